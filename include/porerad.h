@@ -1,0 +1,203 @@
+/* libporerad — B200 (sm_100a) implementation of porerad's surface-radiation path:
+ * surface patches -> seeded Lambertian rays -> first-hit voxel traversal into
+ * integer patch-to-patch counts -> balanced exchange operator -> gray-diffuse
+ * radiosity -> wall and internal net fluxes.
+ *
+ * The reference (moxi000/pore-radiation-ijhmt2026, package `porerad`) exposes no C
+ * interface; its boundary is the Python API of porerad.view_factors and
+ * porerad.exchange.  Each entry point below names the reference function it
+ * replaces (file:line within the reference project).  A Python binding with the
+ * reference's exact names and signatures sits on top (package porerad_b200).
+ *
+ * Conventions
+ *  - Every call returns PR_OK (0) or a PR_ERR_* code; pr_last_error() then holds a
+ *    message for the calling thread.  No call aborts, traps or exits.
+ *  - Array arguments may be host memory (pageable or pinned) or device memory of
+ *    the current device; the library copies with cudaMemcpyDefault.  Calls that
+ *    write host-visible outputs return after the stream has finished them.
+ *  - `stream` is a cudaStream_t (NULL: the legacy default stream).  Objects are
+ *    bound to the device that was current when they were created.  Distinct
+ *    objects may be used concurrently from different host threads on different
+ *    streams; one object must not be used by two calls at the same time.
+ *  - Patch ids are int32 (at most 2^31 - 1 patches), counts are int64 at the API.
+ */
+#ifndef PORERAD_H
+#define PORERAD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PR_API __attribute__((visibility("default")))
+#else
+#define PR_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  PR_OK = 0,
+  PR_ERR_ARG = 1,         /* invalid argument (ValueError in the Python binding) */
+  PR_ERR_CUDA = 2,        /* CUDA runtime failure */
+  PR_ERR_OOM = 3,         /* device memory exhausted */
+  PR_ERR_UNRESOLVED = 4,  /* rays without a receiving patch: view_factors.py:268-269 (RuntimeError) */
+  PR_ERR_ACCOUNTING = 5,  /* counts do not account for every ray: exchange.py:70-71 (ValueError) */
+  PR_ERR_NOT_CLOSED = 6,  /* projected rows do not close: exchange.py:78-80 (RuntimeError) */
+  PR_ERR_BALANCE = 7,     /* diagonal balancing did not converge: exchange.py:197 (RuntimeError) */
+  PR_ERR_SERIES = 8,      /* reflection series did not converge: exchange.py:243-244 (RuntimeError) */
+  PR_ERR_LIMIT = 9        /* a size beyond what this build supports */
+};
+
+/* Balancing method reported by pr_operator_info (exchange.py:153-197). */
+enum { PR_BALANCE_NONE = 0, PR_BALANCE_ANDERSON = 1, PR_BALANCE_MULTIPLICATIVE = 2 };
+
+/* Which product pr_operator_apply forms (exchange.py:82-122). */
+enum {
+  PR_APPLY_RAW = 0,       /* F x          raw_matvec      exchange.py:82-93   */
+  PR_APPLY_RAW_T = 1,     /* F^T x        raw_rmatvec     exchange.py:95-106  */
+  PR_APPLY_SYM = 2,       /* S x          symmetric_matvec exchange.py:108-112 */
+  PR_APPLY_MATVEC = 3,    /* F_p x        matvec          exchange.py:114-117 */
+  PR_APPLY_RMATVEC = 4    /* F_p^T x      rmatvec         exchange.py:119-122 */
+};
+
+/* Radiosity precision (pr_net_patch_power, pr_prescribed_field_channels). */
+enum {
+  PR_PRECISION_FP64 = 0,  /* binary64 reflection series, as the reference */
+  PR_PRECISION_MIXED = 1  /* binary32 sweeps, binary64 residual refinement */
+};
+
+/* Seed of one ray block: numpy.random.PCG64(seed).state, i.e. the 128-bit LCG
+ * state and increment that SeedSequence derives from the integer seed
+ * (view_factors.py:149-151). */
+typedef struct {
+  uint64_t state_hi, state_lo, inc_hi, inc_lo;
+} pr_pcg64;
+
+typedef struct pr_case pr_case;         /* one x-oriented voxel geometry on one GPU */
+typedef struct pr_counts pr_counts;     /* pooled first-hit counts, CSR by origin   */
+typedef struct pr_operator pr_operator; /* projected view-factor operator F_p       */
+
+PR_API const char* pr_last_error(void);
+PR_API int pr_version(void);
+
+/* ---- geometry ------------------------------------------------------------
+ * Replaces build_surface_patches(phases_x, H_m), view_factors.py:70-132.
+ * phases_x: uint8 (nx, ny, nz) C order, 1 = solid, already oriented along x
+ * (orient_along_x, view_factors.py:37-40). */
+PR_API int pr_case_create(const uint8_t* phases_x, int64_t nx, int64_t ny, int64_t nz, double H_m,
+                   void* stream, pr_case** out);
+/* n_patches = SurfacePatches.n_patches (view_factors.py:65-67); n_wall = wall patches. */
+PR_API int pr_case_info(const pr_case* c, int64_t* n_patches, int64_t* n_wall, size_t* device_bytes);
+/* Copies the SurfacePatches fields (view_factors.py:53-63); any pointer may be NULL.
+ * Shapes: solid (nx,ny,nz) u8; patch_class (P) i8; patch_cell (P) i32; patch_face (P) i8;
+ * patch_origin, patch_normal (P,3) f64; patch_area_m2 (P) f64; cell_face_patch
+ * (nx*ny*nz, 6) i32; hot_wall_patch, cold_wall_patch (ny,nz) i32. */
+PR_API int pr_case_patches(const pr_case* c, uint8_t* solid, int8_t* patch_class, int32_t* patch_cell,
+                    int8_t* patch_face, double* patch_origin, double* patch_normal,
+                    double* patch_area_m2, int32_t* cell_face_patch, int32_t* hot_wall_patch,
+                    int32_t* cold_wall_patch, void* stream);
+PR_API void pr_case_destroy(pr_case* c);
+
+/* ---- rays ----------------------------------------------------------------
+ * Replaces generate_rays(patches, patch_start, patch_end, rays_per_patch, seed),
+ * view_factors.py:135-182.  origins, directions: ((patch_end - patch_start) * R, 3) f64. */
+PR_API int pr_generate_rays(const pr_case* c, int64_t patch_start, int64_t patch_end,
+                     int64_t rays_per_patch, const pr_pcg64* seed, double* origins,
+                     double* directions, void* stream);
+
+/* ---- traversal -------------------------------------------------------------
+ * Replaces trace_first_hit(patches, origins, directions), view_factors.py:261-270
+ * (the traversal of view_factors.py:185-258).  receiver (n_rays) i32.  Returns
+ * PR_ERR_UNRESOLVED with *n_failed > 0 when rays did not resolve a receiver. */
+PR_API int pr_trace_first_hit(const pr_case* c, const double* origins, const double* directions,
+                       int64_t n_rays, int32_t* receiver, int64_t* n_failed, void* stream);
+
+/* ---- first-hit counts --------------------------------------------------------
+ * Replaces first_hit_counts(patches, rays_per_patch, seed), view_factors.py:273-287,
+ * for n_seeds blocks at once, pooled as pool_counts (view_factors.py:290-300) pools
+ * them: rays are generated on the fly, traced, and the receivers of each origin
+ * patch reduced into one sorted CSR row.  rays_per_origin = R * n_seeds. */
+PR_API int pr_first_hit_counts(const pr_case* c, int64_t rays_per_patch, const pr_pcg64* seeds,
+                        int n_seeds, void* stream, pr_counts** out);
+/* nnz = pooled (origin, receiver) pairs; rays/steps: rays traced and DDA cells visited. */
+PR_API int pr_counts_info(const pr_counts* k, int64_t* nnz, int64_t* n_patches, int64_t* rays,
+                   int64_t* dda_steps);
+/* The sorted edge list (origin i32, receiver i32, count i64) and rays_per_origin (i64). */
+PR_API int pr_counts_copy(const pr_counts* k, int32_t* origin, int32_t* receiver, int64_t* count,
+                   int64_t* rays_per_origin, void* stream);
+/* Replaces pool_counts(tables, n_patches), view_factors.py:290-300, and the re-pooling at
+ * the top of ExchangeOperator.__init__ (exchange.py:59-67): sums the counts of equal
+ * (origin, receiver) pairs of an arbitrary edge list into sorted CSR rows. */
+PR_API int pr_counts_from_edges(const int32_t* origin, const int32_t* receiver, const int64_t* count,
+                         int64_t n_edges, int64_t n_patches, void* stream, pr_counts** out);
+PR_API void pr_counts_destroy(pr_counts* k);
+
+/* ---- exchange operator -------------------------------------------------------
+ * Replaces ExchangeOperator.__init__, exchange.py:47-80: checks that every row
+ * accounts for its rays (PR_ERR_ACCOUNTING), forms S = 0.5 (A F + F^T A) + delta A,
+ * finds d > 0 with d * (S d) = A (Anderson acceleration on log d; damped
+ * multiplicative iteration as fallback, exchange.py:153-197) and checks the
+ * projected row closure max|F_p 1 - 1| <= 1e-10 (PR_ERR_NOT_CLOSED).  The operator
+ * keeps its own reference to the counts; `counts` may be destroyed afterwards. */
+PR_API int pr_operator_create(const pr_counts* counts, const int64_t* rays_per_origin,
+                       const double* patch_area_m2, double support_diagonal_fraction,
+                       double balance_tolerance, void* stream, pr_operator** out);
+/* scale (P) f64 = ExchangeOperator.scale; the others as the attributes of the same names;
+ * nnz_counts = pooled (origin, receiver) pairs, nnz_symmetric = entries of S on the union
+ * pattern, spmv_calls = sparse products made with this operator so far. */
+PR_API int pr_operator_info(const pr_operator* op, double* scale, int* balance_method,
+                     int* balance_iterations, double* row_sum_error, int64_t* nnz_counts,
+                     int64_t* nnz_symmetric, int64_t* spmv_calls);
+/* y = product(x), see PR_APPLY_*. x, y: (P) f64. */
+PR_API int pr_operator_apply(const pr_operator* op, int which, const double* x, double* y, void* stream);
+/* ExchangeOperator.reciprocity_error(), exchange.py:124-140. */
+PR_API int pr_operator_reciprocity_error(const pr_operator* op, double* out, void* stream);
+/* The sampled edges with their weights n_ij / R_i (ExchangeOperator.origin, .receiver,
+ * .weight, exchange.py:66-72); any pointer may be NULL. */
+PR_API int pr_operator_edges(const pr_operator* op, int32_t* origin, int32_t* receiver, double* weight,
+                      void* stream);
+PR_API void pr_operator_destroy(pr_operator* op);
+
+/* ---- radiosity ----------------------------------------------------------------
+ * Replaces reflection_series(operator, emitted_W, emissivity, relative_tolerance=,
+ * max_reflections=), exchange.py:217-245.  absorbed (P) f64; residual = sum of the
+ * power still in flight; iterations = reflections summed. */
+PR_API int pr_reflection_series(const pr_operator* op, const double* emitted, const double* emissivity,
+                         double relative_tolerance, int64_t max_reflections, double* absorbed,
+                         double* residual_power, int64_t* iterations, void* stream);
+/* Replaces net_patch_power(operator, temperature_K, emissivity, area_m2,
+ * relative_tolerance=, reference_temperature_K=), exchange.py:248-271.
+ * has_reference = 0 means reference_temperature_K=None.  Outputs may be NULL. */
+PR_API int pr_net_patch_power(const pr_operator* op, const double* temperature_K,
+                       const double* emissivity, const double* area_m2,
+                       double relative_tolerance, int has_reference,
+                       double reference_temperature_K, int64_t max_reflections, double* emitted,
+                       double* absorbed, double* net, double* residual_power, int64_t* iterations,
+                       void* stream);
+/* Replaces net_patch_power_jvp(...), exchange.py:274-287.  out (P) f64. */
+PR_API int pr_net_patch_power_jvp(const pr_operator* op, const double* temperature_K,
+                           const double* delta_temperature_K, const double* emissivity,
+                           const double* area_m2, double relative_tolerance, double* out,
+                           void* stream);
+
+/* ---- prescribed-field channels (caller of the path) -------------------------------
+ * Replaces prescribed_field_channels(operator, patches, T_mean_K, delta_T_K, epsilon),
+ * coupled.py:170-194: walls at T_m +/- dT/2, internal patches at the linear field of
+ * their cell (coupled.py:138-143), one radiosity solve with T_ref = T_m, then
+ * q[0..2] = q_h, q_c, q_i (W m^-2) and q[3] = closure_rel.  coarse (optional) =
+ * 8^3 coarse source / cross-section area (coupled.py:146-153, 193), shape of
+ * min(8, n) bins per axis.  precision: PR_PRECISION_*; rtol as the reference (1e-13)
+ * for FP64.  stats (optional, 4 values): reflections or sweeps, SpMV calls, residual
+ * power, estimated relative error of the mixed solve (0 for FP64). */
+PR_API int pr_prescribed_field_channels(const pr_case* c, const pr_operator* op, double T_mean_K,
+                                 double delta_T_K, double epsilon, int precision,
+                                 double relative_tolerance, double* q, double* coarse,
+                                 double* stats, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PORERAD_H */

@@ -1,0 +1,187 @@
+"""ctypes binding of libporerad.so (include/porerad.h).
+
+The library is the only compute path of porerad_b200: if it is missing or no CUDA
+device is visible, every call raises instead of falling back to the CPU.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+from pathlib import Path
+
+import numpy as np
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libporerad.so"
+
+PR_OK = 0
+PR_ERR_ARG = 1
+PR_ERR_CUDA = 2
+PR_ERR_OOM = 3
+PR_ERR_UNRESOLVED = 4
+PR_ERR_ACCOUNTING = 5
+PR_ERR_NOT_CLOSED = 6
+PR_ERR_BALANCE = 7
+PR_ERR_SERIES = 8
+PR_ERR_LIMIT = 9
+
+BALANCE_METHODS = {0: "none", 1: "anderson", 2: "multiplicative"}
+
+APPLY_RAW, APPLY_RAW_T, APPLY_SYM, APPLY_MATVEC, APPLY_RMATVEC = range(5)
+PRECISION_FP64, PRECISION_MIXED = 0, 1
+
+
+class PorerdDeviceError(RuntimeError):
+    """A CUDA failure inside libporerad (not one of the reference's own errors)."""
+
+
+class PCG64Seed(ctypes.Structure):
+    _fields_ = [("state_hi", ctypes.c_uint64), ("state_lo", ctypes.c_uint64),
+                ("inc_hi", ctypes.c_uint64), ("inc_lo", ctypes.c_uint64)]
+
+
+_vp = ctypes.c_void_p
+_i64 = ctypes.c_int64
+_i32 = ctypes.c_int
+_f64 = ctypes.c_double
+
+_SIGNATURES = {
+    "pr_last_error": (ctypes.c_char_p, []),
+    "pr_version": (_i32, []),
+    "pr_case_create": (_i32, [_vp, _i64, _i64, _i64, _f64, _vp, ctypes.POINTER(_vp)]),
+    "pr_case_info": (_i32, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(ctypes.c_size_t)]),
+    "pr_case_patches": (_i32, [_vp] * 11 + [_vp]),
+    "pr_case_destroy": (None, [_vp]),
+    "pr_generate_rays": (_i32, [_vp, _i64, _i64, _i64, _vp, _vp, _vp, _vp]),
+    "pr_trace_first_hit": (_i32, [_vp, _vp, _vp, _i64, _vp, ctypes.POINTER(_i64), _vp]),
+    "pr_first_hit_counts": (_i32, [_vp, _i64, _vp, _i32, _vp, ctypes.POINTER(_vp)]),
+    "pr_counts_info": (_i32, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64),
+                              ctypes.POINTER(_i64)]),
+    "pr_counts_copy": (_i32, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "pr_counts_from_edges": (_i32, [_vp, _vp, _vp, _i64, _i64, _vp, ctypes.POINTER(_vp)]),
+    "pr_counts_destroy": (None, [_vp]),
+    "pr_operator_create": (_i32, [_vp, _vp, _vp, _f64, _f64, _vp, ctypes.POINTER(_vp)]),
+    "pr_operator_info": (_i32, [_vp, _vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32), ctypes.POINTER(_f64),
+                                ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
+    "pr_operator_apply": (_i32, [_vp, _i32, _vp, _vp, _vp]),
+    "pr_operator_reciprocity_error": (_i32, [_vp, ctypes.POINTER(_f64), _vp]),
+    "pr_operator_edges": (_i32, [_vp, _vp, _vp, _vp, _vp]),
+    "pr_operator_destroy": (None, [_vp]),
+    "pr_reflection_series": (_i32, [_vp, _vp, _vp, _f64, _i64, _vp, ctypes.POINTER(_f64), ctypes.POINTER(_i64),
+                                    _vp]),
+    "pr_net_patch_power": (_i32, [_vp, _vp, _vp, _vp, _f64, _i32, _f64, _i64, _vp, _vp, _vp,
+                                  ctypes.POINTER(_f64), ctypes.POINTER(_i64), _vp]),
+    "pr_net_patch_power_jvp": (_i32, [_vp, _vp, _vp, _vp, _vp, _f64, _vp, _vp]),
+    "pr_prescribed_field_channels": (_i32, [_vp, _vp, _f64, _f64, _f64, _i32, _f64, _vp, _vp, _vp, _vp]),
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """The loaded library; raises if it was not built or cannot be loaded."""
+
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not LIB_PATH.is_file():
+                raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m porerad_b200.build` "
+                                   "(porerad_b200 has no CPU implementation)")
+            lib = ctypes.CDLL(str(LIB_PATH), mode=os.RTLD_LOCAL if hasattr(os, "RTLD_LOCAL") else 0)
+            for name, (res, args) in _SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+    return _lib
+
+
+def last_error() -> str:
+    msg = load().pr_last_error()
+    return msg.decode("utf-8", "replace") if msg else ""
+
+
+def check(status: int) -> None:
+    """Map a libporerad status to the exception the reference raises in the same case."""
+
+    if status == PR_OK:
+        return
+    msg = last_error()
+    if status in (PR_ERR_ARG, PR_ERR_ACCOUNTING):
+        raise ValueError(msg)
+    if status in (PR_ERR_UNRESOLVED, PR_ERR_NOT_CLOSED, PR_ERR_BALANCE, PR_ERR_SERIES):
+        raise RuntimeError(msg)
+    if status == PR_ERR_OOM:
+        raise MemoryError(msg)
+    if status == PR_ERR_LIMIT:
+        raise NotImplementedError(msg)
+    raise PorerdDeviceError(msg)
+
+
+def ptr(a) -> int | None:
+    """Data pointer of a C-contiguous NumPy array or CUDA tensor (None stays NULL)."""
+
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("array must be C-contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    raise TypeError(f"unsupported array type {type(a)!r}")
+
+
+def seeds_struct(states) -> ctypes.Array:
+    """pr_pcg64 array from (state, inc) pairs of Python ints."""
+
+    arr = (PCG64Seed * len(states))()
+    for k, (st, inc) in enumerate(states):
+        arr[k].state_hi = (st >> 64) & 0xFFFFFFFFFFFFFFFF
+        arr[k].state_lo = st & 0xFFFFFFFFFFFFFFFF
+        arr[k].inc_hi = (inc >> 64) & 0xFFFFFFFFFFFFFFFF
+        arr[k].inc_lo = inc & 0xFFFFFFFFFFFFFFFF
+    return arr
+
+
+def pcg64_state(seed: int) -> tuple[int, int]:
+    """(state, inc) that numpy.random.PCG64(seed) starts from (SeedSequence seeding)."""
+
+    st = np.random.PCG64(int(seed)).state["state"]
+    return int(st["state"]), int(st["inc"])
+
+
+class Handle:
+    """Owner of one opaque library object; destroyed with its destructor function."""
+
+    __slots__ = ("value", "_destroy", "__weakref__")
+
+    def __init__(self, value: int, destroy: str):
+        self.value = value
+        self._destroy = destroy
+
+    def close(self) -> None:
+        if self.value:
+            getattr(load(), self._destroy)(ctypes.c_void_p(self.value))
+            self.value = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def stream_arg(stream) -> int | None:
+    """cudaStream_t from None (legacy default stream), an int, or a torch.cuda.Stream."""
+
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream or None
+    return int(stream.cuda_stream) or None

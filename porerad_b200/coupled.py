@@ -1,0 +1,210 @@
+"""Prescribed-field radiation channels on a B200: the callers of the radiosity path.
+
+Mirrors the prescribed-field part of ``porerad.coupled`` (porerad/coupled.py:45-219).
+:func:`prescribed_field_channels` runs on the GPU end to end (patch temperatures,
+emission, radiosity, per-class sums and the coarse source in libporerad); the small
+helpers keep the reference's host semantics for callers that use them directly.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from .constants import SIGMA
+from .exchange import ExchangeOperator, RadiosityResult, net_patch_power, net_patch_power_jvp
+from .view_factors import COLD, HOT, INTERNAL, SurfacePatches, _device_of
+
+_TINY = np.finfo(np.float64).tiny
+
+RADIOSITY_RTOL_NEWTON = 1.0e-8
+RADIOSITY_RTOL_FINAL = 1.0e-13
+MIXED_RTOL = 1.0e-12
+"""Relative binary64 residual the mixed-precision solve refines to."""
+
+
+def patch_temperature(patches, T_cells: np.ndarray, T_hot_K: float, T_cold_K: float) -> np.ndarray:
+    """Wall temperatures on wall patches and the owning-cell temperature on internal patches (coupled.py:45-53)."""
+
+    cls = np.asarray(patches.patch_class)
+    T = np.empty(cls.size, dtype=np.float64)
+    inner = cls == INTERNAL
+    T[cls == HOT] = float(T_hot_K)
+    T[cls == COLD] = float(T_cold_K)
+    T[inner] = np.asarray(T_cells, dtype=np.float64).ravel()[np.asarray(patches.patch_cell)[inner]]
+    return T
+
+
+def cell_power(patches, patch_power_W: np.ndarray) -> np.ndarray:
+    """Sum the power of the internal patches into their owning solid cells (coupled.py:56-62)."""
+
+    cls = np.asarray(patches.patch_class)
+    inner = cls == INTERNAL
+    solid = np.asarray(patches.solid)
+    power = np.zeros(solid.size, dtype=np.float64)
+    np.add.at(power, np.asarray(patches.patch_cell)[inner], np.asarray(patch_power_W)[inner])
+    return power.reshape(solid.shape)
+
+
+def emission_diagonal(patches, T_cells: np.ndarray, epsilon: float) -> np.ndarray:
+    """Local emission derivative sum_p 4 eps sigma A_p T^3 of every cell in W/K (coupled.py:65-73)."""
+
+    cls = np.asarray(patches.patch_class)
+    inner = cls == INTERNAL
+    owner = np.asarray(patches.patch_cell)[inner].astype(np.int64)
+    T = np.asarray(T_cells, dtype=np.float64).ravel()[owner]
+    diagonal = np.zeros(np.asarray(patches.solid).size, dtype=np.float64)
+    np.add.at(diagonal, owner, 4.0 * float(epsilon) * SIGMA * np.asarray(patches.patch_area_m2)[inner] * T**3)
+    return diagonal
+
+
+@dataclass
+class RadiationState:
+    """Patch temperatures, net patch power and net cell power of one temperature field (coupled.py:76-83)."""
+
+    patch_temperature_K: np.ndarray
+    patch_net_power_W: np.ndarray
+    cell_net_power_W: np.ndarray
+    radiosity: RadiosityResult
+
+
+def evaluate_radiation(operator: ExchangeOperator, patches, T_cells: np.ndarray, T_hot_K: float, T_cold_K: float,
+                       epsilon: float, *, relative_tolerance: float,
+                       reference_temperature_K: float | None = None) -> RadiationState:
+    """Net radiative power of patches and cells; all surfaces share the emissivity eps (coupled.py:86-105)."""
+
+    T_patch = patch_temperature(patches, T_cells, T_hot_K, T_cold_K)
+    emissivity = np.full(T_patch.size, float(epsilon))
+    radiosity = net_patch_power(operator, T_patch, emissivity, np.asarray(patches.patch_area_m2),
+                                relative_tolerance=relative_tolerance,
+                                reference_temperature_K=reference_temperature_K)
+    return RadiationState(T_patch, radiosity.net_power_W, cell_power(patches, radiosity.net_power_W), radiosity)
+
+
+def radiation_jvp(operator: ExchangeOperator, patches, T_patch: np.ndarray, dT_cells: np.ndarray, epsilon: float, *,
+                  relative_tolerance: float) -> np.ndarray:
+    """Change of the net cell power for a cell temperature perturbation, walls fixed (coupled.py:108-126)."""
+
+    cls = np.asarray(patches.patch_class)
+    internal = cls == INTERNAL
+    dT_patch = np.zeros(cls.size, dtype=np.float64)
+    dT_patch[internal] = np.asarray(dT_cells, dtype=np.float64).ravel()[np.asarray(patches.patch_cell)[internal]]
+    emissivity = np.full(cls.size, float(epsilon))
+    patch_jvp = net_patch_power_jvp(operator, T_patch, dT_patch, emissivity, np.asarray(patches.patch_area_m2),
+                                    relative_tolerance=relative_tolerance)
+    return cell_power(patches, patch_jvp)
+
+
+def cross_section_area(patches) -> float:
+    """Projected wall area N_y N_z (H/N_x)^2 (coupled.py:129-133)."""
+
+    nx, ny, nz = _shape_of(patches)
+    return float(ny * nz) * (patches.H_m / float(nx)) ** 2
+
+
+def linear_cell_temperature(shape: tuple[int, int, int], T_mean_K: float, delta_T_K: float) -> np.ndarray:
+    """Linear field T_h + (T_c - T_h) s/H evaluated at the cell centres (coupled.py:138-143)."""
+
+    nx = int(shape[0])
+    axial = (T_mean_K + delta_T_K / 2.0) - (np.arange(nx, dtype=np.float64) + 0.5) * delta_T_K / nx
+    return np.broadcast_to(axial[:, None, None], tuple(int(n) for n in shape)).copy()
+
+
+def coarse_source(cell_power_W: np.ndarray, bins: int = 8) -> np.ndarray:
+    """Cell power summed over a bins^3 grid of equal blocks (coupled.py:146-153)."""
+
+    array = np.asarray(cell_power_W, dtype=np.float64)
+    parts = [np.array_split(np.arange(n), min(bins, n)) for n in array.shape]
+    return np.asarray(
+        [float(np.sum(array[np.ix_(xs, ys, zs)])) for xs in parts[0] for ys in parts[1] for zs in parts[2]]
+    ).reshape(tuple(len(p) for p in parts))
+
+
+@dataclass
+class PrescribedChannels:
+    """Radiation channels (W m^-2) under the prescribed linear field, q_h + q_c + q_i = 0 (coupled.py:156-167).
+
+    ``stats`` (not in the reference) records how the solve ran: reflections or
+    refinements, sparse products, and the final relative residual.
+    """
+
+    T_mean_K: float
+    delta_T_K: float
+    epsilon: float
+    q_h: float
+    q_c: float
+    q_i: float
+    closure_rel: float
+    coarse_source: np.ndarray = field(repr=False)
+    stats: dict = field(default_factory=dict, repr=False)
+
+
+def _shape_of(patches) -> tuple[int, int, int]:
+    if isinstance(patches, SurfacePatches) and patches._device is not None:
+        return patches._device.shape
+    return tuple(int(s) for s in np.asarray(patches.solid).shape)
+
+
+def prescribed_field_channels(operator: ExchangeOperator, patches, T_mean_K: float, delta_T_K: float,
+                              epsilon: float, *, precision: str = "fp64",
+                              relative_tolerance: float | None = None) -> PrescribedChannels:
+    """Net power leaving the hot wall, the cold wall and the internal surfaces (coupled.py:170-194).
+
+    Walls are held at T_m +/- dT/2 and every internal surface takes the linear
+    field at its owning cell.  One radiosity evaluation to a relative tolerance of
+    1e-13 is made with the isothermal state at T_m subtracted.  ``precision``
+    "mixed" solves with binary32 sweeps refined to a binary64 residual (not in the
+    reference; its relative residual is ``relative_tolerance``, default 1e-12).
+    """
+
+    dev = _device_of(patches)
+    prec = {"fp64": _lib.PRECISION_FP64, "mixed": _lib.PRECISION_MIXED}[precision]
+    rtol = RADIOSITY_RTOL_FINAL if prec == _lib.PRECISION_FP64 else MIXED_RTOL
+    if relative_tolerance is not None:
+        rtol = float(relative_tolerance)
+    nx, ny, nz = dev.shape
+    bins = tuple(min(8, n) for n in (nx, ny, nz))
+    coarse = np.empty(bins)
+    q = np.empty(4)
+    stats = np.zeros(4)
+    _lib.check(_lib.load().pr_prescribed_field_channels(dev.handle, operator.handle, float(T_mean_K),
+                                                        float(delta_T_K), float(epsilon), prec, rtol,
+                                                        q.ctypes.data, coarse.ctypes.data, stats.ctypes.data,
+                                                        None))
+    if prec == _lib.PRECISION_FP64:
+        info = {"reflections": int(stats[0]), "spmv": int(stats[1]), "residual_power_W": float(stats[2])}
+    else:
+        info = {"refinements": int(stats[0]), "spmv": int(stats[1]), "relative_residual": float(stats[2]),
+                "sweeps_per_refinement": int(stats[3])}
+    return PrescribedChannels(float(T_mean_K), float(delta_T_K), float(epsilon), float(q[0]), float(q[1]),
+                              float(q[2]), float(q[3]), coarse, info)
+
+
+def relative_difference(a: float, b: float) -> float:
+    """coupled.py:197-198."""
+
+    return abs(float(a) - float(b)) / max(abs(float(a)), abs(float(b)), _TINY)
+
+
+def ab_differences(set_a: list[PrescribedChannels], set_b: list[PrescribedChannels]) -> tuple[float, float]:
+    """Largest A/B relative difference of the wall channels and of the 8^3 coarse source, L1 (coupled.py:201-213)."""
+
+    channel = max(
+        relative_difference(getattr(a, name), getattr(b, name))
+        for a, b in zip(set_a, set_b) for name in ("q_h", "q_c")
+    )
+    source = max(
+        float(np.sum(np.abs(a.coarse_source - b.coarse_source)))
+        / max(float(np.sum(np.abs(a.coarse_source))), float(np.sum(np.abs(b.coarse_source))), _TINY)
+        for a, b in zip(set_a, set_b)
+    )
+    return channel, source
+
+
+def append_required(channel_difference: float, source_difference: float) -> bool:
+    """One symmetric append of a further ray block to each set when the sets disagree (coupled.py:216-219)."""
+
+    return channel_difference > 0.01 or source_difference > 0.05

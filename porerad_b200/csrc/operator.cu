@@ -1,0 +1,867 @@
+// Exchange operator on the device: pooling of arbitrary edge lists, the ray
+// accounting check, the symmetric exchange matrix, diagonal balancing, the
+// projected products and the reciprocity diagnostic.
+//
+// Follows porerad/exchange.py:37-197:
+//   weight w_ij = n_ij / R_i                                       (exchange.py:72)
+//   S = 0.5 (A F + F^T A) + delta A                                (exchange.py:108-112)
+//   d > 0 with d * (S d) = A, found as y = log d from the residual
+//   f(y) = y + log(S e^y) - log A; convergence when max|f| <= tol, acceptance when
+//   the closure max|d (S d) / A - 1| <= min(max(10 tol, 10 eps), 1e-10); otherwise
+//   the damped multiplicative iteration y += 0.5 (log A - log(d * S d)) until the
+//   closure is <= min(tol, 1e-10) (exchange.py:153-197)
+//   row_sum_error = max|F_p 1 - 1| <= 1e-10                       (exchange.py:78-80)
+// The reference accelerates the log-residual with scipy.optimize.anderson; here it
+// is type-II Anderson acceleration (Walker & Ni 2011) of the damped fixed-point map
+// y <- y - beta f(y), history m = 10, beta = 1/2, least squares by the normal
+// equations with a pseudo-inverse cut at 10 eps of the largest eigenvalue.  The
+// solution d is defined by the equation, so the iterate path may differ from
+// SciPy's; d itself agrees to the balancing tolerance.
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_reduce.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include <cmath>
+#include <vector>
+
+#include "pr_spmv.cuh"
+
+namespace pr {
+
+__global__ void k_sum_partials(const double* __restrict__ partial, int blocks, int K, double* __restrict__ out) {
+  const int k = threadIdx.x;
+  if (k >= K) return;
+  double s = 0.0;
+  for (int b = 0; b < blocks; ++b) s += partial[(int64_t)b * K + k];
+  out[k] = s;
+}
+
+int sum_partials(const double* partial, int blocks, int K, double* out, cudaStream_t s) {
+  k_sum_partials<<<1, 32 * ((K + 31) / 32), 0, s>>>(partial, blocks, K, out);
+  PR_CUDA(cudaGetLastError());
+  return PR_OK;
+}
+
+static int red_grid() { return sm_count() * 4; }
+
+// ------------------------------------------------------------------ pooling
+
+__global__ void k_edge_keys(const int32_t* __restrict__ o, const int32_t* __restrict__ r, int64_t m, int64_t n,
+                            unsigned long long* __restrict__ key, unsigned int* __restrict__ bad) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t a = o[t], b = r[t];
+    if (a < 0 || a >= n || b < 0 || b >= n) {
+      atomicOr(bad, 1u);
+      key[t] = 0;
+    } else {
+      key[t] = (unsigned long long)a * (unsigned long long)n + (unsigned long long)b;
+    }
+  }
+}
+
+__global__ void k_keys_to_csr(const unsigned long long* __restrict__ key, const int64_t* __restrict__ sum, int64_t m,
+                              int64_t n, int32_t* __restrict__ col, int32_t* __restrict__ cnt,
+                              int32_t* __restrict__ row_len, unsigned int* __restrict__ bad) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = (int64_t)(key[t] / (unsigned long long)n);
+    col[t] = (int32_t)(key[t] % (unsigned long long)n);
+    const int64_t c = sum[t];
+    if (c < 0 || c > INT32_MAX) atomicOr(bad, 2u);
+    cnt[t] = (int32_t)c;
+    atomicAdd(row_len + row, 1);
+  }
+}
+
+__global__ void k_zero_i32(int32_t* p, int64_t n) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) p[t] = 0;
+}
+
+__global__ void k_widen_scan_input(const int32_t* __restrict__ in, int64_t* __restrict__ out, int64_t n) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+    out[t] = in[t];
+}
+
+// row_ptr[0] = 0, row_ptr[1..n] = inclusive sum of len (int64)
+static int lengths_to_row_ptr(const int64_t* len, int64_t n, int64_t* row_ptr, cudaStream_t s) {
+  PR_CUDA(cudaMemsetAsync(row_ptr, 0, sizeof(int64_t), s));
+  if (n == 0) return PR_OK;
+  size_t b = 0;
+  PR_CUDA(cub::DeviceScan::InclusiveSum(nullptr, b, len, row_ptr + 1, n, s));
+  DevBuf<uint8_t> tmp;
+  PR_TRY(tmp.alloc(b + 16, s));
+  PR_CUDA(cub::DeviceScan::InclusiveSum(tmp.ptr, b, len, row_ptr + 1, n, s));
+  return PR_OK;
+}
+
+__global__ void k_row_sums(const int64_t* __restrict__ rp, const int32_t* __restrict__ cn, int64_t n,
+                           int64_t* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+    int64_t s = 0;
+    for (int64_t q = rp[i] + lane; q < rp[i + 1]; q += 32) s += cn[q];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) out[i] = s;
+  }
+}
+
+int counts_from_edges(const int32_t* origin, const int32_t* receiver, const int64_t* count, int64_t m, int64_t n,
+                      cudaStream_t s, pr_counts** out) {
+  PR_ARG(n >= 0 && n < INT32_MAX, "n_patches %lld outside the int32 patch ids", (long long)n);
+  PR_ARG(m >= 0, "negative edge count");
+  std::unique_ptr<pr_counts> k(new pr_counts());
+  cudaGetDevice(&k->device);
+  k->csr = std::make_shared<CountCsr>();
+  CountCsr& csr = *k->csr;
+  csr.n_rows = n;
+  PR_TRY(csr.row_ptr.alloc(n + 1, s));
+  DevBuf<int32_t> o, r, row_len;
+  DevBuf<int64_t> c, c_sorted, sums, len64;
+  DevBuf<unsigned long long> key, key_sorted, ukey;
+  DevBuf<unsigned int> bad;
+  DevBuf<int64_t> nruns;
+  PR_TRY(bad.alloc(1, s));
+  PR_CUDA(cudaMemsetAsync(bad.ptr, 0, 4, s));
+  PR_TRY(row_len.alloc(n > 0 ? n : 1, s));
+  k_zero_i32<<<grid_for(n, 256), 256, 0, s>>>(row_len.ptr, n);
+  int64_t u = 0;
+  if (m > 0) {
+    PR_TRY(o.alloc(m, s));
+    PR_TRY(r.alloc(m, s));
+    PR_TRY(c.alloc(m, s));
+    PR_CUDA(cudaMemcpyAsync(o.ptr, origin, m * 4, cudaMemcpyDefault, s));
+    PR_CUDA(cudaMemcpyAsync(r.ptr, receiver, m * 4, cudaMemcpyDefault, s));
+    PR_CUDA(cudaMemcpyAsync(c.ptr, count, m * 8, cudaMemcpyDefault, s));
+    PR_TRY(key.alloc(m, s));
+    PR_TRY(key_sorted.alloc(m, s));
+    PR_TRY(c_sorted.alloc(m, s));
+    k_edge_keys<<<grid_for(m, 256), 256, 0, s>>>(o.ptr, r.ptr, m, n, key.ptr, bad.ptr);
+    PR_CUDA(cudaGetLastError());
+    int end_bit = 1;
+    while (end_bit < 64 && (((unsigned long long)1 << end_bit) < (unsigned long long)n * (unsigned long long)n)) ++end_bit;
+    size_t b = 0;
+    PR_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b, key.ptr, key_sorted.ptr, c.ptr, c_sorted.ptr, m, 0, end_bit, s));
+    DevBuf<uint8_t> tmp;
+    PR_TRY(tmp.alloc(b + 16, s));
+    PR_CUDA(cub::DeviceRadixSort::SortPairs(tmp.ptr, b, key.ptr, key_sorted.ptr, c.ptr, c_sorted.ptr, m, 0, end_bit, s));
+    PR_TRY(ukey.alloc(m, s));
+    PR_TRY(sums.alloc(m, s));
+    PR_TRY(nruns.alloc(1, s));
+    size_t b2 = 0;
+    PR_CUDA(cub::DeviceReduce::ReduceByKey(nullptr, b2, key_sorted.ptr, ukey.ptr, c_sorted.ptr, sums.ptr, nruns.ptr,
+                                           cub::Sum(), m, s));
+    DevBuf<uint8_t> tmp2;
+    PR_TRY(tmp2.alloc(b2 + 16, s));
+    PR_CUDA(cub::DeviceReduce::ReduceByKey(tmp2.ptr, b2, key_sorted.ptr, ukey.ptr, c_sorted.ptr, sums.ptr, nruns.ptr,
+                                           cub::Sum(), m, s));
+    PR_CUDA(cudaMemcpyAsync(&u, nruns.ptr, 8, cudaMemcpyDeviceToHost, s));
+    PR_CUDA(cudaStreamSynchronize(s));
+  }
+  unsigned int hbad = 0;
+  PR_CUDA(cudaMemcpyAsync(&hbad, bad.ptr, 4, cudaMemcpyDeviceToHost, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  PR_ARG(!(hbad & 1u), "edge list holds patch ids outside [0, %lld)", (long long)n);
+  csr.nnz = u;
+  PR_TRY(csr.col.alloc(u, s));
+  PR_TRY(csr.cnt.alloc(u, s));
+  if (u > 0) {
+    k_keys_to_csr<<<grid_for(u, 256), 256, 0, s>>>(ukey.ptr, sums.ptr, u, n, csr.col.ptr, csr.cnt.ptr, row_len.ptr,
+                                                  bad.ptr);
+    PR_CUDA(cudaGetLastError());
+  }
+  PR_TRY(len64.alloc(n > 0 ? n : 1, s));
+  k_widen_scan_input<<<grid_for(n, 256), 256, 0, s>>>(row_len.ptr, len64.ptr, n);
+  PR_TRY(lengths_to_row_ptr(len64.ptr, n, csr.row_ptr.ptr, s));
+  PR_CUDA(cudaMemcpyAsync(&hbad, bad.ptr, 4, cudaMemcpyDeviceToHost, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  PR_ARG(!(hbad & 2u), "pooled counts must be non-negative and below 2^31");
+  // rays per origin = row sums of the pooled counts (callers usually pass their own)
+  PR_TRY(k->rays.alloc(n > 0 ? n : 1, s));
+  k_row_sums<<<grid_for(n * 32, 256), 256, 0, s>>>(csr.row_ptr.ptr, csr.cnt.ptr, n, k->rays.ptr);
+  PR_CUDA(cudaGetLastError());
+  PR_CUDA(cudaStreamSynchronize(s));
+  k->last_stream = s;
+  *out = k.release();
+  return PR_OK;
+}
+
+// ------------------------------------------------------------------ transpose / symmetric pattern
+
+// keys (col << 32 | row) of every entry, in row order
+__global__ void k_transpose_keys(const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col, int64_t n,
+                                 unsigned long long* __restrict__ key) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+    for (int64_t q = row_ptr[i] + lane; q < row_ptr[i + 1]; q += 32)
+      key[q] = ((unsigned long long)(uint32_t)col[q] << 32) | (unsigned long long)(uint32_t)i;
+  }
+}
+
+__global__ void k_split_transposed(const unsigned long long* __restrict__ key, int64_t m, int32_t* __restrict__ tcol,
+                                   int32_t* __restrict__ tlen) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+    tcol[t] = (int32_t)(key[t] & 0xffffffffull);
+    atomicAdd(tlen + (int64_t)(key[t] >> 32), 1);
+  }
+}
+
+int build_transpose(const CountCsr& F, CountCsr& T, cudaStream_t s) {
+  const int64_t n = F.n_rows, m = F.nnz;
+  T.n_rows = n;
+  T.nnz = m;
+  PR_TRY(T.row_ptr.alloc(n + 1, s));
+  PR_TRY(T.col.alloc(m, s));
+  PR_TRY(T.cnt.alloc(m, s));
+  DevBuf<int32_t> tlen;
+  DevBuf<int64_t> tlen64;
+  PR_TRY(tlen.alloc(n > 0 ? n : 1, s));
+  k_zero_i32<<<grid_for(n, 256), 256, 0, s>>>(tlen.ptr, n);
+  if (m > 0) {
+    DevBuf<unsigned long long> key, key_sorted;
+    PR_TRY(key.alloc(m, s));
+    PR_TRY(key_sorted.alloc(m, s));
+    k_transpose_keys<<<grid_for(n * 32, 256), 256, 0, s>>>(F.row_ptr.ptr, F.col.ptr, n, key.ptr);
+    PR_CUDA(cudaGetLastError());
+    int bits = 1;
+    while (bits < 32 && ((int64_t)1 << bits) < n) ++bits;
+    size_t b = 0;
+    PR_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b, key.ptr, key_sorted.ptr, F.cnt.ptr, T.cnt.ptr, m, 0, 32 + bits, s));
+    DevBuf<uint8_t> tmp;
+    PR_TRY(tmp.alloc(b + 16, s));
+    PR_CUDA(cub::DeviceRadixSort::SortPairs(tmp.ptr, b, key.ptr, key_sorted.ptr, F.cnt.ptr, T.cnt.ptr, m, 0, 32 + bits, s));
+    k_split_transposed<<<grid_for(m, 256), 256, 0, s>>>(key_sorted.ptr, m, T.col.ptr, tlen.ptr);
+    PR_CUDA(cudaGetLastError());
+  }
+  PR_TRY(tlen64.alloc(n > 0 ? n : 1, s));
+  k_widen_scan_input<<<grid_for(n, 256), 256, 0, s>>>(tlen.ptr, tlen64.ptr, n);
+  PR_TRY(lengths_to_row_ptr(tlen64.ptr, n, T.row_ptr.ptr, s));
+  return PR_OK;
+}
+
+// |row i of F  union  row i of F^T|
+__global__ void k_union_len(const int64_t* __restrict__ fp, const int32_t* __restrict__ fc,
+                            const int64_t* __restrict__ tp, const int32_t* __restrict__ tc, int64_t n,
+                            int64_t* __restrict__ len) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t a = fp[i], ae = fp[i + 1], b = tp[i], be = tp[i + 1], u = 0;
+    while (a < ae && b < be) {
+      const int32_t x = fc[a], y = tc[b];
+      a += x <= y;
+      b += y <= x;
+      ++u;
+    }
+    len[i] = u + (ae - a) + (be - b);
+  }
+}
+
+// S'_ij = 0.5 (A_i n_ij / R_i + A_j n_ji / R_j) on the union pattern (general form),
+// or the integer pair sums n_ij + n_ji (uniform form).
+template <bool kUniform>
+__global__ void k_union_fill(const int64_t* __restrict__ fp, const int32_t* __restrict__ fc,
+                             const int32_t* __restrict__ fn, const int64_t* __restrict__ tp,
+                             const int32_t* __restrict__ tc, const int32_t* __restrict__ tn,
+                             const int64_t* __restrict__ rays, const double* __restrict__ area, int64_t n,
+                             const int64_t* __restrict__ sp, int32_t* __restrict__ scol, double* __restrict__ sval,
+                             int32_t* __restrict__ spair) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t a = fp[i], ae = fp[i + 1], b = tp[i], be = tp[i + 1], o = sp[i];
+    const double Ai = kUniform ? 0.0 : area[i];
+    const double Ri = kUniform ? 0.0 : (double)rays[i];
+    while (a < ae || b < be) {
+      const int32_t x = a < ae ? fc[a] : INT32_MAX;
+      const int32_t y = b < be ? tc[b] : INT32_MAX;
+      const int32_t j = x < y ? x : y;
+      const int32_t nij = x == j ? fn[a] : 0;
+      const int32_t nji = y == j ? tn[b] : 0;
+      scol[o] = j;
+      if constexpr (kUniform) {
+        spair[o] = nij + nji;
+      } else {
+        const double wij = (double)nij / Ri;
+        const double wji = (double)nji / (double)rays[j];
+        sval[o] = 0.5 * (Ai * wij + area[j] * wji);
+      }
+      ++o;
+      a += x == j;
+      b += y == j;
+    }
+  }
+}
+
+// Row sums of the counts must equal the rays of each origin (exchange.py:68-71).
+__global__ void k_accounting(const int64_t* __restrict__ fp, const int32_t* __restrict__ fn,
+                             const int64_t* __restrict__ rays, int64_t n, unsigned int* __restrict__ bad) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+    int64_t s = 0;
+    for (int64_t q = fp[i] + lane; q < fp[i + 1]; q += 32) s += fn[q];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(PR_FULL, s, o);
+    if (lane == 0 && s != rays[i]) atomicOr(bad, 1u);
+  }
+}
+
+// ------------------------------------------------------------------ balancing kernels
+
+struct BalanceScalars {
+  double max_f;      // max |f|
+  double closure;    // max |d (S d) / A - 1|
+  double bad;        // > 0 when S d is not finite and positive, or y left the log range
+  double pad;
+};
+
+#define PR_LOG_MAX 709.782712893384  // log(DBL_MAX)
+#define PR_LOG_MIN -744.4400719213812  // log(smallest subnormal)
+
+__global__ void k_exp_scale(const double* __restrict__ y, int64_t n, double* __restrict__ d, double* __restrict__ sc) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double v = y[i];
+    if (!(v < PR_LOG_MAX && v > PR_LOG_MIN)) sc[2] = 1.0;  // benign race: any writer sets the flag
+    d[i] = exp(v);
+  }
+}
+
+// One balancing evaluation at y (d = e^y given):  s = S d;  f_new = y + log s - log A;
+// dF = f_new - f_old (when dF != nullptr);  closure |d s / A - 1|;  max |f_new|.
+// In multiplicative mode (mult = 1), also y_next = y + 0.5 (log A - log(d s)).
+template <bool kUniform>
+__global__ void __launch_bounds__(256) k_balance_eval(SymView S, double delta, const double* __restrict__ area,
+                                                      const double* __restrict__ y, const double* __restrict__ d,
+                                                      double* __restrict__ f, double* __restrict__ dF,
+                                                      double* __restrict__ sc, int mult, double* __restrict__ y_next) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  double mf = 0.0, mc = 0.0;
+  bool bad = false;
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < S.n; i += warps) {
+    const double Ai = area[i];
+    const double s = sym_row<kUniform>(S, i, d, lane) + delta * Ai * d[i];
+    if (lane == 0) {
+      if (!(s > 0.0 && isfinite(s))) bad = true;
+      const double fn = y[i] + log(s) - log(Ai);
+      if (dF) dF[i] = fn - f[i];
+      f[i] = fn;
+      const double row = d[i] * s;
+      mf = fmax(mf, fabs(fn));
+      mc = fmax(mc, fabs(row / Ai - 1.0));
+      if (mult) y_next[i] = y[i] + 0.5 * (log(Ai) - log(row));
+    }
+  }
+  if (lane == 0) {
+    atomic_max_nonneg(sc + 0, mf);
+    atomic_max_nonneg(sc + 1, mc);
+    if (bad) sc[2] = 1.0;
+  }
+}
+
+// y_next = y - beta f - sum_c gamma_c (dY_c - beta dF_c);  dY_slot = y_next - y.
+struct AAStep {
+  double gamma[10];
+  int cols;
+  int slot;  // ring slot receiving the new differences
+  double beta;
+};
+
+__global__ void k_aa_update(AAStep st, const double* __restrict__ y, const double* __restrict__ f,
+                            const double* __restrict__ dY, const double* __restrict__ dF, int64_t n,
+                            double* __restrict__ y_next, double* __restrict__ dY_out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double v = y[i] - st.beta * f[i];
+    for (int c = 0; c < st.cols; ++c) v -= st.gamma[c] * (dY[(int64_t)c * n + i] - st.beta * dF[(int64_t)c * n + i]);
+    dY_out[(int64_t)st.slot * n + i] = v - y[i];
+    y_next[i] = v;
+  }
+}
+
+// Dots of the history: row r of the Gram matrix (dF_r . dF_c, c < cols) and the
+// right-hand side (dF_c . f, c < cols) -> partial[block][2 * 10].
+__global__ void __launch_bounds__(256) k_aa_dots(const double* __restrict__ dF, const double* __restrict__ f,
+                                                 int64_t n, int cols, int r, double* __restrict__ partial) {
+  double acc[20];
+#pragma unroll
+  for (int k = 0; k < 20; ++k) acc[k] = 0.0;
+  const double* vr = dF + (int64_t)r * n;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double a = vr[i], fi = f[i];
+#pragma unroll
+    for (int c = 0; c < 10; ++c) {
+      if (c < cols) {
+        const double v = dF[(int64_t)c * n + i];
+        acc[c] = fma(a, v, acc[c]);
+        acc[10 + c] = fma(v, fi, acc[10 + c]);
+      }
+    }
+  }
+  block_sum_store<20>(acc, partial);
+}
+
+// ------------------------------------------------------------------ products
+
+template <bool kUniform>
+__global__ void __launch_bounds__(256) k_sym_apply(SymView S, double delta, const double* __restrict__ area,
+                                                   const double* __restrict__ d, const double* __restrict__ x,
+                                                   int mode, double* __restrict__ u, double* __restrict__ y) {
+  // mode 0: y = S x;  mode 1: y = (d/A) S(u), u = d x;  mode 2: y = d S(u), u = d (x / A)
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const double* v = mode == 0 ? x : u;
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < S.n; i += warps) {
+    const double s = sym_row<kUniform>(S, i, v, lane) + delta * area[i] * v[i];
+    if (lane == 0) y[i] = mode == 0 ? s : (mode == 1 ? (d[i] / area[i]) * s : d[i] * s);
+  }
+}
+
+__global__ void k_prep_u(const double* __restrict__ d, const double* __restrict__ area, const double* __restrict__ x,
+                         int64_t n, int mode, double* __restrict__ u) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    u[i] = mode == 1 ? d[i] * x[i] : d[i] * (x[i] / area[i]);
+}
+
+// F x (transposed = 0) or F^T x (transposed = 1, given the transposed CSR) with w = n / R of the origin.
+__global__ void __launch_bounds__(256) k_raw_apply(const int64_t* __restrict__ rp, const int32_t* __restrict__ cl,
+                                                   const int32_t* __restrict__ cn, const int64_t* __restrict__ rays,
+                                                   int64_t n, int transposed, const double* __restrict__ x,
+                                                   double* __restrict__ y) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+    double acc = 0.0;
+    for (int64_t q = rp[i] + lane; q < rp[i + 1]; q += 32) {
+      const int32_t j = cl[q];
+      const double w = (double)cn[q] / (double)rays[transposed ? j : i];
+      acc = fma(w, x[j], acc);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(PR_FULL, acc, o);
+    if (lane == 0) y[i] = acc;
+  }
+}
+
+// Reciprocity defect over the sampled pairs (exchange.py:124-140).
+__global__ void __launch_bounds__(256) k_reciprocity(const int64_t* __restrict__ fp, const int32_t* __restrict__ fc,
+                                                     const int32_t* __restrict__ fn, const int64_t* __restrict__ rays,
+                                                     const double* __restrict__ area, const double* __restrict__ d,
+                                                     double delta, int64_t n, double* __restrict__ out) {
+  double mdiff = 0.0, mjoint = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t q = fp[i]; q < fp[i + 1]; ++q) {
+      const int32_t j = fc[q];
+      const double w = (double)fn[q] / (double)rays[i];
+      // n_ji by binary search in row j
+      int64_t lo = fp[j], hi = fp[j + 1];
+      while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (fc[mid] < i) lo = mid + 1;
+        else hi = mid;
+      }
+      const double wr = (lo < fp[j + 1] && fc[lo] == (int32_t)i) ? (double)fn[lo] / (double)rays[j] : 0.0;
+      const double Ai = area[i], Aj = area[j];
+      double sij = 0.5 * (Ai * w + Aj * wr);
+      double sji = 0.5 * (Aj * wr + Ai * w);
+      if (j == (int32_t)i) {
+        sij += delta * Ai;
+        sji += delta * Aj;
+      }
+      const double jij = Ai * ((d[i] / Ai) * sij * d[j]);
+      const double jji = Aj * ((d[j] / Aj) * sji * d[i]);
+      mdiff = fmax(mdiff, fabs(jij - jji));
+      mjoint = fmax(mjoint, fabs(jij));
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mdiff = fmax(mdiff, __shfl_xor_sync(PR_FULL, mdiff, o));
+    mjoint = fmax(mjoint, __shfl_xor_sync(PR_FULL, mjoint, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_nonneg(out + 0, mdiff);
+    atomic_max_nonneg(out + 1, mjoint);
+  }
+}
+
+__global__ void k_edges_out(const int64_t* __restrict__ fp, const int32_t* __restrict__ fn,
+                            const int64_t* __restrict__ rays, int64_t n, int32_t* __restrict__ origin,
+                            double* __restrict__ weight) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+    for (int64_t q = fp[i] + lane; q < fp[i + 1]; q += 32) {
+      if (origin) origin[q] = (int32_t)i;
+      if (weight) weight[q] = (double)fn[q] / (double)rays[i];
+    }
+  }
+}
+
+// ------------------------------------------------------------------ host side
+
+static int spmv_grid(int64_t rows) { return grid_for(rows * 32, 256, sm_count() * 8); }
+
+template <typename Fn>
+static void dispatch_uniform(bool uniform, Fn&& fn) {
+  if (uniform) fn(std::integral_constant<bool, true>());
+  else fn(std::integral_constant<bool, false>());
+}
+
+// Symmetric eigen-decomposition (cyclic Jacobi) of a k x k matrix, k <= 10.
+static void jacobi_eig(int k, double* a, double* v, double* w) {
+  for (int i = 0; i < k; ++i)
+    for (int j = 0; j < k; ++j) v[i * k + j] = i == j ? 1.0 : 0.0;
+  for (int sweep = 0; sweep < 64; ++sweep) {
+    double off = 0.0;
+    for (int i = 0; i < k; ++i)
+      for (int j = i + 1; j < k; ++j) off += a[i * k + j] * a[i * k + j];
+    if (off < 1e-300) break;
+    for (int p = 0; p < k; ++p)
+      for (int q = p + 1; q < k; ++q) {
+        const double apq = a[p * k + q];
+        if (apq == 0.0) continue;
+        const double theta = (a[q * k + q] - a[p * k + p]) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+        const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+        for (int r = 0; r < k; ++r) {
+          const double arp = a[r * k + p], arq = a[r * k + q];
+          a[r * k + p] = c * arp - s * arq;
+          a[r * k + q] = s * arp + c * arq;
+        }
+        for (int r = 0; r < k; ++r) {
+          const double apr = a[p * k + r], aqr = a[q * k + r];
+          a[p * k + r] = c * apr - s * aqr;
+          a[q * k + r] = s * apr + c * aqr;
+        }
+        for (int r = 0; r < k; ++r) {
+          const double vrp = v[r * k + p], vrq = v[r * k + q];
+          v[r * k + p] = c * vrp - s * vrq;
+          v[r * k + q] = s * vrp + c * vrq;
+        }
+      }
+  }
+  for (int i = 0; i < k; ++i) w[i] = a[i * k + i];
+}
+
+// Least-squares gamma = pinv(H) b for the k x k Gram matrix H.
+static void solve_gram(int k, const double* H, const double* b, double* gamma) {
+  double a[100], v[100], w[10];
+  for (int i = 0; i < k * k; ++i) a[i] = H[i];
+  jacobi_eig(k, a, v, w);
+  double wmax = 0.0;
+  for (int i = 0; i < k; ++i) wmax = fmax(wmax, fabs(w[i]));
+  const double cut = 10.0 * 2.220446049250313e-16 * wmax;
+  for (int i = 0; i < k; ++i) gamma[i] = 0.0;
+  for (int e = 0; e < k; ++e) {
+    if (!(fabs(w[e]) > cut)) continue;
+    double proj = 0.0;
+    for (int i = 0; i < k; ++i) proj += v[i * k + e] * b[i];
+    proj /= w[e];
+    for (int i = 0; i < k; ++i) gamma[i] += v[i * k + e] * proj;
+  }
+}
+
+struct BalanceWork {
+  int64_t n;
+  DevBuf<double> y, y2, d, f, dY, dF, sc, partial, dots;
+};
+
+static int balance_eval(pr_operator* op, BalanceWork& w, const double* y, double* dF, int mult, double* y_next,
+                        BalanceScalars* out, cudaStream_t s) {
+  const int64_t n = w.n;
+  PR_CUDA(cudaMemsetAsync(w.sc.ptr, 0, 4 * sizeof(double), s));
+  k_exp_scale<<<grid_for(n, 256), 256, 0, s>>>(y, n, w.d.ptr, w.sc.ptr);
+  SymView S = sym_view(op->S);
+  dispatch_uniform(op->S.uniform, [&](auto u) {
+    k_balance_eval<decltype(u)::value><<<spmv_grid(n), 256, 0, s>>>(S, op->delta, op->area.ptr, y, w.d.ptr, w.f.ptr,
+                                                                     dF, w.sc.ptr, mult, y_next);
+  });
+  PR_CUDA(cudaGetLastError());
+  op->spmv_calls++;
+  PR_CUDA(cudaMemcpyAsync(out, w.sc.ptr, sizeof(BalanceScalars), cudaMemcpyDeviceToHost, s));
+  return PR_OK;
+}
+
+static int balance(pr_operator* op, double tol, cudaStream_t s) {
+  const int64_t n = op->n;
+  const int M = 10;
+  const double beta = 0.5;
+  BalanceWork w;
+  w.n = n;
+  PR_TRY(w.y.alloc(n, s));
+  PR_TRY(w.y2.alloc(n, s));
+  PR_TRY(w.d.alloc(n, s));
+  PR_TRY(w.f.alloc(n, s));
+  PR_TRY(w.dY.alloc((size_t)M * n, s));
+  PR_TRY(w.dF.alloc((size_t)M * n, s));
+  PR_TRY(w.sc.alloc(4, s));
+  const int rg = red_grid();
+  PR_TRY(w.partial.alloc((size_t)rg * 20, s));
+  PR_TRY(w.dots.alloc(20, s));
+  PR_CUDA(cudaMemsetAsync(w.y.ptr, 0, n * sizeof(double), s));
+  BalanceScalars sc;
+  PR_TRY(balance_eval(op, w, w.y.ptr, nullptr, 0, nullptr, &sc, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  const double eps = 2.220446049250313e-16;
+  if (!(sc.bad > 0) && sc.closure <= tol) {  // exchange.py:157-159
+    op->method = PR_BALANCE_NONE;
+    op->iterations = 0;
+    PR_CUDA(cudaMemcpyAsync(op->scale.ptr, w.d.ptr, n * 8, cudaMemcpyDeviceToDevice, s));
+    return PR_OK;
+  }
+  // ---- Anderson acceleration
+  bool aa_ok = false;
+  int iters = 0;
+  if (!(sc.bad > 0)) {
+    // History columns live in ring slots 0..cols-1; G and b are indexed by slot.
+    double G[10][10] = {{0}}, b[10] = {0};
+    int cols = 0, oldest = 0;
+    double* y = w.y.ptr;
+    double* y_next = w.y2.ptr;
+    double max_f = sc.max_f;
+    const int maxit = 500;  // scipy.optimize.anderson maxiter of exchange.py:177
+    for (int it = 0; it < maxit && max_f > tol; ++it) {
+      AAStep st;
+      st.cols = cols;
+      st.beta = beta;
+      double gamma[10] = {0};
+      if (cols > 0) {
+        double Hf[100];
+        for (int i = 0; i < cols; ++i)
+          for (int j = 0; j < cols; ++j) Hf[i * cols + j] = G[i][j];
+        solve_gram(cols, Hf, b, gamma);
+      }
+      for (int c = 0; c < 10; ++c) st.gamma[c] = c < cols ? gamma[c] : 0.0;
+      int slot;
+      if (cols < M) {
+        slot = cols;
+      } else {
+        slot = oldest;
+        oldest = (oldest + 1) % M;
+      }
+      st.slot = slot;
+      k_aa_update<<<grid_for(n, 256), 256, 0, s>>>(st, y, w.f.ptr, w.dY.ptr, w.dF.ptr, n, y_next, w.dY.ptr);
+      PR_CUDA(cudaGetLastError());
+      PR_TRY(balance_eval(op, w, y_next, w.dF.ptr + (size_t)slot * n, 0, nullptr, &sc, s));
+      ++iters;
+      std::swap(y, y_next);
+      if (cols < M) ++cols;
+      k_aa_dots<<<rg, 256, 0, s>>>(w.dF.ptr, w.f.ptr, n, cols, slot, w.partial.ptr);
+      PR_CUDA(cudaGetLastError());
+      PR_TRY(sum_partials(w.partial.ptr, rg, 20, w.dots.ptr, s));
+      double hd[20];
+      PR_CUDA(cudaMemcpyAsync(hd, w.dots.ptr, sizeof(hd), cudaMemcpyDeviceToHost, s));
+      PR_CUDA(cudaStreamSynchronize(s));
+      if (sc.bad > 0 || !std::isfinite(sc.max_f)) break;
+      for (int c = 0; c < cols; ++c) {
+        G[slot][c] = hd[c];
+        G[c][slot] = hd[c];
+        b[c] = hd[10 + c];
+      }
+      max_f = sc.max_f;
+    }
+    if (y != w.y.ptr) PR_CUDA(cudaMemcpyAsync(w.y.ptr, y, n * 8, cudaMemcpyDeviceToDevice, s));
+    const double accept = fmin(fmax(10.0 * tol, 10.0 * eps), 1.0e-10);  // exchange.py:180
+    if (!(sc.bad > 0) && max_f <= tol && sc.closure <= accept) {
+      aa_ok = true;
+      // d = exp(y) is in w.d from the last evaluation
+      PR_CUDA(cudaMemcpyAsync(op->scale.ptr, w.d.ptr, n * 8, cudaMemcpyDeviceToDevice, s));
+      op->method = PR_BALANCE_ANDERSON;
+      op->iterations = iters;
+    }
+  }
+  if (aa_ok) return PR_OK;
+  // ---- damped multiplicative iteration from y = 0 (exchange.py:185-196)
+  PR_CUDA(cudaMemsetAsync(w.y.ptr, 0, n * sizeof(double), s));
+  double* y = w.y.ptr;
+  double* y_next = w.y2.ptr;
+  PR_TRY(balance_eval(op, w, y, nullptr, 1, y_next, &sc, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  for (int it = 1; it <= 20000; ++it) {
+    if (sc.bad > 0) break;
+    std::swap(y, y_next);
+    // closure at the updated y, and the next multiplicative step from the same product
+    PR_TRY(balance_eval(op, w, y, nullptr, 1, y_next, &sc, s));
+    PR_CUDA(cudaStreamSynchronize(s));
+    if (sc.bad > 0 || !std::isfinite(sc.closure)) break;
+    if (sc.closure <= fmin(tol, 1.0e-10)) {
+      PR_CUDA(cudaMemcpyAsync(op->scale.ptr, w.d.ptr, n * 8, cudaMemcpyDeviceToDevice, s));
+      op->method = PR_BALANCE_MULTIPLICATIVE;
+      op->iterations = it;
+      return PR_OK;
+    }
+  }
+  set_error("diagonal balancing of the exchange matrix did not converge");
+  return PR_ERR_BALANCE;
+}
+
+static bool all_equal_i64(const std::vector<int64_t>& v) {
+  for (size_t i = 1; i < v.size(); ++i)
+    if (v[i] != v[0]) return false;
+  return true;
+}
+static bool all_equal_f64(const std::vector<double>& v) {
+  for (size_t i = 1; i < v.size(); ++i)
+    if (v[i] != v[0]) return false;
+  return true;
+}
+
+int apply(const pr_operator* op, int which, const double* x_dev, double* y_dev, cudaStream_t s);
+
+int operator_create(const pr_counts* k, const int64_t* rays, const double* area, double delta, double tol,
+                    cudaStream_t s, pr_operator** out) {
+  const int64_t n = k->csr->n_rows;
+  std::unique_ptr<pr_operator> op(new pr_operator());
+  cudaGetDevice(&op->device);
+  op->n = n;
+  op->F = k->csr;
+  op->delta = delta;
+  op->last_stream = s;
+  PR_TRY(op->rays.alloc(n > 0 ? n : 1, s));
+  PR_TRY(op->area.alloc(n > 0 ? n : 1, s));
+  PR_TRY(op->scale.alloc(n > 0 ? n : 1, s));
+  std::vector<int64_t> h_rays(n);
+  std::vector<double> h_area(n);
+  if (n > 0) {
+    PR_CUDA(cudaMemcpyAsync(h_rays.data(), rays, n * 8, cudaMemcpyDefault, s));
+    PR_CUDA(cudaMemcpyAsync(h_area.data(), area, n * 8, cudaMemcpyDefault, s));
+    PR_CUDA(cudaStreamSynchronize(s));
+    PR_CUDA(cudaMemcpyAsync(op->rays.ptr, h_rays.data(), n * 8, cudaMemcpyHostToDevice, s));
+    PR_CUDA(cudaMemcpyAsync(op->area.ptr, h_area.data(), n * 8, cudaMemcpyHostToDevice, s));
+  }
+  const CountCsr& F = *op->F;
+  // accounting (exchange.py:68-71)
+  {
+    DevBuf<unsigned int> bad;
+    PR_TRY(bad.alloc(1, s));
+    PR_CUDA(cudaMemsetAsync(bad.ptr, 0, 4, s));
+    k_accounting<<<spmv_grid(n), 256, 0, s>>>(F.row_ptr.ptr, F.cnt.ptr, op->rays.ptr, n, bad.ptr);
+    PR_CUDA(cudaGetLastError());
+    unsigned int hb = 0;
+    PR_CUDA(cudaMemcpyAsync(&hb, bad.ptr, 4, cudaMemcpyDeviceToHost, s));
+    PR_CUDA(cudaStreamSynchronize(s));
+    if (hb) {
+      set_error("first-hit counts do not account for every emitted ray");
+      return PR_ERR_ACCOUNTING;
+    }
+  }
+  // symmetric matrix on the union pattern
+  {
+    auto T = std::make_shared<CountCsr>();
+    PR_TRY(build_transpose(F, *T, s));
+    DevBuf<int64_t> len;
+    PR_TRY(len.alloc(n > 0 ? n : 1, s));
+    k_union_len<<<grid_for(n, 128), 128, 0, s>>>(F.row_ptr.ptr, F.col.ptr, T->row_ptr.ptr, T->col.ptr, n, len.ptr);
+    PR_CUDA(cudaGetLastError());
+    SymCsr& S = op->S;
+    S.n_rows = n;
+    PR_TRY(S.row_ptr.alloc(n + 1, s));
+    PR_TRY(lengths_to_row_ptr(len.ptr, n, S.row_ptr.ptr, s));
+    int64_t nnz = 0;
+    PR_CUDA(cudaMemcpyAsync(&nnz, S.row_ptr.ptr + n, 8, cudaMemcpyDeviceToHost, s));
+    PR_CUDA(cudaStreamSynchronize(s));
+    S.nnz = nnz;
+    PR_TRY(S.col.alloc(nnz, s));
+    S.uniform = n > 0 && all_equal_i64(h_rays) && all_equal_f64(h_area) && h_rays[0] > 0 && 2 * h_rays[0] < INT32_MAX;
+    if (S.uniform) {
+      PR_TRY(S.pairsum.alloc(nnz, s));
+      S.factor = 0.5 * h_area[0] / (double)h_rays[0];
+      k_union_fill<true><<<grid_for(n, 128), 128, 0, s>>>(F.row_ptr.ptr, F.col.ptr, F.cnt.ptr, T->row_ptr.ptr,
+                                                          T->col.ptr, T->cnt.ptr, op->rays.ptr, op->area.ptr, n,
+                                                          S.row_ptr.ptr, S.col.ptr, nullptr, S.pairsum.ptr);
+    } else {
+      PR_TRY(S.val.alloc(nnz, s));
+      k_union_fill<false><<<grid_for(n, 128), 128, 0, s>>>(F.row_ptr.ptr, F.col.ptr, F.cnt.ptr, T->row_ptr.ptr,
+                                                           T->col.ptr, T->cnt.ptr, op->rays.ptr, op->area.ptr, n,
+                                                           S.row_ptr.ptr, S.col.ptr, S.val.ptr, nullptr);
+    }
+    PR_CUDA(cudaGetLastError());
+    op->FT = T;  // kept for raw_rmatvec
+  }
+  if (n > 0) {
+    PR_TRY(balance(op.get(), tol, s));
+    // row closure of F_p (exchange.py:78-80)
+    DevBuf<double> ones, r;
+    PR_TRY(ones.alloc(n, s));
+    PR_TRY(r.alloc(n, s));
+    std::vector<double> h1(n, 1.0);
+    PR_CUDA(cudaMemcpyAsync(ones.ptr, h1.data(), n * 8, cudaMemcpyHostToDevice, s));
+    PR_TRY(apply(op.get(), PR_APPLY_MATVEC, ones.ptr, r.ptr, s));
+    std::vector<double> hr(n);
+    PR_CUDA(cudaMemcpyAsync(hr.data(), r.ptr, n * 8, cudaMemcpyDeviceToHost, s));
+    PR_CUDA(cudaStreamSynchronize(s));
+    double e = 0.0;
+    for (int64_t i = 0; i < n; ++i) e = fmax(e, fabs(hr[i] - 1.0));
+    op->row_sum_error = e;
+    if (!(e <= 1.0e-10)) {
+      set_error("projected rows do not close: %.3e", e);
+      return PR_ERR_NOT_CLOSED;
+    }
+  }
+  PR_CUDA(cudaStreamSynchronize(s));
+  *out = op.release();
+  return PR_OK;
+}
+
+// y = product(x) with x, y device vectors of length n.
+int apply(const pr_operator* op, int which, const double* x, double* y, cudaStream_t s) {
+  const int64_t n = op->n;
+  if (n == 0) return PR_OK;
+  const CountCsr& F = *op->F;
+  if (which == PR_APPLY_RAW || which == PR_APPLY_RAW_T) {
+    const CountCsr& M = which == PR_APPLY_RAW ? F : *op->FT;
+    k_raw_apply<<<spmv_grid(n), 256, 0, s>>>(M.row_ptr.ptr, M.col.ptr, M.cnt.ptr, op->rays.ptr, n,
+                                             which == PR_APPLY_RAW_T, x, y);
+    PR_CUDA(cudaGetLastError());
+    return PR_OK;
+  }
+  int mode = which == PR_APPLY_SYM ? 0 : (which == PR_APPLY_MATVEC ? 1 : 2);
+  PR_ARG(which >= 0 && which <= PR_APPLY_RMATVEC, "unknown product %d", which);
+  DevBuf<double> u;
+  if (mode != 0) {
+    PR_TRY(u.alloc(n, s));
+    k_prep_u<<<grid_for(n, 256), 256, 0, s>>>(op->scale.ptr, op->area.ptr, x, n, mode, u.ptr);
+    PR_CUDA(cudaGetLastError());
+  }
+  SymView S = sym_view(op->S);
+  dispatch_uniform(op->S.uniform, [&](auto un) {
+    k_sym_apply<decltype(un)::value><<<spmv_grid(n), 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, x,
+                                                                   mode, u.ptr, y);
+  });
+  PR_CUDA(cudaGetLastError());
+  op->spmv_calls++;
+  return PR_OK;
+}
+
+int reciprocity_error(const pr_operator* op, double* out, cudaStream_t s) {
+  const int64_t n = op->n;
+  DevBuf<double> r;
+  PR_TRY(r.alloc(2, s));
+  PR_CUDA(cudaMemsetAsync(r.ptr, 0, 16, s));
+  const CountCsr& F = *op->F;
+  if (n > 0) {
+    k_reciprocity<<<grid_for(n, 256), 256, 0, s>>>(F.row_ptr.ptr, F.col.ptr, F.cnt.ptr, op->rays.ptr, op->area.ptr,
+                                                  op->scale.ptr, op->delta, n, r.ptr);
+    PR_CUDA(cudaGetLastError());
+  }
+  double h[2];
+  PR_CUDA(cudaMemcpyAsync(h, r.ptr, 16, cudaMemcpyDeviceToHost, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  const double tiny = 2.2250738585072014e-308;
+  *out = h[0] / fmax(h[1], tiny);
+  return PR_OK;
+}
+
+int operator_edges(const pr_operator* op, int32_t* origin, int32_t* receiver, double* weight, cudaStream_t s) {
+  const CountCsr& F = *op->F;
+  const int64_t m = F.nnz, n = op->n;
+  if (m == 0) return PR_OK;
+  DevBuf<int32_t> o;
+  DevBuf<double> w;
+  if (origin) PR_TRY(o.alloc(m, s));
+  if (weight) PR_TRY(w.alloc(m, s));
+  k_edges_out<<<spmv_grid(n), 256, 0, s>>>(F.row_ptr.ptr, F.cnt.ptr, op->rays.ptr, n, origin ? o.ptr : nullptr,
+                                           weight ? w.ptr : nullptr);
+  PR_CUDA(cudaGetLastError());
+  if (origin) PR_CUDA(cudaMemcpyAsync(origin, o.ptr, m * 4, cudaMemcpyDefault, s));
+  if (receiver) PR_CUDA(cudaMemcpyAsync(receiver, F.col.ptr, m * 4, cudaMemcpyDefault, s));
+  if (weight) PR_CUDA(cudaMemcpyAsync(weight, w.ptr, m * 8, cudaMemcpyDefault, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  return PR_OK;
+}
+
+}  // namespace pr

@@ -1,0 +1,106 @@
+// Internal plumbing of libporerad: status codes, the thread-local error message,
+// CUDA error checks and stream-ordered device buffers.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+#include <stdarg.h>
+#include <string>
+#include <utility>
+
+#include "../../include/porerad.h"
+
+namespace pr {
+
+void set_error(const char* fmt, ...);
+
+#define PR_CUDA(expr)                                                                      \
+  do {                                                                                     \
+    cudaError_t _e = (expr);                                                               \
+    if (_e != cudaSuccess) {                                                               \
+      ::pr::set_error("CUDA error %s (%s) at %s:%d: %s", cudaGetErrorName(_e),             \
+                      cudaGetErrorString(_e), __FILE__, __LINE__, #expr);                  \
+      return PR_ERR_CUDA;                                                                  \
+    }                                                                                      \
+  } while (0)
+
+#define PR_TRY(expr)            \
+  do {                          \
+    int _s = (expr);            \
+    if (_s != PR_OK) return _s; \
+  } while (0)
+
+#define PR_ARG(cond, ...)                 \
+  do {                                    \
+    if (!(cond)) {                        \
+      ::pr::set_error(__VA_ARGS__);       \
+      return PR_ERR_ARG;                  \
+    }                                     \
+  } while (0)
+
+// A device allocation owned by the library, released in stream order.
+template <typename T>
+struct DevBuf {
+  T* ptr = nullptr;
+  size_t n = 0;
+  cudaStream_t stream = nullptr;
+
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept { *this = std::move(o); }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      ptr = o.ptr;
+      n = o.n;
+      stream = o.stream;
+      o.ptr = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+
+  int alloc(size_t count, cudaStream_t s) {
+    release();
+    stream = s;
+    n = count;
+    if (count == 0) return PR_OK;
+    cudaError_t e = cudaMallocAsync((void**)&ptr, count * sizeof(T), s);
+    if (e != cudaSuccess) {
+      ptr = nullptr;
+      n = 0;
+      set_error("device allocation of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+      return e == cudaErrorMemoryAllocation ? PR_ERR_OOM : PR_ERR_CUDA;
+    }
+    return PR_OK;
+  }
+  void release() {
+    if (ptr) cudaFreeAsync(ptr, stream);
+    ptr = nullptr;
+    n = 0;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+inline int grid_for(int64_t n, int block, int cap = 148 * 32) {
+  int64_t g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (int)g;
+}
+
+inline int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+}  // namespace pr

@@ -1,0 +1,103 @@
+// Device-resident objects behind the opaque handles of porerad.h.
+#pragma once
+#include <memory>
+#include <vector>
+
+#include "pr_internal.cuh"
+
+namespace pr {
+
+// Switches to the object's device for the duration of a call.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// Sorted CSR of integer first-hit counts: row = origin patch, col = receiver patch.
+struct CountCsr {
+  int64_t n_rows = 0, nnz = 0;
+  DevBuf<int64_t> row_ptr;  // n_rows + 1
+  DevBuf<int32_t> col;      // nnz, ascending within a row
+  DevBuf<int32_t> cnt;      // nnz, > 0
+};
+
+// Symmetric exchange matrix S' = 0.5 (A F + F^T A) on the union pattern of F and F^T.
+// The support diagonal delta*A is applied separately.  Values are either binary64
+// (general areas / ray counts) or the integer pair sums n_ij + n_ji with one common
+// factor 0.5 A / R (every patch with the same area and the same ray count).
+struct SymCsr {
+  int64_t n_rows = 0, nnz = 0;
+  DevBuf<int64_t> row_ptr;
+  DevBuf<int32_t> col;
+  DevBuf<double> val;       // general form
+  DevBuf<int32_t> pairsum;  // uniform form
+  bool uniform = false;
+  double factor = 0.0;      // 0.5 A / R in the uniform form
+};
+
+}  // namespace pr
+
+struct pr_case {
+  int device = 0;
+  int64_t nx = 0, ny = 0, nz = 0, n_cells = 0;
+  int64_t n_patches = 0, n_wall = 0;
+  int wpr = 0;  // 32-bit occupancy words per (i, j) row
+  double H = 0.0, area = 0.0;
+  pr::DevBuf<uint8_t> solid;      // n_cells, 0/1
+  pr::DevBuf<uint32_t> occ;       // bit-packed solid flags, (nx*ny) rows of wpr words
+  pr::DevBuf<int8_t> cls;         // patch class 0 hot, 1 cold, 2 internal
+  pr::DevBuf<int8_t> face;        // patch face 0..5, -1 for walls
+  pr::DevBuf<int8_t> code;        // emission normal: 0..5 as +x,-x,+y,-y,+z,-z
+  pr::DevBuf<int32_t> cell;       // owning cell, -1 for walls
+  pr::DevBuf<double> origin;      // (P, 3)
+  pr::DevBuf<int32_t> cfp;        // cell_face_patch (n_cells, 6)
+  pr::DevBuf<int32_t> hot, cold;  // (ny, nz)
+  cudaStream_t last_stream = nullptr;
+  void rebind(cudaStream_t s) {
+    solid.stream = occ.stream = s;
+    cls.stream = face.stream = code.stream = s;
+    cell.stream = origin.stream = cfp.stream = hot.stream = cold.stream = s;
+  }
+  size_t device_bytes() const {
+    return solid.bytes() + occ.bytes() + cls.bytes() + face.bytes() + code.bytes() + cell.bytes() +
+           origin.bytes() + cfp.bytes() + hot.bytes() + cold.bytes();
+  }
+};
+
+struct pr_counts {
+  int device = 0;
+  std::shared_ptr<pr::CountCsr> csr;
+  pr::DevBuf<int64_t> rays;  // rays per origin
+  int64_t rays_traced = 0, dda_steps = 0;
+  cudaStream_t last_stream = nullptr;
+};
+
+struct pr_operator {
+  int device = 0;
+  int64_t n = 0;
+  std::shared_ptr<pr::CountCsr> F;
+  pr::DevBuf<int64_t> rays;   // R_i
+  pr::DevBuf<double> area;    // A_i
+  pr::SymCsr S;
+  pr::DevBuf<double> scale;   // d
+  double delta = 0.0;
+  int method = 0, iterations = 0;
+  double row_sum_error = 0.0;
+  mutable int64_t spmv_calls = 0;
+  // transposed count CSR (kept from the assembly for raw_rmatvec)
+  mutable std::shared_ptr<pr::CountCsr> FT;
+  // binary32 copy of S' for mixed-precision sweeps, built on first use:
+  // packed words (col << bits) | pair sum when they fit 32 bits, else col + float values
+  mutable pr::DevBuf<uint32_t> s32;
+  mutable pr::DevBuf<float> s32val;
+  mutable int s32_bits = -1;  // -1 not built; >= 1 packed; 0 col + float values
+  mutable cudaStream_t last_stream = nullptr;
+};

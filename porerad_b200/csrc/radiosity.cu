@@ -1,0 +1,639 @@
+// Gray-diffuse radiosity on the device.
+//
+// Reflection series (porerad/exchange.py:217-245): flight_0 = E; every reflection
+//   incident = F_p^T flight = d * S(d * (flight / A))          (exchange.py:119-122)
+//   absorbed += eps * incident;  flight = (1 - eps) * incident
+// until sum|flight| <= rtol * max(sum|E|, tiny).  One fused kernel per reflection
+// (SpMV + the three vector updates + block partial sums of |flight| and flight)
+// and a one-thread finish kernel that sums the partials in a fixed order and sets
+// a device flag; reflections launched after convergence return at once, so the
+// host checks the flag only once per batch of launches.
+//
+// Emission (exchange.py:248-271): E = eps sigma A T^4, or with a reference
+// temperature the factored eps sigma A ((T - Tr)(T + Tr)(T T + Tr Tr)).
+// Prescribed field (coupled.py:138-194): walls at T_m +/- dT/2, internal patches at
+// T_h - (i + 0.5) dT / nx of their cell; q_h, q_c, q_i = -sum(net of class) / (ny nz
+// (H / nx)^2); coarse source = cell power summed over min(8, n)^3 blocks split as
+// numpy.array_split does.
+//
+// Mixed precision: the same series with binary32 vectors and binary32 products of
+// the integer pair sums (exact in binary32), wrapped in binary64 iterative
+// refinement of the radiosity J = E + (1 - eps) F_p^T J: the residual
+// r = E - J + (1 - eps) F_p^T J and the absorbed power eps F_p^T J are binary64.
+#include <cmath>
+#include <vector>
+
+#include "pr_spmv.cuh"
+
+namespace pr {
+
+#define PR_SIGMA 5.670374419e-8  // porerad/constants.py:3
+
+struct SeriesState {
+  int done;        // 0 running, 1 converged, 2 reflection cap reached
+  int pad;
+  long long iters;
+  double residual;  // sum of the power in flight at convergence
+  double tol_abs;   // rtol * max(sum|E|, tiny)
+};
+
+template <bool kUniform>
+__global__ void __launch_bounds__(256) k_series_step(SymView S, double delta, const double* __restrict__ area,
+                                                     const double* __restrict__ d, const double* __restrict__ eps,
+                                                     const double* __restrict__ v_in, double* __restrict__ v_out,
+                                                     double* __restrict__ absorbed, double* __restrict__ partial,
+                                                     const SeriesState* __restrict__ state) {
+  if (state->done) return;
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  double acc[2] = {0.0, 0.0};
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < S.n; i += warps) {
+    const double Ai = area[i];
+    const double s = sym_row<kUniform>(S, i, v_in, lane) + delta * Ai * v_in[i];
+    if (lane == 0) {
+      const double inc = d[i] * s;
+      const double e = eps[i];
+      absorbed[i] += e * inc;
+      const double fl = (1.0 - e) * inc;
+      v_out[i] = d[i] * (fl / Ai);
+      acc[0] += fabs(fl);
+      acc[1] += fl;
+    }
+  }
+  block_sum_store<2>(acc, partial);
+}
+
+__global__ void k_series_finish(const double* __restrict__ partial, int blocks, long long max_it,
+                                SeriesState* __restrict__ state) {
+  if (threadIdx.x != 0 || state->done) return;
+  double a = 0.0, t = 0.0;
+  for (int b = 0; b < blocks; ++b) {
+    a += partial[2 * b];
+    t += partial[2 * b + 1];
+  }
+  state->iters += 1;
+  if (a <= state->tol_abs) {
+    state->done = 1;
+    state->residual = t;
+  } else if (state->iters >= max_it) {
+    state->done = 2;
+  }
+}
+
+// v = d * (x / A) and the block partials of |x|
+__global__ void __launch_bounds__(256) k_series_init(const double* __restrict__ x, const double* __restrict__ d,
+                                                     const double* __restrict__ area, int64_t n,
+                                                     double* __restrict__ v, double* __restrict__ absorbed,
+                                                     double* __restrict__ partial) {
+  double acc[1] = {0.0};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    v[i] = d[i] * (x[i] / area[i]);
+    absorbed[i] = 0.0;
+    acc[0] += fabs(x[i]);
+  }
+  block_sum_store<1>(acc, partial);
+}
+
+__global__ void k_series_tol(const double* __restrict__ partial, int blocks, double rtol,
+                             SeriesState* __restrict__ state) {
+  if (threadIdx.x != 0) return;
+  double a = 0.0;
+  for (int b = 0; b < blocks; ++b) a += partial[b];
+  const double tiny = 2.2250738585072014e-308;
+  state->done = 0;
+  state->iters = 0;
+  state->residual = 0.0;
+  state->tol_abs = rtol * fmax(a, tiny);
+}
+
+static int red_blocks() { return sm_count() * 4; }
+static int spmv_blocks(int64_t rows) { return grid_for(rows * 32, 256, sm_count() * 8); }
+
+// FP64 reflection series on device vectors: emitted (n), eps (n) -> absorbed (n).
+int series_fp64(const pr_operator* op, const double* emitted, const double* eps, double rtol, int64_t max_it,
+                double* absorbed, double* residual, int64_t* iterations, cudaStream_t s) {
+  const int64_t n = op->n;
+  const int rb = red_blocks();
+  const int sb = spmv_blocks(n);
+  DevBuf<double> va, vb, partial;
+  DevBuf<SeriesState> st;
+  PR_TRY(va.alloc(n, s));
+  PR_TRY(vb.alloc(n, s));
+  PR_TRY(partial.alloc((size_t)2 * (sb > rb ? sb : rb), s));
+  PR_TRY(st.alloc(1, s));
+  PR_CUDA(cudaMemsetAsync(st.ptr, 0, sizeof(SeriesState), s));
+  k_series_init<<<rb, 256, 0, s>>>(emitted, op->scale.ptr, op->area.ptr, n, va.ptr, absorbed, partial.ptr);
+  PR_CUDA(cudaGetLastError());
+  k_series_tol<<<1, 32, 0, s>>>(partial.ptr, rb, rtol, st.ptr);
+  PR_CUDA(cudaGetLastError());
+  SymView S = sym_view(op->S);
+  double* vin = va.ptr;
+  double* vout = vb.ptr;
+  SeriesState h;
+  int batch = 4;
+  for (int64_t launched = 0;;) {
+    for (int b = 0; b < batch; ++b) {
+      if (op->S.uniform)
+        k_series_step<true><<<sb, 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, eps, vin, vout, absorbed,
+                                               partial.ptr, st.ptr);
+      else
+        k_series_step<false><<<sb, 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, eps, vin, vout, absorbed,
+                                                partial.ptr, st.ptr);
+      k_series_finish<<<1, 32, 0, s>>>(partial.ptr, sb, (long long)max_it, st.ptr);
+      std::swap(vin, vout);
+    }
+    PR_CUDA(cudaGetLastError());
+    launched += batch;
+    PR_CUDA(cudaMemcpyAsync(&h, st.ptr, sizeof(h), cudaMemcpyDeviceToHost, s));
+    PR_CUDA(cudaStreamSynchronize(s));
+    if (h.done) break;
+    if (batch < 64) batch *= 2;
+  }
+  op->spmv_calls += h.iters;
+  if (h.done == 2) {
+    set_error("radiosity reflection series did not converge");
+    return PR_ERR_SERIES;
+  }
+  *residual = h.residual;
+  *iterations = h.iters;
+  return PR_OK;
+}
+
+// ------------------------------------------------------------------ emission / JVP
+
+__global__ void k_emission(const double* __restrict__ T, const double* __restrict__ eps,
+                           const double* __restrict__ area, int64_t n, int has_ref, double ref,
+                           double* __restrict__ e) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double t = T[i];
+    const double pre = eps[i] * PR_SIGMA * area[i];
+    e[i] = has_ref ? pre * ((t - ref) * (t + ref) * (t * t + ref * ref)) : pre * pow(t, 4.0);
+  }
+}
+
+__global__ void k_emission_derivative(const double* __restrict__ T, const double* __restrict__ dT,
+                                      const double* __restrict__ eps, const double* __restrict__ area, int64_t n,
+                                      double* __restrict__ e) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    e[i] = 4.0 * eps[i] * PR_SIGMA * area[i] * pow(T[i], 3.0) * dT[i];
+}
+
+__global__ void k_sub(const double* __restrict__ a, const double* __restrict__ b, int64_t n, double* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = a[i] - b[i];
+}
+
+int net_patch_power(const pr_operator* op, const double* T, const double* eps, const double* area, double rtol,
+                    int has_ref, double ref, int64_t max_it, double* emitted, double* absorbed, double* net,
+                    double* residual, int64_t* iterations, cudaStream_t s) {
+  const int64_t n = op->n;
+  DevBuf<double> dT, de, da, dE, dAb;
+  PR_TRY(dT.alloc(n, s));
+  PR_TRY(de.alloc(n, s));
+  PR_TRY(da.alloc(n, s));
+  PR_TRY(dE.alloc(n, s));
+  PR_TRY(dAb.alloc(n, s));
+  PR_CUDA(cudaMemcpyAsync(dT.ptr, T, n * 8, cudaMemcpyDefault, s));
+  PR_CUDA(cudaMemcpyAsync(de.ptr, eps, n * 8, cudaMemcpyDefault, s));
+  PR_CUDA(cudaMemcpyAsync(da.ptr, area, n * 8, cudaMemcpyDefault, s));
+  k_emission<<<grid_for(n, 256), 256, 0, s>>>(dT.ptr, de.ptr, da.ptr, n, has_ref, ref, dE.ptr);
+  PR_CUDA(cudaGetLastError());
+  double res = 0.0;
+  int64_t it = 0;
+  PR_TRY(series_fp64(op, dE.ptr, de.ptr, rtol, max_it, dAb.ptr, &res, &it, s));
+  if (emitted) PR_CUDA(cudaMemcpyAsync(emitted, dE.ptr, n * 8, cudaMemcpyDefault, s));
+  if (absorbed) PR_CUDA(cudaMemcpyAsync(absorbed, dAb.ptr, n * 8, cudaMemcpyDefault, s));
+  if (net) {
+    k_sub<<<grid_for(n, 256), 256, 0, s>>>(dAb.ptr, dE.ptr, n, dT.ptr);
+    PR_CUDA(cudaMemcpyAsync(net, dT.ptr, n * 8, cudaMemcpyDefault, s));
+  }
+  PR_CUDA(cudaStreamSynchronize(s));
+  if (residual) *residual = res;
+  if (iterations) *iterations = it;
+  return PR_OK;
+}
+
+int net_patch_power_jvp(const pr_operator* op, const double* T, const double* dTin, const double* eps,
+                        const double* area, double rtol, double* out, cudaStream_t s) {
+  const int64_t n = op->n;
+  DevBuf<double> dT, dd, de, da, dE, dAb;
+  PR_TRY(dT.alloc(n, s));
+  PR_TRY(dd.alloc(n, s));
+  PR_TRY(de.alloc(n, s));
+  PR_TRY(da.alloc(n, s));
+  PR_TRY(dE.alloc(n, s));
+  PR_TRY(dAb.alloc(n, s));
+  PR_CUDA(cudaMemcpyAsync(dT.ptr, T, n * 8, cudaMemcpyDefault, s));
+  PR_CUDA(cudaMemcpyAsync(dd.ptr, dTin, n * 8, cudaMemcpyDefault, s));
+  PR_CUDA(cudaMemcpyAsync(de.ptr, eps, n * 8, cudaMemcpyDefault, s));
+  PR_CUDA(cudaMemcpyAsync(da.ptr, area, n * 8, cudaMemcpyDefault, s));
+  k_emission_derivative<<<grid_for(n, 256), 256, 0, s>>>(dT.ptr, dd.ptr, de.ptr, da.ptr, n, dE.ptr);
+  PR_CUDA(cudaGetLastError());
+  double res = 0.0;
+  int64_t it = 0;
+  PR_TRY(series_fp64(op, dE.ptr, de.ptr, rtol, 10000, dAb.ptr, &res, &it, s));
+  k_sub<<<grid_for(n, 256), 256, 0, s>>>(dAb.ptr, dE.ptr, n, dT.ptr);
+  PR_CUDA(cudaMemcpyAsync(out, dT.ptr, n * 8, cudaMemcpyDefault, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  return PR_OK;
+}
+
+int reflection_series(const pr_operator* op, const double* emitted, const double* eps, double rtol, int64_t max_it,
+                      double* absorbed, double* residual, int64_t* iterations, cudaStream_t s) {
+  const int64_t n = op->n;
+  DevBuf<double> dE, de, dAb;
+  PR_TRY(dE.alloc(n, s));
+  PR_TRY(de.alloc(n, s));
+  PR_TRY(dAb.alloc(n, s));
+  PR_CUDA(cudaMemcpyAsync(dE.ptr, emitted, n * 8, cudaMemcpyDefault, s));
+  PR_CUDA(cudaMemcpyAsync(de.ptr, eps, n * 8, cudaMemcpyDefault, s));
+  PR_TRY(series_fp64(op, dE.ptr, de.ptr, rtol, max_it, dAb.ptr, residual, iterations, s));
+  PR_CUDA(cudaMemcpyAsync(absorbed, dAb.ptr, n * 8, cudaMemcpyDefault, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  return PR_OK;
+}
+
+// ------------------------------------------------------------------ prescribed-field channels
+
+// Patch temperature (coupled.py:45-53 with the linear field of coupled.py:138-143),
+// uniform emissivity and the T_ref-subtracted emission (exchange.py:268-270).
+__global__ void k_prescribed_emission(const int8_t* __restrict__ cls, const int32_t* __restrict__ cell,
+                                      const double* __restrict__ area, int64_t n, int64_t nyz, int64_t nx,
+                                      double T_m, double dT, double epsv, double* __restrict__ e,
+                                      double* __restrict__ eps) {
+  const double Th = T_m + dT / 2.0, Tc = T_m - dT / 2.0;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+    double t;
+    const int c = cls[p];
+    if (c == 0) t = Th;
+    else if (c == 1) t = Tc;
+    else {
+      const int64_t i = cell[p] / nyz;
+      t = (T_m + dT / 2.0) - (((double)i + 0.5) * dT) / (double)nx;
+    }
+    e[p] = epsv * PR_SIGMA * area[p] * ((t - T_m) * (t + T_m) * (t * t + T_m * T_m));
+    eps[p] = epsv;
+  }
+}
+
+// block partial sums of net power per class
+__global__ void __launch_bounds__(256) k_class_sums(const int8_t* __restrict__ cls, const double* __restrict__ ab,
+                                                    const double* __restrict__ e, int64_t n,
+                                                    double* __restrict__ partial) {
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+    const double net = ab[p] - e[p];
+    const int c = cls[p];
+    acc[0] += c == 0 ? net : 0.0;
+    acc[1] += c == 1 ? net : 0.0;
+    acc[2] += c == 2 ? net : 0.0;
+  }
+  block_sum_store<3>(acc, partial);
+}
+
+// numpy.array_split(arange(n), b): the first n % b parts have n / b + 1 items.
+__device__ __forceinline__ void split_range(int64_t n, int64_t b, int64_t part, int64_t& lo, int64_t& hi) {
+  const int64_t q = n / b, r = n % b;
+  lo = part * q + (part < r ? part : r);
+  hi = lo + q + (part < r ? 1 : 0);
+}
+
+// One block per coarse bin: sum of the net power of the internal patches of its cells.
+__global__ void __launch_bounds__(256) k_coarse(const int32_t* __restrict__ cfp, const double* __restrict__ ab,
+                                                const double* __restrict__ e, int64_t nx, int64_t ny, int64_t nz,
+                                                int bx, int by, int bz, double scale, double* __restrict__ out) {
+  const int bin = blockIdx.x;
+  const int a = bin / (by * bz), b = (bin / bz) % by, c = bin % bz;
+  int64_t x0, x1, y0, y1, z0, z1;
+  split_range(nx, bx, a, x0, x1);
+  split_range(ny, by, b, y0, y1);
+  split_range(nz, bz, c, z0, z1);
+  const int64_t sy = y1 - y0, sz = z1 - z0;
+  const int64_t cells = (x1 - x0) * sy * sz;
+  double acc[1] = {0.0};
+  for (int64_t t = threadIdx.x; t < cells; t += blockDim.x) {
+    const int64_t x = x0 + t / (sy * sz), y = y0 + (t / sz) % sy, z = z0 + t % sz;
+    const int64_t cell = (x * ny + y) * nz + z;
+    for (int f = 0; f < 6; ++f) {
+      const int32_t p = cfp[cell * 6 + f];
+      if (p >= 0) acc[0] += ab[p] - e[p];
+    }
+  }
+  __shared__ double part[1];
+  block_sum_store<1>(acc, part, 0);
+  if (threadIdx.x == 0) out[bin] = part[0] * scale;
+}
+
+// ------------------------------------------------------------------ mixed precision
+
+__global__ void k_pack_s32(const int32_t* __restrict__ col, const int32_t* __restrict__ pairsum,
+                           const double* __restrict__ val, int64_t m, int bits, uint32_t* __restrict__ w,
+                           float* __restrict__ fv) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < m; q += (int64_t)gridDim.x * blockDim.x) {
+    if (bits > 0) {
+      w[q] = ((uint32_t)col[q] << bits) | (uint32_t)pairsum[q];
+    } else {
+      w[q] = (uint32_t)col[q];
+      fv[q] = pairsum ? (float)pairsum[q] : (float)val[q];
+    }
+  }
+}
+
+__global__ void k_max_i32(const int32_t* __restrict__ a, int64_t m, unsigned int* __restrict__ out) {
+  unsigned int mx = 0;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < m; q += (int64_t)gridDim.x * blockDim.x)
+    mx = max(mx, (unsigned int)a[q]);
+  for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(PR_FULL, mx, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, mx);
+}
+
+static int build_s32(const pr_operator* op, cudaStream_t s) {
+  if (op->s32_bits >= 0) return PR_OK;
+  const SymCsr& S = op->S;
+  const int64_t m = S.nnz;
+  int bits = 0;
+  if (S.uniform && m > 0) {
+    DevBuf<unsigned int> mx;
+    PR_TRY(mx.alloc(1, s));
+    PR_CUDA(cudaMemsetAsync(mx.ptr, 0, 4, s));
+    k_max_i32<<<grid_for(m, 256), 256, 0, s>>>(S.pairsum.ptr, m, mx.ptr);
+    unsigned int h = 0;
+    PR_CUDA(cudaMemcpyAsync(&h, mx.ptr, 4, cudaMemcpyDeviceToHost, s));
+    PR_CUDA(cudaStreamSynchronize(s));
+    int kb = 1;
+    while (kb < 31 && ((unsigned long long)1 << kb) <= h) ++kb;
+    int cb = 1;
+    while (cb < 31 && ((int64_t)1 << cb) < S.n_rows) ++cb;
+    bits = (kb + cb <= 32) ? kb : 0;
+  }
+  PR_TRY(op->s32.alloc(m > 0 ? m : 1, s));
+  if (bits == 0) PR_TRY(op->s32val.alloc(m > 0 ? m : 1, s));
+  if (m > 0) {
+    k_pack_s32<<<grid_for(m, 256), 256, 0, s>>>(S.col.ptr, S.uniform ? S.pairsum.ptr : nullptr, S.val.ptr, m, bits,
+                                                 op->s32.ptr, bits ? nullptr : op->s32val.ptr);
+    PR_CUDA(cudaGetLastError());
+  }
+  op->s32_bits = bits;
+  return PR_OK;
+}
+
+struct S32View {
+  const int64_t* __restrict__ row_ptr;
+  const uint32_t* __restrict__ w;
+  const float* __restrict__ fv;
+  int bits;
+  float factor;  // 1 for float values
+  int64_t n;
+};
+
+template <bool kPacked>
+__device__ __forceinline__ float s32_row(const S32View& S, int64_t i, const float* __restrict__ u, int lane) {
+  const int64_t b = S.row_ptr[i], e = S.row_ptr[i + 1];
+  float acc = 0.0f;
+  const uint32_t mask = (1u << (S.bits & 31)) - 1u;
+  for (int64_t q = b + lane; q < e; q += 32) {
+    const uint32_t w = __ldg(S.w + q);
+    if (kPacked) acc = fmaf((float)(w & mask), __ldg(u + (w >> S.bits)), acc);
+    else acc = fmaf(__ldg(S.fv + q), __ldg(u + w), acc);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(PR_FULL, acc, o);
+  return acc * S.factor;
+}
+
+// One Chebyshev step on (I - om G) x = b in binary32 (Saad, Iterative Methods, Alg. 12.1):
+//   G d = scale * (S' u + delta A u), u = scale d / A;  x += d;  r -= (I - om G) d;
+//   d = c1 d + c2 r;  u_out = scale d / A.
+template <bool kPacked>
+__global__ void __launch_bounds__(256) k_cheb_step(S32View S, float delta, const float* __restrict__ scale,
+                                                   const float* __restrict__ area, const float* __restrict__ om,
+                                                   const float* __restrict__ u_in, float* __restrict__ u_out,
+                                                   float* __restrict__ x, float* __restrict__ r,
+                                                   float* __restrict__ d, float c1, float c2) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < S.n; i += warps) {
+    const float sum = s32_row<kPacked>(S, i, u_in, lane);
+    if (lane == 0) {
+      const float Ai = area[i], sc = scale[i];
+      const float gd = sc * (sum + delta * Ai * u_in[i]);
+      const float di = d[i];
+      const float ad = di - om[i] * gd;
+      x[i] += di;
+      const float ri = r[i] - ad;
+      r[i] = ri;
+      const float dn = c1 * di + c2 * ri;
+      d[i] = dn;
+      u_out[i] = sc * dn / Ai;
+    }
+  }
+}
+
+// J += x (when x != nullptr); u = scale J / A; also the binary32 copies of the coefficients.
+__global__ void k_refine_prep(double* __restrict__ J, const float* __restrict__ x, const double* __restrict__ scale,
+                              const double* __restrict__ area, int64_t n, double* __restrict__ u) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double j = J[i];
+    if (x) {
+      j += (double)x[i];
+      J[i] = j;
+    }
+    u[i] = scale[i] * (j / area[i]);
+  }
+}
+
+// Binary64 residual r = E - J + om G J, absorbed = eps G J; block partials of |r| and |E|;
+// binary32 start of the next correction solve: x = 0, r32 = d32 = r, u32 = scale r / A.
+template <bool kUniform>
+__global__ void __launch_bounds__(256) k_refine_residual(SymView S, double delta, const double* __restrict__ area,
+                                                         const double* __restrict__ scale,
+                                                         const double* __restrict__ eps, const double* __restrict__ E,
+                                                         const double* __restrict__ J, const double* __restrict__ u,
+                                                         double* __restrict__ absorbed, double* __restrict__ partial,
+                                                         float* __restrict__ x32, float* __restrict__ r32,
+                                                         float* __restrict__ d32, float* __restrict__ u32) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  double acc[2] = {0.0, 0.0};
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < S.n; i += warps) {
+    const double Ai = area[i];
+    const double s = sym_row<kUniform>(S, i, u, lane) + delta * Ai * u[i];
+    if (lane == 0) {
+      const double gj = scale[i] * s;
+      const double e = eps[i];
+      const double r = E[i] - J[i] + (1.0 - e) * gj;
+      absorbed[i] = e * gj;
+      acc[0] += fabs(r);
+      acc[1] += fabs(E[i]);
+      x32[i] = 0.0f;
+      r32[i] = (float)r;
+      d32[i] = (float)r;  // d0 = r0 / theta with theta = 1
+      u32[i] = (float)(scale[i] * (r / Ai));
+    }
+  }
+  block_sum_store<2>(acc, partial);
+}
+
+__global__ void k_to_f32(const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c,
+                         int64_t n, float* __restrict__ fa, float* __restrict__ fb, float* __restrict__ fc) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    fa[i] = (float)a[i];
+    fb[i] = (float)b[i];
+    fc[i] = (float)(1.0 - c[i]);
+  }
+}
+
+// Mixed-precision radiosity: binary64 refinement of J with binary32 Chebyshev
+// corrections; absorbed = eps G J from the last binary64 residual.  stats: outer
+// refinements, SpMVs (binary64 + binary32), final |r|_1 / |E|_1, binary32 sweeps per
+// correction.
+int series_mixed(const pr_operator* op, const double* emitted, const double* eps, double rtol, double* absorbed,
+                 double* stats, cudaStream_t s) {
+  const int64_t n = op->n;
+  PR_TRY(build_s32(op, s));
+  // spectral bound of om G: max(1 - eps) (F_p is row-stochastic, similar to symmetric)
+  std::vector<double> he(n);
+  PR_CUDA(cudaMemcpyAsync(he.data(), eps, n * 8, cudaMemcpyDeviceToHost, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  double rho = 0.0;
+  for (int64_t i = 0; i < n; ++i) rho = fmax(rho, 1.0 - he[i]);
+  rho = fmin(fmax(rho, 1e-3), 0.999999);
+  const double kappa = (1.0 + rho) / (1.0 - rho);
+  const double q = (sqrt(kappa) - 1.0) / (sqrt(kappa) + 1.0);
+  const double tol_in = 1.0e-5;
+  int k_in = (int)ceil(log(tol_in / 2.0) / log(q));
+  if (k_in < 2) k_in = 2;
+  if (k_in > 400) k_in = 400;
+
+  DevBuf<double> J, u, partial, sums;
+  DevBuf<float> x32, r32, d32, ua, ub, sc32, ar32, om32;
+  PR_TRY(J.alloc(n, s));
+  PR_TRY(u.alloc(n, s));
+  const int sb = spmv_blocks(n);
+  PR_TRY(partial.alloc((size_t)2 * sb, s));
+  PR_TRY(sums.alloc(2, s));
+  PR_TRY(x32.alloc(n, s));
+  PR_TRY(r32.alloc(n, s));
+  PR_TRY(d32.alloc(n, s));
+  PR_TRY(ua.alloc(n, s));
+  PR_TRY(ub.alloc(n, s));
+  PR_TRY(sc32.alloc(n, s));
+  PR_TRY(ar32.alloc(n, s));
+  PR_TRY(om32.alloc(n, s));
+  k_to_f32<<<grid_for(n, 256), 256, 0, s>>>(op->scale.ptr, op->area.ptr, eps, n, sc32.ptr, ar32.ptr, om32.ptr);
+  PR_CUDA(cudaMemsetAsync(J.ptr, 0, n * 8, s));
+  SymView S = sym_view(op->S);
+  S32View S32;
+  S32.row_ptr = op->S.row_ptr.ptr;
+  S32.w = op->s32.ptr;
+  S32.fv = op->s32val.ptr;
+  S32.bits = op->s32_bits;
+  S32.factor = op->S.uniform ? (float)op->S.factor : 1.0f;
+  S32.n = n;
+  const float c_delta = (float)op->delta;
+  const double sigma1 = 1.0 / rho;  // theta / delta with theta = 1, delta = rho
+  int outer = 0;
+  int64_t sp64 = 0, sp32 = 0;
+  double rel = 0.0;
+  for (;;) {
+    k_refine_prep<<<grid_for(n, 256), 256, 0, s>>>(J.ptr, outer > 0 ? x32.ptr : nullptr, op->scale.ptr,
+                                                    op->area.ptr, n, u.ptr);
+    if (op->S.uniform)
+      k_refine_residual<true><<<sb, 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, eps, emitted, J.ptr,
+                                                 u.ptr, absorbed, partial.ptr, x32.ptr, r32.ptr, d32.ptr, ua.ptr);
+    else
+      k_refine_residual<false><<<sb, 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, eps, emitted, J.ptr,
+                                                  u.ptr, absorbed, partial.ptr, x32.ptr, r32.ptr, d32.ptr, ua.ptr);
+    PR_CUDA(cudaGetLastError());
+    ++sp64;
+    PR_TRY(sum_partials(partial.ptr, sb, 2, sums.ptr, s));
+    double hs[2];
+    PR_CUDA(cudaMemcpyAsync(hs, sums.ptr, 16, cudaMemcpyDeviceToHost, s));
+    PR_CUDA(cudaStreamSynchronize(s));
+    rel = hs[0] / fmax(hs[1], 2.2250738585072014e-308);
+    if (rel <= rtol || outer >= 12) break;
+    // binary32 Chebyshev correction
+    double rho_k = 1.0 / sigma1;
+    float* uin = ua.ptr;
+    float* uout = ub.ptr;
+    for (int k = 0; k < k_in; ++k) {
+      const double rho_n = 1.0 / (2.0 * sigma1 - rho_k);
+      const float c1 = (float)(rho_n * rho_k), c2 = (float)(2.0 * rho_n / rho);
+      if (S32.bits > 0)
+        k_cheb_step<true><<<sb, 256, 0, s>>>(S32, c_delta, sc32.ptr, ar32.ptr, om32.ptr, uin, uout, x32.ptr, r32.ptr,
+                                             d32.ptr, c1, c2);
+      else
+        k_cheb_step<false><<<sb, 256, 0, s>>>(S32, c_delta, sc32.ptr, ar32.ptr, om32.ptr, uin, uout, x32.ptr,
+                                              r32.ptr, d32.ptr, c1, c2);
+      rho_k = rho_n;
+      std::swap(uin, uout);
+      ++sp32;
+    }
+    PR_CUDA(cudaGetLastError());
+    ++outer;
+  }
+  op->spmv_calls += sp64 + sp32;
+  if (!(rel <= rtol)) {
+    set_error("mixed-precision radiosity did not reach the relative residual %.1e (%.1e)", rtol, rel);
+    return PR_ERR_SERIES;
+  }
+  stats[0] = outer;
+  stats[1] = (double)(sp64 + sp32);
+  stats[2] = rel;
+  stats[3] = k_in;
+  return PR_OK;
+}
+
+
+int prescribed_channels(const pr_case* c, const pr_operator* op, double T_m, double dT, double epsv, int precision,
+                        double rtol, double* q, double* coarse, double* stats, cudaStream_t s) {
+  const int64_t n = c->n_patches;
+  PR_ARG(op->n == n, "operator has %lld patches, geometry %lld", (long long)op->n, (long long)n);
+  DevBuf<double> dE, de, dAb, partial, sums;
+  PR_TRY(dE.alloc(n, s));
+  PR_TRY(de.alloc(n, s));
+  PR_TRY(dAb.alloc(n, s));
+  const int rb = red_blocks();
+  PR_TRY(partial.alloc((size_t)3 * rb, s));
+  PR_TRY(sums.alloc(3, s));
+  k_prescribed_emission<<<grid_for(n, 256), 256, 0, s>>>(c->cls.ptr, c->cell.ptr, op->area.ptr, n, c->ny * c->nz,
+                                                        c->nx, T_m, dT, epsv, dE.ptr, de.ptr);
+  PR_CUDA(cudaGetLastError());
+  double st[4] = {0, 0, 0, 0};
+  if (precision == PR_PRECISION_MIXED) {
+    PR_TRY(series_mixed(op, dE.ptr, de.ptr, rtol, dAb.ptr, st, s));
+  } else {
+    double res = 0.0;
+    int64_t it = 0;
+    const int64_t calls0 = op->spmv_calls;
+    PR_TRY(series_fp64(op, dE.ptr, de.ptr, rtol, 10000, dAb.ptr, &res, &it, s));
+    st[0] = (double)it;
+    st[1] = (double)(op->spmv_calls - calls0);
+    st[2] = res;
+  }
+  k_class_sums<<<rb, 256, 0, s>>>(c->cls.ptr, dAb.ptr, dE.ptr, n, partial.ptr);
+  PR_CUDA(cudaGetLastError());
+  PR_TRY(sum_partials(partial.ptr, rb, 3, sums.ptr, s));
+  const double h = c->H / (double)c->nx;
+  const double xs = (double)(c->ny * c->nz) * (h * h);
+  DevBuf<double> dco;
+  int bx = (int)std::min<int64_t>(8, c->nx), by = (int)std::min<int64_t>(8, c->ny), bz = (int)std::min<int64_t>(8, c->nz);
+  if (coarse) {
+    PR_TRY(dco.alloc((size_t)bx * by * bz, s));
+    k_coarse<<<bx * by * bz, 256, 0, s>>>(c->cfp.ptr, dAb.ptr, dE.ptr, c->nx, c->ny, c->nz, bx, by, bz, 1.0 / xs,
+                                           dco.ptr);
+    PR_CUDA(cudaGetLastError());
+  }
+  double hs[3];
+  PR_CUDA(cudaMemcpyAsync(hs, sums.ptr, sizeof(hs), cudaMemcpyDeviceToHost, s));
+  if (coarse) PR_CUDA(cudaMemcpyAsync(coarse, dco.ptr, dco.bytes(), cudaMemcpyDefault, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  const double qh = -hs[0] / xs, qc = -hs[1] / xs, qi = -hs[2] / xs;
+  q[0] = qh;
+  q[1] = qc;
+  q[2] = qi;
+  q[3] = fabs(qh + qc + qi) / fmax(fmax(fabs(qh), fabs(qc)), fmax(fabs(qi), 1.0e-30));
+  if (stats) for (int k = 0; k < 4; ++k) stats[k] = st[k];
+  return PR_OK;
+}
+
+}  // namespace pr

@@ -1,0 +1,581 @@
+// Ray generation, first-hit traversal and per-patch count reduction on sm_100a.
+//
+// Ray stream (generate_rays, porerad/view_factors.py:135-182): ray r of patch p in
+// the block of seed s takes draws (p*R + r)*4 + c, c = 0..3, of that block's PCG64
+// stream.  Each thread jumps its stream there with the power-of-two affine maps of
+// the LCG, so rays are generated on the fly in any order and never stored.
+//   c = 0, 1: origin offsets clip(u, 1e-12, 1 - 1e-12) - 0.5 along the two face
+//             tangents, then y, z wrapped with NumPy's float remainder;
+//   c = 2, 3: radius = sqrt(u2), azimuth = (2 pi) u3, cos(theta) = sqrt(1 - u2);
+//             the direction is divided by sqrt((dx^2 + dy^2) + dz^2).
+// Traversal (_trace_kernel, view_factors.py:202-258): Amanatides-Woo cell walk in
+// binary64 with the 1e-12 tie tolerance, periodic y/z, exits through x < 0 (hot
+// wall) or x >= nx (cold wall), step cap max(10 N^3 + 10, min(8 nx (1 + (|dy|+|dz|)
+// /|dx|) + 100, 1e8)).  Every operation is an explicit round-to-nearest intrinsic,
+// so the arithmetic is the reference's operation for operation.  The occupancy
+// probe reads one bit of the packed grid (L1/L2 resident).
+#include <cub/device/device_scan.cuh>
+
+#include "pr_math.cuh"
+#include "pr_objects.cuh"
+
+namespace pr {
+
+#define PR_TIE 1.0e-12
+#define PR_FAR 1.0e300
+#define PR_TWO_PI 0x1.921fb54442d18p+2  // the binary64 product 2.0 * numpy.pi
+
+struct Geom {
+  const uint32_t* __restrict__ occ;
+  const int32_t* __restrict__ cfp;
+  const int32_t* __restrict__ hot;
+  const int32_t* __restrict__ cold;
+  int32_t nx, ny, nz, wpr;
+  int64_t n_cells;
+};
+
+struct RaySrc {
+  const double* __restrict__ origin;  // (P, 3)
+  const int8_t* __restrict__ code;    // emission normal 0..5
+  const pr_u128* __restrict__ maps;   // per seed: 128 entries (A_{2^i}, C_{2^i})
+  const pr_u128* __restrict__ state;  // per seed
+  const pr_u128* __restrict__ inc;    // per seed
+  double ny_d, nz_d;
+};
+
+__device__ __forceinline__ double clip_edge(double u) {
+  const double lo = 1.0e-12, hi = 1.0 - 1.0e-12;
+  return u < lo ? lo : (u > hi ? hi : u);
+}
+
+// Origin and unit direction of ray r of patch p, block s (view_factors.py:148-181).
+__device__ __forceinline__ void make_ray(const RaySrc& src, int64_t p, int64_t r, int64_t R, int s,
+                                         double o[3], double d[3]) {
+  const pr_u128* maps = src.maps + (int64_t)s * 128;
+  pr_u128 st = pr_pcg_jump(src.state[s], (uint64_t)((p * R + r) * 4), maps);
+  const pr_u128 inc = src.inc[s];
+  const double u0 = pr_pcg_next_double(&st, inc);
+  const double u1 = pr_pcg_next_double(&st, inc);
+  const double u2 = pr_pcg_next_double(&st, inc);
+  const double u3 = pr_pcg_next_double(&st, inc);
+  const int code = src.code[p];
+  const int ax = code >> 1;
+  const double sign = (code & 1) ? -1.0 : 1.0;
+  const int first = ax == 0 ? 1 : 0;
+  const int second = ax == 2 ? 1 : 2;
+  o[0] = src.origin[3 * p];
+  o[1] = src.origin[3 * p + 1];
+  o[2] = src.origin[3 * p + 2];
+  o[first] = pr_add(o[first], pr_sub(clip_edge(u0), 0.5));
+  o[second] = pr_add(o[second], pr_sub(clip_edge(u1), 0.5));
+  o[1] = pr_pymod_pos(o[1], src.ny_d);
+  o[2] = pr_pymod_pos(o[2], src.nz_d);
+  const double radius = pr_sqrt(u2);
+  double sn, cs;
+  pr_sincos(pr_mul(PR_TWO_PI, u3), &sn, &cs);
+  const double la = pr_mul(radius, cs);
+  const double lb = pr_mul(radius, sn);
+  const double polar = pr_sqrt(pr_sub(1.0, u2));
+  d[ax] = sign * polar;
+  d[first] = la;
+  d[second] = sign * lb;
+  const double len = pr_sqrt(pr_add(pr_add(pr_mul(d[0], d[0]), pr_mul(d[1], d[1])), pr_mul(d[2], d[2])));
+  d[0] = pr_div(d[0], len);
+  d[1] = pr_div(d[1], len);
+  d[2] = pr_div(d[2], len);
+}
+
+__device__ __forceinline__ int64_t first_cell(double pos, double dir) {
+  int64_t idx = (int64_t)floor(pos);
+  if (dir < 0.0 && fabs(pr_sub(pos, rint(pos))) <= PR_TIE) idx -= 1;
+  return idx;
+}
+
+__device__ __forceinline__ void axis_setup(double pos, double dir, int64_t idx, int& step, double& tmax,
+                                           double& tdel) {
+  if (dir > 0.0) {
+    step = 1;
+    tmax = pr_div(pr_sub(pr_add((double)idx, 1.0), pos), dir);
+    tdel = pr_div(1.0, dir);
+  } else if (dir < 0.0) {
+    step = -1;
+    tmax = pr_div(pr_sub((double)idx, pos), dir);
+    tdel = pr_div(-1.0, dir);
+  } else {
+    step = 0;
+    tmax = PR_FAR;
+    tdel = PR_FAR;
+  }
+}
+
+__device__ __forceinline__ int64_t imod(int64_t a, int64_t n) {
+  int64_t m = a % n;
+  return m < 0 ? m + n : m;
+}
+
+// First patch hit by the ray, or -1 when it resolves none (the reference's
+// failed flag); *steps counts the cells visited.
+__device__ int32_t dda_first_hit(const Geom& g, double ox, double oy, double oz, double dx, double dy,
+                                 double dz, int64_t* steps) {
+  *steps = 0;
+  if (dx == 0.0) return -1;
+  int64_t i = first_cell(ox, dx);
+  const int64_t j0 = first_cell(oy, dy), k0 = first_cell(oz, dz);
+  int sx, sy, sz;
+  double tx, ty, tz, ddx, ddy, ddz;
+  axis_setup(ox, dx, i, sx, tx, ddx);
+  axis_setup(oy, dy, j0, sy, ty, ddy);
+  axis_setup(oz, dz, k0, sz, tz, ddz);
+  int jj = (int)imod(j0, g.ny), kk = (int)imod(k0, g.nz);
+  double t = 0.0;
+  int face = -1;
+  double scale = pr_add(pr_mul(pr_mul(8.0, (double)g.nx),
+                               pr_add(1.0, pr_div(pr_add(fabs(dy), fabs(dz)), fabs(dx)))), 100.0);
+  if (scale > 100000000.0) scale = 100000000.0;
+  int64_t cap = 10 * g.n_cells + 10;
+  if ((int64_t)scale > cap) cap = (int64_t)scale;
+  int64_t it = 0;
+  for (; it < cap; ++it) {
+    if (i < 0 || i >= g.nx) {
+      const int64_t wj = imod((int64_t)floor(pr_add(oy, pr_mul(dy, t))), g.ny);
+      const int64_t wk = imod((int64_t)floor(pr_add(oz, pr_mul(dz, t))), g.nz);
+      *steps = it + 1;
+      return i < 0 ? g.hot[wj * g.nz + wk] : g.cold[wj * g.nz + wk];
+    }
+    const int64_t row = i * g.ny + jj;
+    const uint32_t word = __ldg(g.occ + row * g.wpr + (kk >> 5));
+    if ((word >> (kk & 31)) & 1u) {
+      *steps = it + 1;
+      return face >= 0 ? __ldg(g.cfp + (row * g.nz + kk) * 6 + face) : -1;
+    }
+    double tn = tx;
+    if (ty < tn) tn = ty;
+    if (tz < tn) tn = tz;
+    const bool cx = fabs(pr_sub(tx, tn)) <= PR_TIE;
+    const bool cy = fabs(pr_sub(ty, tn)) <= PR_TIE;
+    const bool cz = fabs(pr_sub(tz, tn)) <= PR_TIE;
+    if (cx) {
+      i += sx;
+      tx = pr_add(tx, ddx);
+      face = sx > 0 ? 1 : 0;
+    }
+    if (cy) {
+      jj += sy;
+      if (jj == g.ny) jj = 0;
+      else if (jj < 0) jj = g.ny - 1;
+      ty = pr_add(ty, ddy);
+      if (!cx) face = sy > 0 ? 3 : 2;
+    }
+    if (cz) {
+      kk += sz;
+      if (kk == g.nz) kk = 0;
+      else if (kk < 0) kk = g.nz - 1;
+      tz = pr_add(tz, ddz);
+      if (!cx && !cy) face = sz > 0 ? 5 : 4;
+    }
+    t = tn;
+  }
+  *steps = it;
+  return -1;
+}
+
+__device__ __forceinline__ void block_add_i64(int64_t v, unsigned long long* target) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(target, (unsigned long long)v);
+}
+
+// Fused generation + traversal for patches [p0, p0 + np) and n_seeds blocks: ray
+// (p, s, r) writes its receiver to recv[((p - p0) * S + s) * R + r].
+__global__ void __launch_bounds__(256) k_trace_blocks(Geom g, RaySrc src, int64_t p0, int64_t np, int64_t R,
+                                                      int S, int32_t* __restrict__ recv,
+                                                      unsigned long long* __restrict__ counters) {
+  const int64_t n = np * S * R;
+  int64_t my_steps = 0, my_fail = 0;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = q % R;
+    const int64_t ps = q / R;
+    const int s = (int)(ps % S);
+    const int64_t p = p0 + ps / S;
+    double o[3], d[3];
+    make_ray(src, p, r, R, s, o, d);
+    int64_t st = 0;
+    const int32_t hit = dda_first_hit(g, o[0], o[1], o[2], d[0], d[1], d[2], &st);
+    my_steps += st;
+    my_fail += hit < 0;
+    recv[q] = hit;
+  }
+  block_add_i64(my_steps, counters + 0);
+  block_add_i64(my_fail, counters + 1);
+}
+
+__global__ void k_generate(RaySrc src, int64_t p0, int64_t np, int64_t R, double* __restrict__ origins,
+                           double* __restrict__ dirs) {
+  const int64_t n = np * R;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+    double o[3], d[3];
+    make_ray(src, p0 + q / R, q % R, R, 0, o, d);
+    for (int c = 0; c < 3; ++c) {
+      origins[3 * q + c] = o[c];
+      dirs[3 * q + c] = d[c];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_trace_given(Geom g, const double* __restrict__ origins,
+                                                     const double* __restrict__ dirs, int64_t n,
+                                                     int32_t* __restrict__ recv,
+                                                     unsigned long long* __restrict__ counters) {
+  int64_t my_steps = 0, my_fail = 0;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+    int64_t st = 0;
+    const int32_t hit = dda_first_hit(g, origins[3 * q], origins[3 * q + 1], origins[3 * q + 2], dirs[3 * q],
+                                      dirs[3 * q + 1], dirs[3 * q + 2], &st);
+    my_steps += st;
+    my_fail += hit < 0;
+    recv[q] = hit;
+  }
+  block_add_i64(my_steps, counters + 0);
+  block_add_i64(my_fail, counters + 1);
+}
+
+// Per origin patch: sort its L receivers in shared memory (bitonic), run-length
+// encode into (receiver, count) pairs at out[(p - p0) * L ...], nnz[p - p0].
+__global__ void __launch_bounds__(512) k_patch_rle(const int32_t* __restrict__ recv, int64_t np, int L, int Lpad,
+                                                   int32_t* __restrict__ out_col, int32_t* __restrict__ out_cnt,
+                                                   int32_t* __restrict__ nnz) {
+  extern __shared__ int32_t sm[];
+  int32_t* key = sm;          // Lpad
+  int32_t* head = sm + Lpad;  // Lpad (positions of run heads)
+  __shared__ int32_t warp_tot[16];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int64_t p = blockIdx.x; p < np; p += gridDim.x) {
+    const int32_t* src = recv + p * L;
+    for (int i = tid; i < Lpad; i += nt) key[i] = i < L ? src[i] : INT32_MAX;
+    __syncthreads();
+    for (int k = 2; k <= Lpad; k <<= 1) {
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int t = tid; t < (Lpad >> 1); t += nt) {
+          const int a = ((t / j) * 2 * j) + (t % j);
+          const int b = a + j;
+          const bool up = (a & k) == 0;
+          const int32_t x = key[a], y = key[b];
+          if ((x > y) == up) {
+            key[a] = y;
+            key[b] = x;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    // heads: contiguous chunk per thread, then a block-wide exclusive scan
+    const int per = (L + nt - 1) / nt;
+    const int lo = tid * per, hi = min(L, lo + per);
+    int mine = 0;
+    for (int i = lo; i < hi; ++i) mine += (i == 0 || key[i] != key[i - 1]);
+    int incl = mine;
+    const int lane = tid & 31, wid = tid >> 5;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) warp_tot[wid] = incl;
+    __syncthreads();
+    int base = 0, total = 0;
+    for (int w = 0; w < (nt >> 5); ++w) {
+      if (w < wid) base += warp_tot[w];
+      total += warp_tot[w];
+    }
+    int u = base + incl - mine;
+    for (int i = lo; i < hi; ++i)
+      if (i == 0 || key[i] != key[i - 1]) head[u++] = i;
+    __syncthreads();
+    int32_t* oc = out_col + p * L;
+    int32_t* on = out_cnt + p * L;
+    for (int v = tid; v < total; v += nt) {
+      const int h = head[v];
+      const int e = v + 1 < total ? head[v + 1] : L;
+      oc[v] = key[h];
+      on[v] = e - h;
+    }
+    if (tid == 0) nnz[p] = total;
+    __syncthreads();
+  }
+}
+
+// Copy each row's unique pairs from the stage to its CSR position (warp per row).
+__global__ void k_compact_rows(const int32_t* __restrict__ st_col, const int32_t* __restrict__ st_cnt,
+                               const int32_t* __restrict__ nnz, const int64_t* __restrict__ off, int64_t np,
+                               int L, int64_t out_base, int32_t* __restrict__ col, int32_t* __restrict__ cnt) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t p = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); p < np; p += warps) {
+    const int m = nnz[p];
+    const int64_t dst = out_base + off[p];
+    for (int e = lane; e < m; e += 32) {
+      col[dst + e] = st_col[p * L + e];
+      cnt[dst + e] = st_cnt[p * L + e];
+    }
+  }
+}
+
+__global__ void k_i32_to_i64(const int32_t* __restrict__ in, int64_t* __restrict__ out, int64_t n) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+    out[t] = in[t];
+}
+
+__global__ void k_fill_i64(int64_t* __restrict__ out, int64_t n, int64_t v) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+    out[t] = v;
+}
+
+// ---------------------------------------------------------------------------- host
+
+static void host_u128_mul(const pr_u128& a, const pr_u128& b, pr_u128& r) {
+  unsigned __int128 x = ((unsigned __int128)a.hi << 64) | a.lo;
+  unsigned __int128 y = ((unsigned __int128)b.hi << 64) | b.lo;
+  unsigned __int128 z = x * y;
+  r.lo = (uint64_t)z;
+  r.hi = (uint64_t)(z >> 64);
+}
+static pr_u128 host_u128_add(const pr_u128& a, const pr_u128& b) {
+  unsigned __int128 x = ((unsigned __int128)a.hi << 64) | a.lo;
+  unsigned __int128 y = ((unsigned __int128)b.hi << 64) | b.lo;
+  unsigned __int128 z = x + y;
+  return pr_u128{(uint64_t)z, (uint64_t)(z >> 64)};
+}
+
+// Seed tables on the device: maps (S x 128), states (S), increments (S).
+struct SeedTables {
+  DevBuf<pr_u128> maps, state, inc;
+  int build(const pr_pcg64* seeds, int S, cudaStream_t s) {
+    std::vector<pr_u128> h_maps((size_t)S * 128), h_state(S), h_inc(S);
+    for (int q = 0; q < S; ++q) {
+      pr_pcg64 sd;
+      memcpy(&sd, seeds + q, sizeof(sd));  // seeds may be host memory only
+      h_state[q] = pr_u128{sd.state_lo, sd.state_hi};
+      h_inc[q] = pr_u128{sd.inc_lo, sd.inc_hi};
+      pr_u128 A{PR_PCG_MULT_LO, PR_PCG_MULT_HI}, C = h_inc[q];
+      for (int i = 0; i < 64; ++i) {
+        h_maps[(size_t)q * 128 + 2 * i] = A;
+        h_maps[(size_t)q * 128 + 2 * i + 1] = C;
+        // (A, C) o (A, C) = (A A, A C + C)
+        pr_u128 AA, AC;
+        host_u128_mul(A, A, AA);
+        host_u128_mul(A, C, AC);
+        C = host_u128_add(AC, C);
+        A = AA;
+      }
+    }
+    PR_TRY(maps.alloc(h_maps.size(), s));
+    PR_TRY(state.alloc(S, s));
+    PR_TRY(inc.alloc(S, s));
+    PR_CUDA(cudaMemcpyAsync(maps.ptr, h_maps.data(), h_maps.size() * sizeof(pr_u128), cudaMemcpyHostToDevice, s));
+    PR_CUDA(cudaMemcpyAsync(state.ptr, h_state.data(), S * sizeof(pr_u128), cudaMemcpyHostToDevice, s));
+    PR_CUDA(cudaMemcpyAsync(inc.ptr, h_inc.data(), S * sizeof(pr_u128), cudaMemcpyHostToDevice, s));
+    // the host vectors die at return: make the copies complete first
+    PR_CUDA(cudaStreamSynchronize(s));
+    return PR_OK;
+  }
+};
+
+static Geom geom_of(const pr_case* c) {
+  Geom g;
+  g.occ = c->occ.ptr;
+  g.cfp = c->cfp.ptr;
+  g.hot = c->hot.ptr;
+  g.cold = c->cold.ptr;
+  g.nx = (int32_t)c->nx;
+  g.ny = (int32_t)c->ny;
+  g.nz = (int32_t)c->nz;
+  g.wpr = c->wpr;
+  g.n_cells = c->n_cells;
+  return g;
+}
+
+static RaySrc src_of(const pr_case* c, const SeedTables& t) {
+  RaySrc r;
+  r.origin = c->origin.ptr;
+  r.code = c->code.ptr;
+  r.maps = t.maps.ptr;
+  r.state = t.state.ptr;
+  r.inc = t.inc.ptr;
+  r.ny_d = (double)c->ny;
+  r.nz_d = (double)c->nz;
+  return r;
+}
+
+static int trace_grid() { return sm_count() * 8; }
+
+int generate_rays(const pr_case* c, int64_t p0, int64_t p1, int64_t R, const pr_pcg64* seed, double* origins,
+                  double* dirs, cudaStream_t s) {
+  PR_ARG(p0 >= 0 && p1 >= p0 && p1 <= c->n_patches, "patch range [%lld, %lld) outside [0, %lld)",
+         (long long)p0, (long long)p1, (long long)c->n_patches);
+  PR_ARG(R >= 0, "rays_per_patch must be non-negative");
+  const int64_t n = (p1 - p0) * R;
+  if (n == 0) return PR_OK;
+  SeedTables t;
+  PR_TRY(t.build(seed, 1, s));
+  DevBuf<double> o, d;
+  PR_TRY(o.alloc(3 * n, s));
+  PR_TRY(d.alloc(3 * n, s));
+  k_generate<<<grid_for(n, 256, trace_grid()), 256, 0, s>>>(src_of(c, t), p0, p1 - p0, R, o.ptr, d.ptr);
+  PR_CUDA(cudaGetLastError());
+  PR_CUDA(cudaMemcpyAsync(origins, o.ptr, o.bytes(), cudaMemcpyDefault, s));
+  PR_CUDA(cudaMemcpyAsync(dirs, d.ptr, d.bytes(), cudaMemcpyDefault, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  return PR_OK;
+}
+
+int trace_given(const pr_case* c, const double* origins, const double* dirs, int64_t n, int32_t* receiver,
+                int64_t* n_failed, cudaStream_t s) {
+  if (n_failed) *n_failed = 0;
+  if (n == 0) return PR_OK;
+  DevBuf<double> o, d;
+  DevBuf<int32_t> rv;
+  DevBuf<unsigned long long> ctr;
+  PR_TRY(o.alloc(3 * n, s));
+  PR_TRY(d.alloc(3 * n, s));
+  PR_TRY(rv.alloc(n, s));
+  PR_TRY(ctr.alloc(2, s));
+  PR_CUDA(cudaMemcpyAsync(o.ptr, origins, o.bytes(), cudaMemcpyDefault, s));
+  PR_CUDA(cudaMemcpyAsync(d.ptr, dirs, d.bytes(), cudaMemcpyDefault, s));
+  PR_CUDA(cudaMemsetAsync(ctr.ptr, 0, ctr.bytes(), s));
+  k_trace_given<<<grid_for(n, 256, trace_grid()), 256, 0, s>>>(geom_of(c), o.ptr, d.ptr, n, rv.ptr, ctr.ptr);
+  PR_CUDA(cudaGetLastError());
+  unsigned long long h[2];
+  PR_CUDA(cudaMemcpyAsync(receiver, rv.ptr, rv.bytes(), cudaMemcpyDefault, s));
+  PR_CUDA(cudaMemcpyAsync(h, ctr.ptr, sizeof(h), cudaMemcpyDeviceToHost, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  if (n_failed) *n_failed = (int64_t)h[1];
+  if (h[1]) {
+    set_error("%lld rays did not resolve a receiving patch", (long long)h[1]);
+    return PR_ERR_UNRESOLVED;
+  }
+  return PR_OK;
+}
+
+// Largest rays-per-origin segment the shared-memory sort handles (128 KiB of keys + heads).
+static const int kMaxSegment = 16384;
+
+int first_hit_counts(const pr_case* c, int64_t R, const pr_pcg64* seeds, int S, cudaStream_t s, pr_counts** out) {
+  PR_ARG(R > 0 && S > 0, "rays_per_patch and the number of seeds must be positive");
+  const int64_t L64 = R * S;
+  if (L64 > kMaxSegment) {
+    set_error("%lld rays per origin patch exceed the %d supported in one call", (long long)L64, kMaxSegment);
+    return PR_ERR_LIMIT;
+  }
+  const int L = (int)L64;
+  int Lpad = 1;
+  while (Lpad < L) Lpad <<= 1;
+  if (Lpad < 64) Lpad = 64;
+  const int64_t P = c->n_patches;
+
+  SeedTables t;
+  PR_TRY(t.build(seeds, S, s));
+  std::unique_ptr<pr_counts> k(new pr_counts());
+  cudaGetDevice(&k->device);
+  k->csr = std::make_shared<CountCsr>();
+  CountCsr& csr = *k->csr;
+  csr.n_rows = P;
+  PR_TRY(csr.row_ptr.alloc(P + 1, s));
+  PR_TRY(k->rays.alloc(P, s));
+  k_fill_i64<<<grid_for(P, 256), 256, 0, s>>>(k->rays.ptr, P, L64);
+  PR_CUDA(cudaGetLastError());
+  if (P == 0) {
+    PR_CUDA(cudaMemsetAsync(csr.row_ptr.ptr, 0, sizeof(int64_t), s));
+    PR_CUDA(cudaStreamSynchronize(s));
+    *out = k.release();
+    return PR_OK;
+  }
+
+  // Patch chunks of about 2^26 rays bound the receiver and stage buffers.
+  int64_t chunk = ((int64_t)1 << 26) / L64;
+  if (chunk < 1) chunk = 1;
+  if (chunk > P) chunk = P;
+  DevBuf<int32_t> recv, st_col, st_cnt, nnz;
+  DevBuf<int64_t> off;
+  DevBuf<unsigned long long> ctr;
+  PR_TRY(recv.alloc(chunk * L64, s));
+  PR_TRY(st_col.alloc(chunk * L64, s));
+  PR_TRY(st_cnt.alloc(chunk * L64, s));
+  PR_TRY(nnz.alloc(chunk, s));
+  PR_TRY(off.alloc(chunk + 1, s));
+  PR_TRY(ctr.alloc(2, s));
+  PR_CUDA(cudaMemsetAsync(ctr.ptr, 0, ctr.bytes(), s));
+  size_t scan_bytes = 0;
+  PR_CUDA(cub::DeviceScan::InclusiveSum(nullptr, scan_bytes, off.ptr, off.ptr + 1, chunk, s));
+  DevBuf<uint8_t> scan_tmp;
+  PR_TRY(scan_tmp.alloc(scan_bytes + 16, s));
+  const size_t smem = (size_t)2 * Lpad * sizeof(int32_t);
+  PR_CUDA(cudaFuncSetAttribute(k_patch_rle, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int rle_threads = Lpad >= 1024 ? 512 : (Lpad >= 256 ? 256 : 64);
+
+  // per-chunk compacted pieces; concatenated once the total is known
+  struct Piece {
+    DevBuf<int32_t> col, cnt;
+    int64_t n;
+  };
+  std::vector<Piece> pieces;
+  DevBuf<int64_t> nnz_all;  // row lengths of every patch
+  PR_TRY(nnz_all.alloc(P, s));
+  int64_t total = 0;
+  PR_CUDA(cudaMemsetAsync(off.ptr, 0, sizeof(int64_t), s));
+  for (int64_t p0 = 0; p0 < P; p0 += chunk) {
+    const int64_t np = std::min(chunk, P - p0);
+    const int64_t nr = np * L64;
+    k_trace_blocks<<<grid_for(nr, 256, trace_grid()), 256, 0, s>>>(geom_of(c), src_of(c, t), p0, np, R, S,
+                                                                    recv.ptr, ctr.ptr);
+    PR_CUDA(cudaGetLastError());
+    const int rle_grid = (int)std::min<int64_t>(np, (int64_t)sm_count() * 16);
+    k_patch_rle<<<rle_grid, rle_threads, smem, s>>>(recv.ptr, np, L, Lpad, st_col.ptr, st_cnt.ptr, nnz.ptr);
+    PR_CUDA(cudaGetLastError());
+    k_i32_to_i64<<<grid_for(np, 256), 256, 0, s>>>(nnz.ptr, nnz_all.ptr + p0, np);
+    PR_CUDA(cudaGetLastError());
+    PR_CUDA(cub::DeviceScan::InclusiveSum(scan_tmp.ptr, scan_bytes, nnz_all.ptr + p0, off.ptr + 1, np, s));
+    int64_t chunk_total = 0;
+    PR_CUDA(cudaMemcpyAsync(&chunk_total, off.ptr + np, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    PR_CUDA(cudaStreamSynchronize(s));
+    Piece pc;
+    pc.n = chunk_total;
+    PR_TRY(pc.col.alloc(chunk_total, s));
+    PR_TRY(pc.cnt.alloc(chunk_total, s));
+    k_compact_rows<<<grid_for(np * 32, 256), 256, 0, s>>>(st_col.ptr, st_cnt.ptr, nnz.ptr, off.ptr, np, L, 0,
+                                                          pc.col.ptr, pc.cnt.ptr);
+    PR_CUDA(cudaGetLastError());
+    total += chunk_total;
+    pieces.push_back(std::move(pc));
+  }
+  csr.nnz = total;
+  PR_TRY(csr.col.alloc(total, s));
+  PR_TRY(csr.cnt.alloc(total, s));
+  int64_t at = 0;
+  for (auto& pc : pieces) {
+    if (pc.n) {
+      PR_CUDA(cudaMemcpyAsync(csr.col.ptr + at, pc.col.ptr, pc.n * 4, cudaMemcpyDeviceToDevice, s));
+      PR_CUDA(cudaMemcpyAsync(csr.cnt.ptr + at, pc.cnt.ptr, pc.n * 4, cudaMemcpyDeviceToDevice, s));
+    }
+    at += pc.n;
+  }
+  {
+    size_t b = 0;
+    PR_CUDA(cub::DeviceScan::InclusiveSum(nullptr, b, nnz_all.ptr, csr.row_ptr.ptr + 1, P, s));
+    DevBuf<uint8_t> tmp;
+    PR_TRY(tmp.alloc(b + 16, s));
+    PR_CUDA(cudaMemsetAsync(csr.row_ptr.ptr, 0, sizeof(int64_t), s));
+    PR_CUDA(cub::DeviceScan::InclusiveSum(tmp.ptr, b, nnz_all.ptr, csr.row_ptr.ptr + 1, P, s));
+  }
+  unsigned long long h[2];
+  PR_CUDA(cudaMemcpyAsync(h, ctr.ptr, sizeof(h), cudaMemcpyDeviceToHost, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  k->rays_traced = P * L64;
+  k->dda_steps = (int64_t)h[0];
+  k->last_stream = s;
+  if (h[1]) {
+    set_error("%lld rays did not resolve a receiving patch", (long long)h[1]);
+    return PR_ERR_UNRESOLVED;
+  }
+  *out = k.release();
+  return PR_OK;
+}
+
+}  // namespace pr

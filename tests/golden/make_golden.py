@@ -1,0 +1,153 @@
+"""Regenerate the golden fixtures of tests/golden from the reference implementation.
+
+    python tests/golden/make_golden.py [--reference /root/reference]
+
+Runs the unmodified reference package ``porerad`` (moxi000/pore-radiation-ijhmt2026)
+on small seeded inputs and stores its outputs, so that the GPU parity tests can run
+where the reference is not installed:
+
+* ``small_<name>.npz``: phases, the full SurfacePatches table, the rays of one patch
+  range, the receivers of those rays, per-seed and pooled counts, the count hash,
+  the balanced operator (scale, method, row-sum error, reciprocity), one radiosity
+  solve with and without a reference temperature, one JVP, and the prescribed-field
+  channels (q_h, q_c, q_i, closure, coarse source) at two conditions.
+* ``canonical_<name>.npz``: the four canonical 128^3 microstructures of the
+  reference's data/microstructures (CC-BY 4.0, see README.md here), bit-packed.
+* ``count_hashes.json``: the stored first-hit count hashes of data/cases_coupled.csv
+  for those microstructures (columns raw_count_sha256_A/B) with their seeds.
+* ``prescribed_field.json``: archived prescribed-field rows of
+  results/prescribed_field.csv for the committed core microstructure, with its seeds.
+"""
+
+from __future__ import annotations
+
+import argparse
+import csv
+import hashlib
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+
+SMALL_CASES = {
+    # name: (shape, solid fraction, phase seed, H, seeds, rays per patch)
+    "box12": ((12, 10, 9), 0.30, 7, 0.01, [11, 2212], 16),
+    "cube20": ((20, 20, 20), 0.12, 3, 0.004, [5, 912345678901234567], 24),
+    "slab16": ((16, 24, 8), 0.20, 9, 0.02, [77, 78], 12),
+}
+CONDITIONS = [(700.0, 20.0, 0.6), (400.0, 100.0, 0.3)]
+CANONICAL = ["FA_canonical_phi0.10_N128", "FI_canonical_phi0.10_N128", "OF_canonical_phi0.10_N128",
+             "TL_canonical_phi0.10_N128"]
+CORE_CASE = "pf_OF_core_phi0.05_s3_x"
+
+
+def random_phases(shape, phi, seed):
+    rng = np.random.default_rng(seed)
+    field = rng.random(shape)
+    # a little spatial correlation: average with a rolled copy, then threshold at phi
+    field = (field + np.roll(field, 1, axis=0) + np.roll(field, 1, axis=2)) / 3.0
+    thr = np.quantile(field, phi)
+    return (field < thr).astype(np.uint8)
+
+
+def small_case(vf, ex, cp, name, spec):
+    shape, phi, pseed, H, seeds, R = spec
+    phases = random_phases(shape, phi, pseed)
+    patches = vf.build_surface_patches(phases, H)
+    n = patches.n_patches
+    p0, p1 = min(3, n), min(40, n)
+    o, d = vf.generate_rays(patches, p0, p1, R, seeds[0])
+    rec = vf.trace_first_hit(patches, o, d)
+    per_seed = [vf.first_hit_counts(patches, R, s, patch_chunk=max(1, n // 3)) for s in seeds]
+    pooled = vf.pool_counts(per_seed, n)
+    rays = np.full(n, R * len(seeds), np.int64)
+    op = ex.ExchangeOperator(*pooled, rays, patches.patch_area_m2)
+    rng = np.random.default_rng(pseed + 100)
+    T = 600.0 + 100.0 * rng.random(n)
+    eps = np.full(n, 0.7)
+    plain = ex.net_patch_power(op, T, eps, patches.patch_area_m2, relative_tolerance=1e-13)
+    refd = ex.net_patch_power(op, T, eps, patches.patch_area_m2, relative_tolerance=1e-13,
+                              reference_temperature_K=650.0)
+    dT = rng.standard_normal(n)
+    jvp = ex.net_patch_power_jvp(op, T, dT, eps, patches.patch_area_m2, relative_tolerance=1e-13)
+    x = rng.random(n)
+    out = dict(
+        phases=phases, H_m=np.float64(H), seeds=np.asarray(seeds, np.uint64), rays_per_patch=np.int64(R),
+        ray_range=np.asarray([p0, p1], np.int64), ray_origins=o, ray_directions=d, ray_receivers=rec,
+        pooled_origin=pooled[0], pooled_receiver=pooled[1], pooled_count=pooled[2],
+        count_hash=np.bytes_(vf.count_sha256(*pooled, rays)),
+        scale=op.scale, row_sum_error=np.float64(op.row_sum_error),
+        reciprocity_error=np.float64(op.reciprocity_error()),
+        balance_method=np.bytes_(op.balance_method), probe_x=x,
+        probe_raw=op.raw_matvec(x), probe_raw_t=op.raw_rmatvec(x), probe_sym=op.symmetric_matvec(x),
+        probe_matvec=op.matvec(x), probe_rmatvec=op.rmatvec(x),
+        T=T, eps=eps, dT=dT, plain_absorbed=plain.absorbed_power_W, plain_residual=np.float64(plain.residual_power_W),
+        plain_iterations=np.int64(plain.iterations), ref_absorbed=refd.absorbed_power_W,
+        ref_iterations=np.int64(refd.iterations), jvp=jvp,
+    )
+    for k, (o_, r_, c_) in enumerate(per_seed):
+        out[f"seed{k}_origin"], out[f"seed{k}_receiver"], out[f"seed{k}_count"] = o_, r_, c_
+    for field in ("solid", "patch_class", "patch_cell", "patch_face", "patch_origin", "patch_normal",
+                  "patch_area_m2", "cell_face_patch", "hot_wall_patch", "cold_wall_patch"):
+        out["patches_" + field] = getattr(patches, field)
+    ch = []
+    coarse = []
+    for Tm, dTm, e in CONDITIONS:
+        c = cp.prescribed_field_channels(op, patches, Tm, dTm, e)
+        ch.append([Tm, dTm, e, c.q_h, c.q_c, c.q_i, c.closure_rel])
+        coarse.append(c.coarse_source)
+    out["channels"] = np.asarray(ch)
+    out["coarse"] = np.asarray(coarse)
+    np.savez_compressed(HERE / f"small_{name}.npz", **out)
+    print(f"{name}: {n} patches, {pooled[2].size} pairs, {op.balance_method} {op.balance_iterations}")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    args = ap.parse_args()
+    ref = Path(args.reference)
+    sys.path.insert(0, str(ref))
+    from porerad import coupled as cp, exchange as ex, view_factors as vf  # noqa: E402
+
+    for name, spec in SMALL_CASES.items():
+        small_case(vf, ex, cp, name, spec)
+
+    rows = list(csv.DictReader(open(ref / "data" / "cases_coupled.csv")))
+    hashes = {}
+    for r in rows:
+        if r["microstructure"] in CANONICAL and r["raw_count_sha256_A"]:
+            key = f"{r['microstructure']}|{r['transfer_axis']}"
+            hashes[key] = dict(microstructure=r["microstructure"], axis=r["transfer_axis"], H_m=float(r["H_m"]),
+                               rays_per_patch=int(r["rays_per_patch_per_block"]),
+                               seeds_A=[int(s) for s in r["seeds_A"].split(";")],
+                               seeds_B=[int(s) for s in r["seeds_B"].split(";")],
+                               phase_sha256_x=r["phase_sha256_x"], sha256_A=r["raw_count_sha256_A"],
+                               sha256_B=r["raw_count_sha256_B"], source="data/cases_coupled.csv")
+    (HERE / "count_hashes.json").write_text(json.dumps(hashes, indent=1, sort_keys=True))
+    for name in CANONICAL + ["OF_core_phi0.05_s3"]:
+        ph = np.load(ref / "data" / "microstructures" / f"{name}.npz")["phases"]
+        assert ph.dtype == np.uint8 and set(np.unique(ph)) <= {0, 1}
+        np.savez_compressed(HERE / f"canonical_{name}.npz", bits=np.packbits(ph.ravel()),
+                            shape=np.asarray(ph.shape, np.int64),
+                            sha256=np.bytes_(hashlib.sha256(ph.tobytes()).hexdigest()))
+
+    case = next(r for r in csv.DictReader(open(ref / "data" / "cases_prescribed_field.csv"))
+                if r["case_id"] == CORE_CASE)
+    res = [r for r in csv.DictReader(open(ref / "results" / "prescribed_field.csv")) if r["case_id"] == CORE_CASE]
+    pf = dict(case_id=CORE_CASE, microstructure=case["microstructure"], axis=case["transfer_axis"],
+              H_m=float(case["H_m"]), rays_per_patch=int(case["rays_per_patch_per_block"]),
+              seeds=[int(s) for k in ("seeds_A", "seeds_B") for s in case[k].split(";")],
+              phase_sha256_x=case["phase_sha256_x"], delta_T_K=20.0,
+              rows=[dict(T_mean_K=float(r["T_mean_K"]), epsilon=float(r["epsilon"]), q_h=float(r["q_h_W_m2"]),
+                         q_c=float(r["q_c_W_m2"]), q_i=float(r["q_i_W_m2"])) for r in res],
+              source="data/cases_prescribed_field.csv, results/prescribed_field.csv")
+    (HERE / "prescribed_field.json").write_text(json.dumps(pf, indent=1))
+    print("hash cases:", len(hashes))
+
+
+if __name__ == "__main__":
+    main()

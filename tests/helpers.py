@@ -1,0 +1,37 @@
+"""Fixture loaders shared by the tests (golden vectors made by tests/golden/make_golden.py)."""
+
+from __future__ import annotations
+
+import hashlib
+import json
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[1]
+GOLDEN = ROOT / "tests" / "golden"
+
+SMALL = ["box12", "cube20", "slab16"]
+
+
+def load_small(name: str) -> dict:
+    with np.load(GOLDEN / f"small_{name}.npz") as z:
+        return {k: z[k] for k in z.files}
+
+
+def load_canonical(name: str) -> np.ndarray:
+    with np.load(GOLDEN / f"canonical_{name}.npz") as z:
+        shape = tuple(int(s) for s in z["shape"])
+        ph = np.unpackbits(z["bits"])[: int(np.prod(shape))].reshape(shape).astype(np.uint8)
+        assert hashlib.sha256(ph.tobytes()).hexdigest() == z["sha256"].item().decode()
+    return ph
+
+
+def count_hash_cases() -> dict:
+    return json.loads((GOLDEN / "count_hashes.json").read_text())
+
+
+def prescribed_case() -> dict:
+    return json.loads((GOLDEN / "prescribed_field.json").read_text())
+
+
