@@ -1,0 +1,470 @@
+#!/usr/bin/env python
+"""Benchmark of the surface-radiation path on B200: first-hit rays/s and cases/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1] [--impl ours|reference]
+
+Workload c2 (default, the configuration the headline metric is quoted on): open-cell
+foam (OF) N=128^3, phi = 0.10, 64 Poisson seeds, geometry seed 1; 1000 rays per patch
+in two independently seeded sets A and B; eps = 0.6; prescribed field 650 -> 750 K
+along x (T_m 700 K, dT 100 K); H = 1 cm.
+
+One step = one case through the whole path, device-resident: surface patches ->
+fused ray generation + first-hit counts of set A and of set B -> pooled A+B counts ->
+three balanced exchange operators (A, B, A+B) -> mixed-precision radiosity channels
+for each (binary32 Chebyshev sweeps in binary64 refinement) -> q_h, q_c, q_i and
+the A/B wall-channel and coarse-source differences on the host.  ``value`` = rays
+traced per step x steps / device time; ``e2e`` = the same step through the public
+API from pinned host buffers (host->device copy of the phases and device->host copy
+of the results inside the timed region); ``plain`` = the drop-in NumPy API path of
+the reference's case driver (count tables and operators round-trip through host
+arrays, binary64 series).
+
+With --impl reference, the reference's CPU algorithm (the oracle port: NumPy PCG64
+rays + the OpenMP C traversal + np.unique) times a bounded sample of the same
+workload on all host cores.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    "c2": dict(workload="OF N=128^3 phi=0.10 (64 Poisson seeds, geometry seed 1), 1000 rays/patch x sets A,B, "
+                        "eps 0.6, T 650->750 K along x, FP32+FP64-refinement radiosity",
+               arch="OF", n=128, phi=0.10, seed=1, rays=1000, sets=2, eps=0.6, T_m=700.0, dT=100.0, H=0.01),
+    "c1": dict(workload="FI N=64^3 phi=0.10 (r=2, seed 0), 64 rays/patch x 1 set, eps 0.9, T 600->700 K along x, "
+                        "FP64 radiosity",
+               arch="FI", n=64, phi=0.10, seed=0, rays=64, sets=1, eps=0.9, T_m=650.0, dT=100.0, H=0.01),
+}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain drop-in path measurement")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of one baseline sample")
+    return ap.parse_args()
+
+
+def ray_seeds(cfg):
+    from porerad_b200.geometry import ray_set_seed
+
+    return [ray_set_seed(cfg["seed"], s) for s in range(cfg["sets"])]
+
+
+def make_phases(cfg):
+    from porerad_b200 import geometry
+
+    return geometry.make(cfg["arch"], cfg["n"], cfg["phi"], cfg["seed"])
+
+
+# --------------------------------------------------------------------------- our arm
+
+def served_step(phases, cfg, seeds, precision="mixed"):
+    """One case, device-resident; returns host scalars (the only device->host data)."""
+
+    from porerad_b200 import coupled, exchange, view_factors as vf
+
+    geo = vf.DeviceGeometry(phases, cfg["H"])
+    p = vf.SurfacePatches(H_m=cfg["H"], _device=geo)
+    tables = [vf.first_hit_counts_pooled(p, cfg["rays"], [s]) for s in seeds]
+    pooled = tables[0] if len(tables) == 1 else tables[0].merge(tables[1])
+    area = np.full(geo.n_patches, (cfg["H"] / cfg["n"]) ** 2)
+    P = geo.n_patches
+    out = {"rays": sum(t.rays_traced for t in tables), "steps": sum(t.dda_steps for t in tables),
+           "n_patches": P, "nnz": pooled.nnz, "sets": []}
+    n_ops = len(tables) + (1 if len(tables) > 1 else 0)
+    # host->device: phases (e2e form only), 128 jump maps per seed, rays + areas per operator;
+    # device->host: the scale vector per operator, q (4), coarse source (8^3) and stats (4) per solve
+    out["h2d"] = 32 * 130 * len(seeds) + n_ops * P * 16
+    out["d2h"] = n_ops * (P * 8 + 8 * (4 + 512 + 4))
+    ops = []
+    for t in tables if len(tables) > 1 else []:
+        rays = np.full(geo.n_patches, cfg["rays"], np.int64)
+        op = exchange.ExchangeOperator(t, None, None, rays, area)
+        ch = coupled.prescribed_field_channels(op, p, cfg["T_m"], cfg["dT"], cfg["eps"], precision=precision)
+        out["sets"].append(ch)
+        ops.append(op)
+    rays = np.full(geo.n_patches, cfg["rays"] * len(seeds), np.int64)
+    op = exchange.ExchangeOperator(pooled, None, None, rays, area)
+    ch = coupled.prescribed_field_channels(op, p, cfg["T_m"], cfg["dT"], cfg["eps"], precision=precision)
+    out["final"] = ch
+    out["nnz_symmetric"] = op.nnz_symmetric
+    out["balance"] = (op.balance_method, op.balance_iterations, op.row_sum_error)
+    out["_keep"] = (geo, p, tables, pooled, op, ops)
+    return out
+
+
+def release(res):
+    geo, p, tables, pooled, op, ops = res.pop("_keep")
+    for o in ops + [op]:
+        o.close()
+    for t in set(tables + [pooled]):
+        t.close()
+    geo.close()
+
+
+def plain_step(phases_host, cfg, seeds):
+    """The reference case driver's call sequence through the drop-in NumPy API."""
+
+    from porerad_b200 import coupled, exchange, view_factors as vf
+
+    p = vf.build_surface_patches(phases_host, cfg["H"])
+    counts = {s: vf.first_hit_counts(p, cfg["rays"], s) for s in seeds}
+    area = p.patch_area_m2
+    chs = []
+    groups = [[s] for s in seeds] + ([seeds] if len(seeds) > 1 else [])
+    for g in groups:
+        o, r, c = vf.pool_counts([counts[s] for s in g], p.n_patches)
+        op = exchange.ExchangeOperator(o, r, c, np.full(p.n_patches, cfg["rays"] * len(g), np.int64), area)
+        chs.append(coupled.prescribed_field_channels(op, p, cfg["T_m"], cfg["dT"], cfg["eps"]))
+        op.close()
+    return chs
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.is_file():
+        d = json.loads(path.read_text())
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def fp64_peak_tflops(torch) -> float:
+    """Measured binary64 throughput of this GPU: cuBLAS DGEMM 8192^3, best of 5 (CUDA events)."""
+
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2.0 * 8192**3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def ncu_traffic(kernel: str, workload: str):
+    """Per-ray DRAM traffic of a kernel from the committed ncu summary (profiles/), or None."""
+
+    path = ROOT / "profiles" / f"{kernel}_{workload}.md"
+    if not path.is_file():
+        return None
+    for line in path.read_text().splitlines():
+        if line.startswith("dram_bytes_per_ray:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
+def cpu_sample(cfg, seeds, target_s: float):
+    """The oracle (the reference's CPU algorithm) on a bounded patch sample of the workload, all host cores."""
+
+    from oracle import build as ob
+    from oracle import porerad_oracle as orc
+
+    ob.build()
+    cores = orc.set_threads()
+    phases = make_phases(cfg)
+    p = orc.build_surface_patches(phases, cfg["H"])
+    # calibrate on a small slice, then size the sample to about target_s seconds
+    t0 = time.perf_counter()
+    n0 = max(1, min(p.n_patches, 200_000 // cfg["rays"]))
+    o, d = orc.generate_rays(p, 0, n0, cfg["rays"], seeds[0])
+    orc.trace_first_hit(p, o, d)
+    rate = n0 * cfg["rays"] / (time.perf_counter() - t0)
+    n_patch = int(min(p.n_patches, max(1, target_s * rate / (cfg["rays"] * len(seeds)))))
+    t0 = time.perf_counter()
+    rays = 0
+    for s in seeds:
+        orc.first_hit_counts(p, cfg["rays"], s, patch_end=n_patch)
+        rays += n_patch * cfg["rays"]
+    dt = time.perf_counter() - t0
+    return {"value": rays / dt, "unit": "rays/s", "cores": cores, "kind": "port",
+            "sample": f"first-hit counts (NumPy PCG64 rays + OpenMP C traversal + np.unique) of patches "
+                      f"0..{n_patch - 1} of {p.n_patches} x {cfg['rays']} rays x {len(seeds)} sets, {dt:.1f} s"}
+
+
+def run_ours(args, cfg):
+    import torch
+
+    from porerad_b200 import _lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}")
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    lib = _lib.load()
+    seeds = ray_seeds(cfg)
+    phases_host = make_phases(cfg)
+    phases_dev = torch.from_numpy(phases_host).cuda()
+    pinned = torch.from_numpy(phases_host).pin_memory()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    for _ in range(args.warmup):
+        release(served_step(phases_dev, cfg, seeds))
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---- timed region: device-resident inputs
+    lib.pr_timers_reset()
+    lib.pr_timers_enable(1)
+    launches0 = lib.pr_kernel_launches()
+    rays = steps = 0
+    results = []
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            flush.fill_(1)  # 256 MiB write: L2 (126 MB) holds nothing of the previous step
+            res = served_step(phases_dev, cfg, seeds)
+            rays += res["rays"]
+            steps += res["steps"]
+            results.append(res)
+        e1.record()
+        torch.cuda.synchronize()
+    barrier()
+    launches = lib.pr_kernel_launches() - launches0
+    lib.pr_timers_enable(0)
+    ms = e0.elapsed_time(e1)
+    timers = {}
+    for name, tid in (("trace", _lib.TIMER_TRACE), ("rle", _lib.TIMER_RLE), ("balance", _lib.TIMER_BALANCE),
+                      ("series", _lib.TIMER_SERIES), ("cheb", _lib.TIMER_CHEB), ("refine", _lib.TIMER_REFINE)):
+        n, t = _lib.ctypes.c_longlong(), _lib.ctypes.c_double()
+        lib.pr_timers_read(tid, _lib.ctypes.byref(n), _lib.ctypes.byref(t))
+        timers[name] = (int(n.value), float(t.value))
+    last = results[-1]
+    nnz_s = last["nnz_symmetric"]
+    P = last["n_patches"]
+    for r in results:
+        release(r)
+
+    # ---- end to end through the public API from pinned host memory
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_rays = 0
+    for _ in range(args.steps):
+        res = served_step(pinned.numpy(), cfg, seeds)
+        e2e_rays += res["rays"]
+        release(res)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    h2d = int(phases_host.nbytes) + int(res["h2d"])
+    d2h = int(res["d2h"])
+
+    t_max = ms
+    if dist is not None:
+        tt = torch.tensor([ms, e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max, e2e_s = float(tt[0]), float(tt[1])
+    value = rays * world / (t_max * 1e-3)
+    line = None
+    if rank == 0:
+        # accuracy of the mixed solve against the binary64 series on the same operator
+        res64 = served_step(phases_dev, cfg, seeds, precision="fp64")
+        resm = served_step(phases_dev, cfg, seeds, precision="mixed")
+        f64, fm = res64["final"], resm["final"]
+        flux_err = max(abs(fm.q_h - f64.q_h) / abs(f64.q_h), abs(fm.q_c - f64.q_c) / abs(f64.q_c))
+        ab = None
+        if len(seeds) > 1:
+            from porerad_b200 import coupled
+
+            ab = coupled.ab_differences([resm["sets"][0]], [resm["sets"][1]])
+        release(res64)
+        release(resm)
+        plain = None
+        if not args.no_plain:
+            plain_step(phases_host, cfg, seeds)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            plain_step(phases_host, cfg, seeds)
+            torch.cuda.synchronize()
+            plain_s = time.perf_counter() - t0
+            plain = {"cases_per_s": 1.0 / plain_s, "s_per_case": plain_s,
+                     "path": "drop-in NumPy API: build_surface_patches, first_hit_counts per set, pool_counts, "
+                             "ExchangeOperator from host arrays, binary64 prescribed_field_channels"}
+        peaks, kind = measured_peaks()
+        fp64 = fp64_peak_tflops(torch)
+        n_tr, t_tr = timers["trace"]
+        flops = 4.0 * steps + 30.0 * rays
+        achieved = flops / (t_tr * 1e-3) / 1e12 if t_tr > 0 else None
+        per_ray_traffic = ncu_traffic("trace", args.workload)
+        roof = {"kernel": "k_trace_blocks (fused PCG64 ray generation + FP64 DDA)", "bound": "fp64",
+                "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
+                "frac": achieved / fp64 if achieved else None,
+                "traffic": per_ray_traffic * rays / max(n_tr, 1) if per_ray_traffic else None,
+                "launches": n_tr, "ms": t_tr,
+                "work": "4 FP64 ops per DDA step + 30 per ray (generation/setup); steps counted by the kernel",
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                "share_of_step": t_tr / ms}
+        spmv = {}
+        for name in ("balance", "series", "cheb", "refine"):
+            n_k, t_k = timers[name]
+            if n_k == 0:
+                continue
+            bytes_per = nnz_s * (8 if name != "cheb" else 4) + P * (8 + 5 * (8 if name != "cheb" else 4))
+            spmv[name] = {"launches": n_k, "ms": t_k, "GB_per_s": bytes_per * n_k / (t_k * 1e-3) / 1e9}
+        tot_b = sum(v["GB_per_s"] * v["ms"] for v in spmv.values())
+        tot_t = sum(v["ms"] for v in spmv.values())
+        roof_spmv = {"bound": "hbm", "achieved": tot_b / tot_t if tot_t else None, "peak": peaks["hbm_gbs"],
+                     "unit": "GB/s", "frac": (tot_b / tot_t) / peaks["hbm_gbs"] if tot_t else None,
+                     "peak_source": f"MEASURED_PEAKS.json ({kind})", "kernels": spmv,
+                     "share_of_step": tot_t / ms}
+        cpu = None if args.no_cpu else cpu_sample(cfg, seeds, args.cpu_seconds)
+        line = {
+            "metric": "first-hit rays/s (whole case: patches, counts A+B, 3 balanced operators, 3 mixed-precision "
+                      "radiosity solves)",
+            "value": value, "unit": "rays/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 (traversal), f32+f64 (radiosity)", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "archetype": cfg["arch"], "N": cfg["n"], "phi": cfg["phi"],
+                       "rays_per_patch": cfg["rays"], "ray_sets": len(seeds), "n_patches": P,
+                       "pairs_pooled": last["nnz"], "nnz_symmetric": nnz_s, "parallelism": f"replicas x{world}",
+                       "l2": "256 MiB flush write before every timed step; CSR working set > L2"},
+            "cases_per_s": world * args.steps / (t_max * 1e-3),
+            "e2e": {"value": e2e_rays * world / e2e_s, "unit": "rays/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "cases_per_s": world * args.steps / e2e_s},
+            "plain": plain,
+            "served_over_plain": (world * args.steps / e2e_s) / plain["cases_per_s"] if plain else None,
+            "mixed_vs_fp64_rel_flux_error": flux_err,
+            "ab_differences": {"wall_channel": ab[0], "coarse_source": ab[1]} if ab else None,
+            "q": {"q_h": f64.q_h, "q_c": f64.q_c, "q_i": f64.q_i},
+            "balance": {"method": last["balance"][0], "iterations": last["balance"][1],
+                        "row_sum_error": last["balance"][2]},
+            "rays_per_step": rays / args.steps, "dda_steps_per_ray": steps / rays,
+            "roofline": roof, "roofline_spmv": roof_spmv,
+            "clocks": clocks.summary(), "gpu_launches": int(launches), "cpu_baseline": cpu,
+        }
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return line
+
+
+# --------------------------------------------------------------------------- reference arm
+
+def run_reference(args, cfg):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    seeds = ray_seeds(cfg)
+    # warm-up runs of the sample, then K timed samples
+    for _ in range(max(0, args.warmup)):
+        cpu_sample(cfg, seeds, 1.0)
+    vals = []
+    last = None
+    for _ in range(args.steps):
+        last = cpu_sample(cfg, seeds, max(1.0, args.cpu_seconds / 2))
+        vals.append(last["value"])
+    value = float(np.mean(vals))
+    return {
+        "impl": "reference", "metric": "first-hit rays/s", "value": value, "unit": "rays/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "archetype": cfg["arch"], "N": cfg["n"],
+                   "rays_per_patch": cfg["rays"], "ray_sets": len(seeds)},
+        "cpu_baseline": {**last, "value": value},
+        "e2e": {"value": value, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse_args()
+    cfg = WORKLOADS[args.workload]
+    line = run_reference(args, cfg) if args.impl == "reference" else run_ours(args, cfg)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

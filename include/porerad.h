@@ -132,6 +132,9 @@ PR_API int pr_counts_copy(const pr_counts* k, int32_t* origin, int32_t* receiver
  * (origin, receiver) pairs of an arbitrary edge list into sorted CSR rows. */
 PR_API int pr_counts_from_edges(const int32_t* origin, const int32_t* receiver, const int64_t* count,
                          int64_t n_edges, int64_t n_patches, void* stream, pr_counts** out);
+/* pool_counts (view_factors.py:290-300) of two device tables of the same patches, e.g. ray
+ * sets A and B: rows merged, counts, rays per origin, rays traced and DDA steps summed. */
+PR_API int pr_counts_merge(const pr_counts* a, const pr_counts* b, void* stream, pr_counts** out);
 PR_API void pr_counts_destroy(pr_counts* k);
 
 /* ---- exchange operator -------------------------------------------------------
@@ -195,6 +198,17 @@ PR_API int pr_prescribed_field_channels(const pr_case* c, const pr_operator* op,
                                  double delta_T_K, double epsilon, int precision,
                                  double relative_tolerance, double* q, double* coarse,
                                  double* stats, void* stream);
+
+/* ---- instrumentation (no counterpart in the reference) ----------------------------
+ * Kernel classes timed with CUDA events on their launching stream while enabled:
+ * 0 fused ray generation + traversal, 1 per-patch count reduction, 2 balancing
+ * product, 3 reflection-series product, 4 binary32 Chebyshev sweep, 5 binary64
+ * refinement residual. */
+PR_API void pr_timers_enable(int on);
+PR_API void pr_timers_reset(void);
+PR_API int pr_timers_read(int kernel_class, long long* launches, double* total_ms);
+/* Number of the library's own kernel launches so far (CUB primitives not counted). */
+PR_API long long pr_kernel_launches(void);
 
 #ifdef __cplusplus
 }

@@ -216,14 +216,20 @@ def trace_first_hit(patches, origins, directions, *, return_steps: bool = False)
     return (receiver, steps) if return_steps else receiver
 
 
-def first_hit_counts(patches, rays_per_patch: int, seed: int, *, patch_chunk: int = 16384, stats=None):
-    """view_factors.py:273-287: per chunk of patches, unique (origin, receiver) pairs and counts."""
+def first_hit_counts(patches, rays_per_patch: int, seed: int, *, patch_chunk: int = 16384, stats=None,
+                     patch_end: int | None = None):
+    """view_factors.py:273-287: per chunk of patches, unique (origin, receiver) pairs and counts.
+
+    ``patch_end`` (not in the reference) stops after the origins below it, for
+    timing a bounded sample; the pair keys still span all patches.
+    """
 
     n = patches.n_patches
     R = int(rays_per_patch)
+    last = n if patch_end is None else min(int(patch_end), n)
     parts = []
-    for start in range(0, n, int(patch_chunk)):
-        end = min(start + int(patch_chunk), n)
+    for start in range(0, last, int(patch_chunk)):
+        end = min(start + int(patch_chunk), last)
         o, d = generate_rays(patches, start, end, R, seed)
         if stats is not None:
             rec, steps = trace_first_hit(patches, o, d, return_steps=True)

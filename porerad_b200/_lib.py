@@ -61,6 +61,7 @@ _SIGNATURES = {
                               ctypes.POINTER(_i64)]),
     "pr_counts_copy": (_i32, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "pr_counts_from_edges": (_i32, [_vp, _vp, _vp, _i64, _i64, _vp, ctypes.POINTER(_vp)]),
+    "pr_counts_merge": (_i32, [_vp, _vp, _vp, ctypes.POINTER(_vp)]),
     "pr_counts_destroy": (None, [_vp]),
     "pr_operator_create": (_i32, [_vp, _vp, _vp, _f64, _f64, _vp, ctypes.POINTER(_vp)]),
     "pr_operator_info": (_i32, [_vp, _vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32), ctypes.POINTER(_f64),
@@ -75,7 +76,13 @@ _SIGNATURES = {
                                   ctypes.POINTER(_f64), ctypes.POINTER(_i64), _vp]),
     "pr_net_patch_power_jvp": (_i32, [_vp, _vp, _vp, _vp, _vp, _f64, _vp, _vp]),
     "pr_prescribed_field_channels": (_i32, [_vp, _vp, _f64, _f64, _f64, _i32, _f64, _vp, _vp, _vp, _vp]),
+    "pr_timers_enable": (None, [_i32]),
+    "pr_timers_reset": (None, []),
+    "pr_timers_read": (_i32, [_i32, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_f64)]),
+    "pr_kernel_launches": (ctypes.c_longlong, []),
 }
+
+TIMER_TRACE, TIMER_RLE, TIMER_BALANCE, TIMER_SERIES, TIMER_CHEB, TIMER_REFINE = range(6)
 
 _lock = threading.Lock()
 _lib = None

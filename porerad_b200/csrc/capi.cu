@@ -37,6 +37,7 @@ int trace_given(const pr_case* c, const double* origins, const double* dirs, int
 int first_hit_counts(const pr_case* c, int64_t R, const pr_pcg64* seeds, int S, cudaStream_t s, pr_counts** out);
 int counts_from_edges(const int32_t* origin, const int32_t* receiver, const int64_t* count, int64_t m, int64_t n,
                       cudaStream_t s, pr_counts** out);
+int counts_merge(const pr_counts* A, const pr_counts* B, cudaStream_t s, pr_counts** out);
 int operator_create(const pr_counts* k, const int64_t* rays, const double* area, double delta, double tol,
                     cudaStream_t s, pr_operator** out);
 int apply(const pr_operator* op, int which, const double* x, double* y, cudaStream_t s);
@@ -152,7 +153,7 @@ int pr_case_patches(const pr_case* c, uint8_t* solid, int8_t* patch_class, int32
   if ((patch_normal || patch_area_m2) && P) {
     PR_TRY(tmp.alloc(3 * P, s));
     if (patch_normal) {
-      k_normals<<<grid_for(P, 256), 256, 0, s>>>(c->code.ptr, P, tmp.ptr);
+      ::pr::launch_mark(), k_normals<<<grid_for(P, 256), 256, 0, s>>>(c->code.ptr, P, tmp.ptr);
       PR_CUDA(cudaGetLastError());
       PR_CUDA(cudaMemcpyAsync(patch_normal, tmp.ptr, P * 24, cudaMemcpyDefault, s));
     }
@@ -160,7 +161,7 @@ int pr_case_patches(const pr_case* c, uint8_t* solid, int8_t* patch_class, int32
   if (patch_area_m2 && P) {
     DevBuf<double> a;
     PR_TRY(a.alloc(P, s));
-    k_fill_f64<<<grid_for(P, 256), 256, 0, s>>>(a.ptr, P, c->area);
+    ::pr::launch_mark(), k_fill_f64<<<grid_for(P, 256), 256, 0, s>>>(a.ptr, P, c->area);
     PR_CUDA(cudaGetLastError());
     PR_CUDA(cudaMemcpyAsync(patch_area_m2, a.ptr, P * 8, cudaMemcpyDefault, s));
     PR_CUDA(cudaStreamSynchronize(s));
@@ -239,7 +240,7 @@ int pr_counts_copy(const pr_counts* k, int32_t* origin, int32_t* receiver, int64
   if (m > 0 && (origin || count)) {
     if (origin) PR_TRY(o.alloc(m, s));
     if (count) PR_TRY(cn.alloc(m, s));
-    k_expand_rows<<<grid_for(n * 32, 256), 256, 0, s>>>(c.row_ptr.ptr, c.cnt.ptr, n, origin ? o.ptr : nullptr,
+    ::pr::launch_mark(), k_expand_rows<<<grid_for(n * 32, 256), 256, 0, s>>>(c.row_ptr.ptr, c.cnt.ptr, n, origin ? o.ptr : nullptr,
                                                         count ? cn.ptr : nullptr);
     PR_CUDA(cudaGetLastError());
     if (origin) PR_CUDA(cudaMemcpyAsync(origin, o.ptr, m * 4, cudaMemcpyDefault, s));
@@ -258,6 +259,16 @@ int pr_counts_from_edges(const int32_t* origin, const int32_t* receiver, const i
   PR_ARG(n_edges == 0 || (origin && receiver && count), "edge arrays must not be NULL");
   init_pool();
   return counts_from_edges(origin, receiver, count, n_edges, n_patches, (cudaStream_t)stream, out);
+}
+
+int pr_counts_merge(const pr_counts* a, const pr_counts* b, void* stream, pr_counts** out) {
+  PR_CHECK_NULL(a, "a");
+  PR_CHECK_NULL(b, "b");
+  PR_CHECK_NULL(out, "out");
+  *out = nullptr;
+  PR_ARG(a->device == b->device, "count tables live on different devices");
+  PR_ENTRY_GUARD(a);
+  return counts_merge(a, b, (cudaStream_t)stream, out);
 }
 
 void pr_counts_destroy(pr_counts* k) {

@@ -37,7 +37,7 @@ __global__ void k_sum_partials(const double* __restrict__ partial, int blocks, i
 }
 
 int sum_partials(const double* partial, int blocks, int K, double* out, cudaStream_t s) {
-  k_sum_partials<<<1, 32 * ((K + 31) / 32), 0, s>>>(partial, blocks, K, out);
+  ::pr::launch_mark(), k_sum_partials<<<1, 32 * ((K + 31) / 32), 0, s>>>(partial, blocks, K, out);
   PR_CUDA(cudaGetLastError());
   return PR_OK;
 }
@@ -123,7 +123,7 @@ int counts_from_edges(const int32_t* origin, const int32_t* receiver, const int6
   PR_TRY(bad.alloc(1, s));
   PR_CUDA(cudaMemsetAsync(bad.ptr, 0, 4, s));
   PR_TRY(row_len.alloc(n > 0 ? n : 1, s));
-  k_zero_i32<<<grid_for(n, 256), 256, 0, s>>>(row_len.ptr, n);
+  ::pr::launch_mark(), k_zero_i32<<<grid_for(n, 256), 256, 0, s>>>(row_len.ptr, n);
   int64_t u = 0;
   if (m > 0) {
     PR_TRY(o.alloc(m, s));
@@ -135,7 +135,7 @@ int counts_from_edges(const int32_t* origin, const int32_t* receiver, const int6
     PR_TRY(key.alloc(m, s));
     PR_TRY(key_sorted.alloc(m, s));
     PR_TRY(c_sorted.alloc(m, s));
-    k_edge_keys<<<grid_for(m, 256), 256, 0, s>>>(o.ptr, r.ptr, m, n, key.ptr, bad.ptr);
+    ::pr::launch_mark(), k_edge_keys<<<grid_for(m, 256), 256, 0, s>>>(o.ptr, r.ptr, m, n, key.ptr, bad.ptr);
     PR_CUDA(cudaGetLastError());
     int end_bit = 1;
     while (end_bit < 64 && (((unsigned long long)1 << end_bit) < (unsigned long long)n * (unsigned long long)n)) ++end_bit;
@@ -165,21 +165,79 @@ int counts_from_edges(const int32_t* origin, const int32_t* receiver, const int6
   PR_TRY(csr.col.alloc(u, s));
   PR_TRY(csr.cnt.alloc(u, s));
   if (u > 0) {
-    k_keys_to_csr<<<grid_for(u, 256), 256, 0, s>>>(ukey.ptr, sums.ptr, u, n, csr.col.ptr, csr.cnt.ptr, row_len.ptr,
+    ::pr::launch_mark(), k_keys_to_csr<<<grid_for(u, 256), 256, 0, s>>>(ukey.ptr, sums.ptr, u, n, csr.col.ptr, csr.cnt.ptr, row_len.ptr,
                                                   bad.ptr);
     PR_CUDA(cudaGetLastError());
   }
   PR_TRY(len64.alloc(n > 0 ? n : 1, s));
-  k_widen_scan_input<<<grid_for(n, 256), 256, 0, s>>>(row_len.ptr, len64.ptr, n);
+  ::pr::launch_mark(), k_widen_scan_input<<<grid_for(n, 256), 256, 0, s>>>(row_len.ptr, len64.ptr, n);
   PR_TRY(lengths_to_row_ptr(len64.ptr, n, csr.row_ptr.ptr, s));
   PR_CUDA(cudaMemcpyAsync(&hbad, bad.ptr, 4, cudaMemcpyDeviceToHost, s));
   PR_CUDA(cudaStreamSynchronize(s));
   PR_ARG(!(hbad & 2u), "pooled counts must be non-negative and below 2^31");
   // rays per origin = row sums of the pooled counts (callers usually pass their own)
   PR_TRY(k->rays.alloc(n > 0 ? n : 1, s));
-  k_row_sums<<<grid_for(n * 32, 256), 256, 0, s>>>(csr.row_ptr.ptr, csr.cnt.ptr, n, k->rays.ptr);
+  ::pr::launch_mark(), k_row_sums<<<grid_for(n * 32, 256), 256, 0, s>>>(csr.row_ptr.ptr, csr.cnt.ptr, n, k->rays.ptr);
   PR_CUDA(cudaGetLastError());
   PR_CUDA(cudaStreamSynchronize(s));
+  k->last_stream = s;
+  *out = k.release();
+  return PR_OK;
+}
+
+__global__ void k_union_len(const int64_t* __restrict__ fp, const int32_t* __restrict__ fc,
+                            const int64_t* __restrict__ tp, const int32_t* __restrict__ tc, int64_t n,
+                            int64_t* __restrict__ len);
+__global__ void k_merge_fill(const int64_t* __restrict__ ap, const int32_t* __restrict__ ac,
+                             const int32_t* __restrict__ an, const int64_t* __restrict__ bp,
+                             const int32_t* __restrict__ bc, const int32_t* __restrict__ bn, int64_t n,
+                             const int64_t* __restrict__ op, int32_t* __restrict__ oc, int32_t* __restrict__ on,
+                             unsigned int* __restrict__ bad);
+__global__ void k_add_i64(const int64_t* __restrict__ a, const int64_t* __restrict__ b, int64_t n,
+                          int64_t* __restrict__ out);
+
+// pool_counts of two device tables (view_factors.py:290-300): rows merged, counts and rays summed.
+int counts_merge(const pr_counts* A, const pr_counts* B, cudaStream_t s, pr_counts** out) {
+  const CountCsr& a = *A->csr;
+  const CountCsr& b = *B->csr;
+  PR_ARG(a.n_rows == b.n_rows, "count tables of %lld and %lld patches", (long long)a.n_rows, (long long)b.n_rows);
+  const int64_t n = a.n_rows;
+  std::unique_ptr<pr_counts> k(new pr_counts());
+  cudaGetDevice(&k->device);
+  k->csr = std::make_shared<CountCsr>();
+  CountCsr& c = *k->csr;
+  c.n_rows = n;
+  PR_TRY(c.row_ptr.alloc(n + 1, s));
+  DevBuf<int64_t> len;
+  DevBuf<unsigned int> bad;
+  PR_TRY(len.alloc(n > 0 ? n : 1, s));
+  PR_TRY(bad.alloc(1, s));
+  PR_CUDA(cudaMemsetAsync(bad.ptr, 0, 4, s));
+  if (n > 0) {
+    ::pr::launch_mark(), k_union_len<<<grid_for(n, 128), 128, 0, s>>>(a.row_ptr.ptr, a.col.ptr, b.row_ptr.ptr, b.col.ptr, n, len.ptr);
+    PR_CUDA(cudaGetLastError());
+  }
+  PR_TRY(lengths_to_row_ptr(len.ptr, n, c.row_ptr.ptr, s));
+  int64_t nnz = 0;
+  PR_CUDA(cudaMemcpyAsync(&nnz, c.row_ptr.ptr + n, 8, cudaMemcpyDeviceToHost, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  c.nnz = nnz;
+  PR_TRY(c.col.alloc(nnz, s));
+  PR_TRY(c.cnt.alloc(nnz, s));
+  PR_TRY(k->rays.alloc(n > 0 ? n : 1, s));
+  if (n > 0) {
+    ::pr::launch_mark(), k_merge_fill<<<grid_for(n, 128), 128, 0, s>>>(a.row_ptr.ptr, a.col.ptr, a.cnt.ptr, b.row_ptr.ptr, b.col.ptr,
+                                                  b.cnt.ptr, n, c.row_ptr.ptr, c.col.ptr, c.cnt.ptr, bad.ptr);
+    PR_CUDA(cudaGetLastError());
+    ::pr::launch_mark(), k_add_i64<<<grid_for(n, 256), 256, 0, s>>>(A->rays.ptr, B->rays.ptr, n, k->rays.ptr);
+    PR_CUDA(cudaGetLastError());
+  }
+  unsigned int hb = 0;
+  PR_CUDA(cudaMemcpyAsync(&hb, bad.ptr, 4, cudaMemcpyDeviceToHost, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  PR_ARG(!hb, "pooled counts exceed 2^31");
+  k->rays_traced = A->rays_traced + B->rays_traced;
+  k->dda_steps = A->dda_steps + B->dda_steps;
   k->last_stream = s;
   *out = k.release();
   return PR_OK;
@@ -216,12 +274,12 @@ int build_transpose(const CountCsr& F, CountCsr& T, cudaStream_t s) {
   DevBuf<int32_t> tlen;
   DevBuf<int64_t> tlen64;
   PR_TRY(tlen.alloc(n > 0 ? n : 1, s));
-  k_zero_i32<<<grid_for(n, 256), 256, 0, s>>>(tlen.ptr, n);
+  ::pr::launch_mark(), k_zero_i32<<<grid_for(n, 256), 256, 0, s>>>(tlen.ptr, n);
   if (m > 0) {
     DevBuf<unsigned long long> key, key_sorted;
     PR_TRY(key.alloc(m, s));
     PR_TRY(key_sorted.alloc(m, s));
-    k_transpose_keys<<<grid_for(n * 32, 256), 256, 0, s>>>(F.row_ptr.ptr, F.col.ptr, n, key.ptr);
+    ::pr::launch_mark(), k_transpose_keys<<<grid_for(n * 32, 256), 256, 0, s>>>(F.row_ptr.ptr, F.col.ptr, n, key.ptr);
     PR_CUDA(cudaGetLastError());
     int bits = 1;
     while (bits < 32 && ((int64_t)1 << bits) < n) ++bits;
@@ -230,11 +288,11 @@ int build_transpose(const CountCsr& F, CountCsr& T, cudaStream_t s) {
     DevBuf<uint8_t> tmp;
     PR_TRY(tmp.alloc(b + 16, s));
     PR_CUDA(cub::DeviceRadixSort::SortPairs(tmp.ptr, b, key.ptr, key_sorted.ptr, F.cnt.ptr, T.cnt.ptr, m, 0, 32 + bits, s));
-    k_split_transposed<<<grid_for(m, 256), 256, 0, s>>>(key_sorted.ptr, m, T.col.ptr, tlen.ptr);
+    ::pr::launch_mark(), k_split_transposed<<<grid_for(m, 256), 256, 0, s>>>(key_sorted.ptr, m, T.col.ptr, tlen.ptr);
     PR_CUDA(cudaGetLastError());
   }
   PR_TRY(tlen64.alloc(n > 0 ? n : 1, s));
-  k_widen_scan_input<<<grid_for(n, 256), 256, 0, s>>>(tlen.ptr, tlen64.ptr, n);
+  ::pr::launch_mark(), k_widen_scan_input<<<grid_for(n, 256), 256, 0, s>>>(tlen.ptr, tlen64.ptr, n);
   PR_TRY(lengths_to_row_ptr(tlen64.ptr, n, T.row_ptr.ptr, s));
   return PR_OK;
 }
@@ -287,6 +345,35 @@ __global__ void k_union_fill(const int64_t* __restrict__ fp, const int32_t* __re
       b += y == j;
     }
   }
+}
+
+// Pooled counts of two tables on the same patches: union of each row, counts summed.
+__global__ void k_merge_fill(const int64_t* __restrict__ ap, const int32_t* __restrict__ ac,
+                             const int32_t* __restrict__ an, const int64_t* __restrict__ bp,
+                             const int32_t* __restrict__ bc, const int32_t* __restrict__ bn, int64_t n,
+                             const int64_t* __restrict__ op, int32_t* __restrict__ oc, int32_t* __restrict__ on,
+                             unsigned int* __restrict__ bad) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t a = ap[i], ae = ap[i + 1], b = bp[i], be = bp[i + 1], o = op[i];
+    while (a < ae || b < be) {
+      const int32_t x = a < ae ? ac[a] : INT32_MAX;
+      const int32_t y = b < be ? bc[b] : INT32_MAX;
+      const int32_t j = x < y ? x : y;
+      const int64_t c = (int64_t)(x == j ? an[a] : 0) + (int64_t)(y == j ? bn[b] : 0);
+      if (c > INT32_MAX) atomicOr(bad, 1u);
+      oc[o] = j;
+      on[o] = (int32_t)c;
+      ++o;
+      a += x == j;
+      b += y == j;
+    }
+  }
+}
+
+__global__ void k_add_i64(const int64_t* __restrict__ a, const int64_t* __restrict__ b, int64_t n,
+                          int64_t* __restrict__ out) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+    out[t] = a[t] + b[t];
 }
 
 // Row sums of the counts must equal the rays of each origin (exchange.py:68-71).
@@ -564,11 +651,13 @@ static int balance_eval(pr_operator* op, BalanceWork& w, const double* y, double
                         BalanceScalars* out, cudaStream_t s) {
   const int64_t n = w.n;
   PR_CUDA(cudaMemsetAsync(w.sc.ptr, 0, 4 * sizeof(double), s));
-  k_exp_scale<<<grid_for(n, 256), 256, 0, s>>>(y, n, w.d.ptr, w.sc.ptr);
+  ::pr::launch_mark(), k_exp_scale<<<grid_for(n, 256), 256, 0, s>>>(y, n, w.d.ptr, w.sc.ptr);
   SymView S = sym_view(op->S);
   dispatch_uniform(op->S.uniform, [&](auto u) {
-    k_balance_eval<decltype(u)::value><<<spmv_grid(n), 256, 0, s>>>(S, op->delta, op->area.ptr, y, w.d.ptr, w.f.ptr,
+    ::pr::timer_begin(kTimerBalance, s);
+    ::pr::launch_mark(), k_balance_eval<decltype(u)::value><<<spmv_grid(n), 256, 0, s>>>(S, op->delta, op->area.ptr, y, w.d.ptr, w.f.ptr,
                                                                      dF, w.sc.ptr, mult, y_next);
+    ::pr::timer_end(kTimerBalance, s);
   });
   PR_CUDA(cudaGetLastError());
   op->spmv_calls++;
@@ -634,13 +723,13 @@ static int balance(pr_operator* op, double tol, cudaStream_t s) {
         oldest = (oldest + 1) % M;
       }
       st.slot = slot;
-      k_aa_update<<<grid_for(n, 256), 256, 0, s>>>(st, y, w.f.ptr, w.dY.ptr, w.dF.ptr, n, y_next, w.dY.ptr);
+      ::pr::launch_mark(), k_aa_update<<<grid_for(n, 256), 256, 0, s>>>(st, y, w.f.ptr, w.dY.ptr, w.dF.ptr, n, y_next, w.dY.ptr);
       PR_CUDA(cudaGetLastError());
       PR_TRY(balance_eval(op, w, y_next, w.dF.ptr + (size_t)slot * n, 0, nullptr, &sc, s));
       ++iters;
       std::swap(y, y_next);
       if (cols < M) ++cols;
-      k_aa_dots<<<rg, 256, 0, s>>>(w.dF.ptr, w.f.ptr, n, cols, slot, w.partial.ptr);
+      ::pr::launch_mark(), k_aa_dots<<<rg, 256, 0, s>>>(w.dF.ptr, w.f.ptr, n, cols, slot, w.partial.ptr);
       PR_CUDA(cudaGetLastError());
       PR_TRY(sum_partials(w.partial.ptr, rg, 20, w.dots.ptr, s));
       double hd[20];
@@ -729,7 +818,7 @@ int operator_create(const pr_counts* k, const int64_t* rays, const double* area,
     DevBuf<unsigned int> bad;
     PR_TRY(bad.alloc(1, s));
     PR_CUDA(cudaMemsetAsync(bad.ptr, 0, 4, s));
-    k_accounting<<<spmv_grid(n), 256, 0, s>>>(F.row_ptr.ptr, F.cnt.ptr, op->rays.ptr, n, bad.ptr);
+    ::pr::launch_mark(), k_accounting<<<spmv_grid(n), 256, 0, s>>>(F.row_ptr.ptr, F.cnt.ptr, op->rays.ptr, n, bad.ptr);
     PR_CUDA(cudaGetLastError());
     unsigned int hb = 0;
     PR_CUDA(cudaMemcpyAsync(&hb, bad.ptr, 4, cudaMemcpyDeviceToHost, s));
@@ -745,7 +834,7 @@ int operator_create(const pr_counts* k, const int64_t* rays, const double* area,
     PR_TRY(build_transpose(F, *T, s));
     DevBuf<int64_t> len;
     PR_TRY(len.alloc(n > 0 ? n : 1, s));
-    k_union_len<<<grid_for(n, 128), 128, 0, s>>>(F.row_ptr.ptr, F.col.ptr, T->row_ptr.ptr, T->col.ptr, n, len.ptr);
+    ::pr::launch_mark(), k_union_len<<<grid_for(n, 128), 128, 0, s>>>(F.row_ptr.ptr, F.col.ptr, T->row_ptr.ptr, T->col.ptr, n, len.ptr);
     PR_CUDA(cudaGetLastError());
     SymCsr& S = op->S;
     S.n_rows = n;
@@ -760,12 +849,12 @@ int operator_create(const pr_counts* k, const int64_t* rays, const double* area,
     if (S.uniform) {
       PR_TRY(S.pairsum.alloc(nnz, s));
       S.factor = 0.5 * h_area[0] / (double)h_rays[0];
-      k_union_fill<true><<<grid_for(n, 128), 128, 0, s>>>(F.row_ptr.ptr, F.col.ptr, F.cnt.ptr, T->row_ptr.ptr,
+      ::pr::launch_mark(), k_union_fill<true><<<grid_for(n, 128), 128, 0, s>>>(F.row_ptr.ptr, F.col.ptr, F.cnt.ptr, T->row_ptr.ptr,
                                                           T->col.ptr, T->cnt.ptr, op->rays.ptr, op->area.ptr, n,
                                                           S.row_ptr.ptr, S.col.ptr, nullptr, S.pairsum.ptr);
     } else {
       PR_TRY(S.val.alloc(nnz, s));
-      k_union_fill<false><<<grid_for(n, 128), 128, 0, s>>>(F.row_ptr.ptr, F.col.ptr, F.cnt.ptr, T->row_ptr.ptr,
+      ::pr::launch_mark(), k_union_fill<false><<<grid_for(n, 128), 128, 0, s>>>(F.row_ptr.ptr, F.col.ptr, F.cnt.ptr, T->row_ptr.ptr,
                                                            T->col.ptr, T->cnt.ptr, op->rays.ptr, op->area.ptr, n,
                                                            S.row_ptr.ptr, S.col.ptr, S.val.ptr, nullptr);
     }
@@ -804,7 +893,7 @@ int apply(const pr_operator* op, int which, const double* x, double* y, cudaStre
   const CountCsr& F = *op->F;
   if (which == PR_APPLY_RAW || which == PR_APPLY_RAW_T) {
     const CountCsr& M = which == PR_APPLY_RAW ? F : *op->FT;
-    k_raw_apply<<<spmv_grid(n), 256, 0, s>>>(M.row_ptr.ptr, M.col.ptr, M.cnt.ptr, op->rays.ptr, n,
+    ::pr::launch_mark(), k_raw_apply<<<spmv_grid(n), 256, 0, s>>>(M.row_ptr.ptr, M.col.ptr, M.cnt.ptr, op->rays.ptr, n,
                                              which == PR_APPLY_RAW_T, x, y);
     PR_CUDA(cudaGetLastError());
     return PR_OK;
@@ -814,12 +903,12 @@ int apply(const pr_operator* op, int which, const double* x, double* y, cudaStre
   DevBuf<double> u;
   if (mode != 0) {
     PR_TRY(u.alloc(n, s));
-    k_prep_u<<<grid_for(n, 256), 256, 0, s>>>(op->scale.ptr, op->area.ptr, x, n, mode, u.ptr);
+    ::pr::launch_mark(), k_prep_u<<<grid_for(n, 256), 256, 0, s>>>(op->scale.ptr, op->area.ptr, x, n, mode, u.ptr);
     PR_CUDA(cudaGetLastError());
   }
   SymView S = sym_view(op->S);
   dispatch_uniform(op->S.uniform, [&](auto un) {
-    k_sym_apply<decltype(un)::value><<<spmv_grid(n), 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, x,
+    ::pr::launch_mark(), k_sym_apply<decltype(un)::value><<<spmv_grid(n), 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, x,
                                                                    mode, u.ptr, y);
   });
   PR_CUDA(cudaGetLastError());
@@ -834,7 +923,7 @@ int reciprocity_error(const pr_operator* op, double* out, cudaStream_t s) {
   PR_CUDA(cudaMemsetAsync(r.ptr, 0, 16, s));
   const CountCsr& F = *op->F;
   if (n > 0) {
-    k_reciprocity<<<grid_for(n, 256), 256, 0, s>>>(F.row_ptr.ptr, F.col.ptr, F.cnt.ptr, op->rays.ptr, op->area.ptr,
+    ::pr::launch_mark(), k_reciprocity<<<grid_for(n, 256), 256, 0, s>>>(F.row_ptr.ptr, F.col.ptr, F.cnt.ptr, op->rays.ptr, op->area.ptr,
                                                   op->scale.ptr, op->delta, n, r.ptr);
     PR_CUDA(cudaGetLastError());
   }
@@ -854,7 +943,7 @@ int operator_edges(const pr_operator* op, int32_t* origin, int32_t* receiver, do
   DevBuf<double> w;
   if (origin) PR_TRY(o.alloc(m, s));
   if (weight) PR_TRY(w.alloc(m, s));
-  k_edges_out<<<spmv_grid(n), 256, 0, s>>>(F.row_ptr.ptr, F.cnt.ptr, op->rays.ptr, n, origin ? o.ptr : nullptr,
+  ::pr::launch_mark(), k_edges_out<<<spmv_grid(n), 256, 0, s>>>(F.row_ptr.ptr, F.cnt.ptr, op->rays.ptr, n, origin ? o.ptr : nullptr,
                                            weight ? w.ptr : nullptr);
   PR_CUDA(cudaGetLastError());
   if (origin) PR_CUDA(cudaMemcpyAsync(origin, o.ptr, m * 4, cudaMemcpyDefault, s));

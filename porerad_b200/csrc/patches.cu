@@ -162,17 +162,17 @@ int case_build(pr_case* c, const uint8_t* phases, cudaStream_t s) {
   PR_TRY(mask.alloc(n, s));
   PR_TRY(nf.alloc(n, s));
   PR_TRY(off.alloc(n, s));
-  k_cell_faces<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(ph.ptr, c->nx, c->ny, c->nz, c->solid.ptr, mask.ptr, nf.ptr);
+  ::pr::launch_mark(), k_cell_faces<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(ph.ptr, c->nx, c->ny, c->nz, c->solid.ptr, mask.ptr, nf.ptr);
   PR_CUDA(cudaGetLastError());
   c->wpr = (int)((c->nz + 31) / 32);
   const int64_t rows = c->nx * c->ny;
   PR_TRY(c->occ.alloc(rows * c->wpr, s));
-  k_pack_occupancy<<<grid_for(rows * c->wpr, 256, 148 * 16), 256, 0, s>>>(c->solid.ptr, rows, c->nz, c->wpr, c->occ.ptr);
+  ::pr::launch_mark(), k_pack_occupancy<<<grid_for(rows * c->wpr, 256, 148 * 16), 256, 0, s>>>(c->solid.ptr, rows, c->nz, c->wpr, c->occ.ptr);
   PR_CUDA(cudaGetLastError());
 
   PR_TRY(nw.alloc(lat, s));
   PR_TRY(woff.alloc(lat, s));
-  k_wall_counts<<<grid_for(lat, 256), 256, 0, s>>>(c->solid.ptr, c->nx, c->ny, c->nz, nw.ptr);
+  ::pr::launch_mark(), k_wall_counts<<<grid_for(lat, 256), 256, 0, s>>>(c->solid.ptr, c->nx, c->ny, c->nz, nw.ptr);
   PR_CUDA(cudaGetLastError());
   int64_t n_wall = 0, n_int = 0;
   PR_TRY(exclusive_scan_i32(nw.ptr, woff.ptr, lat, &n_wall, s));
@@ -192,11 +192,11 @@ int case_build(pr_case* c, const uint8_t* phases, cudaStream_t s) {
   PR_TRY(c->cfp.alloc(6 * n, s));
   PR_TRY(c->hot.alloc(lat, s));
   PR_TRY(c->cold.alloc(lat, s));
-  k_write_walls<<<grid_for(lat, 256), 256, 0, s>>>(c->solid.ptr, c->nx, c->ny, c->nz, woff.ptr, c->cls.ptr,
+  ::pr::launch_mark(), k_write_walls<<<grid_for(lat, 256), 256, 0, s>>>(c->solid.ptr, c->nx, c->ny, c->nz, woff.ptr, c->cls.ptr,
                                                   c->face.ptr, c->code.ptr, c->cell.ptr, c->origin.ptr,
                                                   c->hot.ptr, c->cold.ptr);
   PR_CUDA(cudaGetLastError());
-  k_write_internal<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(mask.ptr, off.ptr, c->nx, c->ny, c->nz,
+  ::pr::launch_mark(), k_write_internal<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(mask.ptr, off.ptr, c->nx, c->ny, c->nz,
                                                              (int32_t)n_wall, c->cls.ptr, c->face.ptr,
                                                              c->code.ptr, c->cell.ptr, c->origin.ptr, c->cfp.ptr);
   PR_CUDA(cudaGetLastError());

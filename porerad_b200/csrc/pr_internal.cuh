@@ -5,6 +5,7 @@
 #include <stdint.h>
 #include <stdio.h>
 #include <string.h>
+#include <atomic>
 #include <stdarg.h>
 #include <string>
 #include <utility>
@@ -14,6 +15,17 @@
 namespace pr {
 
 void set_error(const char* fmt, ...);
+
+// Count of the library's own kernel launches (CUB primitives not included).
+extern std::atomic<long long> g_launches;
+inline void launch_mark() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+// Optional CUDA-event timers around the hot kernels (see timers.cu).
+enum TimerId { kTimerTrace = 0, kTimerRle = 1, kTimerBalance = 2, kTimerSeries = 3, kTimerCheb = 4,
+               kTimerRefine = 5, kTimerCount = 6 };
+bool timers_on();
+void timer_begin(int id, cudaStream_t s);
+void timer_end(int id, cudaStream_t s);
 
 #define PR_CUDA(expr)                                                                      \
   do {                                                                                     \

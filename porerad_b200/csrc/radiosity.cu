@@ -122,9 +122,9 @@ int series_fp64(const pr_operator* op, const double* emitted, const double* eps,
   PR_TRY(partial.alloc((size_t)2 * (sb > rb ? sb : rb), s));
   PR_TRY(st.alloc(1, s));
   PR_CUDA(cudaMemsetAsync(st.ptr, 0, sizeof(SeriesState), s));
-  k_series_init<<<rb, 256, 0, s>>>(emitted, op->scale.ptr, op->area.ptr, n, va.ptr, absorbed, partial.ptr);
+  ::pr::launch_mark(), k_series_init<<<rb, 256, 0, s>>>(emitted, op->scale.ptr, op->area.ptr, n, va.ptr, absorbed, partial.ptr);
   PR_CUDA(cudaGetLastError());
-  k_series_tol<<<1, 32, 0, s>>>(partial.ptr, rb, rtol, st.ptr);
+  ::pr::launch_mark(), k_series_tol<<<1, 32, 0, s>>>(partial.ptr, rb, rtol, st.ptr);
   PR_CUDA(cudaGetLastError());
   SymView S = sym_view(op->S);
   double* vin = va.ptr;
@@ -134,12 +134,12 @@ int series_fp64(const pr_operator* op, const double* emitted, const double* eps,
   for (int64_t launched = 0;;) {
     for (int b = 0; b < batch; ++b) {
       if (op->S.uniform)
-        k_series_step<true><<<sb, 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, eps, vin, vout, absorbed,
-                                               partial.ptr, st.ptr);
+        { ::pr::timer_begin(kTimerSeries, s); ::pr::launch_mark(), k_series_step<true><<<sb, 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, eps, vin, vout, absorbed,
+                                               partial.ptr, st.ptr); ::pr::timer_end(kTimerSeries, s); }
       else
-        k_series_step<false><<<sb, 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, eps, vin, vout, absorbed,
-                                                partial.ptr, st.ptr);
-      k_series_finish<<<1, 32, 0, s>>>(partial.ptr, sb, (long long)max_it, st.ptr);
+        { ::pr::timer_begin(kTimerSeries, s); ::pr::launch_mark(), k_series_step<false><<<sb, 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, eps, vin, vout, absorbed,
+                                                partial.ptr, st.ptr); ::pr::timer_end(kTimerSeries, s); }
+      ::pr::launch_mark(), k_series_finish<<<1, 32, 0, s>>>(partial.ptr, sb, (long long)max_it, st.ptr);
       std::swap(vin, vout);
     }
     PR_CUDA(cudaGetLastError());
@@ -196,7 +196,7 @@ int net_patch_power(const pr_operator* op, const double* T, const double* eps, c
   PR_CUDA(cudaMemcpyAsync(dT.ptr, T, n * 8, cudaMemcpyDefault, s));
   PR_CUDA(cudaMemcpyAsync(de.ptr, eps, n * 8, cudaMemcpyDefault, s));
   PR_CUDA(cudaMemcpyAsync(da.ptr, area, n * 8, cudaMemcpyDefault, s));
-  k_emission<<<grid_for(n, 256), 256, 0, s>>>(dT.ptr, de.ptr, da.ptr, n, has_ref, ref, dE.ptr);
+  ::pr::launch_mark(), k_emission<<<grid_for(n, 256), 256, 0, s>>>(dT.ptr, de.ptr, da.ptr, n, has_ref, ref, dE.ptr);
   PR_CUDA(cudaGetLastError());
   double res = 0.0;
   int64_t it = 0;
@@ -204,7 +204,7 @@ int net_patch_power(const pr_operator* op, const double* T, const double* eps, c
   if (emitted) PR_CUDA(cudaMemcpyAsync(emitted, dE.ptr, n * 8, cudaMemcpyDefault, s));
   if (absorbed) PR_CUDA(cudaMemcpyAsync(absorbed, dAb.ptr, n * 8, cudaMemcpyDefault, s));
   if (net) {
-    k_sub<<<grid_for(n, 256), 256, 0, s>>>(dAb.ptr, dE.ptr, n, dT.ptr);
+    ::pr::launch_mark(), k_sub<<<grid_for(n, 256), 256, 0, s>>>(dAb.ptr, dE.ptr, n, dT.ptr);
     PR_CUDA(cudaMemcpyAsync(net, dT.ptr, n * 8, cudaMemcpyDefault, s));
   }
   PR_CUDA(cudaStreamSynchronize(s));
@@ -227,12 +227,12 @@ int net_patch_power_jvp(const pr_operator* op, const double* T, const double* dT
   PR_CUDA(cudaMemcpyAsync(dd.ptr, dTin, n * 8, cudaMemcpyDefault, s));
   PR_CUDA(cudaMemcpyAsync(de.ptr, eps, n * 8, cudaMemcpyDefault, s));
   PR_CUDA(cudaMemcpyAsync(da.ptr, area, n * 8, cudaMemcpyDefault, s));
-  k_emission_derivative<<<grid_for(n, 256), 256, 0, s>>>(dT.ptr, dd.ptr, de.ptr, da.ptr, n, dE.ptr);
+  ::pr::launch_mark(), k_emission_derivative<<<grid_for(n, 256), 256, 0, s>>>(dT.ptr, dd.ptr, de.ptr, da.ptr, n, dE.ptr);
   PR_CUDA(cudaGetLastError());
   double res = 0.0;
   int64_t it = 0;
   PR_TRY(series_fp64(op, dE.ptr, de.ptr, rtol, 10000, dAb.ptr, &res, &it, s));
-  k_sub<<<grid_for(n, 256), 256, 0, s>>>(dAb.ptr, dE.ptr, n, dT.ptr);
+  ::pr::launch_mark(), k_sub<<<grid_for(n, 256), 256, 0, s>>>(dAb.ptr, dE.ptr, n, dT.ptr);
   PR_CUDA(cudaMemcpyAsync(out, dT.ptr, n * 8, cudaMemcpyDefault, s));
   PR_CUDA(cudaStreamSynchronize(s));
   return PR_OK;
@@ -356,7 +356,7 @@ static int build_s32(const pr_operator* op, cudaStream_t s) {
     DevBuf<unsigned int> mx;
     PR_TRY(mx.alloc(1, s));
     PR_CUDA(cudaMemsetAsync(mx.ptr, 0, 4, s));
-    k_max_i32<<<grid_for(m, 256), 256, 0, s>>>(S.pairsum.ptr, m, mx.ptr);
+    ::pr::launch_mark(), k_max_i32<<<grid_for(m, 256), 256, 0, s>>>(S.pairsum.ptr, m, mx.ptr);
     unsigned int h = 0;
     PR_CUDA(cudaMemcpyAsync(&h, mx.ptr, 4, cudaMemcpyDeviceToHost, s));
     PR_CUDA(cudaStreamSynchronize(s));
@@ -369,7 +369,7 @@ static int build_s32(const pr_operator* op, cudaStream_t s) {
   PR_TRY(op->s32.alloc(m > 0 ? m : 1, s));
   if (bits == 0) PR_TRY(op->s32val.alloc(m > 0 ? m : 1, s));
   if (m > 0) {
-    k_pack_s32<<<grid_for(m, 256), 256, 0, s>>>(S.col.ptr, S.uniform ? S.pairsum.ptr : nullptr, S.val.ptr, m, bits,
+    ::pr::launch_mark(), k_pack_s32<<<grid_for(m, 256), 256, 0, s>>>(S.col.ptr, S.uniform ? S.pairsum.ptr : nullptr, S.val.ptr, m, bits,
                                                  op->s32.ptr, bits ? nullptr : op->s32val.ptr);
     PR_CUDA(cudaGetLastError());
   }
@@ -519,7 +519,7 @@ int series_mixed(const pr_operator* op, const double* emitted, const double* eps
   PR_TRY(sc32.alloc(n, s));
   PR_TRY(ar32.alloc(n, s));
   PR_TRY(om32.alloc(n, s));
-  k_to_f32<<<grid_for(n, 256), 256, 0, s>>>(op->scale.ptr, op->area.ptr, eps, n, sc32.ptr, ar32.ptr, om32.ptr);
+  ::pr::launch_mark(), k_to_f32<<<grid_for(n, 256), 256, 0, s>>>(op->scale.ptr, op->area.ptr, eps, n, sc32.ptr, ar32.ptr, om32.ptr);
   PR_CUDA(cudaMemsetAsync(J.ptr, 0, n * 8, s));
   SymView S = sym_view(op->S);
   S32View S32;
@@ -535,14 +535,14 @@ int series_mixed(const pr_operator* op, const double* emitted, const double* eps
   int64_t sp64 = 0, sp32 = 0;
   double rel = 0.0;
   for (;;) {
-    k_refine_prep<<<grid_for(n, 256), 256, 0, s>>>(J.ptr, outer > 0 ? x32.ptr : nullptr, op->scale.ptr,
+    ::pr::launch_mark(), k_refine_prep<<<grid_for(n, 256), 256, 0, s>>>(J.ptr, outer > 0 ? x32.ptr : nullptr, op->scale.ptr,
                                                     op->area.ptr, n, u.ptr);
     if (op->S.uniform)
-      k_refine_residual<true><<<sb, 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, eps, emitted, J.ptr,
-                                                 u.ptr, absorbed, partial.ptr, x32.ptr, r32.ptr, d32.ptr, ua.ptr);
+      { ::pr::timer_begin(kTimerRefine, s); ::pr::launch_mark(), k_refine_residual<true><<<sb, 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, eps, emitted, J.ptr,
+                                                 u.ptr, absorbed, partial.ptr, x32.ptr, r32.ptr, d32.ptr, ua.ptr); ::pr::timer_end(kTimerRefine, s); }
     else
-      k_refine_residual<false><<<sb, 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, eps, emitted, J.ptr,
-                                                  u.ptr, absorbed, partial.ptr, x32.ptr, r32.ptr, d32.ptr, ua.ptr);
+      { ::pr::timer_begin(kTimerRefine, s); ::pr::launch_mark(), k_refine_residual<false><<<sb, 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, eps, emitted, J.ptr,
+                                                  u.ptr, absorbed, partial.ptr, x32.ptr, r32.ptr, d32.ptr, ua.ptr); ::pr::timer_end(kTimerRefine, s); }
     PR_CUDA(cudaGetLastError());
     ++sp64;
     PR_TRY(sum_partials(partial.ptr, sb, 2, sums.ptr, s));
@@ -559,11 +559,11 @@ int series_mixed(const pr_operator* op, const double* emitted, const double* eps
       const double rho_n = 1.0 / (2.0 * sigma1 - rho_k);
       const float c1 = (float)(rho_n * rho_k), c2 = (float)(2.0 * rho_n / rho);
       if (S32.bits > 0)
-        k_cheb_step<true><<<sb, 256, 0, s>>>(S32, c_delta, sc32.ptr, ar32.ptr, om32.ptr, uin, uout, x32.ptr, r32.ptr,
-                                             d32.ptr, c1, c2);
+        { ::pr::timer_begin(kTimerCheb, s); ::pr::launch_mark(), k_cheb_step<true><<<sb, 256, 0, s>>>(S32, c_delta, sc32.ptr, ar32.ptr, om32.ptr, uin, uout, x32.ptr, r32.ptr,
+                                             d32.ptr, c1, c2); ::pr::timer_end(kTimerCheb, s); }
       else
-        k_cheb_step<false><<<sb, 256, 0, s>>>(S32, c_delta, sc32.ptr, ar32.ptr, om32.ptr, uin, uout, x32.ptr,
-                                              r32.ptr, d32.ptr, c1, c2);
+        { ::pr::timer_begin(kTimerCheb, s); ::pr::launch_mark(), k_cheb_step<false><<<sb, 256, 0, s>>>(S32, c_delta, sc32.ptr, ar32.ptr, om32.ptr, uin, uout, x32.ptr,
+                                              r32.ptr, d32.ptr, c1, c2); ::pr::timer_end(kTimerCheb, s); }
       rho_k = rho_n;
       std::swap(uin, uout);
       ++sp32;
@@ -595,7 +595,7 @@ int prescribed_channels(const pr_case* c, const pr_operator* op, double T_m, dou
   const int rb = red_blocks();
   PR_TRY(partial.alloc((size_t)3 * rb, s));
   PR_TRY(sums.alloc(3, s));
-  k_prescribed_emission<<<grid_for(n, 256), 256, 0, s>>>(c->cls.ptr, c->cell.ptr, op->area.ptr, n, c->ny * c->nz,
+  ::pr::launch_mark(), k_prescribed_emission<<<grid_for(n, 256), 256, 0, s>>>(c->cls.ptr, c->cell.ptr, op->area.ptr, n, c->ny * c->nz,
                                                         c->nx, T_m, dT, epsv, dE.ptr, de.ptr);
   PR_CUDA(cudaGetLastError());
   double st[4] = {0, 0, 0, 0};
@@ -610,7 +610,7 @@ int prescribed_channels(const pr_case* c, const pr_operator* op, double T_m, dou
     st[1] = (double)(op->spmv_calls - calls0);
     st[2] = res;
   }
-  k_class_sums<<<rb, 256, 0, s>>>(c->cls.ptr, dAb.ptr, dE.ptr, n, partial.ptr);
+  ::pr::launch_mark(), k_class_sums<<<rb, 256, 0, s>>>(c->cls.ptr, dAb.ptr, dE.ptr, n, partial.ptr);
   PR_CUDA(cudaGetLastError());
   PR_TRY(sum_partials(partial.ptr, rb, 3, sums.ptr, s));
   const double h = c->H / (double)c->nx;
@@ -619,7 +619,7 @@ int prescribed_channels(const pr_case* c, const pr_operator* op, double T_m, dou
   int bx = (int)std::min<int64_t>(8, c->nx), by = (int)std::min<int64_t>(8, c->ny), bz = (int)std::min<int64_t>(8, c->nz);
   if (coarse) {
     PR_TRY(dco.alloc((size_t)bx * by * bz, s));
-    k_coarse<<<bx * by * bz, 256, 0, s>>>(c->cfp.ptr, dAb.ptr, dE.ptr, c->nx, c->ny, c->nz, bx, by, bz, 1.0 / xs,
+    ::pr::launch_mark(), k_coarse<<<bx * by * bz, 256, 0, s>>>(c->cfp.ptr, dAb.ptr, dE.ptr, c->nx, c->ny, c->nz, bx, by, bz, 1.0 / xs,
                                            dco.ptr);
     PR_CUDA(cudaGetLastError());
   }

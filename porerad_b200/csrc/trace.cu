@@ -48,9 +48,22 @@ __device__ __forceinline__ double clip_edge(double u) {
   return u < lo ? lo : (u > hi ? hi : u);
 }
 
+// NumPy's float remainder by b > 0 for the origins, whose values lie in (-b, 2b):
+// a - b is exact there (Sterbenz), a + b is the single rounded add NumPy makes for a
+// negative fmod result, and a zero result is +0.0.  Other values take the general path.
+__device__ __forceinline__ double wrap_origin(double a, double b) {
+  if (a > -b && a < 2.0 * b) {
+    if (a >= b) return pr_sub(a, b);
+    if (a < 0.0) return pr_add(a, b);
+    return a == 0.0 ? 0.0 : a;
+  }
+  return pr_pymod_pos(a, b);
+}
+
 // Origin and unit direction of ray r of patch p, block s (view_factors.py:148-181).
+// Tangent axes (first, second) of a normal along x, y, z: (y, z), (x, z), (x, y).
 __device__ __forceinline__ void make_ray(const RaySrc& src, int64_t p, int64_t r, int64_t R, int s,
-                                         double o[3], double d[3]) {
+                                         double& ox, double& oy, double& oz, double& dx, double& dy, double& dz) {
   const pr_u128* maps = src.maps + (int64_t)s * 128;
   pr_u128 st = pr_pcg_jump(src.state[s], (uint64_t)((p * R + r) * 4), maps);
   const pr_u128 inc = src.inc[s];
@@ -61,28 +74,40 @@ __device__ __forceinline__ void make_ray(const RaySrc& src, int64_t p, int64_t r
   const int code = src.code[p];
   const int ax = code >> 1;
   const double sign = (code & 1) ? -1.0 : 1.0;
-  const int first = ax == 0 ? 1 : 0;
-  const int second = ax == 2 ? 1 : 2;
-  o[0] = src.origin[3 * p];
-  o[1] = src.origin[3 * p + 1];
-  o[2] = src.origin[3 * p + 2];
-  o[first] = pr_add(o[first], pr_sub(clip_edge(u0), 0.5));
-  o[second] = pr_add(o[second], pr_sub(clip_edge(u1), 0.5));
-  o[1] = pr_pymod_pos(o[1], src.ny_d);
-  o[2] = pr_pymod_pos(o[2], src.nz_d);
+  ox = src.origin[3 * p];
+  oy = src.origin[3 * p + 1];
+  oz = src.origin[3 * p + 2];
+  const double ta = pr_sub(clip_edge(u0), 0.5);
+  const double tb = pr_sub(clip_edge(u1), 0.5);
+  if (ax == 0) {
+    oy = pr_add(oy, ta);
+    oz = pr_add(oz, tb);
+  } else if (ax == 1) {
+    ox = pr_add(ox, ta);
+    oz = pr_add(oz, tb);
+  } else {
+    ox = pr_add(ox, ta);
+    oy = pr_add(oy, tb);
+  }
+  oy = wrap_origin(oy, src.ny_d);
+  oz = wrap_origin(oz, src.nz_d);
   const double radius = pr_sqrt(u2);
   double sn, cs;
   pr_sincos(pr_mul(PR_TWO_PI, u3), &sn, &cs);
   const double la = pr_mul(radius, cs);
-  const double lb = pr_mul(radius, sn);
-  const double polar = pr_sqrt(pr_sub(1.0, u2));
-  d[ax] = sign * polar;
-  d[first] = la;
-  d[second] = sign * lb;
-  const double len = pr_sqrt(pr_add(pr_add(pr_mul(d[0], d[0]), pr_mul(d[1], d[1])), pr_mul(d[2], d[2])));
-  d[0] = pr_div(d[0], len);
-  d[1] = pr_div(d[1], len);
-  d[2] = pr_div(d[2], len);
+  const double lb = sign * pr_mul(radius, sn);
+  const double dn = sign * pr_sqrt(pr_sub(1.0, u2));
+  if (ax == 0) {
+    dx = dn; dy = la; dz = lb;
+  } else if (ax == 1) {
+    dx = la; dy = dn; dz = lb;
+  } else {
+    dx = la; dy = lb; dz = dn;
+  }
+  const double len = pr_sqrt(pr_add(pr_add(pr_mul(dx, dx), pr_mul(dy, dy)), pr_mul(dz, dz)));
+  dx = pr_div(dx, len);
+  dy = pr_div(dy, len);
+  dz = pr_div(dz, len);
 }
 
 __device__ __forceinline__ int64_t first_cell(double pos, double dir) {
@@ -196,10 +221,10 @@ __global__ void __launch_bounds__(256) k_trace_blocks(Geom g, RaySrc src, int64_
     const int64_t ps = q / R;
     const int s = (int)(ps % S);
     const int64_t p = p0 + ps / S;
-    double o[3], d[3];
-    make_ray(src, p, r, R, s, o, d);
+    double ox, oy, oz, dx, dy, dz;
+    make_ray(src, p, r, R, s, ox, oy, oz, dx, dy, dz);
     int64_t st = 0;
-    const int32_t hit = dda_first_hit(g, o[0], o[1], o[2], d[0], d[1], d[2], &st);
+    const int32_t hit = dda_first_hit(g, ox, oy, oz, dx, dy, dz, &st);
     my_steps += st;
     my_fail += hit < 0;
     recv[q] = hit;
@@ -212,12 +237,14 @@ __global__ void k_generate(RaySrc src, int64_t p0, int64_t np, int64_t R, double
                            double* __restrict__ dirs) {
   const int64_t n = np * R;
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
-    double o[3], d[3];
-    make_ray(src, p0 + q / R, q % R, R, 0, o, d);
-    for (int c = 0; c < 3; ++c) {
-      origins[3 * q + c] = o[c];
-      dirs[3 * q + c] = d[c];
-    }
+    double ox, oy, oz, dx, dy, dz;
+    make_ray(src, p0 + q / R, q % R, R, 0, ox, oy, oz, dx, dy, dz);
+    origins[3 * q] = ox;
+    origins[3 * q + 1] = oy;
+    origins[3 * q + 2] = oz;
+    dirs[3 * q] = dx;
+    dirs[3 * q + 1] = dy;
+    dirs[3 * q + 2] = dz;
   }
 }
 
@@ -418,7 +445,7 @@ int generate_rays(const pr_case* c, int64_t p0, int64_t p1, int64_t R, const pr_
   DevBuf<double> o, d;
   PR_TRY(o.alloc(3 * n, s));
   PR_TRY(d.alloc(3 * n, s));
-  k_generate<<<grid_for(n, 256, trace_grid()), 256, 0, s>>>(src_of(c, t), p0, p1 - p0, R, o.ptr, d.ptr);
+  ::pr::launch_mark(), k_generate<<<grid_for(n, 256, trace_grid()), 256, 0, s>>>(src_of(c, t), p0, p1 - p0, R, o.ptr, d.ptr);
   PR_CUDA(cudaGetLastError());
   PR_CUDA(cudaMemcpyAsync(origins, o.ptr, o.bytes(), cudaMemcpyDefault, s));
   PR_CUDA(cudaMemcpyAsync(dirs, d.ptr, d.bytes(), cudaMemcpyDefault, s));
@@ -440,7 +467,7 @@ int trace_given(const pr_case* c, const double* origins, const double* dirs, int
   PR_CUDA(cudaMemcpyAsync(o.ptr, origins, o.bytes(), cudaMemcpyDefault, s));
   PR_CUDA(cudaMemcpyAsync(d.ptr, dirs, d.bytes(), cudaMemcpyDefault, s));
   PR_CUDA(cudaMemsetAsync(ctr.ptr, 0, ctr.bytes(), s));
-  k_trace_given<<<grid_for(n, 256, trace_grid()), 256, 0, s>>>(geom_of(c), o.ptr, d.ptr, n, rv.ptr, ctr.ptr);
+  ::pr::launch_mark(), k_trace_given<<<grid_for(n, 256, trace_grid()), 256, 0, s>>>(geom_of(c), o.ptr, d.ptr, n, rv.ptr, ctr.ptr);
   PR_CUDA(cudaGetLastError());
   unsigned long long h[2];
   PR_CUDA(cudaMemcpyAsync(receiver, rv.ptr, rv.bytes(), cudaMemcpyDefault, s));
@@ -479,7 +506,7 @@ int first_hit_counts(const pr_case* c, int64_t R, const pr_pcg64* seeds, int S, 
   csr.n_rows = P;
   PR_TRY(csr.row_ptr.alloc(P + 1, s));
   PR_TRY(k->rays.alloc(P, s));
-  k_fill_i64<<<grid_for(P, 256), 256, 0, s>>>(k->rays.ptr, P, L64);
+  ::pr::launch_mark(), k_fill_i64<<<grid_for(P, 256), 256, 0, s>>>(k->rays.ptr, P, L64);
   PR_CUDA(cudaGetLastError());
   if (P == 0) {
     PR_CUDA(cudaMemsetAsync(csr.row_ptr.ptr, 0, sizeof(int64_t), s));
@@ -523,13 +550,17 @@ int first_hit_counts(const pr_case* c, int64_t R, const pr_pcg64* seeds, int S, 
   for (int64_t p0 = 0; p0 < P; p0 += chunk) {
     const int64_t np = std::min(chunk, P - p0);
     const int64_t nr = np * L64;
-    k_trace_blocks<<<grid_for(nr, 256, trace_grid()), 256, 0, s>>>(geom_of(c), src_of(c, t), p0, np, R, S,
+    ::pr::timer_begin(kTimerTrace, s);
+    ::pr::launch_mark(), k_trace_blocks<<<grid_for(nr, 256, trace_grid()), 256, 0, s>>>(geom_of(c), src_of(c, t), p0, np, R, S,
                                                                     recv.ptr, ctr.ptr);
+    ::pr::timer_end(kTimerTrace, s);
     PR_CUDA(cudaGetLastError());
     const int rle_grid = (int)std::min<int64_t>(np, (int64_t)sm_count() * 16);
-    k_patch_rle<<<rle_grid, rle_threads, smem, s>>>(recv.ptr, np, L, Lpad, st_col.ptr, st_cnt.ptr, nnz.ptr);
+    ::pr::timer_begin(kTimerRle, s);
+    ::pr::launch_mark(), k_patch_rle<<<rle_grid, rle_threads, smem, s>>>(recv.ptr, np, L, Lpad, st_col.ptr, st_cnt.ptr, nnz.ptr);
+    ::pr::timer_end(kTimerRle, s);
     PR_CUDA(cudaGetLastError());
-    k_i32_to_i64<<<grid_for(np, 256), 256, 0, s>>>(nnz.ptr, nnz_all.ptr + p0, np);
+    ::pr::launch_mark(), k_i32_to_i64<<<grid_for(np, 256), 256, 0, s>>>(nnz.ptr, nnz_all.ptr + p0, np);
     PR_CUDA(cudaGetLastError());
     PR_CUDA(cub::DeviceScan::InclusiveSum(scan_tmp.ptr, scan_bytes, nnz_all.ptr + p0, off.ptr + 1, np, s));
     int64_t chunk_total = 0;
@@ -539,7 +570,7 @@ int first_hit_counts(const pr_case* c, int64_t R, const pr_pcg64* seeds, int S, 
     pc.n = chunk_total;
     PR_TRY(pc.col.alloc(chunk_total, s));
     PR_TRY(pc.cnt.alloc(chunk_total, s));
-    k_compact_rows<<<grid_for(np * 32, 256), 256, 0, s>>>(st_col.ptr, st_cnt.ptr, nnz.ptr, off.ptr, np, L, 0,
+    ::pr::launch_mark(), k_compact_rows<<<grid_for(np * 32, 256), 256, 0, s>>>(st_col.ptr, st_cnt.ptr, nnz.ptr, off.ptr, np, L, 0,
                                                           pc.col.ptr, pc.cnt.ptr);
     PR_CUDA(cudaGetLastError());
     total += chunk_total;

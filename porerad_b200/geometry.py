@@ -1,0 +1,138 @@
+"""Seeded synthetic voxel microstructures of the four benchmark archetypes (uint8, 1 = solid).
+
+These are the workload inputs of the benchmark and tests, generated on the host
+with NumPy from an integer seed.  They follow the archetype definitions of the
+benchmark configurations (not the reference's own generators, porerad/geometry.py):
+
+* FI: isotropic random-axis solid cylinders of radius r placed until the solid
+  fraction reaches phi;
+* FA: cylinders of radius r aligned with z, placed until phi;
+* OF: open-cell foam, struts along the edges of the periodic Voronoi tessellation of
+  64 Poisson seed points, dilated until phi;
+* TL: tortuous layers, 4-voxel-thick sheets normal to z perforated by random
+  8-voxel holes, holes added until phi.
+
+Every field is periodic in y and z (and x) so any axis can be the transfer axis.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+ARCHETYPES = ("OF", "FI", "FA", "TL")
+
+
+def _ball(radius: float) -> np.ndarray:
+    r = int(np.ceil(radius))
+    g = np.arange(-r, r + 1)
+    dx, dy, dz = np.meshgrid(g, g, g, indexing="ij")
+    keep = dx * dx + dy * dy + dz * dz <= radius * radius
+    return np.stack((dx[keep], dy[keep], dz[keep]), axis=1)
+
+
+def _stamp_segment(solid: np.ndarray, p0: np.ndarray, direction: np.ndarray, length: float, ball: np.ndarray) -> None:
+    n = np.asarray(solid.shape)
+    t = np.arange(-length / 2.0, length / 2.0 + 0.25, 0.25)
+    centres = np.rint(p0[None, :] + t[:, None] * direction[None, :]).astype(np.int64)
+    centres = np.unique(centres, axis=0)
+    pts = (centres[:, None, :] + ball[None, :, :]).reshape(-1, 3) % n
+    solid[pts[:, 0], pts[:, 1], pts[:, 2]] = 1
+
+
+def fibers(n: int, phi: float, seed: int, *, radius: float = 2.0, aligned: bool = False) -> np.ndarray:
+    """FI (isotropic axes) or FA (axes along z) cylinders of the given radius until phi is reached."""
+
+    rng = np.random.default_rng(seed)
+    solid = np.zeros((n, n, n), np.uint8)
+    ball = _ball(radius)
+    target = phi * solid.size
+    count = 0
+    while count < target:
+        p0 = rng.random(3) * n
+        if aligned:
+            d = np.array([0.0, 0.0, 1.0])
+            length = float(n)
+        else:
+            v = rng.standard_normal(3)
+            d = v / np.linalg.norm(v)
+            length = float(n) * np.sqrt(3.0)
+        _stamp_segment(solid, p0, d, length, ball)
+        count = int(solid.sum())
+    return solid
+
+
+def foam(n: int, phi: float, seed: int, *, n_seeds: int = 64) -> np.ndarray:
+    """OF: struts on the edges of a periodic Voronoi tessellation, thickened until phi.
+
+    A voxel belongs to a Voronoi edge where its three nearest seeds are nearly
+    equidistant; the strut field d3 - d1 (distance to the third minus the first
+    nearest seed) is thresholded at the phi-quantile.
+    """
+
+    from scipy.spatial import cKDTree
+
+    rng = np.random.default_rng(seed)
+    pts = rng.random((n_seeds, 3)) * n
+    tree = cKDTree(pts, boxsize=n)
+    g = np.arange(n) + 0.5
+    cx, cy, cz = np.meshgrid(g, g, g, indexing="ij")
+    centres = np.stack((cx.ravel(), cy.ravel(), cz.ravel()), axis=1)
+    dist, _ = tree.query(centres, k=3)
+    field = (dist[:, 2] - dist[:, 0]).reshape(n, n, n)
+    thr = np.quantile(field, phi)
+    return (field <= thr).astype(np.uint8)
+
+
+def layers(n: int, phi: float, seed: int, *, thickness: int = 4, hole: int = 8) -> np.ndarray:
+    """TL: sheets normal to z, evenly spaced from a random offset, perforated by random holes until phi."""
+
+    rng = np.random.default_rng(seed)
+    solid = np.zeros((n, n, n), np.uint8)
+    m = max(1, int(np.ceil(phi * n / thickness)))
+    offset = int(rng.integers(0, n))
+    for s in range(m):
+        z0 = (offset + (s * n) // m) % n
+        for dz in range(thickness):
+            solid[:, :, (z0 + dz) % n] = 1
+    target = phi * solid.size
+    r = hole / 2.0
+    g = np.arange(-hole, hole + 1)
+    dx, dy = np.meshgrid(g, g, indexing="ij")
+    disk = np.stack((dx[dx * dx + dy * dy <= r * r], dy[dx * dx + dy * dy <= r * r]), axis=1)
+    sheet_z = [(offset + (s * n) // m) % n for s in range(m)]
+    while solid.sum() > target:
+        z0 = sheet_z[int(rng.integers(0, m))]
+        c = rng.integers(0, n, size=2)
+        xy = (c[None, :] + disk) % n
+        for dz in range(thickness):
+            solid[xy[:, 0], xy[:, 1], (z0 + dz) % n] = 0
+    return solid
+
+
+def make(archetype: str, n: int, phi: float, seed: int) -> np.ndarray:
+    """One archetype microstructure of size n^3 (uint8, 1 = solid)."""
+
+    if archetype == "FI":
+        return fibers(n, phi, seed)
+    if archetype == "FA":
+        return fibers(n, phi, seed, aligned=True)
+    if archetype == "OF":
+        return foam(n, phi, seed)
+    if archetype == "TL":
+        return layers(n, phi, seed)
+    raise ValueError(f"unknown archetype {archetype!r}; expected one of {ARCHETYPES}")
+
+
+def splitmix64(x: int) -> int:
+    """SplitMix64 finaliser: 64-bit ray-set seeds derived from a case seed."""
+
+    x = (x + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+    x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+    x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+    return x ^ (x >> 31)
+
+
+def ray_set_seed(case_seed: int, set_index: int, block: int = 0) -> int:
+    """Seed of ray block ``block`` of ray set ``set_index`` (0 = A, 1 = B, ...) of a case (below 2^63)."""
+
+    return splitmix64(splitmix64(splitmix64(int(case_seed)) ^ int(set_index)) ^ int(block)) >> 1

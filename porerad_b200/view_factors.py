@@ -38,18 +38,26 @@ def orient_along_x(array: np.ndarray, axis: str) -> np.ndarray:
 class DeviceGeometry:
     """One x-oriented voxel geometry resident on the current CUDA device (a ``pr_case``)."""
 
-    def __init__(self, phases_x: np.ndarray, H_m: float, *, stream=None):
-        ph = np.asarray(phases_x)
-        if ph.ndim != 3:
-            raise ValueError("phases_x must be a 3-D array")
-        if ph.dtype != np.uint8:
-            ph = (ph == 1).astype(np.uint8)
-        ph = np.ascontiguousarray(ph)
+    def __init__(self, phases_x, H_m: float, *, stream=None):
+        if getattr(phases_x, "is_cuda", False):
+            # a contiguous uint8 CUDA tensor already resident in HBM
+            if str(phases_x.dtype) != "torch.uint8" or not phases_x.is_contiguous() or phases_x.dim() != 3:
+                raise ValueError("device phases must be a contiguous 3-D uint8 tensor")
+            src = int(phases_x.data_ptr())
+            shape = tuple(int(s) for s in phases_x.shape)
+        else:
+            ph = np.asarray(phases_x)
+            if ph.ndim != 3:
+                raise ValueError("phases_x must be a 3-D array")
+            if ph.dtype != np.uint8:
+                ph = (ph == 1).astype(np.uint8)
+            ph = np.ascontiguousarray(ph)
+            src = ph.ctypes.data
+            shape = tuple(int(s) for s in ph.shape)
         lib = _lib.load()
         out = ctypes.c_void_p()
-        nx, ny, nz = (int(s) for s in ph.shape)
-        _lib.check(lib.pr_case_create(ph.ctypes.data, nx, ny, nz, float(H_m), _lib.stream_arg(stream),
-                                      ctypes.byref(out)))
+        nx, ny, nz = shape
+        _lib.check(lib.pr_case_create(src, nx, ny, nz, float(H_m), _lib.stream_arg(stream), ctypes.byref(out)))
         self._h = _lib.Handle(out.value, "pr_case_destroy")
         self.shape = (nx, ny, nz)
         self.H_m = float(H_m)
@@ -255,6 +263,13 @@ class CountTable:
     def sha256(self) -> str:
         o, r, c, rays = self.to_numpy(with_rays=True)
         return count_sha256(o, r, c, rays)
+
+    def merge(self, other: "CountTable") -> "CountTable":
+        """Pooled counts of this table and ``other`` (same patches), computed on the device."""
+
+        out = ctypes.c_void_p()
+        _lib.check(_lib.load().pr_counts_merge(self.handle, other.handle, None, ctypes.byref(out)))
+        return CountTable(out.value)
 
 
 def first_hit_counts_pooled(patches, rays_per_patch: int, seeds) -> CountTable:
