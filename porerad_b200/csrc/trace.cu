@@ -21,7 +21,18 @@
 
 namespace pr {
 
+// Per-seed table of LCG jump maps (A, C): state -> A state + C.
+//   [0, 128):   the maps of 2^i steps, i = 0..63
+//   [128, 192): the maps of 4 l steps, l = 0..31 (lane offsets inside a batch of 32 rays)
+//   [192, 194): the map of 128 steps (one batch of 32 rays)
+static constexpr int kMapStride = 256;
+static constexpr int kMapSmall = 128;
+static constexpr int kMapBatch = 192;
+
 #define PR_TIE 1.0e-12
+#ifndef PR_FULL
+#define PR_FULL 0xffffffffu
+#endif
 #define PR_FAR 1.0e300
 #define PR_TWO_PI 0x1.921fb54442d18p+2  // the binary64 product 2.0 * numpy.pi
 
@@ -37,7 +48,7 @@ struct Geom {
 struct RaySrc {
   const double* __restrict__ origin;  // (P, 3)
   const int8_t* __restrict__ code;    // emission normal 0..5
-  const pr_u128* __restrict__ maps;   // per seed: 128 entries (A_{2^i}, C_{2^i})
+  const pr_u128* __restrict__ maps;   // per seed: kMapStride entries, see SeedTables
   const pr_u128* __restrict__ state;  // per seed
   const pr_u128* __restrict__ inc;    // per seed
   double ny_d, nz_d;
@@ -64,7 +75,7 @@ __device__ __forceinline__ double wrap_origin(double a, double b) {
 // Tangent axes (first, second) of a normal along x, y, z: (y, z), (x, z), (x, y).
 __device__ __forceinline__ void make_ray(const RaySrc& src, int64_t p, int64_t r, int64_t R, int s,
                                          double& ox, double& oy, double& oz, double& dx, double& dy, double& dz) {
-  const pr_u128* maps = src.maps + (int64_t)s * 128;
+  const pr_u128* maps = src.maps + (int64_t)s * kMapStride;
   pr_u128 st = pr_pcg_jump(src.state[s], (uint64_t)((p * R + r) * 4), maps);
   const pr_u128 inc = src.inc[s];
   const double u0 = pr_pcg_next_double(&st, inc);
@@ -209,30 +220,6 @@ __device__ __forceinline__ void block_add_i64(int64_t v, unsigned long long* tar
   if ((threadIdx.x & 31) == 0 && v) atomicAdd(target, (unsigned long long)v);
 }
 
-// Fused generation + traversal for patches [p0, p0 + np) and n_seeds blocks: ray
-// (p, s, r) writes its receiver to recv[((p - p0) * S + s) * R + r].
-__global__ void __launch_bounds__(256) k_trace_blocks(Geom g, RaySrc src, int64_t p0, int64_t np, int64_t R,
-                                                      int S, int32_t* __restrict__ recv,
-                                                      unsigned long long* __restrict__ counters) {
-  const int64_t n = np * S * R;
-  int64_t my_steps = 0, my_fail = 0;
-  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r = q % R;
-    const int64_t ps = q / R;
-    const int s = (int)(ps % S);
-    const int64_t p = p0 + ps / S;
-    double ox, oy, oz, dx, dy, dz;
-    make_ray(src, p, r, R, s, ox, oy, oz, dx, dy, dz);
-    int64_t st = 0;
-    const int32_t hit = dda_first_hit(g, ox, oy, oz, dx, dy, dz, &st);
-    my_steps += st;
-    my_fail += hit < 0;
-    recv[q] = hit;
-  }
-  block_add_i64(my_steps, counters + 0);
-  block_add_i64(my_fail, counters + 1);
-}
-
 __global__ void k_generate(RaySrc src, int64_t p0, int64_t np, int64_t R, double* __restrict__ origins,
                            double* __restrict__ dirs) {
   const int64_t n = np * R;
@@ -265,19 +252,282 @@ __global__ void __launch_bounds__(256) k_trace_given(Geom g, const double* __res
   block_add_i64(my_fail, counters + 1);
 }
 
-// Per origin patch: sort its L receivers in shared memory (bitonic), run-length
-// encode into (receiver, count) pairs at out[(p - p0) * L ...], nnz[p - p0].
-__global__ void __launch_bounds__(512) k_patch_rle(const int32_t* __restrict__ recv, int64_t np, int L, int Lpad,
-                                                   int32_t* __restrict__ out_col, int32_t* __restrict__ out_cnt,
-                                                   int32_t* __restrict__ nnz) {
+// ---------------------------------------------------------------------------
+// Pooled traversal.  A chunk of rays is numbered seed-major, g = (s * np + (p - p0)) * R + r,
+// so inside one seed block consecutive rays are 4 draws apart in their PCG64 stream.
+// Each warp grabs units of kUnit consecutive rays from a global counter, generates
+// them 32 at a time with all lanes converged (one 128-step map advances the batch base,
+// one small map per lane), runs the DDA setup there too, and parks the ready states
+// in a warp-private shared-memory pool.  Idle lanes take rays from the pool between
+// bursts of kBurst DDA steps, so the warp no longer waits for its longest ray.
+static constexpr int kPool = 64;   // pool slots per warp (two batches)
+static constexpr int kWarps = 4;   // warps per block
+static constexpr int kBurst = 4;   // DDA steps between refills
+static constexpr int kUnit = 512;  // rays per work grab
+
+struct WarpPool {
+  double tx[kPool], ty[kPool], tz[kPool], ddx[kPool], ddy[kPool], ddz[kPool];
+  double oy[kPool], oz[kPool], dy[kPool], dz[kPool];
+  int i[kPool], jj[kPool], kk[kPool], meta[kPool], cap[kPool], q[kPool];
+  double eoy[32], eoz[32], edy[32], edz[32];  // wall-exit data of each lane's current ray
+};
+
+struct ChunkDesc {
+  int64_t n;        // rays in the chunk = S * np * R
+  int64_t np;       // patches in the chunk
+  int64_t p0;       // first patch
+  int64_t R;        // rays per patch per seed
+};
+
+// Ray (origin, direction) of patch p from a positioned stream (view_factors.py:148-181).
+__device__ __forceinline__ void ray_from_stream(const RaySrc& src, pr_u128 st, pr_u128 inc, int64_t p, double& ox,
+                                                double& oy, double& oz, double& dx, double& dy, double& dz) {
+  const double u0 = pr_pcg_next_double(&st, inc);
+  const double u1 = pr_pcg_next_double(&st, inc);
+  const double u2 = pr_pcg_next_double(&st, inc);
+  const double u3 = pr_pcg_next_double(&st, inc);
+  const int code = src.code[p];
+  const int ax = code >> 1;
+  const double sign = (code & 1) ? -1.0 : 1.0;
+  ox = src.origin[3 * p];
+  oy = src.origin[3 * p + 1];
+  oz = src.origin[3 * p + 2];
+  const double ta = pr_sub(clip_edge(u0), 0.5);
+  const double tb = pr_sub(clip_edge(u1), 0.5);
+  if (ax == 0) {
+    oy = pr_add(oy, ta);
+    oz = pr_add(oz, tb);
+  } else if (ax == 1) {
+    ox = pr_add(ox, ta);
+    oz = pr_add(oz, tb);
+  } else {
+    ox = pr_add(ox, ta);
+    oy = pr_add(oy, tb);
+  }
+  oy = wrap_origin(oy, src.ny_d);
+  oz = wrap_origin(oz, src.nz_d);
+  const double radius = pr_sqrt(u2);
+  double sn, cs;
+  pr_sincos(pr_mul(PR_TWO_PI, u3), &sn, &cs);
+  const double la = pr_mul(radius, cs);
+  const double lb = sign * pr_mul(radius, sn);
+  const double dn = sign * pr_sqrt(pr_sub(1.0, u2));
+  if (ax == 0) {
+    dx = dn; dy = la; dz = lb;
+  } else if (ax == 1) {
+    dx = la; dy = dn; dz = lb;
+  } else {
+    dx = la; dy = lb; dz = dn;
+  }
+  const double len = pr_sqrt(pr_add(pr_add(pr_mul(dx, dx), pr_mul(dy, dy)), pr_mul(dz, dz)));
+  dx = pr_div(dx, len);
+  dy = pr_div(dy, len);
+  dz = pr_div(dz, len);
+}
+
+__global__ void __launch_bounds__(kWarps * 32) k_trace_pool(Geom g, RaySrc src, ChunkDesc cd,
+                                                            int32_t* __restrict__ recv,
+                                                            unsigned long long* __restrict__ counters) {
+  __shared__ WarpPool pools[kWarps];
+  WarpPool& pool = pools[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const int64_t npR = cd.np * cd.R;
+  const uint64_t base_draw = (uint64_t)cd.p0 * (uint64_t)cd.R;  // ray index of the chunk's first ray in a stream
+  const int cap_all = (int)min((int64_t)INT32_MAX, 10 * g.n_cells + 10);
+
+  int64_t unit_next = 0, unit_end = 0;  // warp-uniform
+  int head = 0, tail = 0;               // warp-uniform pool cursors
+  bool more = true;                     // warp-uniform
+  pr_u128 base_st{0, 0};
+  int base_s = -1;
+  uint64_t base_m = 0;
+
+  bool active = false;
+  double tx = 0, ty = 0, tz = 0, ddx = 0, ddy = 0, ddz = 0, t = 0;
+  int i = 0, jj = 0, kk = 0, sx = 0, sy = 0, sz = 0, face = -1, it = 0, cap = 0, q = 0;
+  long long my_steps = 0, my_fail = 0;
+
+  for (;;) {
+    // ---- generate one batch of 32 rays when the pool has room for it
+    if (more && tail - head <= kPool - 32) {
+      if (unit_next >= unit_end) {
+        unsigned long long u = 0;
+        if (lane == 0) u = atomicAdd(counters + 2, (unsigned long long)kUnit);
+        u = __shfl_sync(PR_FULL, u, 0);
+        if ((int64_t)u >= cd.n) {
+          more = false;
+        } else {
+          unit_next = (int64_t)u;
+          unit_end = min((int64_t)u + kUnit, cd.n);
+        }
+      }
+      if (more) {
+        const int64_t g0 = unit_next;
+        const int cnt = (int)min((int64_t)32, unit_end - g0);
+        unit_next += cnt;
+        // batch base stream (warp-uniform)
+        const int s0 = (int)(g0 / npR);
+        const uint64_t m0 = (base_draw + (uint64_t)(g0 - (int64_t)s0 * npR)) * 4u;
+        const pr_u128* maps0 = src.maps + (int64_t)s0 * kMapStride;
+        if (base_s == s0 && m0 == base_m + 128u) {
+          base_st = pr_u128_affine(maps0[kMapBatch], maps0[kMapBatch + 1], base_st);
+        } else {
+          base_st = pr_pcg_jump(src.state[s0], m0, maps0);
+        }
+        base_s = s0;
+        base_m = m0;
+        if (lane < cnt) {
+          const int64_t gq = g0 + lane;
+          const int sq = (int)(gq / npR);
+          const int64_t rem = gq - (int64_t)sq * npR;
+          const int64_t p = cd.p0 + rem / cd.R;
+          pr_u128 st;
+          if (sq == s0) {
+            st = pr_u128_affine(maps0[kMapSmall + 2 * lane], maps0[kMapSmall + 2 * lane + 1], base_st);
+          } else {
+            const pr_u128* mq = src.maps + (int64_t)sq * kMapStride;
+            st = pr_pcg_jump(src.state[sq], (base_draw + (uint64_t)rem) * 4u, mq);
+          }
+          double ox, oy, oz, dx, dy, dz;
+          ray_from_stream(src, st, src.inc[sq], p, ox, oy, oz, dx, dy, dz);
+          // DDA setup (view_factors.py:213-224)
+          const int slot = (tail + lane) & (kPool - 1);
+          int c = 0, si = 0, sj = 0, sk = 0, ci = 0, cj = 0, ck = 0;
+          double a = 0, b = 0, e = 0, da = 0, db = 0, de = 0;
+          if (dx != 0.0) {
+            const int64_t i0 = first_cell(ox, dx), j0 = first_cell(oy, dy), k0 = first_cell(oz, dz);
+            axis_setup(ox, dx, i0, si, a, da);
+            axis_setup(oy, dy, j0, sj, b, db);
+            axis_setup(oz, dz, k0, sk, e, de);
+            ci = (int)max((int64_t)-1, min(i0, (int64_t)g.nx));
+            cj = (int)imod(j0, g.ny);
+            ck = (int)imod(k0, g.nz);
+            double scale = pr_add(pr_mul(pr_mul(8.0, (double)g.nx),
+                                         pr_add(1.0, pr_div(pr_add(fabs(dy), fabs(dz)), fabs(dx)))), 100.0);
+            if (scale > 100000000.0) scale = 100000000.0;
+            c = cap_all;
+            if ((int64_t)scale > (int64_t)c) c = (int)scale;
+          }
+          pool.tx[slot] = a; pool.ty[slot] = b; pool.tz[slot] = e;
+          pool.ddx[slot] = da; pool.ddy[slot] = db; pool.ddz[slot] = de;
+          pool.oy[slot] = oy; pool.oz[slot] = oz; pool.dy[slot] = dy; pool.dz[slot] = dz;
+          pool.i[slot] = ci; pool.jj[slot] = cj; pool.kk[slot] = ck;
+          pool.meta[slot] = (si + 1) | ((sj + 1) << 2) | ((sk + 1) << 4);
+          pool.cap[slot] = c;
+          pool.q[slot] = (int)gq;
+        }
+        tail += cnt;
+        __syncwarp();
+      }
+    }
+    // ---- idle lanes take ready rays
+    const unsigned idle = __ballot_sync(PR_FULL, !active);
+    const int avail = tail - head;
+    if (!active) {
+      const int rank = __popc(idle & lt);
+      if (rank < avail) {
+        const int slot = (head + rank) & (kPool - 1);
+        tx = pool.tx[slot]; ty = pool.ty[slot]; tz = pool.tz[slot];
+        ddx = pool.ddx[slot]; ddy = pool.ddy[slot]; ddz = pool.ddz[slot];
+        i = pool.i[slot]; jj = pool.jj[slot]; kk = pool.kk[slot];
+        const int meta = pool.meta[slot];
+        sx = (meta & 3) - 1;
+        sy = ((meta >> 2) & 3) - 1;
+        sz = ((meta >> 4) & 3) - 1;
+        cap = pool.cap[slot];
+        q = pool.q[slot];
+        pool.eoy[lane] = pool.oy[slot];
+        pool.eoz[lane] = pool.oz[slot];
+        pool.edy[lane] = pool.dy[slot];
+        pool.edz[lane] = pool.dz[slot];
+        t = 0.0;
+        face = -1;
+        it = 0;
+        active = true;
+      }
+    }
+    head += min(__popc(idle), avail);
+    __syncwarp();
+    if (!more && head == tail && !__any_sync(PR_FULL, active)) break;
+    // ---- a burst of DDA steps (view_factors.py:225-255)
+#pragma unroll 1
+    for (int b = 0; b < kBurst; ++b) {
+      if (!active) continue;
+      int32_t hit = -2;
+      if (it >= cap) {
+        hit = -1;
+      } else {
+        ++it;
+        if ((unsigned)i >= (unsigned)g.nx) {
+          const int64_t wj = imod((int64_t)floor(pr_add(pool.eoy[lane], pr_mul(pool.edy[lane], t))), g.ny);
+          const int64_t wk = imod((int64_t)floor(pr_add(pool.eoz[lane], pr_mul(pool.edz[lane], t))), g.nz);
+          hit = i < 0 ? __ldg(g.hot + wj * g.nz + wk) : __ldg(g.cold + wj * g.nz + wk);
+        } else {
+          const int row = i * g.ny + jj;
+          const uint32_t word = __ldg(g.occ + row * g.wpr + (kk >> 5));
+          if ((word >> (kk & 31)) & 1u) {
+            hit = face >= 0 ? __ldg(g.cfp + ((int64_t)row * g.nz + kk) * 6 + face) : -1;
+          } else {
+            double tn = tx;
+            if (ty < tn) tn = ty;
+            if (tz < tn) tn = tz;
+            const bool cx = fabs(pr_sub(tx, tn)) <= PR_TIE;
+            const bool cy = fabs(pr_sub(ty, tn)) <= PR_TIE;
+            const bool cz = fabs(pr_sub(tz, tn)) <= PR_TIE;
+            if (cx) {
+              i += sx;
+              tx = pr_add(tx, ddx);
+              face = sx > 0 ? 1 : 0;
+            }
+            if (cy) {
+              jj += sy;
+              jj = jj == g.ny ? 0 : (jj < 0 ? g.ny - 1 : jj);
+              ty = pr_add(ty, ddy);
+              if (!cx) face = sy > 0 ? 3 : 2;
+            }
+            if (cz) {
+              kk += sz;
+              kk = kk == g.nz ? 0 : (kk < 0 ? g.nz - 1 : kk);
+              tz = pr_add(tz, ddz);
+              if (!cx && !cy) face = sz > 0 ? 5 : 4;
+            }
+            t = tn;
+          }
+        }
+      }
+      if (hit != -2) {
+        recv[q] = hit;
+        my_steps += it;
+        my_fail += hit < 0;
+        active = false;
+      }
+    }
+  }
+  block_add_i64(my_steps, counters + 0);
+  block_add_i64(my_fail, counters + 1);
+}
+
+// Per origin patch: gather its L = S * R receivers (seed-major chunk layout), sort them
+// in shared memory (bitonic), run-length encode into (receiver, count) pairs at
+// out[(p - p0) * L ...], nnz[p - p0].
+__global__ void __launch_bounds__(512) k_patch_rle(const int32_t* __restrict__ recv, int64_t np, int L, int R,
+                                                   int Lpad, int32_t* __restrict__ out_col,
+                                                   int32_t* __restrict__ out_cnt, int32_t* __restrict__ nnz) {
   extern __shared__ int32_t sm[];
   int32_t* key = sm;          // Lpad
   int32_t* head = sm + Lpad;  // Lpad (positions of run heads)
   __shared__ int32_t warp_tot[16];
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int64_t p = blockIdx.x; p < np; p += gridDim.x) {
-    const int32_t* src = recv + p * L;
-    for (int i = tid; i < Lpad; i += nt) key[i] = i < L ? src[i] : INT32_MAX;
+    for (int i = tid; i < Lpad; i += nt) {
+      if (i < L) {
+        const int sd = i / R;
+        key[i] = recv[((int64_t)sd * np + p) * R + (i - sd * R)];
+      } else {
+        key[i] = INT32_MAX;
+      }
+    }
     __syncthreads();
     for (int k = 2; k <= Lpad; k <<= 1) {
       for (int j = k >> 1; j > 0; j >>= 1) {
@@ -371,26 +621,51 @@ static pr_u128 host_u128_add(const pr_u128& a, const pr_u128& b) {
   return pr_u128{(uint64_t)z, (uint64_t)(z >> 64)};
 }
 
-// Seed tables on the device: maps (S x 128), states (S), increments (S).
+static pr_u128 host_affine(const pr_u128& A, const pr_u128& C, const pr_u128& x) {
+  pr_u128 m;
+  host_u128_mul(A, x, m);
+  return host_u128_add(m, C);
+}
+
+// Seed tables on the device: kMapStride maps per seed, states (S), increments (S).
 struct SeedTables {
   DevBuf<pr_u128> maps, state, inc;
   int build(const pr_pcg64* seeds, int S, cudaStream_t s) {
-    std::vector<pr_u128> h_maps((size_t)S * 128), h_state(S), h_inc(S);
+    std::vector<pr_u128> h_maps((size_t)S * kMapStride), h_state(S), h_inc(S);
     for (int q = 0; q < S; ++q) {
       pr_pcg64 sd;
       memcpy(&sd, seeds + q, sizeof(sd));  // seeds may be host memory only
       h_state[q] = pr_u128{sd.state_lo, sd.state_hi};
       h_inc[q] = pr_u128{sd.inc_lo, sd.inc_hi};
-      pr_u128 A{PR_PCG_MULT_LO, PR_PCG_MULT_HI}, C = h_inc[q];
+      pr_u128* m = h_maps.data() + (size_t)q * kMapStride;
+      const pr_u128 A1{PR_PCG_MULT_LO, PR_PCG_MULT_HI}, C1 = h_inc[q];
+      pr_u128 A = A1, C = C1;
       for (int i = 0; i < 64; ++i) {
-        h_maps[(size_t)q * 128 + 2 * i] = A;
-        h_maps[(size_t)q * 128 + 2 * i + 1] = C;
+        m[2 * i] = A;
+        m[2 * i + 1] = C;
         // (A, C) o (A, C) = (A A, A C + C)
         pr_u128 AA, AC;
         host_u128_mul(A, A, AA);
         host_u128_mul(A, C, AC);
         C = host_u128_add(AC, C);
         A = AA;
+      }
+      // maps of n = 4 l steps by repeated composition with the one-step map
+      pr_u128 An{1, 0}, Cn{0, 0};
+      for (int n = 0; n <= 128; ++n) {
+        if (n % 4 == 0 && n / 4 < 32) {
+          m[kMapSmall + 2 * (n / 4)] = An;
+          m[kMapSmall + 2 * (n / 4) + 1] = Cn;
+        }
+        if (n == 128) {
+          m[kMapBatch] = An;
+          m[kMapBatch + 1] = Cn;
+        }
+        // (A1, C1) o (An, Cn) = (A1 An, A1 Cn + C1)
+        pr_u128 t;
+        host_u128_mul(A1, An, t);
+        Cn = host_affine(A1, C1, Cn);
+        An = t;
       }
     }
     PR_TRY(maps.alloc(h_maps.size(), s));
@@ -432,6 +707,17 @@ static RaySrc src_of(const pr_case* c, const SeedTables& t) {
 }
 
 static int trace_grid() { return sm_count() * 8; }
+
+// Persistent grid of the pooled traversal: as many blocks as fit on every SM.
+static int pool_grid() {
+  static int blocks = 0;
+  if (blocks == 0) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_pool, kWarps * 32, 0);
+    blocks = sm_count() * (per_sm > 0 ? per_sm : 1);
+  }
+  return blocks;
+}
 
 int generate_rays(const pr_case* c, int64_t p0, int64_t p1, int64_t R, const pr_pcg64* seed, double* origins,
                   double* dirs, cudaStream_t s) {
@@ -527,7 +813,7 @@ int first_hit_counts(const pr_case* c, int64_t R, const pr_pcg64* seeds, int S, 
   PR_TRY(st_cnt.alloc(chunk * L64, s));
   PR_TRY(nnz.alloc(chunk, s));
   PR_TRY(off.alloc(chunk + 1, s));
-  PR_TRY(ctr.alloc(2, s));
+  PR_TRY(ctr.alloc(3, s));
   PR_CUDA(cudaMemsetAsync(ctr.ptr, 0, ctr.bytes(), s));
   size_t scan_bytes = 0;
   PR_CUDA(cub::DeviceScan::InclusiveSum(nullptr, scan_bytes, off.ptr, off.ptr + 1, chunk, s));
@@ -550,14 +836,17 @@ int first_hit_counts(const pr_case* c, int64_t R, const pr_pcg64* seeds, int S, 
   for (int64_t p0 = 0; p0 < P; p0 += chunk) {
     const int64_t np = std::min(chunk, P - p0);
     const int64_t nr = np * L64;
+    ChunkDesc cd{nr, np, p0, R};
+    PR_CUDA(cudaMemsetAsync(ctr.ptr + 2, 0, sizeof(unsigned long long), s));
     ::pr::timer_begin(kTimerTrace, s);
-    ::pr::launch_mark(), k_trace_blocks<<<grid_for(nr, 256, trace_grid()), 256, 0, s>>>(geom_of(c), src_of(c, t), p0, np, R, S,
-                                                                    recv.ptr, ctr.ptr);
+    ::pr::launch_mark(), k_trace_pool<<<pool_grid(), kWarps * 32, 0, s>>>(geom_of(c), src_of(c, t), cd, recv.ptr,
+                                                                          ctr.ptr);
     ::pr::timer_end(kTimerTrace, s);
     PR_CUDA(cudaGetLastError());
     const int rle_grid = (int)std::min<int64_t>(np, (int64_t)sm_count() * 16);
     ::pr::timer_begin(kTimerRle, s);
-    ::pr::launch_mark(), k_patch_rle<<<rle_grid, rle_threads, smem, s>>>(recv.ptr, np, L, Lpad, st_col.ptr, st_cnt.ptr, nnz.ptr);
+    ::pr::launch_mark(), k_patch_rle<<<rle_grid, rle_threads, smem, s>>>(recv.ptr, np, L, (int)R, Lpad, st_col.ptr, st_cnt.ptr,
+                                                                     nnz.ptr);
     ::pr::timer_end(kTimerRle, s);
     PR_CUDA(cudaGetLastError());
     ::pr::launch_mark(), k_i32_to_i64<<<grid_for(np, 256), 256, 0, s>>>(nnz.ptr, nnz_all.ptr + p0, np);
