@@ -309,6 +309,7 @@ def run_ours(args, cfg):
             res = served_step(phases_dev, cfg, seeds)
             rays += res["rays"]
             steps += res["steps"]
+            release(res)  # stream-ordered frees: the next step reuses the pool
             results.append(res)
         e1.record()
         torch.cuda.synchronize()
@@ -325,8 +326,6 @@ def run_ours(args, cfg):
     last = results[-1]
     nnz_s = last["nnz_symmetric"]
     P = last["n_patches"]
-    for r in results:
-        release(r)
 
     # ---- end to end through the public API from pinned host memory
     barrier()

@@ -185,10 +185,10 @@ int counts_from_edges(const int32_t* origin, const int32_t* receiver, const int6
   return PR_OK;
 }
 
-__global__ void k_union_len(const int64_t* __restrict__ fp, const int32_t* __restrict__ fc,
-                            const int64_t* __restrict__ tp, const int32_t* __restrict__ tc, int64_t n,
+__global__ void k_merge_len(const int64_t* __restrict__ ap, const int32_t* __restrict__ ac,
+                            const int64_t* __restrict__ bp, const int32_t* __restrict__ bc, int64_t n,
                             int64_t* __restrict__ len);
-__global__ void k_merge_fill(const int64_t* __restrict__ ap, const int32_t* __restrict__ ac,
+__global__ void k_merge_rank(const int64_t* __restrict__ ap, const int32_t* __restrict__ ac,
                              const int32_t* __restrict__ an, const int64_t* __restrict__ bp,
                              const int32_t* __restrict__ bc, const int32_t* __restrict__ bn, int64_t n,
                              const int64_t* __restrict__ op, int32_t* __restrict__ oc, int32_t* __restrict__ on,
@@ -214,7 +214,8 @@ int counts_merge(const pr_counts* A, const pr_counts* B, cudaStream_t s, pr_coun
   PR_TRY(bad.alloc(1, s));
   PR_CUDA(cudaMemsetAsync(bad.ptr, 0, 4, s));
   if (n > 0) {
-    ::pr::launch_mark(), k_union_len<<<grid_for(n, 128), 128, 0, s>>>(a.row_ptr.ptr, a.col.ptr, b.row_ptr.ptr, b.col.ptr, n, len.ptr);
+    ::pr::launch_mark(), k_merge_len<<<grid_for(n * 32, 256), 256, 0, s>>>(a.row_ptr.ptr, a.col.ptr, b.row_ptr.ptr, b.col.ptr, n,
+                                                                    len.ptr);
     PR_CUDA(cudaGetLastError());
   }
   PR_TRY(lengths_to_row_ptr(len.ptr, n, c.row_ptr.ptr, s));
@@ -226,7 +227,7 @@ int counts_merge(const pr_counts* A, const pr_counts* B, cudaStream_t s, pr_coun
   PR_TRY(c.cnt.alloc(nnz, s));
   PR_TRY(k->rays.alloc(n > 0 ? n : 1, s));
   if (n > 0) {
-    ::pr::launch_mark(), k_merge_fill<<<grid_for(n, 128), 128, 0, s>>>(a.row_ptr.ptr, a.col.ptr, a.cnt.ptr, b.row_ptr.ptr, b.col.ptr,
+    ::pr::launch_mark(), k_merge_rank<<<grid_for(n * 32, 256), 256, 0, s>>>(a.row_ptr.ptr, a.col.ptr, a.cnt.ptr, b.row_ptr.ptr, b.col.ptr,
                                                   b.cnt.ptr, n, c.row_ptr.ptr, c.col.ptr, c.cnt.ptr, bad.ptr);
     PR_CUDA(cudaGetLastError());
     ::pr::launch_mark(), k_add_i64<<<grid_for(n, 256), 256, 0, s>>>(A->rays.ptr, B->rays.ptr, n, k->rays.ptr);
@@ -297,75 +298,126 @@ int build_transpose(const CountCsr& F, CountCsr& T, cudaStream_t s) {
   return PR_OK;
 }
 
-// |row i of F  union  row i of F^T|
-__global__ void k_union_len(const int64_t* __restrict__ fp, const int32_t* __restrict__ fc,
-                            const int64_t* __restrict__ tp, const int32_t* __restrict__ tc, int64_t n,
-                            int64_t* __restrict__ len) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    int64_t a = fp[i], ae = fp[i + 1], b = tp[i], be = tp[i + 1], u = 0;
-    while (a < ae && b < be) {
-      const int32_t x = fc[a], y = tc[b];
-      a += x <= y;
-      b += y <= x;
-      ++u;
-    }
-    len[i] = u + (ae - a) + (be - b);
-  }
+// Row offsets of S: len_S(i) = len_F(i) + len_T(i).
+__global__ void k_sym_row_ptr(const int64_t* __restrict__ fp, const int64_t* __restrict__ tp, int64_t n,
+                              int64_t* __restrict__ sp) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= n; i += (int64_t)gridDim.x * blockDim.x)
+    sp[i] = fp[i] + tp[i];
 }
 
-// S'_ij = 0.5 (A_i n_ij / R_i + A_j n_ji / R_j) on the union pattern (general form),
-// or the integer pair sums n_ij + n_ji (uniform form).
-template <bool kUniform>
-__global__ void k_union_fill(const int64_t* __restrict__ fp, const int32_t* __restrict__ fc,
-                             const int32_t* __restrict__ fn, const int64_t* __restrict__ tp,
-                             const int32_t* __restrict__ tc, const int32_t* __restrict__ tn,
-                             const int64_t* __restrict__ rays, const double* __restrict__ area, int64_t n,
-                             const int64_t* __restrict__ sp, int32_t* __restrict__ scol, double* __restrict__ sval,
-                             int32_t* __restrict__ spair) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    int64_t a = fp[i], ae = fp[i + 1], b = tp[i], be = tp[i + 1], o = sp[i];
-    const double Ai = kUniform ? 0.0 : area[i];
-    const double Ri = kUniform ? 0.0 : (double)rays[i];
-    while (a < ae || b < be) {
-      const int32_t x = a < ae ? fc[a] : INT32_MAX;
-      const int32_t y = b < be ? tc[b] : INT32_MAX;
-      const int32_t j = x < y ? x : y;
-      const int32_t nij = x == j ? fn[a] : 0;
-      const int32_t nji = y == j ? tn[b] : 0;
-      scol[o] = j;
-      if constexpr (kUniform) {
-        spair[o] = nij + nji;
+// Row i of S: the entries of row i of F (value 0.5 A_i n_ij / R_i) then those of row i of
+// F^T (value 0.5 A_j n_ji / R_j); one warp per row, coalesced copies.
+__global__ void k_sym_fill(const int64_t* __restrict__ fp, const int32_t* __restrict__ fc,
+                           const int32_t* __restrict__ fn, const int64_t* __restrict__ tp,
+                           const int32_t* __restrict__ tc, const int32_t* __restrict__ tn,
+                           const int64_t* __restrict__ rays, const double* __restrict__ area, int64_t n,
+                           const int64_t* __restrict__ sp, int mode, int bits, uint32_t* __restrict__ words,
+                           int32_t* __restrict__ cnt, double* __restrict__ val) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+    const int64_t o = sp[i], fb = fp[i], lf = fp[i + 1] - fb, tb = tp[i], lt = tp[i + 1] - tb;
+    for (int64_t e = lane; e < lf + lt; e += 32) {
+      const bool f = e < lf;
+      const int64_t src = f ? fb + e : tb + (e - lf);
+      const uint32_t col = (uint32_t)(f ? fc[src] : tc[src]);
+      const int32_t c = f ? fn[src] : tn[src];
+      if (mode == kPacked) {
+        words[o + e] = (col << bits) | (uint32_t)c;
       } else {
-        const double wij = (double)nij / Ri;
-        const double wji = (double)nji / (double)rays[j];
-        sval[o] = 0.5 * (Ai * wij + area[j] * wji);
+        words[o + e] = col;
+        if (mode == kCounts) {
+          cnt[o + e] = c;
+        } else {
+          const int64_t owner = f ? i : (int64_t)col;
+          val[o + e] = 0.5 * area[owner] * ((double)c / (double)rays[owner]);
+        }
       }
-      ++o;
-      a += x == j;
-      b += y == j;
     }
   }
 }
 
-// Pooled counts of two tables on the same patches: union of each row, counts summed.
-__global__ void k_merge_fill(const int64_t* __restrict__ ap, const int32_t* __restrict__ ac,
+__device__ __forceinline__ int64_t lower_bound_i32(const int32_t* __restrict__ a, int64_t lo, int64_t hi, int32_t x) {
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (a[mid] < x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// |row i of A  union  row i of B| = |a| + |b| - |a intersect b|, one warp per row.
+__global__ void k_merge_len(const int64_t* __restrict__ ap, const int32_t* __restrict__ ac,
+                            const int64_t* __restrict__ bp, const int32_t* __restrict__ bc, int64_t n,
+                            int64_t* __restrict__ len) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+    const int64_t a0 = ap[i], a1 = ap[i + 1], b0 = bp[i], b1 = bp[i + 1];
+    int dup = 0;
+    for (int64_t k = a0 + lane; k < a1; k += 32) {
+      const int64_t pb = lower_bound_i32(bc, b0, b1, ac[k]);
+      dup += pb < b1 && bc[pb] == ac[k];
+    }
+    for (int o = 16; o > 0; o >>= 1) dup += __shfl_xor_sync(0xffffffffu, dup, o);
+    if (lane == 0) len[i] = (a1 - a0) + (b1 - b0) - dup;
+  }
+}
+
+// Pooled row i of A and B by ranking: an entry of A lands at k + #(b < a_k) - #(common < a_k),
+// an entry of B absent from A at m + #(a < b_m) - #(common < b_m); a common column carries
+// both counts.  The common-prefix counts come from warp ballots over tiles of 32.
+__global__ void k_merge_rank(const int64_t* __restrict__ ap, const int32_t* __restrict__ ac,
                              const int32_t* __restrict__ an, const int64_t* __restrict__ bp,
                              const int32_t* __restrict__ bc, const int32_t* __restrict__ bn, int64_t n,
                              const int64_t* __restrict__ op, int32_t* __restrict__ oc, int32_t* __restrict__ on,
                              unsigned int* __restrict__ bad) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    int64_t a = ap[i], ae = ap[i + 1], b = bp[i], be = bp[i + 1], o = op[i];
-    while (a < ae || b < be) {
-      const int32_t x = a < ae ? ac[a] : INT32_MAX;
-      const int32_t y = b < be ? bc[b] : INT32_MAX;
-      const int32_t j = x < y ? x : y;
-      const int64_t c = (int64_t)(x == j ? an[a] : 0) + (int64_t)(y == j ? bn[b] : 0);
-      if (c > INT32_MAX) atomicOr(bad, 1u);
-      oc[o] = j;
-      on[o] = (int32_t)c;
-      ++o;
-      a += x == j;
-      b += y == j;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+    const int64_t a0 = ap[i], a1 = ap[i + 1], b0 = bp[i], b1 = bp[i + 1], o = op[i];
+    int64_t carry = 0;
+    for (int64_t base = 0; base < a1 - a0; base += 32) {
+      const int64_t k = base + lane;
+      const bool valid = k < a1 - a0;
+      int32_t x = 0;
+      int64_t pb = b0;
+      bool match = false;
+      if (valid) {
+        x = ac[a0 + k];
+        pb = lower_bound_i32(bc, b0, b1, x);
+        match = pb < b1 && bc[pb] == x;
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, valid && match);
+      if (valid) {
+        const int64_t pos = k + (pb - b0) - (carry + __popc(m & lt));
+        const int64_t c = (int64_t)an[a0 + k] + (match ? (int64_t)bn[pb] : 0);
+        if (c > INT32_MAX) atomicOr(bad, 1u);
+        oc[o + pos] = x;
+        on[o + pos] = (int32_t)c;
+      }
+      carry += __popc(m);
+    }
+    carry = 0;
+    for (int64_t base = 0; base < b1 - b0; base += 32) {
+      const int64_t k = base + lane;
+      const bool valid = k < b1 - b0;
+      int32_t y = 0;
+      int64_t pa = a0;
+      bool match = false;
+      if (valid) {
+        y = bc[b0 + k];
+        pa = lower_bound_i32(ac, a0, a1, y);
+        match = pa < a1 && ac[pa] == y;
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, valid && match);
+      if (valid && !match) {
+        const int64_t pos = k + (pa - a0) - (carry + __popc(m & lt));
+        oc[o + pos] = y;
+        on[o + pos] = bn[b0 + k];
+      }
+      carry += __popc(m);
     }
   }
 }
@@ -412,7 +464,7 @@ __global__ void k_exp_scale(const double* __restrict__ y, int64_t n, double* __r
 // One balancing evaluation at y (d = e^y given):  s = S d;  f_new = y + log s - log A;
 // dF = f_new - f_old (when dF != nullptr);  closure |d s / A - 1|;  max |f_new|.
 // In multiplicative mode (mult = 1), also y_next = y + 0.5 (log A - log(d s)).
-template <bool kUniform>
+template <int kMode>
 __global__ void __launch_bounds__(256) k_balance_eval(SymView S, double delta, const double* __restrict__ area,
                                                       const double* __restrict__ y, const double* __restrict__ d,
                                                       double* __restrict__ f, double* __restrict__ dF,
@@ -423,7 +475,7 @@ __global__ void __launch_bounds__(256) k_balance_eval(SymView S, double delta, c
   bool bad = false;
   for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < S.n; i += warps) {
     const double Ai = area[i];
-    const double s = sym_row<kUniform>(S, i, d, lane) + delta * Ai * d[i];
+    const double s = sym_row<kMode>(S, i, d, lane) + delta * Ai * d[i];
     if (lane == 0) {
       if (!(s > 0.0 && isfinite(s))) bad = true;
       const double fn = y[i] + log(s) - log(Ai);
@@ -485,7 +537,7 @@ __global__ void __launch_bounds__(256) k_aa_dots(const double* __restrict__ dF, 
 
 // ------------------------------------------------------------------ products
 
-template <bool kUniform>
+template <int kMode>
 __global__ void __launch_bounds__(256) k_sym_apply(SymView S, double delta, const double* __restrict__ area,
                                                    const double* __restrict__ d, const double* __restrict__ x,
                                                    int mode, double* __restrict__ u, double* __restrict__ y) {
@@ -494,7 +546,7 @@ __global__ void __launch_bounds__(256) k_sym_apply(SymView S, double delta, cons
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   const double* v = mode == 0 ? x : u;
   for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < S.n; i += warps) {
-    const double s = sym_row<kUniform>(S, i, v, lane) + delta * area[i] * v[i];
+    const double s = sym_row<kMode>(S, i, v, lane) + delta * area[i] * v[i];
     if (lane == 0) y[i] = mode == 0 ? s : (mode == 1 ? (d[i] / area[i]) * s : d[i] * s);
   }
 }
@@ -582,11 +634,6 @@ __global__ void k_edges_out(const int64_t* __restrict__ fp, const int32_t* __res
 
 static int spmv_grid(int64_t rows) { return grid_for(rows * 32, 256, sm_count() * 8); }
 
-template <typename Fn>
-static void dispatch_uniform(bool uniform, Fn&& fn) {
-  if (uniform) fn(std::integral_constant<bool, true>());
-  else fn(std::integral_constant<bool, false>());
-}
 
 // Symmetric eigen-decomposition (cyclic Jacobi) of a k x k matrix, k <= 10.
 static void jacobi_eig(int k, double* a, double* v, double* w) {
@@ -653,7 +700,7 @@ static int balance_eval(pr_operator* op, BalanceWork& w, const double* y, double
   PR_CUDA(cudaMemsetAsync(w.sc.ptr, 0, 4 * sizeof(double), s));
   ::pr::launch_mark(), k_exp_scale<<<grid_for(n, 256), 256, 0, s>>>(y, n, w.d.ptr, w.sc.ptr);
   SymView S = sym_view(op->S);
-  dispatch_uniform(op->S.uniform, [&](auto u) {
+  dispatch_mode(op->S.mode, [&](auto u) {
     ::pr::timer_begin(kTimerBalance, s);
     ::pr::launch_mark(), k_balance_eval<decltype(u)::value><<<spmv_grid(n), 256, 0, s>>>(S, op->delta, op->area.ptr, y, w.d.ptr, w.f.ptr,
                                                                      dF, w.sc.ptr, mult, y_next);
@@ -828,37 +875,43 @@ int operator_create(const pr_counts* k, const int64_t* rays, const double* area,
       return PR_ERR_ACCOUNTING;
     }
   }
-  // symmetric matrix on the union pattern
+  // symmetric matrix: row i = row i of F followed by row i of F^T
   {
     auto T = std::make_shared<CountCsr>();
     PR_TRY(build_transpose(F, *T, s));
-    DevBuf<int64_t> len;
-    PR_TRY(len.alloc(n > 0 ? n : 1, s));
-    ::pr::launch_mark(), k_union_len<<<grid_for(n, 128), 128, 0, s>>>(F.row_ptr.ptr, F.col.ptr, T->row_ptr.ptr, T->col.ptr, n, len.ptr);
-    PR_CUDA(cudaGetLastError());
     SymCsr& S = op->S;
     S.n_rows = n;
+    S.nnz = F.nnz + T->nnz;
     PR_TRY(S.row_ptr.alloc(n + 1, s));
-    PR_TRY(lengths_to_row_ptr(len.ptr, n, S.row_ptr.ptr, s));
-    int64_t nnz = 0;
-    PR_CUDA(cudaMemcpyAsync(&nnz, S.row_ptr.ptr + n, 8, cudaMemcpyDeviceToHost, s));
-    PR_CUDA(cudaStreamSynchronize(s));
-    S.nnz = nnz;
-    PR_TRY(S.col.alloc(nnz, s));
-    S.uniform = n > 0 && all_equal_i64(h_rays) && all_equal_f64(h_area) && h_rays[0] > 0 && 2 * h_rays[0] < INT32_MAX;
-    if (S.uniform) {
-      PR_TRY(S.pairsum.alloc(nnz, s));
+    PR_TRY(S.words.alloc(S.nnz > 0 ? S.nnz : 1, s));
+    const bool uniform = n > 0 && all_equal_i64(h_rays) && all_equal_f64(h_area) && h_rays[0] > 0;
+    int64_t max_rays = 0;
+    for (int64_t r : h_rays) max_rays = std::max(max_rays, r);
+    int cb = 1, kb = 1;
+    while (cb < 32 && ((int64_t)1 << cb) < n) ++cb;
+    while (kb < 32 && ((int64_t)1 << kb) <= max_rays) ++kb;
+    if (uniform) {
       S.factor = 0.5 * h_area[0] / (double)h_rays[0];
-      ::pr::launch_mark(), k_union_fill<true><<<grid_for(n, 128), 128, 0, s>>>(F.row_ptr.ptr, F.col.ptr, F.cnt.ptr, T->row_ptr.ptr,
-                                                          T->col.ptr, T->cnt.ptr, op->rays.ptr, op->area.ptr, n,
-                                                          S.row_ptr.ptr, S.col.ptr, nullptr, S.pairsum.ptr);
+      if (cb + kb <= 32) {
+        S.mode = kPacked;
+        S.bits = kb;
+      } else {
+        S.mode = kCounts;
+        PR_TRY(S.cnt.alloc(S.nnz > 0 ? S.nnz : 1, s));
+      }
     } else {
-      PR_TRY(S.val.alloc(nnz, s));
-      ::pr::launch_mark(), k_union_fill<false><<<grid_for(n, 128), 128, 0, s>>>(F.row_ptr.ptr, F.col.ptr, F.cnt.ptr, T->row_ptr.ptr,
-                                                           T->col.ptr, T->cnt.ptr, op->rays.ptr, op->area.ptr, n,
-                                                           S.row_ptr.ptr, S.col.ptr, S.val.ptr, nullptr);
+      S.mode = kValues;
+      PR_TRY(S.val.alloc(S.nnz > 0 ? S.nnz : 1, s));
     }
-    PR_CUDA(cudaGetLastError());
+    if (n > 0) {
+      ::pr::launch_mark(), k_sym_row_ptr<<<grid_for(n + 1, 256), 256, 0, s>>>(F.row_ptr.ptr, T->row_ptr.ptr, n,
+                                                                              S.row_ptr.ptr);
+      PR_CUDA(cudaGetLastError());
+      ::pr::launch_mark(), k_sym_fill<<<grid_for(n * 32, 256), 256, 0, s>>>(
+          F.row_ptr.ptr, F.col.ptr, F.cnt.ptr, T->row_ptr.ptr, T->col.ptr, T->cnt.ptr, op->rays.ptr, op->area.ptr, n,
+          S.row_ptr.ptr, S.mode, S.bits, S.words.ptr, S.cnt.ptr, S.val.ptr);
+      PR_CUDA(cudaGetLastError());
+    }
     op->FT = T;  // kept for raw_rmatvec
   }
   if (n > 0) {
@@ -907,7 +960,7 @@ int apply(const pr_operator* op, int which, const double* x, double* y, cudaStre
     PR_CUDA(cudaGetLastError());
   }
   SymView S = sym_view(op->S);
-  dispatch_uniform(op->S.uniform, [&](auto un) {
+  dispatch_mode(op->S.mode, [&](auto un) {
     ::pr::launch_mark(), k_sym_apply<decltype(un)::value><<<spmv_grid(n), 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, x,
                                                                    mode, u.ptr, y);
   });

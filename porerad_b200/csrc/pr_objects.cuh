@@ -29,18 +29,25 @@ struct CountCsr {
   DevBuf<int32_t> cnt;      // nnz, > 0
 };
 
-// Symmetric exchange matrix S' = 0.5 (A F + F^T A) on the union pattern of F and F^T.
-// The support diagonal delta*A is applied separately.  Values are either binary64
-// (general areas / ray counts) or the integer pair sums n_ij + n_ji with one common
-// factor 0.5 A / R (every patch with the same area and the same ray count).
+// Symmetric exchange matrix S' = 0.5 (A F + F^T A) without the support diagonal
+// (delta A, applied separately).  Row i holds row i of F followed by row i of F^T, so
+// S'_ij x_j is the sum over both segments; no union of the two patterns is formed.
+// Entry storage, by mode:
+//   kPacked:  one 32-bit word (col << bits) | n per entry, value factor * n
+//             (every patch with the same area and ray count, and col/count bits fit);
+//   kCounts:  col (int32) + n (int32), value factor * n (same uniform case, wide ids);
+//   kValues:  col (int32) + binary64 value 0.5 A n / R of the entry's origin patch.
+enum SymMode { kPacked = 0, kCounts = 1, kValues = 2 };
+
 struct SymCsr {
   int64_t n_rows = 0, nnz = 0;
   DevBuf<int64_t> row_ptr;
-  DevBuf<int32_t> col;
-  DevBuf<double> val;       // general form
-  DevBuf<int32_t> pairsum;  // uniform form
-  bool uniform = false;
-  double factor = 0.0;      // 0.5 A / R in the uniform form
+  DevBuf<uint32_t> words;  // packed words, or the column of every entry
+  DevBuf<int32_t> cnt;     // kCounts
+  DevBuf<double> val;      // kValues
+  int mode = kPacked;
+  int bits = 0;            // count bits of a packed word
+  double factor = 0.0;     // 0.5 A / R in the uniform modes
 };
 
 }  // namespace pr
@@ -94,10 +101,5 @@ struct pr_operator {
   mutable int64_t spmv_calls = 0;
   // transposed count CSR (kept from the assembly for raw_rmatvec)
   mutable std::shared_ptr<pr::CountCsr> FT;
-  // binary32 copy of S' for mixed-precision sweeps, built on first use:
-  // packed words (col << bits) | pair sum when they fit 32 bits, else col + float values
-  mutable pr::DevBuf<uint32_t> s32;
-  mutable pr::DevBuf<float> s32val;
-  mutable int s32_bits = -1;  // -1 not built; >= 1 packed; 0 col + float values
   mutable cudaStream_t last_stream = nullptr;
 };

@@ -1,10 +1,12 @@
 // Sparse products over the symmetric exchange matrix and deterministic reductions.
 //
-// S x = S' x + delta A x, S' = 0.5 (A F + F^T A) on the union pattern of F and F^T
-// (porerad/exchange.py:108-112).  One warp owns one row: lanes stride over the
-// row's entries (coalesced col/value loads, gathers of x from L2) and the partial
-// sums meet in a fixed shuffle tree, so every product is bitwise reproducible.
+// S x = S' x + delta A x, S' = 0.5 (A F + F^T A) (porerad/exchange.py:108-112), row i
+// stored as row i of F followed by row i of F^T.  One warp owns one row: lanes stride
+// over the row's entries (coalesced 32-bit word loads, gathers of x from L2) and the
+// partial sums meet in a fixed shuffle tree, so every product is bitwise reproducible.
 #pragma once
+#include <type_traits>
+
 #include "pr_objects.cuh"
 
 namespace pr {
@@ -13,9 +15,11 @@ namespace pr {
 
 struct SymView {
   const int64_t* __restrict__ row_ptr;
-  const int32_t* __restrict__ col;
+  const uint32_t* __restrict__ words;
+  const int32_t* __restrict__ cnt;
   const double* __restrict__ val;
-  const int32_t* __restrict__ pairsum;
+  uint32_t mask;  // count mask of packed words
+  int bits;
   double factor;
   int64_t n;
 };
@@ -23,25 +27,60 @@ struct SymView {
 inline SymView sym_view(const SymCsr& S) {
   SymView v;
   v.row_ptr = S.row_ptr.ptr;
-  v.col = S.col.ptr;
+  v.words = S.words.ptr;
+  v.cnt = S.cnt.ptr;
   v.val = S.val.ptr;
-  v.pairsum = S.pairsum.ptr;
+  v.bits = S.bits;
+  v.mask = S.bits > 0 && S.bits < 32 ? ((1u << S.bits) - 1u) : 0xffffffffu;
   v.factor = S.factor;
   v.n = S.n_rows;
   return v;
 }
 
-// sum_j S'_ij x_j, the full sum on every lane of the warp.
-template <bool kUniform, typename Tx>
+// sum_j S'_ij x_j in binary64, the full sum on every lane of the warp.
+template <int kMode, typename Tx>
 __device__ __forceinline__ double sym_row(const SymView& S, int64_t i, const Tx* __restrict__ x, int lane) {
   const int64_t b = S.row_ptr[i], e = S.row_ptr[i + 1];
   double acc = 0.0;
   for (int64_t q = b + lane; q < e; q += 32) {
-    const double v = kUniform ? (double)__ldg(S.pairsum + q) : __ldg(S.val + q);
-    acc = fma(v, (double)__ldg(x + __ldg(S.col + q)), acc);
+    const uint32_t w = __ldg(S.words + q);
+    if constexpr (kMode == kPacked) {
+      acc = fma((double)(w & S.mask), (double)__ldg(x + (w >> S.bits)), acc);
+    } else if constexpr (kMode == kCounts) {
+      acc = fma((double)__ldg(S.cnt + q), (double)__ldg(x + w), acc);
+    } else {
+      acc = fma(__ldg(S.val + q), (double)__ldg(x + w), acc);
+    }
   }
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(PR_FULL, acc, o);
-  return kUniform ? acc * S.factor : acc;
+  return kMode == kValues ? acc : acc * S.factor;
+}
+
+// The same sum in binary32 (mixed-precision sweeps).
+template <int kMode>
+__device__ __forceinline__ float sym_row32(const SymView& S, int64_t i, const float* __restrict__ x, int lane) {
+  const int64_t b = S.row_ptr[i], e = S.row_ptr[i + 1];
+  float acc = 0.0f;
+  for (int64_t q = b + lane; q < e; q += 32) {
+    const uint32_t w = __ldg(S.words + q);
+    if constexpr (kMode == kPacked) {
+      acc = fmaf((float)(w & S.mask), __ldg(x + (w >> S.bits)), acc);
+    } else if constexpr (kMode == kCounts) {
+      acc = fmaf((float)__ldg(S.cnt + q), __ldg(x + w), acc);
+    } else {
+      acc = fmaf((float)__ldg(S.val + q), __ldg(x + w), acc);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(PR_FULL, acc, o);
+  return kMode == kValues ? acc : acc * (float)S.factor;
+}
+
+// Calls fn(std::integral_constant<int, mode>) for the matrix's storage mode.
+template <typename Fn>
+inline void dispatch_mode(int mode, Fn&& fn) {
+  if (mode == kPacked) fn(std::integral_constant<int, kPacked>());
+  else if (mode == kCounts) fn(std::integral_constant<int, kCounts>());
+  else fn(std::integral_constant<int, kValues>());
 }
 
 // atomic max of a non-negative double (bit patterns of non-negative doubles order as integers)

@@ -16,10 +16,10 @@
 // (H / nx)^2); coarse source = cell power summed over min(8, n)^3 blocks split as
 // numpy.array_split does.
 //
-// Mixed precision: the same series with binary32 vectors and binary32 products of
-// the integer pair sums (exact in binary32), wrapped in binary64 iterative
-// refinement of the radiosity J = E + (1 - eps) F_p^T J: the residual
-// r = E - J + (1 - eps) F_p^T J and the absorbed power eps F_p^T J are binary64.
+// Mixed precision: binary32 Chebyshev sweeps over the same packed matrix (the integer
+// counts are exact in binary32) inside binary64 iterative refinement of the radiosity
+// J = E + (1 - eps) F_p^T J: the residual r = E - J + (1 - eps) F_p^T J and the absorbed
+// power eps F_p^T J are binary64.
 #include <cmath>
 #include <vector>
 
@@ -37,7 +37,7 @@ struct SeriesState {
   double tol_abs;   // rtol * max(sum|E|, tiny)
 };
 
-template <bool kUniform>
+template <int kMode>
 __global__ void __launch_bounds__(256) k_series_step(SymView S, double delta, const double* __restrict__ area,
                                                      const double* __restrict__ d, const double* __restrict__ eps,
                                                      const double* __restrict__ v_in, double* __restrict__ v_out,
@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(256) k_series_step(SymView S, double delta, co
   double acc[2] = {0.0, 0.0};
   for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < S.n; i += warps) {
     const double Ai = area[i];
-    const double s = sym_row<kUniform>(S, i, v_in, lane) + delta * Ai * v_in[i];
+    const double s = sym_row<kMode>(S, i, v_in, lane) + delta * Ai * v_in[i];
     if (lane == 0) {
       const double inc = d[i] * s;
       const double e = eps[i];
@@ -133,12 +133,12 @@ int series_fp64(const pr_operator* op, const double* emitted, const double* eps,
   int batch = 4;
   for (int64_t launched = 0;;) {
     for (int b = 0; b < batch; ++b) {
-      if (op->S.uniform)
-        { ::pr::timer_begin(kTimerSeries, s); ::pr::launch_mark(), k_series_step<true><<<sb, 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, eps, vin, vout, absorbed,
-                                               partial.ptr, st.ptr); ::pr::timer_end(kTimerSeries, s); }
-      else
-        { ::pr::timer_begin(kTimerSeries, s); ::pr::launch_mark(), k_series_step<false><<<sb, 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, eps, vin, vout, absorbed,
-                                                partial.ptr, st.ptr); ::pr::timer_end(kTimerSeries, s); }
+      ::pr::timer_begin(kTimerSeries, s);
+      dispatch_mode(op->S.mode, [&](auto m) {
+        ::pr::launch_mark(), k_series_step<decltype(m)::value><<<sb, 256, 0, s>>>(
+            S, op->delta, op->area.ptr, op->scale.ptr, eps, vin, vout, absorbed, partial.ptr, st.ptr);
+      });
+      ::pr::timer_end(kTimerSeries, s);
       ::pr::launch_mark(), k_series_finish<<<1, 32, 0, s>>>(partial.ptr, sb, (long long)max_it, st.ptr);
       std::swap(vin, vout);
     }
@@ -326,85 +326,11 @@ __global__ void __launch_bounds__(256) k_coarse(const int32_t* __restrict__ cfp,
 
 // ------------------------------------------------------------------ mixed precision
 
-__global__ void k_pack_s32(const int32_t* __restrict__ col, const int32_t* __restrict__ pairsum,
-                           const double* __restrict__ val, int64_t m, int bits, uint32_t* __restrict__ w,
-                           float* __restrict__ fv) {
-  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < m; q += (int64_t)gridDim.x * blockDim.x) {
-    if (bits > 0) {
-      w[q] = ((uint32_t)col[q] << bits) | (uint32_t)pairsum[q];
-    } else {
-      w[q] = (uint32_t)col[q];
-      fv[q] = pairsum ? (float)pairsum[q] : (float)val[q];
-    }
-  }
-}
-
-__global__ void k_max_i32(const int32_t* __restrict__ a, int64_t m, unsigned int* __restrict__ out) {
-  unsigned int mx = 0;
-  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < m; q += (int64_t)gridDim.x * blockDim.x)
-    mx = max(mx, (unsigned int)a[q]);
-  for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(PR_FULL, mx, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, mx);
-}
-
-static int build_s32(const pr_operator* op, cudaStream_t s) {
-  if (op->s32_bits >= 0) return PR_OK;
-  const SymCsr& S = op->S;
-  const int64_t m = S.nnz;
-  int bits = 0;
-  if (S.uniform && m > 0) {
-    DevBuf<unsigned int> mx;
-    PR_TRY(mx.alloc(1, s));
-    PR_CUDA(cudaMemsetAsync(mx.ptr, 0, 4, s));
-    ::pr::launch_mark(), k_max_i32<<<grid_for(m, 256), 256, 0, s>>>(S.pairsum.ptr, m, mx.ptr);
-    unsigned int h = 0;
-    PR_CUDA(cudaMemcpyAsync(&h, mx.ptr, 4, cudaMemcpyDeviceToHost, s));
-    PR_CUDA(cudaStreamSynchronize(s));
-    int kb = 1;
-    while (kb < 31 && ((unsigned long long)1 << kb) <= h) ++kb;
-    int cb = 1;
-    while (cb < 31 && ((int64_t)1 << cb) < S.n_rows) ++cb;
-    bits = (kb + cb <= 32) ? kb : 0;
-  }
-  PR_TRY(op->s32.alloc(m > 0 ? m : 1, s));
-  if (bits == 0) PR_TRY(op->s32val.alloc(m > 0 ? m : 1, s));
-  if (m > 0) {
-    ::pr::launch_mark(), k_pack_s32<<<grid_for(m, 256), 256, 0, s>>>(S.col.ptr, S.uniform ? S.pairsum.ptr : nullptr, S.val.ptr, m, bits,
-                                                 op->s32.ptr, bits ? nullptr : op->s32val.ptr);
-    PR_CUDA(cudaGetLastError());
-  }
-  op->s32_bits = bits;
-  return PR_OK;
-}
-
-struct S32View {
-  const int64_t* __restrict__ row_ptr;
-  const uint32_t* __restrict__ w;
-  const float* __restrict__ fv;
-  int bits;
-  float factor;  // 1 for float values
-  int64_t n;
-};
-
-template <bool kPacked>
-__device__ __forceinline__ float s32_row(const S32View& S, int64_t i, const float* __restrict__ u, int lane) {
-  const int64_t b = S.row_ptr[i], e = S.row_ptr[i + 1];
-  float acc = 0.0f;
-  const uint32_t mask = (1u << (S.bits & 31)) - 1u;
-  for (int64_t q = b + lane; q < e; q += 32) {
-    const uint32_t w = __ldg(S.w + q);
-    if (kPacked) acc = fmaf((float)(w & mask), __ldg(u + (w >> S.bits)), acc);
-    else acc = fmaf(__ldg(S.fv + q), __ldg(u + w), acc);
-  }
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(PR_FULL, acc, o);
-  return acc * S.factor;
-}
-
 // One Chebyshev step on (I - om G) x = b in binary32 (Saad, Iterative Methods, Alg. 12.1):
 //   G d = scale * (S' u + delta A u), u = scale d / A;  x += d;  r -= (I - om G) d;
 //   d = c1 d + c2 r;  u_out = scale d / A.
-template <bool kPacked>
-__global__ void __launch_bounds__(256) k_cheb_step(S32View S, float delta, const float* __restrict__ scale,
+template <int kMode>
+__global__ void __launch_bounds__(256) k_cheb_step(SymView S, float delta, const float* __restrict__ scale,
                                                    const float* __restrict__ area, const float* __restrict__ om,
                                                    const float* __restrict__ u_in, float* __restrict__ u_out,
                                                    float* __restrict__ x, float* __restrict__ r,
@@ -412,7 +338,7 @@ __global__ void __launch_bounds__(256) k_cheb_step(S32View S, float delta, const
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < S.n; i += warps) {
-    const float sum = s32_row<kPacked>(S, i, u_in, lane);
+    const float sum = sym_row32<kMode>(S, i, u_in, lane);
     if (lane == 0) {
       const float Ai = area[i], sc = scale[i];
       const float gd = sc * (sum + delta * Ai * u_in[i]);
@@ -443,7 +369,7 @@ __global__ void k_refine_prep(double* __restrict__ J, const float* __restrict__ 
 
 // Binary64 residual r = E - J + om G J, absorbed = eps G J; block partials of |r| and |E|;
 // binary32 start of the next correction solve: x = 0, r32 = d32 = r, u32 = scale r / A.
-template <bool kUniform>
+template <int kMode>
 __global__ void __launch_bounds__(256) k_refine_residual(SymView S, double delta, const double* __restrict__ area,
                                                          const double* __restrict__ scale,
                                                          const double* __restrict__ eps, const double* __restrict__ E,
@@ -456,7 +382,7 @@ __global__ void __launch_bounds__(256) k_refine_residual(SymView S, double delta
   double acc[2] = {0.0, 0.0};
   for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < S.n; i += warps) {
     const double Ai = area[i];
-    const double s = sym_row<kUniform>(S, i, u, lane) + delta * Ai * u[i];
+    const double s = sym_row<kMode>(S, i, u, lane) + delta * Ai * u[i];
     if (lane == 0) {
       const double gj = scale[i] * s;
       const double e = eps[i];
@@ -489,7 +415,6 @@ __global__ void k_to_f32(const double* __restrict__ a, const double* __restrict_
 int series_mixed(const pr_operator* op, const double* emitted, const double* eps, double rtol, double* absorbed,
                  double* stats, cudaStream_t s) {
   const int64_t n = op->n;
-  PR_TRY(build_s32(op, s));
   // spectral bound of om G: max(1 - eps) (F_p is row-stochastic, similar to symmetric)
   std::vector<double> he(n);
   PR_CUDA(cudaMemcpyAsync(he.data(), eps, n * 8, cudaMemcpyDeviceToHost, s));
@@ -522,13 +447,6 @@ int series_mixed(const pr_operator* op, const double* emitted, const double* eps
   ::pr::launch_mark(), k_to_f32<<<grid_for(n, 256), 256, 0, s>>>(op->scale.ptr, op->area.ptr, eps, n, sc32.ptr, ar32.ptr, om32.ptr);
   PR_CUDA(cudaMemsetAsync(J.ptr, 0, n * 8, s));
   SymView S = sym_view(op->S);
-  S32View S32;
-  S32.row_ptr = op->S.row_ptr.ptr;
-  S32.w = op->s32.ptr;
-  S32.fv = op->s32val.ptr;
-  S32.bits = op->s32_bits;
-  S32.factor = op->S.uniform ? (float)op->S.factor : 1.0f;
-  S32.n = n;
   const float c_delta = (float)op->delta;
   const double sigma1 = 1.0 / rho;  // theta / delta with theta = 1, delta = rho
   int outer = 0;
@@ -537,12 +455,13 @@ int series_mixed(const pr_operator* op, const double* emitted, const double* eps
   for (;;) {
     ::pr::launch_mark(), k_refine_prep<<<grid_for(n, 256), 256, 0, s>>>(J.ptr, outer > 0 ? x32.ptr : nullptr, op->scale.ptr,
                                                     op->area.ptr, n, u.ptr);
-    if (op->S.uniform)
-      { ::pr::timer_begin(kTimerRefine, s); ::pr::launch_mark(), k_refine_residual<true><<<sb, 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, eps, emitted, J.ptr,
-                                                 u.ptr, absorbed, partial.ptr, x32.ptr, r32.ptr, d32.ptr, ua.ptr); ::pr::timer_end(kTimerRefine, s); }
-    else
-      { ::pr::timer_begin(kTimerRefine, s); ::pr::launch_mark(), k_refine_residual<false><<<sb, 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, eps, emitted, J.ptr,
-                                                  u.ptr, absorbed, partial.ptr, x32.ptr, r32.ptr, d32.ptr, ua.ptr); ::pr::timer_end(kTimerRefine, s); }
+    ::pr::timer_begin(kTimerRefine, s);
+    dispatch_mode(op->S.mode, [&](auto m) {
+      ::pr::launch_mark(), k_refine_residual<decltype(m)::value><<<sb, 256, 0, s>>>(
+          S, op->delta, op->area.ptr, op->scale.ptr, eps, emitted, J.ptr, u.ptr, absorbed, partial.ptr, x32.ptr,
+          r32.ptr, d32.ptr, ua.ptr);
+    });
+    ::pr::timer_end(kTimerRefine, s);
     PR_CUDA(cudaGetLastError());
     ++sp64;
     PR_TRY(sum_partials(partial.ptr, sb, 2, sums.ptr, s));
@@ -558,12 +477,12 @@ int series_mixed(const pr_operator* op, const double* emitted, const double* eps
     for (int k = 0; k < k_in; ++k) {
       const double rho_n = 1.0 / (2.0 * sigma1 - rho_k);
       const float c1 = (float)(rho_n * rho_k), c2 = (float)(2.0 * rho_n / rho);
-      if (S32.bits > 0)
-        { ::pr::timer_begin(kTimerCheb, s); ::pr::launch_mark(), k_cheb_step<true><<<sb, 256, 0, s>>>(S32, c_delta, sc32.ptr, ar32.ptr, om32.ptr, uin, uout, x32.ptr, r32.ptr,
-                                             d32.ptr, c1, c2); ::pr::timer_end(kTimerCheb, s); }
-      else
-        { ::pr::timer_begin(kTimerCheb, s); ::pr::launch_mark(), k_cheb_step<false><<<sb, 256, 0, s>>>(S32, c_delta, sc32.ptr, ar32.ptr, om32.ptr, uin, uout, x32.ptr,
-                                              r32.ptr, d32.ptr, c1, c2); ::pr::timer_end(kTimerCheb, s); }
+      ::pr::timer_begin(kTimerCheb, s);
+      dispatch_mode(op->S.mode, [&](auto m) {
+        ::pr::launch_mark(), k_cheb_step<decltype(m)::value><<<sb, 256, 0, s>>>(
+            S, c_delta, sc32.ptr, ar32.ptr, om32.ptr, uin, uout, x32.ptr, r32.ptr, d32.ptr, c1, c2);
+      });
+      ::pr::timer_end(kTimerCheb, s);
       rho_k = rho_n;
       std::swap(uin, uout);
       ++sp32;

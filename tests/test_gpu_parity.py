@@ -248,3 +248,50 @@ def test_empty_and_degenerate_inputs():
     assert int(c.sum()) == q.n_patches * 8
     e = vf.pool_counts([], 7)
     assert all(a.size == 0 for a in e)
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_device_merge_of_count_tables(name):
+    vf = _vf()
+    case = load_small(name)
+    p = _patches(case)
+    R = int(case["rays_per_patch"])
+    a, b = (vf.first_hit_counts_pooled(p, R, [int(s)]) for s in case["seeds"][:2])
+    merged = a.merge(b)
+    assert merged.sha256() == case["count_hash"].item().decode()
+    assert merged.rays_traced == a.rays_traced + b.rays_traced
+
+
+def test_operator_general_areas_against_oracle(oracle):
+    """Unequal patch areas select the binary64-value storage of S; checked against the oracle."""
+
+    from porerad_b200 import exchange
+
+    case = load_small("box12")
+    n = case["patches_patch_class"].size
+    R = int(case["rays_per_patch"]) * len(case["seeds"])
+    rays = np.full(n, R, np.int64)
+    area = case["patches_patch_area_m2"] * (1.0 + 0.5 * np.random.default_rng(4).random(n))
+    args = (case["pooled_origin"], case["pooled_receiver"], case["pooled_count"], rays, area)
+    op = exchange.ExchangeOperator(*args)
+    ref = oracle.ExchangeOperator(*args)
+    assert _rel(op.scale, ref.scale) <= SCALE_RTOL
+    x = case["probe_x"]
+    assert _rel(op.symmetric_matvec(x), ref.symmetric_matvec(x)) <= PRODUCT_RTOL
+    assert _rel(op.rmatvec(x), ref.rmatvec(x)) <= SCALE_RTOL
+    assert abs(op.reciprocity_error() - ref.reciprocity_error()) <= 1e-12
+
+
+def test_operator_wide_counts_storage():
+    """Counts and rays scaled by 2^16 keep every weight but no longer fit packed 32-bit words."""
+
+    from porerad_b200 import exchange
+
+    case = load_small("cube20")
+    n = case["patches_patch_class"].size
+    R = int(case["rays_per_patch"]) * len(case["seeds"])
+    k = 1 << 16
+    op = exchange.ExchangeOperator(case["pooled_origin"], case["pooled_receiver"], case["pooled_count"] * k,
+                                   np.full(n, R * k, np.int64), case["patches_patch_area_m2"])
+    assert _rel(op.scale, case["scale"]) <= SCALE_RTOL
+    assert _rel(op.symmetric_matvec(case["probe_x"]), case["probe_sym"]) <= PRODUCT_RTOL
