@@ -170,6 +170,22 @@ PR_API void pr_operator_destroy(pr_operator* op);
 PR_API int pr_reflection_series(const pr_operator* op, const double* emitted, const double* emissivity,
                          double relative_tolerance, int64_t max_reflections, double* absorbed,
                          double* residual_power, int64_t* iterations, void* stream);
+/* No counterpart in the reference.  The reflection series of pr_reflection_series for
+ * callers that cannot call cudaMalloc: a host whose device memory is owned by another
+ * allocator (for example a framework pool that reserves the GPU's memory up front), or
+ * code that must not take the allocator's implicit synchronisation in the middle of its
+ * stream work.  It allocates nothing: its scratch (two vectors, block partial sums and
+ * the convergence state) is one static device array held by every GPU that loads the
+ * library until the process exits, sized for at most 262144 patches; larger operators
+ * are rejected with PR_ERR_LIMIT.  emitted, emissivity and absorbed must be device
+ * memory of the operator's device.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) and should come before any stream capture.
+ * Every call shares the one array: calls that overlap on the GPU (other streams, other
+ * host threads) race and must be serialised by the caller. */
+PR_API int pr_reflection_series_noalloc(const pr_operator* op, const double* emitted,
+                                        const double* emissivity, double relative_tolerance,
+                                        int64_t max_reflections, double* absorbed,
+                                        double* residual_power, int64_t* iterations, void* stream);
 /* Replaces net_patch_power(operator, temperature_K, emissivity, area_m2,
  * relative_tolerance=, reference_temperature_K=), exchange.py:248-271.
  * has_reference = 0 means reference_temperature_K=None.  Outputs may be NULL. */

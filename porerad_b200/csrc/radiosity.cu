@@ -21,6 +21,7 @@
 // J = E + (1 - eps) F_p^T J: the residual r = E - J + (1 - eps) F_p^T J and the absorbed
 // power eps F_p^T J are binary64.
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "pr_spmv.cuh"
@@ -556,3 +557,139 @@ int prescribed_channels(const pr_case* c, const pr_operator* op, double T_m, dou
 }
 
 }  // namespace pr
+
+// ------------------------------------------------------------------ reflection series without allocation
+//
+// For callers that cannot call cudaMalloc: a host whose device memory is owned by
+// another allocator (a framework pool that reserves the GPU's memory up front), or a
+// caller that must not take the allocator's implicit synchronisation in the middle of
+// its own stream work.  The scratch of the series (two ping-pong vectors, block
+// partial sums and the convergence state) lives in one file-scope device array
+// instead, sized for at most kNoAllocMaxPatches patches.
+namespace pr {
+
+static constexpr int64_t kNoAllocMaxPatches = 262144;  // 2 x 262144 x 8 B of vectors
+static constexpr int64_t kNoAllocPartials = 2 * 148 * 8 * 2;  // block partials, two values per block
+static constexpr int64_t kNoAllocDoubles = 2 * kNoAllocMaxPatches + kNoAllocPartials + 8;
+
+static __device__ __align__(256) double g_series_scratch[kNoAllocDoubles];
+
+// Device address of the scratch array on the current device, looked up once per device.
+static int noalloc_scratch(double** out) {
+  static std::mutex mu;
+  static double* addr[64] = {nullptr};
+  int dev = 0;
+  PR_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    set_error("device %d outside the supported range", dev);
+    return PR_ERR_LIMIT;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    PR_CUDA(cudaGetSymbolAddress(&p, g_series_scratch));
+    addr[dev] = (double*)p;
+  }
+  *out = addr[dev];
+  return PR_OK;
+}
+
+static bool is_device_pointer(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+static int series_fp64_noalloc(const pr_operator* op, const double* emitted, const double* eps, double rtol,
+                               int64_t max_it, double* absorbed, double* residual, int64_t* iterations,
+                               cudaStream_t s) {
+  const int64_t n = op->n;
+  if (n > kNoAllocMaxPatches) {
+    set_error("pr_reflection_series_noalloc: %lld patches exceed the %lld of its static scratch; use "
+              "pr_reflection_series", (long long)n, (long long)kNoAllocMaxPatches);
+    return PR_ERR_LIMIT;
+  }
+  const int rb = red_blocks();
+  const int sb = spmv_blocks(n);
+  if ((int64_t)2 * (sb > rb ? sb : rb) > kNoAllocPartials) {
+    set_error("pr_reflection_series_noalloc: %d blocks exceed its partial-sum scratch", sb > rb ? sb : rb);
+    return PR_ERR_LIMIT;
+  }
+  double* base = nullptr;
+  PR_TRY(noalloc_scratch(&base));
+  double* va = base;
+  double* vb = base + kNoAllocMaxPatches;
+  double* partial = base + 2 * kNoAllocMaxPatches;
+  SeriesState* st = (SeriesState*)(base + 2 * kNoAllocMaxPatches + kNoAllocPartials);
+  // the array keeps the previous call's contents: the convergence state must start at zero
+  PR_CUDA(cudaMemsetAsync(st, 0, sizeof(SeriesState), s));
+  if (n == 0) {
+    *residual = 0.0;
+    *iterations = 0;
+    return PR_OK;
+  }
+  ::pr::launch_mark(), k_series_init<<<rb, 256, 0, s>>>(emitted, op->scale.ptr, op->area.ptr, n, va, absorbed, partial);
+  PR_CUDA(cudaGetLastError());
+  ::pr::launch_mark(), k_series_tol<<<1, 32, 0, s>>>(partial, rb, rtol, st);
+  PR_CUDA(cudaGetLastError());
+  SymView S = sym_view(op->S);
+  double* vin = va;
+  double* vout = vb;
+  SeriesState h;
+  int batch = 4;
+  for (;;) {
+    for (int b = 0; b < batch; ++b) {
+      dispatch_mode(op->S.mode, [&](auto m) {
+        ::pr::launch_mark(), k_series_step<decltype(m)::value><<<sb, 256, 0, s>>>(
+            S, op->delta, op->area.ptr, op->scale.ptr, eps, vin, vout, absorbed, partial, st);
+      });
+      ::pr::launch_mark(), k_series_finish<<<1, 32, 0, s>>>(partial, sb, (long long)max_it, st);
+      std::swap(vin, vout);
+    }
+    PR_CUDA(cudaGetLastError());
+    PR_CUDA(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s));
+    PR_CUDA(cudaStreamSynchronize(s));
+    if (h.done) break;
+    if (batch < 64) batch *= 2;
+  }
+  op->spmv_calls += h.iters;
+  if (h.done == 2) {
+    set_error("radiosity reflection series did not converge");
+    return PR_ERR_SERIES;
+  }
+  *residual = h.residual;
+  *iterations = h.iters;
+  return PR_OK;
+}
+
+}  // namespace pr
+
+extern "C" PR_API int pr_reflection_series_noalloc(const pr_operator* op, const double* emitted,
+                                                   const double* emissivity, double relative_tolerance,
+                                                   int64_t max_reflections, double* absorbed,
+                                                   double* residual_power, int64_t* iterations, void* stream) {
+  using namespace pr;
+  if (!op || !emitted || !emissivity || !absorbed) {
+    set_error("pr_reflection_series_noalloc: operator, emitted, emissivity and absorbed must not be NULL");
+    return PR_ERR_ARG;
+  }
+  if (max_reflections < 1) {
+    set_error("max_reflections must be at least 1");
+    return PR_ERR_ARG;
+  }
+  DeviceGuard guard(op->device);
+  if (!is_device_pointer(emitted) || !is_device_pointer(emissivity) || !is_device_pointer(absorbed)) {
+    set_error("pr_reflection_series_noalloc: emitted, emissivity and absorbed must be device memory");
+    return PR_ERR_ARG;
+  }
+  double res = 0.0;
+  int64_t it = 0;
+  const int st = series_fp64_noalloc(op, emitted, emissivity, relative_tolerance, max_reflections, absorbed, &res,
+                                     &it, (cudaStream_t)stream);
+  if (residual_power) *residual_power = res;
+  if (iterations) *iterations = it;
+  return st;
+}
