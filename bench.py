@@ -266,18 +266,13 @@ def run_ours(args, cfg):
 
     from porerad_b200 import _lib
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from porerad_b200 import replicas
+
+    world, rank, local = replicas.world_size(), replicas.rank(), replicas.local_rank()
     if world != args.gpus:
         raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}")
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    replicas.init("nccl")
     lib = _lib.load()
     seeds = ray_seeds(cfg)
     phases_host = make_phases(cfg)
@@ -289,9 +284,7 @@ def run_ours(args, cfg):
         release(served_step(phases_dev, cfg, seeds))
     torch.cuda.synchronize()
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
+    barrier = replicas.barrier
 
     # ---- timed region: device-resident inputs
     lib.pr_timers_reset()
@@ -341,11 +334,7 @@ def run_ours(args, cfg):
     h2d = int(phases_host.nbytes) + int(res["h2d"])
     d2h = int(res["d2h"])
 
-    t_max = ms
-    if dist is not None:
-        tt = torch.tensor([ms, e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max, e2e_s = float(tt[0]), float(tt[1])
+    t_max, e2e_s = replicas.max_over_ranks([ms, e2e_s])
     value = rays * world / (t_max * 1e-3)
     line = None
     if rank == 0:
@@ -424,18 +413,17 @@ def run_ours(args, cfg):
             "roofline": roof, "roofline_spmv": roof_spmv,
             "clocks": clocks.summary(), "gpu_launches": int(launches), "cpu_baseline": cpu,
         }
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finalize()
     return line
 
 
 # --------------------------------------------------------------------------- reference arm
 
 def run_reference(args, cfg):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return None
+    from porerad_b200 import replicas
+
+    if replicas.rank() != 0:
+        return None  # the CPU reference runs once, on rank 0
     seeds = ray_seeds(cfg)
     # warm-up runs of the sample, then K timed samples
     for _ in range(max(0, args.warmup)):

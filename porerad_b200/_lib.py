@@ -184,6 +184,35 @@ class Handle:
             pass
 
 
+_tls = threading.local()
+
+
+class use_stream:
+    """Context manager: calls made by this thread inside it run on ``stream``.
+
+    ``stream`` is a torch.cuda.Stream, a raw cudaStream_t (int) or None (the legacy
+    default stream).  Worker threads of the serving loop each hold their own stream so
+    that cases overlap on the device.
+    """
+
+    def __init__(self, stream):
+        self.stream = stream_arg(stream)
+
+    def __enter__(self):
+        self.prev = getattr(_tls, "stream", None)
+        _tls.stream = self.stream
+        return self
+
+    def __exit__(self, *exc):
+        _tls.stream = self.prev
+
+
+def stream() -> int | None:
+    """The cudaStream_t of the calling thread (None = legacy default stream)."""
+
+    return getattr(_tls, "stream", None)
+
+
 def stream_arg(stream) -> int | None:
     """cudaStream_t from None (legacy default stream), an int, or a torch.cuda.Stream."""
 

@@ -22,7 +22,7 @@ _TINY = np.finfo(np.float64).tiny
 
 RADIOSITY_RTOL_NEWTON = 1.0e-8
 RADIOSITY_RTOL_FINAL = 1.0e-13
-MIXED_RTOL = 1.0e-12
+MIXED_RTOL = 1.0e-10
 """Relative binary64 residual the mixed-precision solve refines to."""
 
 
@@ -157,7 +157,7 @@ def prescribed_field_channels(operator: ExchangeOperator, patches, T_mean_K: flo
     field at its owning cell.  One radiosity evaluation to a relative tolerance of
     1e-13 is made with the isothermal state at T_m subtracted.  ``precision``
     "mixed" solves with binary32 sweeps refined to a binary64 residual (not in the
-    reference; its relative residual is ``relative_tolerance``, default 1e-12).
+    reference; its relative residual is ``relative_tolerance``, default 1e-10).
     """
 
     dev = _device_of(patches)
@@ -173,7 +173,7 @@ def prescribed_field_channels(operator: ExchangeOperator, patches, T_mean_K: flo
     _lib.check(_lib.load().pr_prescribed_field_channels(dev.handle, operator.handle, float(T_mean_K),
                                                         float(delta_T_K), float(epsilon), prec, rtol,
                                                         q.ctypes.data, coarse.ctypes.data, stats.ctypes.data,
-                                                        None))
+                                                        _lib.stream()))
     if prec == _lib.PRECISION_FP64:
         info = {"reflections": int(stats[0]), "spmv": int(stats[1]), "residual_power_W": float(stats[2])}
     else:

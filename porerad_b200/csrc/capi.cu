@@ -294,7 +294,8 @@ int pr_operator_info(const pr_operator* op, double* scale, int* balance_method, 
   PR_CHECK_NULL(op, "operator");
   PR_ENTRY_GUARD(op);
   if (scale && op->n) {
-    PR_CUDA(cudaMemcpy(scale, op->scale.ptr, op->n * 8, cudaMemcpyDefault));
+    PR_CUDA(cudaMemcpyAsync(scale, op->scale.ptr, op->n * 8, cudaMemcpyDefault, op->last_stream));
+    PR_CUDA(cudaStreamSynchronize(op->last_stream));
   }
   if (balance_method) *balance_method = op->method;
   if (balance_iterations) *balance_iterations = op->iterations;

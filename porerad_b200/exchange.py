@@ -61,7 +61,7 @@ class ExchangeOperator:
         try:
             _lib.check(_lib.load().pr_operator_create(table.handle, rays.ctypes.data, area.ctypes.data,
                                                       float(support_diagonal_fraction), float(balance_tolerance),
-                                                      None, ctypes.byref(out)))
+                                                      _lib.stream(), ctypes.byref(out)))
         finally:
             if own_table:
                 table.close()
@@ -106,7 +106,7 @@ class ExchangeOperator:
             o = np.empty(m, np.int32)
             r = np.empty(m, np.int32)
             w = np.empty(m, np.float64)
-            _lib.check(_lib.load().pr_operator_edges(self.handle, o.ctypes.data, r.ctypes.data, w.ctypes.data, None))
+            _lib.check(_lib.load().pr_operator_edges(self.handle, o.ctypes.data, r.ctypes.data, w.ctypes.data, _lib.stream()))
             self._edges = (o, r, w)
         return self._edges
 
@@ -125,7 +125,7 @@ class ExchangeOperator:
     def _apply(self, which: int, x) -> np.ndarray:
         xx = np.ascontiguousarray(np.broadcast_to(np.asarray(x, dtype=np.float64), (self.n_patches,)))
         y = np.empty(self.n_patches)
-        _lib.check(_lib.load().pr_operator_apply(self.handle, which, xx.ctypes.data, y.ctypes.data, None))
+        _lib.check(_lib.load().pr_operator_apply(self.handle, which, xx.ctypes.data, y.ctypes.data, _lib.stream()))
         return y
 
     def raw_matvec(self, x: np.ndarray) -> np.ndarray:
@@ -157,7 +157,7 @@ class ExchangeOperator:
         """Largest relative defect of A_i F_p,ij = A_j F_p,ji over all sampled pairs (exchange.py:124-140)."""
 
         out = ctypes.c_double()
-        _lib.check(_lib.load().pr_operator_reciprocity_error(self.handle, ctypes.byref(out), None))
+        _lib.check(_lib.load().pr_operator_reciprocity_error(self.handle, ctypes.byref(out), _lib.stream()))
         return float(out.value)
 
     def _closure_error(self, y: np.ndarray) -> float:
@@ -211,7 +211,7 @@ def reflection_series(operator: ExchangeOperator, emitted_W: np.ndarray, emissiv
     res, it = ctypes.c_double(), ctypes.c_int64()
     _lib.check(_lib.load().pr_reflection_series(operator.handle, e.ctypes.data, eps.ctypes.data,
                                                 float(relative_tolerance), int(max_reflections),
-                                                absorbed.ctypes.data, ctypes.byref(res), ctypes.byref(it), None))
+                                                absorbed.ctypes.data, ctypes.byref(res), ctypes.byref(it), _lib.stream()))
     return RadiosityResult(e, absorbed, absorbed - e, float(res.value), int(it.value))
 
 
@@ -236,7 +236,7 @@ def net_patch_power(operator: ExchangeOperator, temperature_K: np.ndarray, emiss
                                               float(relative_tolerance), int(has_ref),
                                               float(reference_temperature_K) if has_ref else 0.0, 10000,
                                               emitted.ctypes.data, absorbed.ctypes.data, net.ctypes.data,
-                                              ctypes.byref(res), ctypes.byref(it), None))
+                                              ctypes.byref(res), ctypes.byref(it), _lib.stream()))
     return RadiosityResult(emitted, absorbed, net, float(res.value), int(it.value))
 
 
@@ -252,5 +252,5 @@ def net_patch_power_jvp(operator: ExchangeOperator, temperature_K: np.ndarray, d
     out = np.empty(n)
     _lib.check(_lib.load().pr_net_patch_power_jvp(operator.handle, T.ctypes.data, dT.ctypes.data, eps.ctypes.data,
                                                   area.ctypes.data, float(relative_tolerance), out.ctypes.data,
-                                                  None))
+                                                  _lib.stream()))
     return out

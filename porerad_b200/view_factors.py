@@ -57,7 +57,8 @@ class DeviceGeometry:
         lib = _lib.load()
         out = ctypes.c_void_p()
         nx, ny, nz = shape
-        _lib.check(lib.pr_case_create(src, nx, ny, nz, float(H_m), _lib.stream_arg(stream), ctypes.byref(out)))
+        st = _lib.stream_arg(stream) if stream is not None else _lib.stream()
+        _lib.check(lib.pr_case_create(src, nx, ny, nz, float(H_m), st, ctypes.byref(out)))
         self._h = _lib.Handle(out.value, "pr_case_destroy")
         self.shape = (nx, ny, nz)
         self.H_m = float(H_m)
@@ -88,7 +89,7 @@ class DeviceGeometry:
         }
         out = {n: np.empty(*shapes[n]) for n in names}
         args = [_lib.ptr(out.get(n)) for n in _FIELDS]
-        _lib.check(_lib.load().pr_case_patches(self.handle, *args, None))
+        _lib.check(_lib.load().pr_case_patches(self.handle, *args, _lib.stream()))
         return out
 
 
@@ -208,7 +209,7 @@ def generate_rays(patches, patch_start: int, patch_end: int, rays_per_patch: int
     directions = np.empty((n, 3))
     seeds = _lib.seeds_struct([_lib.pcg64_state(seed)])
     _lib.check(_lib.load().pr_generate_rays(dev.handle, p0, p1, R, ctypes.addressof(seeds), origins.ctypes.data,
-                                            directions.ctypes.data, None))
+                                            directions.ctypes.data, _lib.stream()))
     return origins, directions
 
 
@@ -222,7 +223,7 @@ def trace_first_hit(patches, origins: np.ndarray, directions: np.ndarray) -> np.
     receiver = np.empty(n, dtype=np.int32)
     failed = ctypes.c_int64()
     status = _lib.load().pr_trace_first_hit(dev.handle, o.ctypes.data, d.ctypes.data, n, receiver.ctypes.data,
-                                            ctypes.byref(failed), None)
+                                            ctypes.byref(failed), _lib.stream())
     if status == _lib.PR_ERR_UNRESOLVED:
         raise RuntimeError(f"{int(failed.value)} rays did not resolve a receiving patch")
     _lib.check(status)
@@ -257,7 +258,7 @@ class CountTable:
         c = np.empty(self.nnz, np.int64)
         rays = np.empty(self.n_patches, np.int64) if with_rays else None
         _lib.check(_lib.load().pr_counts_copy(self.handle, o.ctypes.data, r.ctypes.data, c.ctypes.data,
-                                              _lib.ptr(rays), None))
+                                              _lib.ptr(rays), _lib.stream()))
         return (o, r, c, rays) if with_rays else (o, r, c)
 
     def sha256(self) -> str:
@@ -268,7 +269,7 @@ class CountTable:
         """Pooled counts of this table and ``other`` (same patches), computed on the device."""
 
         out = ctypes.c_void_p()
-        _lib.check(_lib.load().pr_counts_merge(self.handle, other.handle, None, ctypes.byref(out)))
+        _lib.check(_lib.load().pr_counts_merge(self.handle, other.handle, _lib.stream(), ctypes.byref(out)))
         return CountTable(out.value)
 
 
@@ -280,7 +281,7 @@ def first_hit_counts_pooled(patches, rays_per_patch: int, seeds) -> CountTable:
     arr = _lib.seeds_struct([_lib.pcg64_state(s) for s in seeds])
     out = ctypes.c_void_p()
     _lib.check(_lib.load().pr_first_hit_counts(dev.handle, int(rays_per_patch), ctypes.addressof(arr), len(seeds),
-                                               None, ctypes.byref(out)))
+                                               _lib.stream(), ctypes.byref(out)))
     return CountTable(out.value)
 
 
@@ -333,7 +334,7 @@ def pool_to_device(origin, receiver, count, n_patches: int) -> CountTable:
         raise ValueError("origin, receiver and count must have the same length")
     out = ctypes.c_void_p()
     _lib.check(_lib.load().pr_counts_from_edges(o32.ctypes.data, r32.ctypes.data, c64.ctypes.data, int(o32.size), n,
-                                                None, ctypes.byref(out)))
+                                                _lib.stream(), ctypes.byref(out)))
     return CountTable(out.value)
 
 
