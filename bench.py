@@ -44,6 +44,15 @@ WORKLOADS = {
     "c2": dict(workload="OF N=128^3 phi=0.10 (64 Poisson seeds, geometry seed 1), 1000 rays/patch x sets A,B, "
                         "eps 0.6, T 650->750 K along x, FP32+FP64-refinement radiosity",
                arch="OF", n=128, phi=0.10, seed=1, rays=1000, sets=2, eps=0.6, T_m=700.0, dT=100.0, H=0.01),
+    "c4": dict(workload="serving: Poisson stream of geometry-axis cases, N in {96,128,160,192}, archetypes OF/FI/FA/TL, "
+                        "phi U(0.05,0.20), seeds 0-99, eps U(0.3,0.95), T_mean U(500,900) K with 100 K span, "
+                        "250-1000 rays/patch; served = continuous batching, mixed precision",
+               requests=16, stream_seed=2026, slots=4, H=0.01),
+    "c5": dict(workload="coupled-size stress: TL and FA N=192^3 phi=0.10, 1000 rays/patch x sets A,B,C, eps 0.6, "
+                        "T 690->710 K along x; then 20 solves at T_cell + N(0, 5 K) per voxel (seed 2) on the resident "
+                        "operator, FP32+FP64-refinement vs FP64 flux error per solve",
+               archs=("TL", "FA"), n=192, phi=0.10, seed=0, rays=1000, sets=3, eps=0.6, T_m=700.0, dT=20.0, H=0.01,
+               solves=20, sigma_K=5.0),
     "c1": dict(workload="FI N=64^3 phi=0.10 (r=2, seed 0), 64 rays/patch x 1 set, eps 0.9, T 600->700 K along x, "
                         "FP64 radiosity",
                arch="FI", n=64, phi=0.10, seed=0, rays=64, sets=1, eps=0.9, T_m=650.0, dT=100.0, H=0.01),
@@ -417,6 +426,197 @@ def run_ours(args, cfg):
     return line
 
 
+# --------------------------------------------------------------------------- serving (c4)
+
+def c4_specs(cfg):
+    """The request stream: (archetype, N, phi, geometry seed, axis, eps, T_mean, rays) per request."""
+
+    from porerad_b200.geometry import ARCHETYPES
+
+    rng = np.random.default_rng(cfg["stream_seed"])
+    out = []
+    for _ in range(cfg["requests"]):
+        out.append(dict(arch=str(rng.choice(ARCHETYPES)), n=int(rng.choice([96, 128, 160, 192])),
+                        phi=float(rng.uniform(0.05, 0.20)), seed=int(rng.integers(0, 100)),
+                        axis=str(rng.choice(["x", "y", "z"])), eps=float(rng.uniform(0.3, 0.95)),
+                        T_mean=float(rng.uniform(500.0, 900.0)), rays=int(rng.integers(250, 1001))))
+    return out
+
+
+def _c4_geometry(spec):
+    from porerad_b200 import geometry
+
+    ph = geometry.make(spec["arch"], spec["n"], spec["phi"], spec["seed"])
+    return np.ascontiguousarray(np.moveaxis(ph, "xyz".index(spec["axis"]), 0))
+
+
+def plain_case(req):
+    """One request through the drop-in NumPy API (the reference driver's sequence, binary64 series)."""
+
+    from porerad_b200 import coupled, exchange, view_factors as vf
+
+    p = vf.build_surface_patches(req.phases, req.H_m)
+    tables = [vf.first_hit_counts(p, req.rays_per_patch, s) for s in req.seeds]
+    o, r, c = vf.pool_counts(tables, p.n_patches)
+    op = exchange.ExchangeOperator(o, r, c, np.full(p.n_patches, req.rays_per_patch * len(req.seeds), np.int64),
+                                   p.patch_area_m2)
+    ch = coupled.prescribed_field_channels(op, p, req.T_mean_K, req.delta_T_K, req.epsilon)
+    op.close()
+    return ch
+
+
+def run_c4(args, cfg):
+    import multiprocessing
+
+    specs = c4_specs(cfg)
+    with multiprocessing.get_context("spawn").Pool(min(8, os.cpu_count() or 1)) as pool:
+        phases = pool.map(_c4_geometry, specs)
+    import torch
+
+    from porerad_b200 import _lib, serving
+    from porerad_b200.geometry import ray_set_seed
+
+    torch.cuda.set_device(0)
+    reqs = [serving.CaseRequest(ph, cfg["H"], sp["rays"], [ray_set_seed(sp["seed"] * 131 + k, 0)], sp["T_mean"],
+                                100.0, sp["eps"], precision="mixed", tag=k)
+            for k, (sp, ph) in enumerate(zip(specs, phases))]
+    lib = _lib.load()
+    # warm-up: one small case per slot count
+    with serving.Server(slots=1) as srv:
+        srv.submit(reqs[0]).result()
+    # saturated: every request arrives at t0
+    launches0 = lib.pr_kernel_launches()
+    with ClockSampler(0) as clocks:
+        t0 = time.perf_counter()
+        with serving.Server(slots=cfg["slots"]) as srv:
+            futs = [srv.submit(r, t_submit=t0) for r in reqs]
+            sat = [f.result() for f in futs]
+        t_sat = time.perf_counter() - t0
+        peak_reserved = srv.admission.peak
+    launches = lib.pr_kernel_launches() - launches0
+    served_rate = len(reqs) / t_sat
+    rays = sum(r.rays for r in sat)
+    # plain path, sequential, on the same requests
+    plain_case(reqs[0])
+    service = []
+    for r in reqs:
+        t = time.perf_counter()
+        plain_case(r)
+        service.append(time.perf_counter() - t)
+    plain_rate = len(reqs) / sum(service)
+    # Poisson arrivals at 0.8 x the plain rate, replayed in real time against the server
+    lam = 0.8 * plain_rate
+    arr = np.cumsum(np.random.default_rng(cfg["stream_seed"] + 1).exponential(1.0 / lam, size=len(reqs)))
+    arr -= arr[0]
+    t0 = time.perf_counter()
+    with serving.Server(slots=cfg["slots"]) as srv:
+        futs = []
+        for a, r in zip(arr, reqs):
+            delay = t0 + a - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            futs.append(srv.submit(r, t_submit=t0 + a))
+        pois = [f.result() for f in futs]
+    lat = [r.latency_s for r in pois]
+    # the plain path under the same arrivals: one FIFO server with the measured service times
+    done, plain_lat = 0.0, []
+    for a, sv in zip(arr, service):
+        done = max(done, a) + sv
+        plain_lat.append(done - a)
+    sat_lat = [r.latency_s for r in sat]
+    return {
+        "metric": "served cases/s (continuous batching, mixed precision), saturated request stream",
+        "value": served_rate, "unit": "cases/s", "n_gpus": 1, "steps": len(reqs), "warmup": 1,
+        "ms_per_step": 1e3 * t_sat / len(reqs), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (traversal), f32+f64 (radiosity)", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "requests": len(reqs), "slots": cfg["slots"],
+                   "stream_seed": cfg["stream_seed"], "hbm_peak_reserved_GB": peak_reserved / 1e9},
+        "rays_per_s_served": rays / t_sat,
+        "plain": {"cases_per_s": plain_rate, "p50_s": serving.percentile(service, 50)},
+        "served_over_plain": served_rate / plain_rate,
+        "saturated_latency_s": {"p50": serving.percentile(sat_lat, 50), "p99": serving.percentile(sat_lat, 99)},
+        "poisson": {"rate_per_s": lam, "served_p50_s": serving.percentile(lat, 50),
+                    "served_p99_s": serving.percentile(lat, 99),
+                    "plain_p50_s": serving.percentile(plain_lat, 50), "plain_p99_s": serving.percentile(plain_lat, 99),
+                    "plain_latency": "FIFO queue over the measured plain service times"},
+        "clocks": clocks.summary(), "gpu_launches": int(launches),
+    }
+
+
+# --------------------------------------------------------------------------- coupled-size stress (c5)
+
+def run_c5(args, cfg):
+    import torch
+
+    from porerad_b200 import _lib, coupled, exchange, geometry, view_factors as vf
+    from porerad_b200.geometry import ray_set_seed
+
+    torch.cuda.set_device(0)
+    lib = _lib.load()
+    n = cfg["n"]
+    base = coupled.linear_cell_temperature((n, n, n), cfg["T_m"], cfg["dT"])
+    rng = np.random.default_rng(2)
+    fields = [torch.from_numpy(base + rng.normal(0.0, cfg["sigma_K"], base.shape)).cuda() for _ in range(cfg["solves"])]
+    Th, Tc = cfg["T_m"] + cfg["dT"] / 2.0, cfg["T_m"] - cfg["dT"] / 2.0
+    # warm-up on a small case
+    w = vf.build_surface_patches(geometry.make("FA", 48, cfg["phi"], 0), cfg["H"])
+    t = vf.first_hit_counts_pooled(w, 64, [1])
+    wo = exchange.ExchangeOperator(t, None, None, np.full(w.n_patches, 64, np.int64), w.patch_area_m2)
+    coupled.cell_field_channels(wo, w, base[:48, :48, :48].copy(), Th, Tc, cfg["eps"], precision="mixed")
+    wo.close(); t.close()
+    out = {}
+    total_rays, total_ms = 0, 0.0
+    launches0 = lib.pr_kernel_launches()
+    with ClockSampler(0) as clocks:
+        for arch in cfg["archs"]:
+            phases = torch.from_numpy(geometry.make(arch, n, cfg["phi"], cfg["seed"])).cuda()
+            seeds = [ray_set_seed(cfg["seed"] + 7919 * (arch == "FA"), k) for k in range(cfg["sets"])]
+            torch.cuda.synchronize()
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record()
+            geo = vf.DeviceGeometry(phases, cfg["H"])
+            p = vf.SurfacePatches(H_m=cfg["H"], _device=geo)
+            tables = [vf.first_hit_counts_pooled(p, cfg["rays"], [s]) for s in seeds]
+            rays = sum(tb.rays_traced for tb in tables)
+            pooled = tables[0]
+            for tb in tables[1:]:
+                merged = pooled.merge(tb)
+                pooled.close()
+                tb.close()
+                pooled = merged
+            op = exchange.ExchangeOperator(pooled, None, None, np.full(geo.n_patches, cfg["rays"] * cfg["sets"],
+                                                                       np.int64),
+                                           np.full(geo.n_patches, (cfg["H"] / n) ** 2))
+            e1.record()
+            mixed = [coupled.cell_field_channels(op, p, f, Th, Tc, cfg["eps"], reference_temperature_K=cfg["T_m"],
+                                                 precision="mixed") for f in fields]
+            e2.record()
+            torch.cuda.synchronize()
+            build_ms, solve_ms = e0.elapsed_time(e1), e1.elapsed_time(e2)
+            fp64 = [coupled.cell_field_channels(op, p, f, Th, Tc, cfg["eps"], reference_temperature_K=cfg["T_m"])
+                    for f in fields]
+            errs = [max(abs(m.q_h - d.q_h) / abs(d.q_h), abs(m.q_c - d.q_c) / abs(d.q_c)) for m, d in zip(mixed, fp64)]
+            out[arch] = {"n_patches": geo.n_patches, "rays": rays, "pairs_pooled": pooled.nnz,
+                         "nnz_symmetric": op.nnz_symmetric, "build_ms": build_ms,
+                         "solve_ms_each": solve_ms / len(fields), "balance": [op.balance_method, op.balance_iterations],
+                         "mixed_vs_fp64_rel_flux_error_max": max(errs), "per_solve_error": errs,
+                         "q_first": [fp64[0].q_h, fp64[0].q_c, fp64[0].q_i]}
+            total_rays += rays
+            total_ms += build_ms + solve_ms
+            op.close()
+            pooled.close()
+            geo.close()
+            del phases
+    return {
+        "metric": "first-hit rays/s (N=192 stress: build + 20 resident-operator solves per geometry)",
+        "value": total_rays / (total_ms * 1e-3), "unit": "rays/s", "n_gpus": 1, "steps": len(cfg["archs"]),
+        "warmup": 1, "ms_per_step": total_ms / len(cfg["archs"]), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (traversal), f32+f64 (radiosity)", "data": "synthetic",
+        "config": {"workload": cfg["workload"]}, "cases": out, "clocks": clocks.summary(),
+        "gpu_launches": int(lib.pr_kernel_launches() - launches0),
+    }
+
+
 # --------------------------------------------------------------------------- reference arm
 
 def run_reference(args, cfg):
@@ -448,7 +648,14 @@ def run_reference(args, cfg):
 def main():
     args = parse_args()
     cfg = WORKLOADS[args.workload]
-    line = run_reference(args, cfg) if args.impl == "reference" else run_ours(args, cfg)
+    if args.impl == "reference":
+        line = run_reference(args, cfg)
+    elif args.workload == "c4":
+        line = run_c4(args, cfg)
+    elif args.workload == "c5":
+        line = run_c5(args, cfg)
+    else:
+        line = run_ours(args, cfg)
     if line is not None:
         print(json.dumps(line), flush=True)
 

@@ -215,6 +215,18 @@ PR_API int pr_prescribed_field_channels(const pr_case* c, const pr_operator* op,
                                  double relative_tolerance, double* q, double* coarse,
                                  double* stats, void* stream);
 
+/* Replaces evaluate_radiation(operator, patches, T_cells, T_hot_K, T_cold_K, epsilon,
+ * relative_tolerance=, reference_temperature_K=), coupled.py:86-105, followed by the channel
+ * sums of coupled.py:185-193, for an arbitrary cell temperature field: walls at T_hot_K /
+ * T_cold_K, internal patches at T_cells (nx*ny*nz f64) of their owning cell.  Outputs as
+ * pr_prescribed_field_channels.  The resident operator is reused across calls, as a
+ * Newton-Krylov outer loop calls the radiosity at every trial field. */
+PR_API int pr_cell_field_channels(const pr_case* c, const pr_operator* op, const double* T_cells,
+                                  double T_hot_K, double T_cold_K, double epsilon, int has_reference,
+                                  double reference_temperature_K, int precision,
+                                  double relative_tolerance, double* q, double* coarse, double* stats,
+                                  void* stream);
+
 /* ---- instrumentation (no counterpart in the reference) ----------------------------
  * Kernel classes timed with CUDA events on their launching stream while enabled:
  * 0 fused ray generation + traversal, 1 per-patch count reduction, 2 balancing

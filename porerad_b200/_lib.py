@@ -76,6 +76,7 @@ _SIGNATURES = {
                                   ctypes.POINTER(_f64), ctypes.POINTER(_i64), _vp]),
     "pr_net_patch_power_jvp": (_i32, [_vp, _vp, _vp, _vp, _vp, _f64, _vp, _vp]),
     "pr_prescribed_field_channels": (_i32, [_vp, _vp, _f64, _f64, _f64, _i32, _f64, _vp, _vp, _vp, _vp]),
+    "pr_cell_field_channels": (_i32, [_vp, _vp, _vp, _f64, _f64, _f64, _i32, _f64, _i32, _f64, _vp, _vp, _vp, _vp]),
     "pr_timers_enable": (None, [_i32]),
     "pr_timers_reset": (None, []),
     "pr_timers_read": (_i32, [_i32, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_f64)]),

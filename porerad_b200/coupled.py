@@ -208,3 +208,43 @@ def append_required(channel_difference: float, source_difference: float) -> bool
     """One symmetric append of a further ray block to each set when the sets disagree (coupled.py:216-219)."""
 
     return channel_difference > 0.01 or source_difference > 0.05
+
+
+def cell_field_channels(operator: ExchangeOperator, patches, T_cells, T_hot_K: float, T_cold_K: float,
+                        epsilon: float, *, reference_temperature_K: float | None = None, precision: str = "fp64",
+                        relative_tolerance: float | None = None) -> PrescribedChannels:
+    """Channels q_h, q_c, q_i of an arbitrary cell temperature field on the device (not in the reference).
+
+    The radiation evaluation of evaluate_radiation (coupled.py:86-105) followed by the
+    channel sums of prescribed_field_channels (coupled.py:185-193): walls at T_hot_K /
+    T_cold_K, internal patches at the temperature of their owning cell, one solve on the
+    resident operator.  ``T_cells`` is a float64 array (nx, ny, nz) on the host or a
+    CUDA tensor; the returned ``T_mean_K``/``delta_T_K`` are the wall mean and span.
+    """
+
+    dev = _device_of(patches)
+    prec = {"fp64": _lib.PRECISION_FP64, "mixed": _lib.PRECISION_MIXED}[precision]
+    rtol = RADIOSITY_RTOL_FINAL if prec == _lib.PRECISION_FP64 else MIXED_RTOL
+    if relative_tolerance is not None:
+        rtol = float(relative_tolerance)
+    if getattr(T_cells, "is_cuda", False):
+        if T_cells.numel() != int(np.prod(dev.shape)) or str(T_cells.dtype) != "torch.float64":
+            raise ValueError("T_cells must hold nx*ny*nz float64 values")
+        src = T_cells
+    else:
+        src = np.ascontiguousarray(np.asarray(T_cells, dtype=np.float64))
+        if src.size != int(np.prod(dev.shape)):
+            raise ValueError("T_cells must hold nx*ny*nz values")
+    nx, ny, nz = dev.shape
+    coarse = np.empty(tuple(min(8, n) for n in (nx, ny, nz)))
+    q = np.empty(4)
+    stats = np.zeros(4)
+    has_ref = reference_temperature_K is not None
+    _lib.check(_lib.load().pr_cell_field_channels(dev.handle, operator.handle, _lib.ptr(src), float(T_hot_K),
+                                                  float(T_cold_K), float(epsilon), int(has_ref),
+                                                  float(reference_temperature_K) if has_ref else 0.0, prec, rtol,
+                                                  q.ctypes.data, coarse.ctypes.data, stats.ctypes.data,
+                                                  _lib.stream()))
+    info = {"sweeps_or_reflections": int(stats[0]), "spmv": int(stats[1]), "residual": float(stats[2])}
+    return PrescribedChannels(0.5 * (T_hot_K + T_cold_K), float(T_hot_K - T_cold_K), float(epsilon), float(q[0]),
+                              float(q[1]), float(q[2]), float(q[3]), coarse, info)

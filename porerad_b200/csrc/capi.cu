@@ -52,6 +52,9 @@ int net_patch_power_jvp(const pr_operator* op, const double* T, const double* dT
                         const double* area, double rtol, double* out, cudaStream_t s);
 int prescribed_channels(const pr_case* c, const pr_operator* op, double T_m, double dT, double epsv, int precision,
                         double rtol, double* q, double* coarse, double* stats, cudaStream_t s);
+int cell_field_channels(const pr_case* c, const pr_operator* op, const double* T_cells, double Th, double Tc,
+                        double epsv, int has_ref, double ref, int precision, double rtol, double* q, double* coarse,
+                        double* stats, cudaStream_t s);
 
 }  // namespace pr
 
@@ -400,6 +403,21 @@ int pr_prescribed_field_channels(const pr_case* c, const pr_operator* op, double
   PR_ENTRY_GUARD(c);
   return prescribed_channels(c, op, T_mean_K, delta_T_K, epsilon, precision, relative_tolerance, q, coarse, stats,
                              (cudaStream_t)stream);
+}
+
+int pr_cell_field_channels(const pr_case* c, const pr_operator* op, const double* T_cells, double T_hot_K,
+                           double T_cold_K, double epsilon, int has_reference, double reference_temperature_K,
+                           int precision, double relative_tolerance, double* q, double* coarse, double* stats,
+                           void* stream) {
+  PR_CHECK_NULL(c, "case");
+  PR_CHECK_NULL(op, "operator");
+  PR_CHECK_NULL(T_cells, "T_cells");
+  PR_CHECK_NULL(q, "q");
+  PR_ARG(precision == PR_PRECISION_FP64 || precision == PR_PRECISION_MIXED, "unknown precision %d", precision);
+  PR_ARG(c->device == op->device, "case and operator live on different devices");
+  PR_ENTRY_GUARD(c);
+  return cell_field_channels(c, op, T_cells, T_hot_K, T_cold_K, epsilon, has_reference, reference_temperature_K,
+                             precision, relative_tolerance, q, coarse, stats, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -258,22 +258,33 @@ int reflection_series(const pr_operator* op, const double* emitted, const double
 
 // Patch temperature (coupled.py:45-53 with the linear field of coupled.py:138-143),
 // uniform emissivity and the T_ref-subtracted emission (exchange.py:268-270).
-__global__ void k_prescribed_emission(const int8_t* __restrict__ cls, const int32_t* __restrict__ cell,
-                                      const double* __restrict__ area, int64_t n, int64_t nyz, int64_t nx,
-                                      double T_m, double dT, double epsv, double* __restrict__ e,
-                                      double* __restrict__ eps) {
-  const double Th = T_m + dT / 2.0, Tc = T_m - dT / 2.0;
+// Patch temperature and emission for the channel solves.  T_cells == nullptr: the linear
+// prescribed field (walls at T_m +/- dT/2, coupled.py:138-143, 178-184); otherwise the given
+// cell field with walls at Th, Tc (coupled.py:45-53).  Emission with a reference
+// temperature in the factored form of exchange.py:268-270, else eps sigma A T^4.
+struct FieldSpec {
+  const double* T_cells;
+  double T_m, dT, Th, Tc, eps, ref;
+  int has_ref;
+};
+
+__global__ void k_field_emission(const int8_t* __restrict__ cls, const int32_t* __restrict__ cell,
+                                 const double* __restrict__ area, int64_t n, int64_t nyz, int64_t nx, FieldSpec f,
+                                 double* __restrict__ e, double* __restrict__ eps) {
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
     double t;
     const int c = cls[p];
-    if (c == 0) t = Th;
-    else if (c == 1) t = Tc;
+    if (c == 0) t = f.Th;
+    else if (c == 1) t = f.Tc;
+    else if (f.T_cells) t = f.T_cells[cell[p]];
     else {
       const int64_t i = cell[p] / nyz;
-      t = (T_m + dT / 2.0) - (((double)i + 0.5) * dT) / (double)nx;
+      t = (f.T_m + f.dT / 2.0) - (((double)i + 0.5) * f.dT) / (double)nx;
     }
-    e[p] = epsv * PR_SIGMA * area[p] * ((t - T_m) * (t + T_m) * (t * t + T_m * T_m));
-    eps[p] = epsv;
+    const double pre = f.eps * PR_SIGMA * area[p];
+    const double r = f.ref;
+    e[p] = f.has_ref ? pre * ((t - r) * (t + r) * (t * t + r * r)) : pre * pow(t, 4.0);
+    eps[p] = f.eps;
   }
 }
 
@@ -504,8 +515,8 @@ int series_mixed(const pr_operator* op, const double* emitted, const double* eps
 }
 
 
-int prescribed_channels(const pr_case* c, const pr_operator* op, double T_m, double dT, double epsv, int precision,
-                        double rtol, double* q, double* coarse, double* stats, cudaStream_t s) {
+static int field_channels(const pr_case* c, const pr_operator* op, const FieldSpec& f, int precision, double rtol,
+                          double* q, double* coarse, double* stats, cudaStream_t s) {
   const int64_t n = c->n_patches;
   PR_ARG(op->n == n, "operator has %lld patches, geometry %lld", (long long)op->n, (long long)n);
   DevBuf<double> dE, de, dAb, partial, sums;
@@ -515,8 +526,8 @@ int prescribed_channels(const pr_case* c, const pr_operator* op, double T_m, dou
   const int rb = red_blocks();
   PR_TRY(partial.alloc((size_t)3 * rb, s));
   PR_TRY(sums.alloc(3, s));
-  ::pr::launch_mark(), k_prescribed_emission<<<grid_for(n, 256), 256, 0, s>>>(c->cls.ptr, c->cell.ptr, op->area.ptr, n, c->ny * c->nz,
-                                                        c->nx, T_m, dT, epsv, dE.ptr, de.ptr);
+  ::pr::launch_mark(), k_field_emission<<<grid_for(n, 256), 256, 0, s>>>(c->cls.ptr, c->cell.ptr, op->area.ptr, n,
+                                                                         c->ny * c->nz, c->nx, f, dE.ptr, de.ptr);
   PR_CUDA(cudaGetLastError());
   double st[4] = {0, 0, 0, 0};
   if (precision == PR_PRECISION_MIXED) {
@@ -554,6 +565,22 @@ int prescribed_channels(const pr_case* c, const pr_operator* op, double T_m, dou
   q[3] = fabs(qh + qc + qi) / fmax(fmax(fabs(qh), fabs(qc)), fmax(fabs(qi), 1.0e-30));
   if (stats) for (int k = 0; k < 4; ++k) stats[k] = st[k];
   return PR_OK;
+}
+
+int prescribed_channels(const pr_case* c, const pr_operator* op, double T_m, double dT, double epsv, int precision,
+                        double rtol, double* q, double* coarse, double* stats, cudaStream_t s) {
+  FieldSpec f{nullptr, T_m, dT, T_m + dT / 2.0, T_m - dT / 2.0, epsv, T_m, 1};
+  return field_channels(c, op, f, precision, rtol, q, coarse, stats, s);
+}
+
+int cell_field_channels(const pr_case* c, const pr_operator* op, const double* T_cells, double Th, double Tc,
+                        double epsv, int has_ref, double ref, int precision, double rtol, double* q, double* coarse,
+                        double* stats, cudaStream_t s) {
+  DevBuf<double> dT;
+  PR_TRY(dT.alloc(c->n_cells, s));
+  PR_CUDA(cudaMemcpyAsync(dT.ptr, T_cells, c->n_cells * 8, cudaMemcpyDefault, s));
+  FieldSpec f{dT.ptr, 0.0, 0.0, Th, Tc, epsv, ref, has_ref};
+  return field_channels(c, op, f, precision, rtol, q, coarse, stats, s);
 }
 
 }  // namespace pr

@@ -295,3 +295,35 @@ def test_operator_wide_counts_storage():
                                    np.full(n, R * k, np.int64), case["patches_patch_area_m2"])
     assert _rel(op.scale, case["scale"]) <= SCALE_RTOL
     assert _rel(op.symmetric_matvec(case["probe_x"]), case["probe_sym"]) <= PRODUCT_RTOL
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_cell_field_channels_against_oracle(oracle, name):
+    """An arbitrary cell field (walls fixed) against the oracle's evaluate_radiation + channel sums."""
+
+    from porerad_b200 import coupled, exchange
+
+    case = load_small(name)
+    p = _patches(case)
+    R = int(case["rays_per_patch"]) * len(case["seeds"])
+    args = (case["pooled_origin"], case["pooled_receiver"], case["pooled_count"],
+            np.full(p.n_patches, R, np.int64), case["patches_patch_area_m2"])
+    op = exchange.ExchangeOperator(*args)
+    ref_op = oracle.ExchangeOperator(*args)
+    q = oracle.build_surface_patches(case["phases"], float(case["H_m"]))
+    rng = np.random.default_rng(2)
+    T_cells = 700.0 + 5.0 * rng.standard_normal(case["phases"].shape)
+    for ref_T, prec in ((700.0, "fp64"), (None, "fp64"), (700.0, "mixed")):
+        got = coupled.cell_field_channels(op, p, T_cells, 710.0, 690.0, 0.6, reference_temperature_K=ref_T,
+                                          precision=prec)
+        Tp = oracle.patch_temperature(q, T_cells, 710.0, 690.0)
+        rad = oracle.net_patch_power(ref_op, Tp, np.full(q.n_patches, 0.6), q.patch_area_m2,
+                                     relative_tolerance=1e-13, reference_temperature_K=ref_T)
+        area = oracle.cross_section_area(q)
+        want = [-float(np.sum(rad.net_power_W[q.patch_class == k])) / area for k in (0, 1, 2)]
+        scale = max(abs(w) for w in want)
+        tol = MIXED_RTOL if prec == "mixed" else FLUX_RTOL
+        if ref_T is None:
+            tol = max(tol, 1e-7)  # absolute emission T^4 without the reference subtraction: q is a small difference
+        for g, w in zip((got.q_h, got.q_c, got.q_i), want):
+            assert abs(g - w) <= tol * scale
