@@ -376,7 +376,7 @@ def run_ours(args, cfg):
         flops = 4.0 * steps + 30.0 * rays
         achieved = flops / (t_tr * 1e-3) / 1e12 if t_tr > 0 else None
         per_ray_traffic = ncu_traffic("trace", args.workload)
-        roof = {"kernel": "k_trace_blocks (fused PCG64 ray generation + FP64 DDA)", "bound": "fp64",
+        roof = {"kernel": "k_trace_pool (fused PCG64 ray generation + FP64 DDA, pooled lanes)", "bound": "fp64",
                 "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
                 "frac": achieved / fp64 if achieved else None,
                 "traffic": per_ray_traffic * rays / max(n_tr, 1) if per_ray_traffic else None,
@@ -389,7 +389,8 @@ def run_ours(args, cfg):
             n_k, t_k = timers[name]
             if n_k == 0:
                 continue
-            bytes_per = nnz_s * (8 if name != "cheb" else 4) + P * (8 + 5 * (8 if name != "cheb" else 4))
+            # packed 4-byte words per entry, row offsets, and the P-vectors each kernel streams
+            bytes_per = nnz_s * 4 + P * (8 + 5 * (8 if name != "cheb" else 4))
             spmv[name] = {"launches": n_k, "ms": t_k, "GB_per_s": bytes_per * n_k / (t_k * 1e-3) / 1e9}
         tot_b = sum(v["GB_per_s"] * v["ms"] for v in spmv.values())
         tot_t = sum(v["ms"] for v in spmv.values())
@@ -419,7 +420,7 @@ def run_ours(args, cfg):
             "balance": {"method": last["balance"][0], "iterations": last["balance"][1],
                         "row_sum_error": last["balance"][2]},
             "rays_per_step": rays / args.steps, "dda_steps_per_ray": steps / rays,
-            "roofline": roof, "roofline_spmv": roof_spmv,
+            "roofline": roof, "roofline_spmv": roof_spmv, "trace_variant": _lib.trace_variant()[1],
             "clocks": clocks.summary(), "gpu_launches": int(launches), "cpu_baseline": cpu,
         }
     replicas.finalize()

@@ -235,6 +235,12 @@ PR_API int pr_cell_field_channels(const pr_case* c, const pr_operator* op, const
 PR_API void pr_timers_enable(int on);
 PR_API void pr_timers_reset(void);
 PR_API int pr_timers_read(int kernel_class, long long* launches, double* total_ms);
+/* Traversal autotuning (no counterpart in the reference): the fused traversal has several
+ * compiled variants (registers per thread, DDA steps between lane refills); by default the
+ * first count pass of a problem class (grid size, rays per origin) times each on its first
+ * chunk and keeps the fastest.  Results do not depend on the variant. */
+PR_API int pr_trace_set_variant(int variant);  /* -1 = autotune (default) */
+PR_API int pr_trace_variant_info(int* count, int* last_used, const char** name);
 /* Number of the library's own kernel launches so far (CUB primitives not counted). */
 PR_API long long pr_kernel_launches(void);
 

@@ -81,6 +81,8 @@ _SIGNATURES = {
     "pr_timers_reset": (None, []),
     "pr_timers_read": (_i32, [_i32, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_f64)]),
     "pr_kernel_launches": (ctypes.c_longlong, []),
+    "pr_trace_set_variant": (_i32, [_i32]),
+    "pr_trace_variant_info": (_i32, [ctypes.POINTER(_i32), ctypes.POINTER(_i32), ctypes.POINTER(ctypes.c_char_p)]),
 }
 
 TIMER_TRACE, TIMER_RLE, TIMER_BALANCE, TIMER_SERIES, TIMER_CHEB, TIMER_REFINE = range(6)
@@ -206,6 +208,14 @@ class use_stream:
 
     def __exit__(self, *exc):
         _tls.stream = self.prev
+
+
+def trace_variant() -> tuple[int, str]:
+    """(index, name) of the traversal variant the last count pass used (chosen by the autotuner)."""
+
+    n, last, name = ctypes.c_int(), ctypes.c_int(), ctypes.c_char_p()
+    check(load().pr_trace_variant_info(ctypes.byref(n), ctypes.byref(last), ctypes.byref(name)))
+    return int(last.value), name.value.decode()
 
 
 def stream() -> int | None:

@@ -246,55 +246,70 @@ int counts_merge(const pr_counts* A, const pr_counts* B, cudaStream_t s, pr_coun
 
 // ------------------------------------------------------------------ transpose / symmetric pattern
 
-// keys (col << 32 | row) of every entry, in row order
-__global__ void k_transpose_keys(const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col, int64_t n,
-                                 unsigned long long* __restrict__ key) {
+// (row << 32 | count) of every entry of F, in row order
+__global__ void k_row_count_values(const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ cnt, int64_t n,
+                                   unsigned long long* __restrict__ val) {
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps)
     for (int64_t q = row_ptr[i] + lane; q < row_ptr[i + 1]; q += 32)
-      key[q] = ((unsigned long long)(uint32_t)col[q] << 32) | (unsigned long long)(uint32_t)i;
-  }
+      val[q] = ((unsigned long long)(uint32_t)i << 32) | (unsigned long long)(uint32_t)cnt[q];
 }
 
-__global__ void k_split_transposed(const unsigned long long* __restrict__ key, int64_t m, int32_t* __restrict__ tcol,
-                                   int32_t* __restrict__ tlen) {
+__global__ void k_split_values(const unsigned long long* __restrict__ val, int64_t m, int32_t* __restrict__ col,
+                               int32_t* __restrict__ cnt) {
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
-    tcol[t] = (int32_t)(key[t] & 0xffffffffull);
-    atomicAdd(tlen + (int64_t)(key[t] >> 32), 1);
+    col[t] = (int32_t)(val[t] >> 32);
+    cnt[t] = (int32_t)(val[t] & 0xffffffffull);
   }
 }
 
+// row_ptr[c] = first position of key c in the sorted keys (lower bound), c = 0..n
+__global__ void k_row_ptr_from_sorted(const uint32_t* __restrict__ keys, int64_t m, int64_t n,
+                                      int64_t* __restrict__ row_ptr) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c <= n; c += (int64_t)gridDim.x * blockDim.x) {
+    int64_t lo = 0, hi = m;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if ((int64_t)keys[mid] < c) lo = mid + 1;
+      else hi = mid;
+    }
+    row_ptr[c] = lo;
+  }
+}
+
+// F^T by one stable radix sort of F's entries (already in row order) keyed on the column
+// alone: equal columns keep their row order, so every row of F^T comes out sorted.
 int build_transpose(const CountCsr& F, CountCsr& T, cudaStream_t s) {
   const int64_t n = F.n_rows, m = F.nnz;
   T.n_rows = n;
   T.nnz = m;
   PR_TRY(T.row_ptr.alloc(n + 1, s));
-  PR_TRY(T.col.alloc(m, s));
-  PR_TRY(T.cnt.alloc(m, s));
-  DevBuf<int32_t> tlen;
-  DevBuf<int64_t> tlen64;
-  PR_TRY(tlen.alloc(n > 0 ? n : 1, s));
-  ::pr::launch_mark(), k_zero_i32<<<grid_for(n, 256), 256, 0, s>>>(tlen.ptr, n);
-  if (m > 0) {
-    DevBuf<unsigned long long> key, key_sorted;
-    PR_TRY(key.alloc(m, s));
-    PR_TRY(key_sorted.alloc(m, s));
-    ::pr::launch_mark(), k_transpose_keys<<<grid_for(n * 32, 256), 256, 0, s>>>(F.row_ptr.ptr, F.col.ptr, n, key.ptr);
-    PR_CUDA(cudaGetLastError());
-    int bits = 1;
-    while (bits < 32 && ((int64_t)1 << bits) < n) ++bits;
-    size_t b = 0;
-    PR_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b, key.ptr, key_sorted.ptr, F.cnt.ptr, T.cnt.ptr, m, 0, 32 + bits, s));
-    DevBuf<uint8_t> tmp;
-    PR_TRY(tmp.alloc(b + 16, s));
-    PR_CUDA(cub::DeviceRadixSort::SortPairs(tmp.ptr, b, key.ptr, key_sorted.ptr, F.cnt.ptr, T.cnt.ptr, m, 0, 32 + bits, s));
-    ::pr::launch_mark(), k_split_transposed<<<grid_for(m, 256), 256, 0, s>>>(key_sorted.ptr, m, T.col.ptr, tlen.ptr);
-    PR_CUDA(cudaGetLastError());
+  PR_TRY(T.col.alloc(m > 0 ? m : 1, s));
+  PR_TRY(T.cnt.alloc(m > 0 ? m : 1, s));
+  if (m == 0) {
+    PR_CUDA(cudaMemsetAsync(T.row_ptr.ptr, 0, (n + 1) * sizeof(int64_t), s));
+    return PR_OK;
   }
-  PR_TRY(tlen64.alloc(n > 0 ? n : 1, s));
-  ::pr::launch_mark(), k_widen_scan_input<<<grid_for(n, 256), 256, 0, s>>>(tlen.ptr, tlen64.ptr, n);
-  PR_TRY(lengths_to_row_ptr(tlen64.ptr, n, T.row_ptr.ptr, s));
+  DevBuf<uint32_t> keys_out;
+  DevBuf<unsigned long long> val, val_out;
+  PR_TRY(keys_out.alloc(m, s));
+  PR_TRY(val.alloc(m, s));
+  PR_TRY(val_out.alloc(m, s));
+  ::pr::launch_mark(), k_row_count_values<<<grid_for(n * 32, 256), 256, 0, s>>>(F.row_ptr.ptr, F.cnt.ptr, n, val.ptr);
+  PR_CUDA(cudaGetLastError());
+  int bits = 1;
+  while (bits < 32 && ((int64_t)1 << bits) < n) ++bits;
+  const uint32_t* keys_in = (const uint32_t*)F.col.ptr;
+  size_t b = 0;
+  PR_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b, keys_in, keys_out.ptr, val.ptr, val_out.ptr, m, 0, bits, s));
+  DevBuf<uint8_t> tmp;
+  PR_TRY(tmp.alloc(b + 16, s));
+  PR_CUDA(cub::DeviceRadixSort::SortPairs(tmp.ptr, b, keys_in, keys_out.ptr, val.ptr, val_out.ptr, m, 0, bits, s));
+  ::pr::launch_mark(), k_split_values<<<grid_for(m, 256), 256, 0, s>>>(val_out.ptr, m, T.col.ptr, T.cnt.ptr);
+  PR_CUDA(cudaGetLastError());
+  ::pr::launch_mark(), k_row_ptr_from_sorted<<<grid_for(n + 1, 256), 256, 0, s>>>(keys_out.ptr, m, n, T.row_ptr.ptr);
+  PR_CUDA(cudaGetLastError());
   return PR_OK;
 }
 
@@ -836,6 +851,47 @@ static bool all_equal_f64(const std::vector<double>& v) {
   return true;
 }
 
+__global__ void k_pack_words(uint32_t* __restrict__ words, const int32_t* __restrict__ cnt, int64_t m, int bits) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x)
+    words[t] = (words[t] << bits) | (uint32_t)cnt[t];
+}
+
+// S' on the union of the patterns of F and F^T with the pair counts n_ij + n_ji (ranked
+// row merge), packed into 32-bit words when the bits fit.
+static int sym_union(const CountCsr& F, const CountCsr& T, pr_operator* op, cudaStream_t s) {
+  SymCsr& S = op->S;
+  const int64_t n = F.n_rows;
+  DevBuf<int64_t> len;
+  DevBuf<unsigned int> bad;
+  PR_TRY(len.alloc(n, s));
+  PR_TRY(bad.alloc(1, s));
+  PR_CUDA(cudaMemsetAsync(bad.ptr, 0, 4, s));
+  ::pr::launch_mark(), k_merge_len<<<grid_for(n * 32, 256), 256, 0, s>>>(F.row_ptr.ptr, F.col.ptr, T.row_ptr.ptr,
+                                                                         T.col.ptr, n, len.ptr);
+  PR_CUDA(cudaGetLastError());
+  PR_TRY(lengths_to_row_ptr(len.ptr, n, S.row_ptr.ptr, s));
+  int64_t nnz = 0;
+  PR_CUDA(cudaMemcpyAsync(&nnz, S.row_ptr.ptr + n, 8, cudaMemcpyDeviceToHost, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  S.nnz = nnz;
+  PR_TRY(S.words.alloc(nnz > 0 ? nnz : 1, s));
+  PR_TRY(S.cnt.alloc(nnz > 0 ? nnz : 1, s));
+  ::pr::launch_mark(), k_merge_rank<<<grid_for(n * 32, 256), 256, 0, s>>>(
+      F.row_ptr.ptr, F.col.ptr, F.cnt.ptr, T.row_ptr.ptr, T.col.ptr, T.cnt.ptr, n, S.row_ptr.ptr,
+      (int32_t*)S.words.ptr, S.cnt.ptr, bad.ptr);
+  PR_CUDA(cudaGetLastError());
+  if (S.mode == kPacked && nnz > 0) {
+    ::pr::launch_mark(), k_pack_words<<<grid_for(nnz, 256), 256, 0, s>>>(S.words.ptr, S.cnt.ptr, nnz, S.bits);
+    PR_CUDA(cudaGetLastError());
+    S.cnt.release();
+  }
+  unsigned int hb = 0;
+  PR_CUDA(cudaMemcpyAsync(&hb, bad.ptr, 4, cudaMemcpyDeviceToHost, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  PR_ARG(!hb, "pair counts exceed 2^31");
+  return PR_OK;
+}
+
 int apply(const pr_operator* op, int which, const double* x_dev, double* y_dev, cudaStream_t s);
 
 int operator_create(const pr_counts* k, const int64_t* rays, const double* area, double delta, double tol,
@@ -881,29 +937,24 @@ int operator_create(const pr_counts* k, const int64_t* rays, const double* area,
     PR_TRY(build_transpose(F, *T, s));
     SymCsr& S = op->S;
     S.n_rows = n;
-    S.nnz = F.nnz + T->nnz;
     PR_TRY(S.row_ptr.alloc(n + 1, s));
-    PR_TRY(S.words.alloc(S.nnz > 0 ? S.nnz : 1, s));
     const bool uniform = n > 0 && all_equal_i64(h_rays) && all_equal_f64(h_area) && h_rays[0] > 0;
     int64_t max_rays = 0;
     for (int64_t r : h_rays) max_rays = std::max(max_rays, r);
     int cb = 1, kb = 1;
     while (cb < 32 && ((int64_t)1 << cb) < n) ++cb;
-    while (kb < 32 && ((int64_t)1 << kb) <= max_rays) ++kb;
+    while (kb < 32 && ((int64_t)1 << kb) <= 2 * max_rays) ++kb;  // pair sums n_ij + n_ji <= 2 R
     if (uniform) {
       S.factor = 0.5 * h_area[0] / (double)h_rays[0];
-      if (cb + kb <= 32) {
-        S.mode = kPacked;
-        S.bits = kb;
-      } else {
-        S.mode = kCounts;
-        PR_TRY(S.cnt.alloc(S.nnz > 0 ? S.nnz : 1, s));
-      }
+      S.mode = cb + kb <= 32 ? kPacked : kCounts;
+      S.bits = S.mode == kPacked ? kb : 0;
     } else {
       S.mode = kValues;
+      S.nnz = F.nnz + T->nnz;
+      PR_TRY(S.words.alloc(S.nnz > 0 ? S.nnz : 1, s));
       PR_TRY(S.val.alloc(S.nnz > 0 ? S.nnz : 1, s));
     }
-    if (n > 0) {
+    if (n > 0 && S.mode == kValues) {
       ::pr::launch_mark(), k_sym_row_ptr<<<grid_for(n + 1, 256), 256, 0, s>>>(F.row_ptr.ptr, T->row_ptr.ptr, n,
                                                                               S.row_ptr.ptr);
       PR_CUDA(cudaGetLastError());
@@ -911,6 +962,9 @@ int operator_create(const pr_counts* k, const int64_t* rays, const double* area,
           F.row_ptr.ptr, F.col.ptr, F.cnt.ptr, T->row_ptr.ptr, T->col.ptr, T->cnt.ptr, op->rays.ptr, op->area.ptr, n,
           S.row_ptr.ptr, S.mode, S.bits, S.words.ptr, S.cnt.ptr, S.val.ptr);
       PR_CUDA(cudaGetLastError());
+    } else if (n > 0) {
+      // equal areas and ray counts: S'_ij = factor (n_ij + n_ji) on the union of the patterns
+      PR_TRY(sym_union(F, *T, op.get(), s));
     }
     op->FT = T;  // kept for raw_rmatvec
   }

@@ -16,6 +16,10 @@
 // probe reads one bit of the packed grid (L1/L2 resident).
 #include <cub/device/device_scan.cuh>
 
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "pr_math.cuh"
 #include "pr_objects.cuh"
 
@@ -262,7 +266,6 @@ __global__ void __launch_bounds__(256) k_trace_given(Geom g, const double* __res
 // bursts of kBurst DDA steps, so the warp no longer waits for its longest ray.
 static constexpr int kPool = 64;   // pool slots per warp (two batches)
 static constexpr int kWarps = 4;   // warps per block
-static constexpr int kBurst = 4;   // DDA steps between refills
 static constexpr int kUnit = 512;  // rays per work grab
 
 struct WarpPool {
@@ -325,9 +328,10 @@ __device__ __forceinline__ void ray_from_stream(const RaySrc& src, pr_u128 st, p
   dz = pr_div(dz, len);
 }
 
-__global__ void __launch_bounds__(kWarps * 32) k_trace_pool(Geom g, RaySrc src, ChunkDesc cd,
-                                                            int32_t* __restrict__ recv,
-                                                            unsigned long long* __restrict__ counters) {
+template <int kMinBlocks, int kBurst>
+__global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(Geom g, RaySrc src, ChunkDesc cd,
+                                                                        int32_t* __restrict__ recv,
+                                                                        unsigned long long* __restrict__ counters) {
   __shared__ WarpPool pools[kWarps];
   WarpPool& pool = pools[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
@@ -708,15 +712,125 @@ static RaySrc src_of(const pr_case* c, const SeedTables& t) {
 
 static int trace_grid() { return sm_count() * 8; }
 
-// Persistent grid of the pooled traversal: as many blocks as fit on every SM.
-static int pool_grid() {
-  static int blocks = 0;
-  if (blocks == 0) {
+// Variants of the pooled traversal (minimum resident blocks per SM x DDA steps per burst).
+// Every variant writes the same receivers; the autotuner below picks the fastest per
+// problem class by timing them on the first chunk of the first call.
+using TraceKernel = void (*)(Geom, RaySrc, ChunkDesc, int32_t*, unsigned long long*);
+struct TraceVariant {
+  TraceKernel kernel;
+  const char* name;
+};
+static const TraceVariant kVariants[] = {
+    {k_trace_pool<5, 4>, "5blk-burst4"},
+    {k_trace_pool<5, 8>, "5blk-burst8"},
+    {k_trace_pool<5, 2>, "5blk-burst2"},
+    {k_trace_pool<6, 4>, "6blk-burst4"},
+    {k_trace_pool<8, 4>, "8blk-burst4"},
+    {k_trace_pool<4, 4>, "4blk-burst4"},
+};
+static constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
+
+// Persistent grid of a variant: as many blocks as fit on every SM.
+static int variant_grid(int v) {
+  static int blocks[kNumVariants] = {0};
+  if (blocks[v] == 0) {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_pool, kWarps * 32, 0);
-    blocks = sm_count() * (per_sm > 0 ? per_sm : 1);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kVariants[v].kernel, kWarps * 32, 0);
+    blocks[v] = sm_count() * (per_sm > 0 ? per_sm : 1);
   }
-  return blocks;
+  return blocks[v];
+}
+
+struct TuneKey {
+  int64_t nx, ny, nz, L;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(nx, ny, nz, L) < std::tie(o.nx, o.ny, o.nz, o.L);
+  }
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, int> g_tuned;
+static int g_forced_variant = -1;
+static int g_last_variant = 0;
+
+}  // namespace pr
+
+extern "C" {
+// Force one traversal variant (0 .. count - 1), or -1 for the autotuner (default).
+PR_API int pr_trace_set_variant(int v) {
+  if (v < -1 || v >= pr::kNumVariants) {
+    pr::set_error("traversal variant %d outside [-1, %d)", v, pr::kNumVariants);
+    return PR_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lk(pr::g_tune_mu);
+  pr::g_forced_variant = v;
+  return PR_OK;
+}
+// Number of variants, the variant used by the last count pass, and its name (may be NULL).
+PR_API int pr_trace_variant_info(int* count, int* last, const char** name) {
+  std::lock_guard<std::mutex> lk(pr::g_tune_mu);
+  if (count) *count = pr::kNumVariants;
+  if (last) *last = pr::g_last_variant;
+  if (name) *name = pr::kVariants[pr::g_last_variant].name;
+  return PR_OK;
+}
+}
+
+namespace pr {
+
+static int launch_variant(int v, const pr_case* c, const RaySrc& src, const ChunkDesc& cd, int32_t* recv,
+                          unsigned long long* ctr, cudaStream_t s) {
+  PR_CUDA(cudaMemsetAsync(ctr + 2, 0, sizeof(unsigned long long), s));
+  ::pr::launch_mark(), kVariants[v].kernel<<<variant_grid(v), kWarps * 32, 0, s>>>(geom_of(c), src, cd, recv, ctr);
+  PR_CUDA(cudaGetLastError());
+  return PR_OK;
+}
+
+// Variant for this problem class: forced, cached, or measured now on the given chunk
+// (each variant traces it once, timed with events; the counters are restored after).
+static int choose_variant(const pr_case* c, int64_t L, const RaySrc& src, const ChunkDesc& cd, int32_t* recv,
+                          unsigned long long* ctr, cudaStream_t s, int* out) {
+  const TuneKey key{c->nx, c->ny, c->nz, L};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    if (g_forced_variant >= 0) {
+      *out = g_forced_variant;
+      return PR_OK;
+    }
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) {
+      *out = it->second;
+      return PR_OK;
+    }
+  }
+  unsigned long long saved[2];
+  PR_CUDA(cudaMemcpyAsync(saved, ctr, sizeof(saved), cudaMemcpyDeviceToHost, s));
+  cudaEvent_t e0, e1;
+  PR_CUDA(cudaEventCreate(&e0));
+  PR_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int best_v = 0;
+  for (int v = 0; v < kNumVariants; ++v) {
+    PR_CUDA(cudaEventRecord(e0, s));
+    PR_TRY(launch_variant(v, c, src, cd, recv, ctr, s));
+    PR_CUDA(cudaEventRecord(e1, s));
+    PR_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    PR_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best) {
+      best = ms;
+      best_v = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  PR_CUDA(cudaMemcpyAsync(ctr, saved, sizeof(saved), cudaMemcpyHostToDevice, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[key] = best_v;
+  }
+  *out = best_v;
+  return PR_OK;
 }
 
 int generate_rays(const pr_case* c, int64_t p0, int64_t p1, int64_t R, const pr_pcg64* seed, double* origins,
@@ -770,6 +884,21 @@ int trace_given(const pr_case* c, const double* origins, const double* dirs, int
 // Largest rays-per-origin segment the shared-memory sort handles (128 KiB of keys + heads).
 static const int kMaxSegment = 16384;
 
+// The per-patch sort's dynamic shared-memory limit is a per-device function attribute shared
+// by every host thread: raise it once per device to the largest segment and never lower it.
+static int enable_rle_smem() {
+  static std::mutex mu;
+  static bool done[64] = {false};
+  int dev = 0;
+  PR_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev >= 0 && dev < 64 && done[dev]) return PR_OK;
+  PR_CUDA(cudaFuncSetAttribute(k_patch_rle, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(2 * kMaxSegment * sizeof(int32_t))));
+  if (dev >= 0 && dev < 64) done[dev] = true;
+  return PR_OK;
+}
+
 int first_hit_counts(const pr_case* c, int64_t R, const pr_pcg64* seeds, int S, cudaStream_t s, pr_counts** out) {
   PR_ARG(R > 0 && S > 0, "rays_per_patch and the number of seeds must be positive");
   const int64_t L64 = R * S;
@@ -820,7 +949,7 @@ int first_hit_counts(const pr_case* c, int64_t R, const pr_pcg64* seeds, int S, 
   DevBuf<uint8_t> scan_tmp;
   PR_TRY(scan_tmp.alloc(scan_bytes + 16, s));
   const size_t smem = (size_t)2 * Lpad * sizeof(int32_t);
-  PR_CUDA(cudaFuncSetAttribute(k_patch_rle, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  PR_TRY(enable_rle_smem());
   const int rle_threads = Lpad >= 1024 ? 512 : (Lpad >= 256 ? 256 : 64);
 
   // per-chunk compacted pieces; concatenated once the total is known
@@ -832,17 +961,17 @@ int first_hit_counts(const pr_case* c, int64_t R, const pr_pcg64* seeds, int S, 
   DevBuf<int64_t> nnz_all;  // row lengths of every patch
   PR_TRY(nnz_all.alloc(P, s));
   int64_t total = 0;
+  int variant = 0;
   PR_CUDA(cudaMemsetAsync(off.ptr, 0, sizeof(int64_t), s));
   for (int64_t p0 = 0; p0 < P; p0 += chunk) {
     const int64_t np = std::min(chunk, P - p0);
     const int64_t nr = np * L64;
     ChunkDesc cd{nr, np, p0, R};
-    PR_CUDA(cudaMemsetAsync(ctr.ptr + 2, 0, sizeof(unsigned long long), s));
+    const RaySrc src = src_of(c, t);
+    if (p0 == 0) PR_TRY(choose_variant(c, L64, src, cd, recv.ptr, ctr.ptr, s, &variant));
     ::pr::timer_begin(kTimerTrace, s);
-    ::pr::launch_mark(), k_trace_pool<<<pool_grid(), kWarps * 32, 0, s>>>(geom_of(c), src_of(c, t), cd, recv.ptr,
-                                                                          ctr.ptr);
+    PR_TRY(launch_variant(variant, c, src, cd, recv.ptr, ctr.ptr, s));
     ::pr::timer_end(kTimerTrace, s);
-    PR_CUDA(cudaGetLastError());
     const int rle_grid = (int)std::min<int64_t>(np, (int64_t)sm_count() * 16);
     ::pr::timer_begin(kTimerRle, s);
     ::pr::launch_mark(), k_patch_rle<<<rle_grid, rle_threads, smem, s>>>(recv.ptr, np, L, (int)R, Lpad, st_col.ptr, st_cnt.ptr,
@@ -887,6 +1016,10 @@ int first_hit_counts(const pr_case* c, int64_t R, const pr_pcg64* seeds, int S, 
   unsigned long long h[2];
   PR_CUDA(cudaMemcpyAsync(h, ctr.ptr, sizeof(h), cudaMemcpyDeviceToHost, s));
   PR_CUDA(cudaStreamSynchronize(s));
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_last_variant = variant;
+  }
   k->rays_traced = P * L64;
   k->dda_steps = (int64_t)h[0];
   k->last_stream = s;

@@ -327,3 +327,27 @@ def test_cell_field_channels_against_oracle(oracle, name):
             tol = max(tol, 1e-7)  # absolute emission T^4 without the reference subtraction: q is a small difference
         for g, w in zip((got.q_h, got.q_c, got.q_i), want):
             assert abs(g - w) <= tol * scale
+
+
+def test_every_traversal_variant_gives_the_same_counts():
+    """The autotuner may pick any compiled variant: all must produce the reference's counts."""
+
+    from porerad_b200 import _lib
+
+    vf = _vf()
+    case = load_small("cube20")
+    p = _patches(case)
+    R = int(case["rays_per_patch"])
+    n = ctypes_int = None
+    import ctypes
+
+    count = ctypes.c_int()
+    _lib.check(_lib.load().pr_trace_variant_info(ctypes.byref(count), None, None))
+    try:
+        for v in range(count.value):
+            _lib.check(_lib.load().pr_trace_set_variant(v))
+            t = vf.first_hit_counts_pooled(p, R, [int(s) for s in case["seeds"]])
+            assert t.sha256() == case["count_hash"].item().decode(), v
+            assert _lib.trace_variant()[0] == v
+    finally:
+        _lib.load().pr_trace_set_variant(-1)
