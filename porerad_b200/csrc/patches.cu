@@ -47,17 +47,17 @@ __global__ void k_cell_faces(const uint8_t* __restrict__ phases, int64_t nx, int
   }
 }
 
-// One 64-bit word per 4x4x4 brick: bit ((i & 3) << 4) | ((j & 3) << 2) | (k & 3) of brick
-// ((i >> 2) * nby + (j >> 2)) * nbz + (k >> 2) is solid[i, j, k]; cells past the grid are 0.
-__global__ void k_pack_bricks(const uint8_t* __restrict__ solid, int64_t nx, int64_t ny, int64_t nz, int nbx,
-                              int nby, int nbz, uint64_t* __restrict__ occ) {
-  const int64_t n = (int64_t)nbx * nby * nbz;
+// One 32-bit word per (row, w): bit b = solid[i, j, 32 w + b].
+__global__ void k_pack_occupancy(const uint8_t* __restrict__ solid, int64_t rows, int64_t nz, int wpr,
+                                 uint32_t* __restrict__ occ) {
+  const int64_t n = rows * wpr;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t bk = t % nbz, bj = (t / nbz) % nby, bi = t / ((int64_t)nby * nbz);
-    uint64_t word = 0;
-    for (int b = 0; b < 64; ++b) {
-      const int64_t i = bi * 4 + (b >> 4), j = bj * 4 + ((b >> 2) & 3), k = bk * 4 + (b & 3);
-      if (i < nx && j < ny && k < nz && solid[(i * ny + j) * nz + k]) word |= 1ull << b;
+    const int64_t row = t / wpr;
+    const int w = (int)(t % wpr);
+    uint32_t word = 0;
+    for (int b = 0; b < 32; ++b) {
+      const int64_t k = (int64_t)w * 32 + b;
+      if (k < nz && solid[row * nz + k]) word |= 1u << b;
     }
     occ[t] = word;
   }
@@ -164,13 +164,10 @@ int case_build(pr_case* c, const uint8_t* phases, cudaStream_t s) {
   PR_TRY(off.alloc(n, s));
   ::pr::launch_mark(), k_cell_faces<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(ph.ptr, c->nx, c->ny, c->nz, c->solid.ptr, mask.ptr, nf.ptr);
   PR_CUDA(cudaGetLastError());
-  c->nbx = (int)((c->nx + 3) / 4);
-  c->nby = (int)((c->ny + 3) / 4);
-  c->nbz = (int)((c->nz + 3) / 4);
-  const int64_t bricks = (int64_t)c->nbx * c->nby * c->nbz;
-  PR_TRY(c->occ.alloc(bricks, s));
-  ::pr::launch_mark(), k_pack_bricks<<<grid_for(bricks, 256, 148 * 16), 256, 0, s>>>(c->solid.ptr, c->nx, c->ny, c->nz,
-                                                                                    c->nbx, c->nby, c->nbz, c->occ.ptr);
+  c->wpr = (int)((c->nz + 31) / 32);
+  const int64_t rows = c->nx * c->ny;
+  PR_TRY(c->occ.alloc(rows * c->wpr, s));
+  ::pr::launch_mark(), k_pack_occupancy<<<grid_for(rows * c->wpr, 256, 148 * 16), 256, 0, s>>>(c->solid.ptr, rows, c->nz, c->wpr, c->occ.ptr);
   PR_CUDA(cudaGetLastError());
 
   PR_TRY(nw.alloc(lat, s));

@@ -41,24 +41,13 @@ static constexpr int kMapBatch = 192;
 #define PR_TWO_PI 0x1.921fb54442d18p+2  // the binary64 product 2.0 * numpy.pi
 
 struct Geom {
-  const uint64_t* __restrict__ occ;  // 4x4x4 bricks
+  const uint32_t* __restrict__ occ;
   const int32_t* __restrict__ cfp;
   const int32_t* __restrict__ hot;
   const int32_t* __restrict__ cold;
-  int32_t nx, ny, nz, nby, nbz;
+  int32_t nx, ny, nz, wpr;
   int64_t n_cells;
 };
-
-// Solid flag of cell (i, j, k) from its 4x4x4 brick; the lane keeps the last brick word and
-// reloads only when the walk leaves that brick.
-__device__ __forceinline__ bool solid_cell(const Geom& g, int i, int j, int k, int& brick, uint64_t& word) {
-  const int b = ((i >> 2) * g.nby + (j >> 2)) * g.nbz + (k >> 2);
-  if (b != brick) {
-    brick = b;
-    word = __ldg(g.occ + b);
-  }
-  return (word >> (((i & 3) << 4) | ((j & 3) << 2) | (k & 3))) & 1ull;
-}
 
 struct RaySrc {
   const double* __restrict__ origin;  // (P, 3)
@@ -186,8 +175,6 @@ __device__ int32_t dda_first_hit(const Geom& g, double ox, double oy, double oz,
   int64_t cap = 10 * g.n_cells + 10;
   if ((int64_t)scale > cap) cap = (int64_t)scale;
   int64_t it = 0;
-  int brick = -1;
-  uint64_t bword = 0;
   for (; it < cap; ++it) {
     if (i < 0 || i >= g.nx) {
       const int64_t wj = imod((int64_t)floor(pr_add(oy, pr_mul(dy, t))), g.ny);
@@ -195,9 +182,11 @@ __device__ int32_t dda_first_hit(const Geom& g, double ox, double oy, double oz,
       *steps = it + 1;
       return i < 0 ? g.hot[wj * g.nz + wk] : g.cold[wj * g.nz + wk];
     }
-    if (solid_cell(g, (int)i, jj, kk, brick, bword)) {
+    const int64_t row = i * g.ny + jj;
+    const uint32_t word = __ldg(g.occ + row * g.wpr + (kk >> 5));
+    if ((word >> (kk & 31)) & 1u) {
       *steps = it + 1;
-      return face >= 0 ? __ldg(g.cfp + (((int64_t)i * g.ny + jj) * g.nz + kk) * 6 + face) : -1;
+      return face >= 0 ? __ldg(g.cfp + (row * g.nz + kk) * 6 + face) : -1;
     }
     double tn = tx;
     if (ty < tn) tn = ty;
@@ -361,8 +350,6 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(Geom g, 
   bool active = false;
   double tx = 0, ty = 0, tz = 0, ddx = 0, ddy = 0, ddz = 0, t = 0;
   int i = 0, jj = 0, kk = 0, sx = 0, sy = 0, sz = 0, face = -1, it = 0, cap = 0, q = 0;
-  int brick = -1;
-  uint64_t bword = 0;
   long long my_steps = 0, my_fail = 0;
 
   for (;;) {
@@ -481,8 +468,10 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(Geom g, 
           const int64_t wk = imod((int64_t)floor(pr_add(pool.eoz[lane], pr_mul(pool.edz[lane], t))), g.nz);
           hit = i < 0 ? __ldg(g.hot + wj * g.nz + wk) : __ldg(g.cold + wj * g.nz + wk);
         } else {
-          if (solid_cell(g, i, jj, kk, brick, bword)) {
-            hit = face >= 0 ? __ldg(g.cfp + (((int64_t)i * g.ny + jj) * g.nz + kk) * 6 + face) : -1;
+          const int row = i * g.ny + jj;
+          const uint32_t word = __ldg(g.occ + row * g.wpr + (kk >> 5));
+          if ((word >> (kk & 31)) & 1u) {
+            hit = face >= 0 ? __ldg(g.cfp + ((int64_t)row * g.nz + kk) * 6 + face) : -1;
           } else {
             double tn = tx;
             if (ty < tn) tn = ty;
@@ -704,8 +693,7 @@ static Geom geom_of(const pr_case* c) {
   g.nx = (int32_t)c->nx;
   g.ny = (int32_t)c->ny;
   g.nz = (int32_t)c->nz;
-  g.nby = c->nby;
-  g.nbz = c->nbz;
+  g.wpr = c->wpr;
   g.n_cells = c->n_cells;
   return g;
 }
