@@ -48,6 +48,11 @@ WORKLOADS = {
                         "phi U(0.05,0.20), seeds 0-99, eps U(0.3,0.95), T_mean U(500,900) K with 100 K span, "
                         "250-1000 rays/patch; served = continuous batching, mixed precision",
                requests=16, stream_seed=2026, slots=4, H=0.01),
+    "c3": dict(workload="batched sweep: 48 geometries = OF/FI/FA/TL x phi {0.05,0.10,0.20} x seeds 0-3, N=128^3, "
+                        "500 rays/patch, eps from {0.3,0.6,0.9} and axis from {x,y,z} (RNG seed 3); all first-hit "
+                        "counts in shared persistent traversal launches, operators and mixed-precision solves "
+                        "overlapped on 4 streams",
+               n=128, rays=500, phis=(0.05, 0.10, 0.20), seeds=4, H=0.01, T_m=700.0, dT=20.0, slots=4, pick_seed=3),
     "c5": dict(workload="coupled-size stress: TL and FA N=192^3 phi=0.10, 1000 rays/patch x sets A,B,C, eps 0.6, "
                         "T 690->710 K along x; then 20 solves at T_cell + N(0, 5 K) per voxel (seed 2) on the resident "
                         "operator, FP32+FP64-refinement vs FP64 flux error per solve",
@@ -544,6 +549,89 @@ def run_c4(args, cfg):
     }
 
 
+# --------------------------------------------------------------------------- batched sweep (c3)
+
+def c3_specs(cfg):
+    from porerad_b200.geometry import ARCHETYPES
+
+    rng = np.random.default_rng(cfg["pick_seed"])
+    out = []
+    for arch in ARCHETYPES:
+        for phi in cfg["phis"]:
+            for seed in range(cfg["seeds"]):
+                out.append(dict(arch=arch, n=cfg["n"], phi=phi, seed=seed, axis=str(rng.choice(["x", "y", "z"])),
+                                eps=float(rng.choice([0.3, 0.6, 0.9]))))
+    return out
+
+
+def run_c3(args, cfg):
+    import concurrent.futures
+    import multiprocessing
+
+    specs = c3_specs(cfg)
+    with multiprocessing.get_context("spawn").Pool(min(8, os.cpu_count() or 1)) as pool:
+        phases = pool.map(_c4_geometry, specs)
+    import torch
+
+    from porerad_b200 import _lib, coupled, exchange, view_factors as vf
+    from porerad_b200.geometry import ray_set_seed
+
+    torch.cuda.set_device(0)
+    lib = _lib.load()
+    dev_phases = [torch.from_numpy(ph).cuda() for ph in phases]
+    seeds = [[ray_set_seed(1000 + k, 0)] for k in range(len(specs))]
+    R, H = cfg["rays"], cfg["H"]
+    streams = [torch.cuda.Stream() for _ in range(cfg["slots"])]
+
+    def solve(k, geo, table):
+        with _lib.use_stream(streams[k % len(streams)]):
+            p = vf.SurfacePatches(H_m=H, _device=geo)
+            op = exchange.ExchangeOperator(table, None, None, np.full(geo.n_patches, R, np.int64),
+                                           np.full(geo.n_patches, (H / cfg["n"]) ** 2))
+            ch = coupled.prescribed_field_channels(op, p, cfg["T_m"], cfg["dT"], specs[k]["eps"], precision="mixed")
+            op.close()
+            table.close()
+            return ch
+
+    def sweep():
+        geos = [vf.DeviceGeometry(ph, H) for ph in dev_phases]
+        pats = [vf.SurfacePatches(H_m=H, _device=g) for g in geos]
+        tables = vf.first_hit_counts_batch(pats, R, seeds)
+        torch.cuda.synchronize()
+        with concurrent.futures.ThreadPoolExecutor(cfg["slots"]) as ex:
+            chs = list(ex.map(lambda a: solve(*a), [(k, g, t) for k, (g, t) in enumerate(zip(geos, tables))]))
+        torch.cuda.synchronize()
+        rays = sum(g.n_patches for g in geos) * R
+        patches = [g.n_patches for g in geos]
+        for g in geos:
+            g.close()
+        return rays, chs, patches
+
+    sweep()  # warm-up (autotuning, pools)
+    lib.pr_timers_reset()
+    lib.pr_timers_enable(1)
+    launches0 = lib.pr_kernel_launches()
+    with ClockSampler(0) as clocks:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rays, chs, patches = sweep()
+        dt = time.perf_counter() - t0
+    lib.pr_timers_enable(0)
+    n, ms = _lib.ctypes.c_longlong(), _lib.ctypes.c_double()
+    lib.pr_timers_read(_lib.TIMER_TRACE, _lib.ctypes.byref(n), _lib.ctypes.byref(ms))
+    return {
+        "metric": "first-hit rays/s and cases/s of the 48-case batched sweep (one count pass, overlapped solves)",
+        "value": rays / dt, "unit": "rays/s", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": dt * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (traversal), f32+f64 (radiosity)", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "cases": len(specs), "patches_min": min(patches),
+                   "patches_max": max(patches), "rays": rays},
+        "cases_per_s": len(specs) / dt, "trace_launches": int(n.value), "trace_ms": ms.value,
+        "trace_variant": _lib.trace_variant()[1], "max_closure_rel": max(c.closure_rel for c in chs),
+        "clocks": clocks.summary(), "gpu_launches": int(lib.pr_kernel_launches() - launches0),
+    }
+
+
 # --------------------------------------------------------------------------- coupled-size stress (c5)
 
 def run_c5(args, cfg):
@@ -651,6 +739,8 @@ def main():
     cfg = WORKLOADS[args.workload]
     if args.impl == "reference":
         line = run_reference(args, cfg)
+    elif args.workload == "c3":
+        line = run_c3(args, cfg)
     elif args.workload == "c4":
         line = run_c4(args, cfg)
     elif args.workload == "c5":

@@ -121,6 +121,12 @@ PR_API int pr_trace_first_hit(const pr_case* c, const double* origins, const dou
  * patch reduced into one sorted CSR row.  rays_per_origin = R * n_seeds. */
 PR_API int pr_first_hit_counts(const pr_case* c, int64_t rays_per_patch, const pr_pcg64* seeds,
                         int n_seeds, void* stream, pr_counts** out);
+/* pr_first_hit_counts for n_cases geometries at once (batched sweeps, serving): the rays of
+ * all cases share persistent launches of the traversal, waves of up to 2^27 rays that mix
+ * chunks of cases of different sizes.  seeds holds n_seeds per case (case-major); out
+ * receives one count table per case, each identical to the single-case call's. */
+PR_API int pr_first_hit_counts_batch(const pr_case* const* cases, int n_cases, int64_t rays_per_patch,
+                                     const pr_pcg64* seeds, int n_seeds, void* stream, pr_counts** out);
 /* nnz = pooled (origin, receiver) pairs; rays/steps: rays traced and DDA cells visited. */
 PR_API int pr_counts_info(const pr_counts* k, int64_t* nnz, int64_t* n_patches, int64_t* rays,
                    int64_t* dda_steps);

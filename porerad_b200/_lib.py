@@ -57,6 +57,7 @@ _SIGNATURES = {
     "pr_generate_rays": (_i32, [_vp, _i64, _i64, _i64, _vp, _vp, _vp, _vp]),
     "pr_trace_first_hit": (_i32, [_vp, _vp, _vp, _i64, _vp, ctypes.POINTER(_i64), _vp]),
     "pr_first_hit_counts": (_i32, [_vp, _i64, _vp, _i32, _vp, ctypes.POINTER(_vp)]),
+    "pr_first_hit_counts_batch": (_i32, [_vp, _i32, _i64, _vp, _i32, _vp, _vp]),
     "pr_counts_info": (_i32, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64),
                               ctypes.POINTER(_i64)]),
     "pr_counts_copy": (_i32, [_vp, _vp, _vp, _vp, _vp, _vp]),

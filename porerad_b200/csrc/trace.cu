@@ -275,15 +275,28 @@ struct WarpPool {
   double eoy[32], eoz[32], edy[32], edz[32];  // wall-exit data of each lane's current ray
 };
 
-struct ChunkDesc {
-  int64_t n;        // rays in the chunk = S * np * R
-  int64_t np;       // patches in the chunk
-  int64_t p0;       // first patch
-  int64_t R;        // rays per patch per seed
+// One chunk of a launch: the rays of patches [p0, p0 + np) of one case, numbered seed-major
+// inside the chunk (g = (s * np + p - p0) * R + r) and placed at global ray indices
+// [start, start + n) of the launch, start a multiple of kUnit.  A launch (a wave) may hold
+// chunks of many cases of different sizes.
+struct WaveChunk {
+  const uint32_t* occ;
+  const int32_t* cfp;
+  const int32_t* hot;
+  const int32_t* cold;
+  const double* origin;
+  const int8_t* code;
+  const pr_u128* maps;   // kMapStride maps per seed of this case
+  const pr_u128* state;  // per seed
+  const pr_u128* inc;    // per seed
+  int32_t* recv;         // receivers of this chunk, seed-major
+  int64_t n, np, p0, R, start, n_cells;
+  int32_t nx, ny, nz, wpr;
+  double ny_d, nz_d;
 };
 
 // Ray (origin, direction) of patch p from a positioned stream (view_factors.py:148-181).
-__device__ __forceinline__ void ray_from_stream(const RaySrc& src, pr_u128 st, pr_u128 inc, int64_t p, double& ox,
+__device__ __forceinline__ void ray_from_stream(const WaveChunk& src, pr_u128 st, pr_u128 inc, int64_t p, double& ox,
                                                 double& oy, double& oz, double& dx, double& dy, double& dz) {
   const double u0 = pr_pcg_next_double(&st, inc);
   const double u1 = pr_pcg_next_double(&st, inc);
@@ -328,19 +341,48 @@ __device__ __forceinline__ void ray_from_stream(const RaySrc& src, pr_u128 st, p
   dz = pr_div(dz, len);
 }
 
+__device__ __forceinline__ void flush_chunk_counters(long long& steps, long long& fails,
+                                                     unsigned long long* __restrict__ ctr, int lane) {
+  for (int o = 16; o > 0; o >>= 1) {
+    steps += __shfl_xor_sync(PR_FULL, steps, o);
+    fails += __shfl_xor_sync(PR_FULL, fails, o);
+  }
+  if (lane == 0) {
+    if (steps) atomicAdd(ctr, (unsigned long long)steps);
+    if (fails) atomicAdd(ctr + 1, (unsigned long long)fails);
+  }
+  steps = 0;
+  fails = 0;
+}
+
+// chunk holding global ray index u (chunks sorted by start)
+__device__ __forceinline__ int find_chunk(const WaveChunk* __restrict__ chunks, int n_chunks, int64_t u) {
+  int lo = 0, hi = n_chunks - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (chunks[mid].start <= u) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// The pooled traversal over a table of chunks.  A warp works on one chunk at a time: when
+// its next work unit belongs to another chunk it stops generating, drains its lanes and
+// pool, flushes the chunk's step/failure counters (chunk_ctr[2 c], [2 c + 1]) and switches.
 template <int kMinBlocks, int kBurst>
-__global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(Geom g, RaySrc src, ChunkDesc cd,
-                                                                        int32_t* __restrict__ recv,
-                                                                        unsigned long long* __restrict__ counters) {
+__global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const WaveChunk* __restrict__ chunks,
+                                                                        int n_chunks, int64_t total,
+                                                                        unsigned long long* __restrict__ work,
+                                                                        unsigned long long* __restrict__ chunk_ctr) {
   __shared__ WarpPool pools[kWarps];
   WarpPool& pool = pools[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
-  const int64_t npR = cd.np * cd.R;
-  const uint64_t base_draw = (uint64_t)cd.p0 * (uint64_t)cd.R;  // ray index of the chunk's first ray in a stream
-  const int cap_all = (int)min((int64_t)INT32_MAX, 10 * g.n_cells + 10);
 
-  int64_t unit_next = 0, unit_end = 0;  // warp-uniform
+  int64_t unit_next = 0, unit_end = 0;  // warp-uniform: the work unit being generated
+  int unit_chunk = -1, cur = -1;        // warp-uniform: its chunk, and the chunk of the rays in flight
+  const uint32_t* occ = nullptr;        // warp-uniform geometry of chunk cur
+  int nx = 0, ny = 0, nz = 0, wpr = 0;
   int head = 0, tail = 0;               // warp-uniform pool cursors
   bool more = true;                     // warp-uniform
   pr_u128 base_st{0, 0};
@@ -353,31 +395,46 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(Geom g, 
   long long my_steps = 0, my_fail = 0;
 
   for (;;) {
+    // ---- switch to the chunk of the pending unit once nothing of the previous one is in flight
+    if (unit_chunk != cur && unit_next < unit_end && head == tail && !__any_sync(PR_FULL, active)) {
+      if (cur >= 0) flush_chunk_counters(my_steps, my_fail, chunk_ctr + 2 * cur, lane);
+      cur = unit_chunk;
+      occ = chunks[cur].occ;
+      nx = chunks[cur].nx;
+      ny = chunks[cur].ny;
+      nz = chunks[cur].nz;
+      wpr = chunks[cur].wpr;
+      base_s = -1;
+    }
     // ---- generate one batch of 32 rays when the pool has room for it
     if (more && tail - head <= kPool - 32) {
       if (unit_next >= unit_end) {
         unsigned long long u = 0;
-        if (lane == 0) u = atomicAdd(counters + 2, (unsigned long long)kUnit);
+        if (lane == 0) u = atomicAdd(work, (unsigned long long)kUnit);
         u = __shfl_sync(PR_FULL, u, 0);
-        if ((int64_t)u >= cd.n) {
+        if ((int64_t)u >= total) {
           more = false;
         } else {
+          unit_chunk = find_chunk(chunks, n_chunks, (int64_t)u);
           unit_next = (int64_t)u;
-          unit_end = min((int64_t)u + kUnit, cd.n);
+          unit_end = min((int64_t)u + kUnit, chunks[unit_chunk].start + chunks[unit_chunk].n);
         }
       }
-      if (more) {
-        const int64_t g0 = unit_next;
-        const int cnt = (int)min((int64_t)32, unit_end - g0);
+      if (more && unit_chunk == cur && unit_next < unit_end) {
+        const WaveChunk& C = chunks[cur];
+        const int64_t npR = C.np * C.R;
+        const uint64_t base_draw = (uint64_t)C.p0 * (uint64_t)C.R;  // stream ray index of the chunk's first ray
+        const int64_t g0 = unit_next - C.start;                      // chunk-local index of the batch
+        const int cnt = (int)min((int64_t)32, unit_end - unit_next);
         unit_next += cnt;
         // batch base stream (warp-uniform)
         const int s0 = (int)(g0 / npR);
         const uint64_t m0 = (base_draw + (uint64_t)(g0 - (int64_t)s0 * npR)) * 4u;
-        const pr_u128* maps0 = src.maps + (int64_t)s0 * kMapStride;
+        const pr_u128* maps0 = C.maps + (int64_t)s0 * kMapStride;
         if (base_s == s0 && m0 == base_m + 128u) {
           base_st = pr_u128_affine(maps0[kMapBatch], maps0[kMapBatch + 1], base_st);
         } else {
-          base_st = pr_pcg_jump(src.state[s0], m0, maps0);
+          base_st = pr_pcg_jump(C.state[s0], m0, maps0);
         }
         base_s = s0;
         base_m = m0;
@@ -385,16 +442,16 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(Geom g, 
           const int64_t gq = g0 + lane;
           const int sq = (int)(gq / npR);
           const int64_t rem = gq - (int64_t)sq * npR;
-          const int64_t p = cd.p0 + rem / cd.R;
+          const int64_t p = C.p0 + rem / C.R;
           pr_u128 st;
           if (sq == s0) {
             st = pr_u128_affine(maps0[kMapSmall + 2 * lane], maps0[kMapSmall + 2 * lane + 1], base_st);
           } else {
-            const pr_u128* mq = src.maps + (int64_t)sq * kMapStride;
-            st = pr_pcg_jump(src.state[sq], (base_draw + (uint64_t)rem) * 4u, mq);
+            const pr_u128* mq = C.maps + (int64_t)sq * kMapStride;
+            st = pr_pcg_jump(C.state[sq], (base_draw + (uint64_t)rem) * 4u, mq);
           }
           double ox, oy, oz, dx, dy, dz;
-          ray_from_stream(src, st, src.inc[sq], p, ox, oy, oz, dx, dy, dz);
+          ray_from_stream(C, st, C.inc[sq], p, ox, oy, oz, dx, dy, dz);
           // DDA setup (view_factors.py:213-224)
           const int slot = (tail + lane) & (kPool - 1);
           int c = 0, si = 0, sj = 0, sk = 0, ci = 0, cj = 0, ck = 0;
@@ -404,13 +461,13 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(Geom g, 
             axis_setup(ox, dx, i0, si, a, da);
             axis_setup(oy, dy, j0, sj, b, db);
             axis_setup(oz, dz, k0, sk, e, de);
-            ci = (int)max((int64_t)-1, min(i0, (int64_t)g.nx));
-            cj = (int)imod(j0, g.ny);
-            ck = (int)imod(k0, g.nz);
-            double scale = pr_add(pr_mul(pr_mul(8.0, (double)g.nx),
+            ci = (int)max((int64_t)-1, min(i0, (int64_t)nx));
+            cj = (int)imod(j0, ny);
+            ck = (int)imod(k0, nz);
+            double scale = pr_add(pr_mul(pr_mul(8.0, (double)nx),
                                          pr_add(1.0, pr_div(pr_add(fabs(dy), fabs(dz)), fabs(dx)))), 100.0);
             if (scale > 100000000.0) scale = 100000000.0;
-            c = cap_all;
+            c = (int)min((int64_t)INT32_MAX, 10 * C.n_cells + 10);
             if ((int64_t)scale > (int64_t)c) c = (int)scale;
           }
           pool.tx[slot] = a; pool.ty[slot] = b; pool.tz[slot] = e;
@@ -463,15 +520,15 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(Geom g, 
         hit = -1;
       } else {
         ++it;
-        if ((unsigned)i >= (unsigned)g.nx) {
-          const int64_t wj = imod((int64_t)floor(pr_add(pool.eoy[lane], pr_mul(pool.edy[lane], t))), g.ny);
-          const int64_t wk = imod((int64_t)floor(pr_add(pool.eoz[lane], pr_mul(pool.edz[lane], t))), g.nz);
-          hit = i < 0 ? __ldg(g.hot + wj * g.nz + wk) : __ldg(g.cold + wj * g.nz + wk);
+        if ((unsigned)i >= (unsigned)nx) {
+          const int64_t wj = imod((int64_t)floor(pr_add(pool.eoy[lane], pr_mul(pool.edy[lane], t))), ny);
+          const int64_t wk = imod((int64_t)floor(pr_add(pool.eoz[lane], pr_mul(pool.edz[lane], t))), nz);
+          hit = i < 0 ? __ldg(chunks[cur].hot + wj * nz + wk) : __ldg(chunks[cur].cold + wj * nz + wk);
         } else {
-          const int row = i * g.ny + jj;
-          const uint32_t word = __ldg(g.occ + row * g.wpr + (kk >> 5));
+          const int row = i * ny + jj;
+          const uint32_t word = __ldg(occ + row * wpr + (kk >> 5));
           if ((word >> (kk & 31)) & 1u) {
-            hit = face >= 0 ? __ldg(g.cfp + ((int64_t)row * g.nz + kk) * 6 + face) : -1;
+            hit = face >= 0 ? __ldg(chunks[cur].cfp + ((int64_t)row * nz + kk) * 6 + face) : -1;
           } else {
             double tn = tx;
             if (ty < tn) tn = ty;
@@ -486,13 +543,13 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(Geom g, 
             }
             if (cy) {
               jj += sy;
-              jj = jj == g.ny ? 0 : (jj < 0 ? g.ny - 1 : jj);
+              jj = jj == ny ? 0 : (jj < 0 ? ny - 1 : jj);
               ty = pr_add(ty, ddy);
               if (!cx) face = sy > 0 ? 3 : 2;
             }
             if (cz) {
               kk += sz;
-              kk = kk == g.nz ? 0 : (kk < 0 ? g.nz - 1 : kk);
+              kk = kk == nz ? 0 : (kk < 0 ? nz - 1 : kk);
               tz = pr_add(tz, ddz);
               if (!cx && !cy) face = sz > 0 ? 5 : 4;
             }
@@ -501,29 +558,48 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(Geom g, 
         }
       }
       if (hit != -2) {
-        recv[q] = hit;
+        chunks[cur].recv[q] = hit;
         my_steps += it;
         my_fail += hit < 0;
         active = false;
       }
     }
   }
-  block_add_i64(my_steps, counters + 0);
-  block_add_i64(my_fail, counters + 1);
+  if (cur >= 0) flush_chunk_counters(my_steps, my_fail, chunk_ctr + 2 * cur, lane);
 }
 
 // Per origin patch: gather its L = S * R receivers (seed-major chunk layout), sort them
 // in shared memory (bitonic), run-length encode into (receiver, count) pairs at
 // out[(p - p0) * L ...], nnz[p - p0].
-__global__ void __launch_bounds__(512) k_patch_rle(const int32_t* __restrict__ recv, int64_t np, int L, int R,
-                                                   int Lpad, int32_t* __restrict__ out_col,
-                                                   int32_t* __restrict__ out_cnt, int32_t* __restrict__ nnz) {
+struct RleChunk {
+  const int32_t* recv;  // receivers of the chunk (seed-major)
+  int64_t np;           // patches
+  int64_t patch0;       // index of its first patch among the wave's patches
+  int64_t ray0;         // offset of its rays (and stage entries) in the wave's buffers
+};
+
+__global__ void __launch_bounds__(512) k_patch_rle(const RleChunk* __restrict__ rc, int n_chunks,
+                                                   int64_t total_patches, int L, int R, int Lpad,
+                                                   int32_t* __restrict__ st_col, int32_t* __restrict__ st_cnt,
+                                                   int32_t* __restrict__ nnz) {
   extern __shared__ int32_t sm[];
   int32_t* key = sm;          // Lpad
   int32_t* head = sm + Lpad;  // Lpad (positions of run heads)
   __shared__ int32_t warp_tot[16];
   const int tid = threadIdx.x, nt = blockDim.x;
-  for (int64_t p = blockIdx.x; p < np; p += gridDim.x) {
+  for (int64_t gp = blockIdx.x; gp < total_patches; gp += gridDim.x) {
+    int c = 0;
+    {
+      int lo = 0, hi = n_chunks - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (rc[mid].patch0 <= gp) lo = mid;
+        else hi = mid - 1;
+      }
+      c = lo;
+    }
+    const int64_t p = gp - rc[c].patch0, np = rc[c].np;
+    const int32_t* recv = rc[c].recv;
     for (int i = tid; i < Lpad; i += nt) {
       if (i < L) {
         const int sd = i / R;
@@ -570,15 +646,15 @@ __global__ void __launch_bounds__(512) k_patch_rle(const int32_t* __restrict__ r
     for (int i = lo; i < hi; ++i)
       if (i == 0 || key[i] != key[i - 1]) head[u++] = i;
     __syncthreads();
-    int32_t* oc = out_col + p * L;
-    int32_t* on = out_cnt + p * L;
+    int32_t* oc = st_col + rc[c].ray0 + p * L;
+    int32_t* on = st_cnt + rc[c].ray0 + p * L;
     for (int v = tid; v < total; v += nt) {
       const int h = head[v];
       const int e = v + 1 < total ? head[v + 1] : L;
       oc[v] = key[h];
       on[v] = e - h;
     }
-    if (tid == 0) nnz[p] = total;
+    if (tid == 0) nnz[gp] = total;
     __syncthreads();
   }
 }
@@ -715,7 +791,7 @@ static int trace_grid() { return sm_count() * 8; }
 // Variants of the pooled traversal (minimum resident blocks per SM x DDA steps per burst).
 // Every variant writes the same receivers; the autotuner below picks the fastest per
 // problem class by timing them on the first chunk of the first call.
-using TraceKernel = void (*)(Geom, RaySrc, ChunkDesc, int32_t*, unsigned long long*);
+using TraceKernel = void (*)(const WaveChunk*, int, int64_t, unsigned long long*, unsigned long long*);
 struct TraceVariant {
   TraceKernel kernel;
   const char* name;
@@ -742,9 +818,9 @@ static int variant_grid(int v) {
 }
 
 struct TuneKey {
-  int64_t nx, ny, nz, L;
+  int64_t nx, ny, nz, L, cases;
   bool operator<(const TuneKey& o) const {
-    return std::tie(nx, ny, nz, L) < std::tie(o.nx, o.ny, o.nz, o.L);
+    return std::tie(nx, ny, nz, L, cases) < std::tie(o.nx, o.ny, o.nz, o.L, o.cases);
   }
 };
 static std::mutex g_tune_mu;
@@ -777,19 +853,25 @@ PR_API int pr_trace_variant_info(int* count, int* last, const char** name) {
 
 namespace pr {
 
-static int launch_variant(int v, const pr_case* c, const RaySrc& src, const ChunkDesc& cd, int32_t* recv,
-                          unsigned long long* ctr, cudaStream_t s) {
-  PR_CUDA(cudaMemsetAsync(ctr + 2, 0, sizeof(unsigned long long), s));
-  ::pr::launch_mark(), kVariants[v].kernel<<<variant_grid(v), kWarps * 32, 0, s>>>(geom_of(c), src, cd, recv, ctr);
+struct WaveLaunch {
+  const WaveChunk* chunks;  // device table
+  int n_chunks;
+  int64_t total;            // global ray indices [0, total)
+  unsigned long long* work; // work-unit counter
+  unsigned long long* ctr;  // 2 per chunk: DDA steps, failed rays
+};
+
+static int launch_variant(int v, const WaveLaunch& w, cudaStream_t s) {
+  PR_CUDA(cudaMemsetAsync(w.work, 0, sizeof(unsigned long long), s));
+  ::pr::launch_mark(), kVariants[v].kernel<<<variant_grid(v), kWarps * 32, 0, s>>>(w.chunks, w.n_chunks, w.total,
+                                                                                  w.work, w.ctr);
   PR_CUDA(cudaGetLastError());
   return PR_OK;
 }
 
-// Variant for this problem class: forced, cached, or measured now on the given chunk
-// (each variant traces it once, timed with events; the counters are restored after).
-static int choose_variant(const pr_case* c, int64_t L, const RaySrc& src, const ChunkDesc& cd, int32_t* recv,
-                          unsigned long long* ctr, cudaStream_t s, int* out) {
-  const TuneKey key{c->nx, c->ny, c->nz, L};
+// Variant for this problem class: forced, cached, or measured now on the given wave (each
+// variant traces it once, timed with events; the per-chunk counters are cleared after).
+static int choose_variant(const TuneKey& key, const WaveLaunch& w, cudaStream_t s, int* out) {
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     if (g_forced_variant >= 0) {
@@ -802,8 +884,6 @@ static int choose_variant(const pr_case* c, int64_t L, const RaySrc& src, const 
       return PR_OK;
     }
   }
-  unsigned long long saved[2];
-  PR_CUDA(cudaMemcpyAsync(saved, ctr, sizeof(saved), cudaMemcpyDeviceToHost, s));
   cudaEvent_t e0, e1;
   PR_CUDA(cudaEventCreate(&e0));
   PR_CUDA(cudaEventCreate(&e1));
@@ -811,7 +891,7 @@ static int choose_variant(const pr_case* c, int64_t L, const RaySrc& src, const 
   int best_v = 0;
   for (int v = 0; v < kNumVariants; ++v) {
     PR_CUDA(cudaEventRecord(e0, s));
-    PR_TRY(launch_variant(v, c, src, cd, recv, ctr, s));
+    PR_TRY(launch_variant(v, w, s));
     PR_CUDA(cudaEventRecord(e1, s));
     PR_CUDA(cudaEventSynchronize(e1));
     float ms = 0.f;
@@ -823,8 +903,7 @@ static int choose_variant(const pr_case* c, int64_t L, const RaySrc& src, const 
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  PR_CUDA(cudaMemcpyAsync(ctr, saved, sizeof(saved), cudaMemcpyHostToDevice, s));
-  PR_CUDA(cudaStreamSynchronize(s));
+  PR_CUDA(cudaMemsetAsync(w.ctr, 0, 2 * sizeof(unsigned long long) * w.n_chunks, s));
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tuned[key] = best_v;
@@ -899,7 +978,28 @@ static int enable_rle_smem() {
   return PR_OK;
 }
 
-int first_hit_counts(const pr_case* c, int64_t R, const pr_pcg64* seeds, int S, cudaStream_t s, pr_counts** out) {
+// Rays of one launch (a wave): chunks of one or more cases are packed until this bound.
+static const int64_t kWaveRays = (int64_t)1 << 27;
+// Patches per chunk: a chunk holds at most 2^26 rays.
+static const int64_t kChunkRays = (int64_t)1 << 26;
+
+// Per-case accumulation of a batched count pass.
+struct CaseCounts {
+  std::unique_ptr<pr_counts> k;
+  DevBuf<int64_t> nnz_all;  // row lengths
+  struct Piece {
+    DevBuf<int32_t> col, cnt;
+    int64_t n = 0;
+  };
+  std::vector<Piece> pieces;  // compacted chunks in patch order
+};
+
+// first_hit_counts for n_cases geometries at once (view_factors.py:273-300 per case): every
+// case traces rays_per_patch rays per patch for each of its S seeds (seeds[c * S + s]);
+// chunks of all cases share persistent launches of the pooled traversal.
+int counts_batch(const pr_case* const* cases, int nc, int64_t R, const pr_pcg64* seeds, int S, cudaStream_t s,
+                 pr_counts** out) {
+  PR_ARG(nc > 0, "no cases");
   PR_ARG(R > 0 && S > 0, "rays_per_patch and the number of seeds must be positive");
   const int64_t L64 = R * S;
   if (L64 > kMaxSegment) {
@@ -910,125 +1010,224 @@ int first_hit_counts(const pr_case* c, int64_t R, const pr_pcg64* seeds, int S, 
   int Lpad = 1;
   while (Lpad < L) Lpad <<= 1;
   if (Lpad < 64) Lpad = 64;
-  const int64_t P = c->n_patches;
+  int dev0 = 0;
+  cudaGetDevice(&dev0);
 
-  SeedTables t;
-  PR_TRY(t.build(seeds, S, s));
-  std::unique_ptr<pr_counts> k(new pr_counts());
-  cudaGetDevice(&k->device);
-  k->csr = std::make_shared<CountCsr>();
-  CountCsr& csr = *k->csr;
-  csr.n_rows = P;
-  PR_TRY(csr.row_ptr.alloc(P + 1, s));
-  PR_TRY(k->rays.alloc(P, s));
-  ::pr::launch_mark(), k_fill_i64<<<grid_for(P, 256), 256, 0, s>>>(k->rays.ptr, P, L64);
-  PR_CUDA(cudaGetLastError());
-  if (P == 0) {
-    PR_CUDA(cudaMemsetAsync(csr.row_ptr.ptr, 0, sizeof(int64_t), s));
-    PR_CUDA(cudaStreamSynchronize(s));
-    *out = k.release();
-    return PR_OK;
+  // seed tables and per-case outputs
+  std::vector<SeedTables> tables(nc);
+  std::vector<CaseCounts> cc(nc);
+  for (int c = 0; c < nc; ++c) {
+    PR_ARG(cases[c] != nullptr, "case %d is NULL", c);
+    PR_ARG(cases[c]->device == dev0, "case %d lives on another device", c);
+    PR_TRY(tables[c].build(seeds + (size_t)c * S, S, s));
+    const int64_t P = cases[c]->n_patches;
+    cc[c].k.reset(new pr_counts());
+    cc[c].k->device = dev0;
+    cc[c].k->csr = std::make_shared<CountCsr>();
+    cc[c].k->csr->n_rows = P;
+    PR_TRY(cc[c].k->csr->row_ptr.alloc(P + 1, s));
+    PR_TRY(cc[c].k->rays.alloc(P > 0 ? P : 1, s));
+    PR_TRY(cc[c].nnz_all.alloc(P > 0 ? P : 1, s));
+    if (P > 0) {
+      ::pr::launch_mark(), k_fill_i64<<<grid_for(P, 256), 256, 0, s>>>(cc[c].k->rays.ptr, P, L64);
+      PR_CUDA(cudaGetLastError());
+    }
   }
 
-  // Patch chunks of about 2^26 rays bound the receiver and stage buffers.
-  int64_t chunk = ((int64_t)1 << 26) / L64;
-  if (chunk < 1) chunk = 1;
-  if (chunk > P) chunk = P;
+  // chunks: (case, first patch, patches)
+  struct Chunk {
+    int c;
+    int64_t p0, np;
+  };
+  std::vector<Chunk> chunks;
+  const int64_t chunk_patches = std::max<int64_t>(1, kChunkRays / L64);
+  for (int c = 0; c < nc; ++c)
+    for (int64_t p0 = 0; p0 < cases[c]->n_patches; p0 += chunk_patches)
+      chunks.push_back({c, p0, std::min(chunk_patches, cases[c]->n_patches - p0)});
+
+  // wave buffers
+  int64_t wave_cap = 0;
+  for (const Chunk& ch : chunks) wave_cap = std::max(wave_cap, ch.np * L64);
+  wave_cap = std::max(wave_cap, std::min<int64_t>(kWaveRays, [&] {
+                        int64_t t = 0;
+                        for (const Chunk& ch : chunks) t += ch.np * L64;
+                        return t;
+                      }()));
   DevBuf<int32_t> recv, st_col, st_cnt, nnz;
   DevBuf<int64_t> off;
-  DevBuf<unsigned long long> ctr;
-  PR_TRY(recv.alloc(chunk * L64, s));
-  PR_TRY(st_col.alloc(chunk * L64, s));
-  PR_TRY(st_cnt.alloc(chunk * L64, s));
-  PR_TRY(nnz.alloc(chunk, s));
-  PR_TRY(off.alloc(chunk + 1, s));
-  PR_TRY(ctr.alloc(3, s));
+  DevBuf<unsigned long long> work, ctr;
+  DevBuf<WaveChunk> dchunks;
+  DevBuf<RleChunk> drle;
+  const int64_t max_wave_patches = wave_cap / L64 + (int64_t)chunks.size();
+  PR_TRY(recv.alloc(wave_cap, s));
+  PR_TRY(st_col.alloc(wave_cap, s));
+  PR_TRY(st_cnt.alloc(wave_cap, s));
+  PR_TRY(nnz.alloc(max_wave_patches, s));
+  PR_TRY(off.alloc(max_wave_patches + 1, s));
+  PR_TRY(work.alloc(1, s));
+  PR_TRY(ctr.alloc(2 * chunks.size(), s));
+  PR_TRY(dchunks.alloc(chunks.size(), s));
+  PR_TRY(drle.alloc(chunks.size(), s));
   PR_CUDA(cudaMemsetAsync(ctr.ptr, 0, ctr.bytes(), s));
+  PR_TRY(enable_rle_smem());
+  const size_t smem = (size_t)2 * Lpad * sizeof(int32_t);
+  const int rle_threads = Lpad >= 1024 ? 512 : (Lpad >= 256 ? 256 : 64);
   size_t scan_bytes = 0;
-  PR_CUDA(cub::DeviceScan::InclusiveSum(nullptr, scan_bytes, off.ptr, off.ptr + 1, chunk, s));
+  PR_CUDA(cub::DeviceScan::InclusiveSum(nullptr, scan_bytes, off.ptr, off.ptr + 1, max_wave_patches, s));
   DevBuf<uint8_t> scan_tmp;
   PR_TRY(scan_tmp.alloc(scan_bytes + 16, s));
-  const size_t smem = (size_t)2 * Lpad * sizeof(int32_t);
-  PR_TRY(enable_rle_smem());
-  const int rle_threads = Lpad >= 1024 ? 512 : (Lpad >= 256 ? 256 : 64);
 
-  // per-chunk compacted pieces; concatenated once the total is known
-  struct Piece {
-    DevBuf<int32_t> col, cnt;
-    int64_t n;
-  };
-  std::vector<Piece> pieces;
-  DevBuf<int64_t> nnz_all;  // row lengths of every patch
-  PR_TRY(nnz_all.alloc(P, s));
-  int64_t total = 0;
   int variant = 0;
-  PR_CUDA(cudaMemsetAsync(off.ptr, 0, sizeof(int64_t), s));
-  for (int64_t p0 = 0; p0 < P; p0 += chunk) {
-    const int64_t np = std::min(chunk, P - p0);
-    const int64_t nr = np * L64;
-    ChunkDesc cd{nr, np, p0, R};
-    const RaySrc src = src_of(c, t);
-    if (p0 == 0) PR_TRY(choose_variant(c, L64, src, cd, recv.ptr, ctr.ptr, s, &variant));
+  bool tuned = false;
+  std::vector<WaveChunk> hw;
+  std::vector<RleChunk> hr;
+  std::vector<int64_t> totals;
+  for (size_t w0 = 0; w0 < chunks.size();) {
+    // pack a wave
+    size_t w1 = w0;
+    int64_t rays = 0;
+    while (w1 < chunks.size() && (w1 == w0 || rays + chunks[w1].np * L64 <= wave_cap)) rays += chunks[w1++].np * L64;
+    const int nw = (int)(w1 - w0);
+    hw.assign(nw, WaveChunk{});
+    hr.assign(nw, RleChunk{});
+    int64_t start = 0, ray0 = 0, patch0 = 0;
+    for (int k = 0; k < nw; ++k) {
+      const Chunk& ch = chunks[w0 + k];
+      const pr_case* c = cases[ch.c];
+      WaveChunk& W = hw[k];
+      W.occ = c->occ.ptr;
+      W.cfp = c->cfp.ptr;
+      W.hot = c->hot.ptr;
+      W.cold = c->cold.ptr;
+      W.origin = c->origin.ptr;
+      W.code = c->code.ptr;
+      W.maps = tables[ch.c].maps.ptr;
+      W.state = tables[ch.c].state.ptr;
+      W.inc = tables[ch.c].inc.ptr;
+      W.recv = recv.ptr + ray0;
+      W.n = ch.np * L64;
+      W.np = ch.np;
+      W.p0 = ch.p0;
+      W.R = R;
+      W.start = start;
+      W.n_cells = c->n_cells;
+      W.nx = (int32_t)c->nx;
+      W.ny = (int32_t)c->ny;
+      W.nz = (int32_t)c->nz;
+      W.wpr = c->wpr;
+      W.ny_d = (double)c->ny;
+      W.nz_d = (double)c->nz;
+      hr[k] = RleChunk{recv.ptr + ray0, ch.np, patch0, ray0};
+      start += (W.n + kUnit - 1) / kUnit * kUnit;
+      ray0 += W.n;
+      patch0 += ch.np;
+    }
+    const int64_t total = hw[nw - 1].start + hw[nw - 1].n;
+    PR_CUDA(cudaMemcpyAsync(dchunks.ptr, hw.data(), nw * sizeof(WaveChunk), cudaMemcpyHostToDevice, s));
+    PR_CUDA(cudaMemcpyAsync(drle.ptr, hr.data(), nw * sizeof(RleChunk), cudaMemcpyHostToDevice, s));
+    unsigned long long* wave_ctr = ctr.ptr + 2 * w0;
+    WaveLaunch wl{dchunks.ptr, nw, total, work.ptr, wave_ctr};
+    if (!tuned) {
+      const pr_case* c0 = cases[chunks[w0].c];
+      PR_TRY(choose_variant(TuneKey{c0->nx, c0->ny, c0->nz, L64, nc}, wl, s, &variant));
+      tuned = true;
+    }
     ::pr::timer_begin(kTimerTrace, s);
-    PR_TRY(launch_variant(variant, c, src, cd, recv.ptr, ctr.ptr, s));
+    PR_TRY(launch_variant(variant, wl, s));
     ::pr::timer_end(kTimerTrace, s);
-    const int rle_grid = (int)std::min<int64_t>(np, (int64_t)sm_count() * 16);
+    const int rle_grid = (int)std::min<int64_t>(patch0, (int64_t)sm_count() * 16);
     ::pr::timer_begin(kTimerRle, s);
-    ::pr::launch_mark(), k_patch_rle<<<rle_grid, rle_threads, smem, s>>>(recv.ptr, np, L, (int)R, Lpad, st_col.ptr, st_cnt.ptr,
-                                                                     nnz.ptr);
+    ::pr::launch_mark(), k_patch_rle<<<rle_grid, rle_threads, smem, s>>>(drle.ptr, nw, patch0, L, (int)R, Lpad,
+                                                                     st_col.ptr, st_cnt.ptr, nnz.ptr);
     ::pr::timer_end(kTimerRle, s);
     PR_CUDA(cudaGetLastError());
-    ::pr::launch_mark(), k_i32_to_i64<<<grid_for(np, 256), 256, 0, s>>>(nnz.ptr, nnz_all.ptr + p0, np);
-    PR_CUDA(cudaGetLastError());
-    PR_CUDA(cub::DeviceScan::InclusiveSum(scan_tmp.ptr, scan_bytes, nnz_all.ptr + p0, off.ptr + 1, np, s));
-    int64_t chunk_total = 0;
-    PR_CUDA(cudaMemcpyAsync(&chunk_total, off.ptr + np, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    PR_CUDA(cudaStreamSynchronize(s));
-    Piece pc;
-    pc.n = chunk_total;
-    PR_TRY(pc.col.alloc(chunk_total, s));
-    PR_TRY(pc.cnt.alloc(chunk_total, s));
-    ::pr::launch_mark(), k_compact_rows<<<grid_for(np * 32, 256), 256, 0, s>>>(st_col.ptr, st_cnt.ptr, nnz.ptr, off.ptr, np, L, 0,
-                                                          pc.col.ptr, pc.cnt.ptr);
-    PR_CUDA(cudaGetLastError());
-    total += chunk_total;
-    pieces.push_back(std::move(pc));
-  }
-  csr.nnz = total;
-  PR_TRY(csr.col.alloc(total, s));
-  PR_TRY(csr.cnt.alloc(total, s));
-  int64_t at = 0;
-  for (auto& pc : pieces) {
-    if (pc.n) {
-      PR_CUDA(cudaMemcpyAsync(csr.col.ptr + at, pc.col.ptr, pc.n * 4, cudaMemcpyDeviceToDevice, s));
-      PR_CUDA(cudaMemcpyAsync(csr.cnt.ptr + at, pc.cnt.ptr, pc.n * 4, cudaMemcpyDeviceToDevice, s));
+    // per chunk: row lengths into the case, exclusive offsets for the compaction
+    totals.assign(nw, 0);
+    for (int k = 0; k < nw; ++k) {
+      const Chunk& ch = chunks[w0 + k];
+      const RleChunk& rc = hr[k];
+      ::pr::launch_mark(), k_i32_to_i64<<<grid_for(ch.np, 256), 256, 0, s>>>(nnz.ptr + rc.patch0,
+                                                                            cc[ch.c].nnz_all.ptr + ch.p0, ch.np);
+      PR_CUDA(cudaGetLastError());
+      int64_t* o = off.ptr + rc.patch0 + k;  // np + 1 slots per chunk
+      PR_CUDA(cudaMemsetAsync(o, 0, sizeof(int64_t), s));
+      PR_CUDA(cub::DeviceScan::InclusiveSum(scan_tmp.ptr, scan_bytes, cc[ch.c].nnz_all.ptr + ch.p0, o + 1, ch.np, s));
+      PR_CUDA(cudaMemcpyAsync(&totals[k], o + ch.np, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     }
-    at += pc.n;
+    PR_CUDA(cudaStreamSynchronize(s));
+    for (int k = 0; k < nw; ++k) {
+      const Chunk& ch = chunks[w0 + k];
+      const RleChunk& rc = hr[k];
+      CaseCounts::Piece pc;
+      pc.n = totals[k];
+      PR_TRY(pc.col.alloc(pc.n > 0 ? pc.n : 1, s));
+      PR_TRY(pc.cnt.alloc(pc.n > 0 ? pc.n : 1, s));
+      ::pr::launch_mark(), k_compact_rows<<<grid_for(ch.np * 32, 256), 256, 0, s>>>(
+          st_col.ptr + rc.ray0, st_cnt.ptr + rc.ray0, nnz.ptr + rc.patch0, off.ptr + rc.patch0 + k, ch.np, L, 0,
+          pc.col.ptr, pc.cnt.ptr);
+      PR_CUDA(cudaGetLastError());
+      cc[ch.c].pieces.push_back(std::move(pc));
+    }
+    // the compactions read the stage buffers: finish them before the next wave reuses them
+    PR_CUDA(cudaStreamSynchronize(s));
+    w0 = w1;
   }
-  {
-    size_t b = 0;
-    PR_CUDA(cub::DeviceScan::InclusiveSum(nullptr, b, nnz_all.ptr, csr.row_ptr.ptr + 1, P, s));
-    DevBuf<uint8_t> tmp;
-    PR_TRY(tmp.alloc(b + 16, s));
+
+  // per case: concatenate the pieces, row offsets, counters
+  std::vector<unsigned long long> hctr(2 * chunks.size());
+  PR_CUDA(cudaMemcpyAsync(hctr.data(), ctr.ptr, ctr.bytes(), cudaMemcpyDeviceToHost, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  int64_t failed = 0;
+  std::vector<int64_t> steps(nc, 0), fails(nc, 0);
+  for (size_t k = 0; k < chunks.size(); ++k) {
+    steps[chunks[k].c] += (int64_t)hctr[2 * k];
+    fails[chunks[k].c] += (int64_t)hctr[2 * k + 1];
+  }
+  for (int c = 0; c < nc; ++c) {
+    CountCsr& csr = *cc[c].k->csr;
+    const int64_t P = csr.n_rows;
+    int64_t total = 0;
+    for (auto& pc : cc[c].pieces) total += pc.n;
+    csr.nnz = total;
+    PR_TRY(csr.col.alloc(total > 0 ? total : 1, s));
+    PR_TRY(csr.cnt.alloc(total > 0 ? total : 1, s));
+    int64_t at = 0;
+    for (auto& pc : cc[c].pieces) {
+      if (pc.n) {
+        PR_CUDA(cudaMemcpyAsync(csr.col.ptr + at, pc.col.ptr, pc.n * 4, cudaMemcpyDeviceToDevice, s));
+        PR_CUDA(cudaMemcpyAsync(csr.cnt.ptr + at, pc.cnt.ptr, pc.n * 4, cudaMemcpyDeviceToDevice, s));
+      }
+      at += pc.n;
+    }
+    cc[c].pieces.clear();
     PR_CUDA(cudaMemsetAsync(csr.row_ptr.ptr, 0, sizeof(int64_t), s));
-    PR_CUDA(cub::DeviceScan::InclusiveSum(tmp.ptr, b, nnz_all.ptr, csr.row_ptr.ptr + 1, P, s));
+    if (P > 0) {
+      size_t b = 0;
+      PR_CUDA(cub::DeviceScan::InclusiveSum(nullptr, b, cc[c].nnz_all.ptr, csr.row_ptr.ptr + 1, P, s));
+      DevBuf<uint8_t> tmp;
+      PR_TRY(tmp.alloc(b + 16, s));
+      PR_CUDA(cub::DeviceScan::InclusiveSum(tmp.ptr, b, cc[c].nnz_all.ptr, csr.row_ptr.ptr + 1, P, s));
+    }
+    cc[c].k->rays_traced = P * L64;
+    cc[c].k->dda_steps = steps[c];
+    cc[c].k->last_stream = s;
+    failed += fails[c];
   }
-  unsigned long long h[2];
-  PR_CUDA(cudaMemcpyAsync(h, ctr.ptr, sizeof(h), cudaMemcpyDeviceToHost, s));
   PR_CUDA(cudaStreamSynchronize(s));
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_last_variant = variant;
   }
-  k->rays_traced = P * L64;
-  k->dda_steps = (int64_t)h[0];
-  k->last_stream = s;
-  if (h[1]) {
-    set_error("%lld rays did not resolve a receiving patch", (long long)h[1]);
+  if (failed) {
+    set_error("%lld rays did not resolve a receiving patch", (long long)failed);
     return PR_ERR_UNRESOLVED;
   }
-  *out = k.release();
+  for (int c = 0; c < nc; ++c) out[c] = cc[c].k.release();
   return PR_OK;
+}
+
+int first_hit_counts(const pr_case* c, int64_t R, const pr_pcg64* seeds, int S, cudaStream_t s, pr_counts** out) {
+  return counts_batch(&c, 1, R, seeds, S, s, out);
 }
 
 }  // namespace pr

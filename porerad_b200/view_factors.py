@@ -285,6 +285,26 @@ def first_hit_counts_pooled(patches, rays_per_patch: int, seeds) -> CountTable:
     return CountTable(out.value)
 
 
+def first_hit_counts_batch(patches_list, rays_per_patch: int, seeds_per_case) -> list[CountTable]:
+    """Pooled counts of many geometries in shared traversal launches (batched sweeps).
+
+    ``seeds_per_case[c]`` lists the seeds of case ``c`` (the same number for every case);
+    each returned table equals ``first_hit_counts_pooled(patches_list[c], R, seeds)``.
+    """
+
+    devs = [_device_of(p) for p in patches_list]
+    seeds = [[int(s) for s in ss] for ss in seeds_per_case]
+    if len(seeds) != len(devs) or len({len(ss) for ss in seeds}) != 1:
+        raise ValueError("one list of seeds per case, all of the same length")
+    arr = _lib.seeds_struct([_lib.pcg64_state(s) for ss in seeds for s in ss])
+    handles = (ctypes.c_void_p * len(devs))(*[d.handle for d in devs])
+    out = (ctypes.c_void_p * len(devs))()
+    _lib.check(_lib.load().pr_first_hit_counts_batch(ctypes.addressof(handles), len(devs), int(rays_per_patch),
+                                                     ctypes.addressof(arr), len(seeds[0]), _lib.stream(),
+                                                     ctypes.addressof(out)))
+    return [CountTable(h) for h in out]
+
+
 def first_hit_counts(patches, rays_per_patch: int, seed: int, *,
                      patch_chunk: int = 16384) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
     """Integer counts (origin, receiver, n) of one seeded ray block, sorted by edge (view_factors.py:273-287).

@@ -351,3 +351,28 @@ def test_every_traversal_variant_gives_the_same_counts():
             assert _lib.trace_variant()[0] == v
     finally:
         _lib.load().pr_trace_set_variant(-1)
+
+
+def test_batched_counts_equal_single_case_counts():
+    """Cases of different shapes and sizes traced in shared launches give each case's own counts."""
+
+    from porerad_b200 import geometry
+
+    vf = _vf()
+    pats, seeds, want = [], [], []
+    for k, name in enumerate(SMALL):
+        case = load_small(name)
+        pats.append(_patches(case))
+        seeds.append([int(s) for s in case["seeds"][:2]])
+    for k, arch in enumerate(geometry.ARCHETYPES):
+        pats.append(vf.build_surface_patches(geometry.make(arch, 24 + 8 * k, 0.15, k), 0.005))
+        seeds.append([1000 + k, 2000 + k])
+    R = 24
+    for p, ss in zip(pats, seeds):
+        t = vf.first_hit_counts_pooled(p, R, ss)
+        want.append((t.sha256(), t.dda_steps))
+        t.close()
+    got = vf.first_hit_counts_batch(pats, R, seeds)
+    for g, (h, st) in zip(got, want):
+        assert g.sha256() == h
+        assert g.dda_steps == st
