@@ -171,9 +171,9 @@ int pr_case_patches(const pr_case* c, uint8_t* solid, int8_t* patch_class, int32
     PR_CUDA(cudaMemcpyAsync(patch_area_m2, a.ptr, P * 8, cudaMemcpyDefault, s));
     PR_CUDA(cudaStreamSynchronize(s));
   }
-  if (cell_face_patch) PR_CUDA(cudaMemcpyAsync(cell_face_patch, c->cfp.ptr, c->n_cells * 24, cudaMemcpyDefault, s));
-  if (hot_wall_patch) PR_CUDA(cudaMemcpyAsync(hot_wall_patch, c->hot.ptr, lat * 4, cudaMemcpyDefault, s));
-  if (cold_wall_patch) PR_CUDA(cudaMemcpyAsync(cold_wall_patch, c->cold.ptr, lat * 4, cudaMemcpyDefault, s));
+  if (cell_face_patch) PR_CUDA(cudaMemcpyAsync(cell_face_patch, c->cfp(), c->n_cells * 24, cudaMemcpyDefault, s));
+  if (hot_wall_patch) PR_CUDA(cudaMemcpyAsync(hot_wall_patch, c->hot(), lat * 4, cudaMemcpyDefault, s));
+  if (cold_wall_patch) PR_CUDA(cudaMemcpyAsync(cold_wall_patch, c->cold(), lat * 4, cudaMemcpyDefault, s));
   PR_CUDA(cudaStreamSynchronize(s));
   return PR_OK;
 }

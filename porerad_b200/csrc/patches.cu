@@ -189,16 +189,14 @@ int case_build(pr_case* c, const uint8_t* phases, cudaStream_t s) {
   PR_TRY(c->code.alloc(P, s));
   PR_TRY(c->cell.alloc(P, s));
   PR_TRY(c->origin.alloc(3 * P, s));
-  PR_TRY(c->cfp.alloc(6 * n, s));
-  PR_TRY(c->hot.alloc(lat, s));
-  PR_TRY(c->cold.alloc(lat, s));
+  PR_TRY(c->ftab.alloc(6 * n + 2 * lat, s));
   ::pr::launch_mark(), k_write_walls<<<grid_for(lat, 256), 256, 0, s>>>(c->solid.ptr, c->nx, c->ny, c->nz, woff.ptr, c->cls.ptr,
                                                   c->face.ptr, c->code.ptr, c->cell.ptr, c->origin.ptr,
-                                                  c->hot.ptr, c->cold.ptr);
+                                                  c->hot(), c->cold());
   PR_CUDA(cudaGetLastError());
   ::pr::launch_mark(), k_write_internal<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(mask.ptr, off.ptr, c->nx, c->ny, c->nz,
                                                              (int32_t)n_wall, c->cls.ptr, c->face.ptr,
-                                                             c->code.ptr, c->cell.ptr, c->origin.ptr, c->cfp.ptr);
+                                                             c->code.ptr, c->cell.ptr, c->origin.ptr, c->cfp());
   PR_CUDA(cudaGetLastError());
   return PR_OK;
 }

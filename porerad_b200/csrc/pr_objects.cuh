@@ -65,17 +65,21 @@ struct pr_case {
   pr::DevBuf<int8_t> code;        // emission normal: 0..5 as +x,-x,+y,-y,+z,-z
   pr::DevBuf<int32_t> cell;       // owning cell, -1 for walls
   pr::DevBuf<double> origin;      // (P, 3)
-  pr::DevBuf<int32_t> cfp;        // cell_face_patch (n_cells, 6)
-  pr::DevBuf<int32_t> hot, cold;  // (ny, nz)
+  // Face table: cell_face_patch (n_cells, 6), then the hot and the cold wall patch of each
+  // (j, k) lattice site.  A first hit is recorded as an index into this table (its hit code).
+  pr::DevBuf<int32_t> ftab;
   cudaStream_t last_stream = nullptr;
+  int32_t* cfp() const { return ftab.ptr; }
+  int32_t* hot() const { return ftab.ptr + 6 * n_cells; }
+  int32_t* cold() const { return ftab.ptr + 6 * n_cells + ny * nz; }
   void rebind(cudaStream_t s) {
     solid.stream = occ.stream = s;
     cls.stream = face.stream = code.stream = s;
-    cell.stream = origin.stream = cfp.stream = hot.stream = cold.stream = s;
+    cell.stream = origin.stream = ftab.stream = s;
   }
   size_t device_bytes() const {
     return solid.bytes() + occ.bytes() + cls.bytes() + face.bytes() + code.bytes() + cell.bytes() +
-           origin.bytes() + cfp.bytes() + hot.bytes() + cold.bytes();
+           origin.bytes() + ftab.bytes();
   }
 };
 

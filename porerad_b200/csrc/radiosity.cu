@@ -550,7 +550,7 @@ static int field_channels(const pr_case* c, const pr_operator* op, const FieldSp
   int bx = (int)std::min<int64_t>(8, c->nx), by = (int)std::min<int64_t>(8, c->ny), bz = (int)std::min<int64_t>(8, c->nz);
   if (coarse) {
     PR_TRY(dco.alloc((size_t)bx * by * bz, s));
-    ::pr::launch_mark(), k_coarse<<<bx * by * bz, 256, 0, s>>>(c->cfp.ptr, dAb.ptr, dE.ptr, c->nx, c->ny, c->nz, bx, by, bz, 1.0 / xs,
+    ::pr::launch_mark(), k_coarse<<<bx * by * bz, 256, 0, s>>>(c->cfp(), dAb.ptr, dE.ptr, c->nx, c->ny, c->nz, bx, by, bz, 1.0 / xs,
                                            dco.ptr);
     PR_CUDA(cudaGetLastError());
   }

@@ -278,18 +278,14 @@ struct WarpPool {
 // One chunk of a launch: the rays of patches [p0, p0 + np) of one case, numbered seed-major
 // inside the chunk (g = (s * np + p - p0) * R + r) and placed at global ray indices
 // [start, start + n) of the launch, start a multiple of kUnit.  A launch (a wave) may hold
-// chunks of many cases of different sizes.
+// chunks of many cases of different sizes.  Its rays' hit codes go to recv[start + g].
 struct WaveChunk {
   const uint32_t* occ;
-  const int32_t* cfp;
-  const int32_t* hot;
-  const int32_t* cold;
   const double* origin;
   const int8_t* code;
   const pr_u128* maps;   // kMapStride maps per seed of this case
   const pr_u128* state;  // per seed
   const pr_u128* inc;    // per seed
-  int32_t* recv;         // receivers of this chunk, seed-major
   int64_t n, np, p0, R, start, n_cells;
   int32_t nx, ny, nz, wpr;
   double ny_d, nz_d;
@@ -372,6 +368,7 @@ __device__ __forceinline__ int find_chunk(const WaveChunk* __restrict__ chunks, 
 template <int kMinBlocks, int kBurst>
 __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const WaveChunk* __restrict__ chunks,
                                                                         int n_chunks, int64_t total,
+                                                                        int32_t* __restrict__ recv,
                                                                         unsigned long long* __restrict__ work,
                                                                         unsigned long long* __restrict__ chunk_ctr) {
   __shared__ WarpPool pools[kWarps];
@@ -476,7 +473,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const Wa
           pool.i[slot] = ci; pool.jj[slot] = cj; pool.kk[slot] = ck;
           pool.meta[slot] = (si + 1) | ((sj + 1) << 2) | ((sk + 1) << 4);
           pool.cap[slot] = c;
-          pool.q[slot] = (int)gq;
+          pool.q[slot] = (int)(C.start + gq);  // wave-wide ray index (< 2^31)
         }
         tail += cnt;
         __syncwarp();
@@ -521,14 +518,16 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const Wa
       } else {
         ++it;
         if ((unsigned)i >= (unsigned)nx) {
-          const int64_t wj = imod((int64_t)floor(pr_add(pool.eoy[lane], pr_mul(pool.edy[lane], t))), ny);
-          const int64_t wk = imod((int64_t)floor(pr_add(pool.eoz[lane], pr_mul(pool.edz[lane], t))), nz);
-          hit = i < 0 ? __ldg(chunks[cur].hot + wj * nz + wk) : __ldg(chunks[cur].cold + wj * nz + wk);
+          // hit code of a wall: 6 n_cells + (0 hot | ny nz cold) + j nz + k
+          const int wj = (int)imod((int64_t)floor(pr_add(pool.eoy[lane], pr_mul(pool.edy[lane], t))), ny);
+          const int wk = (int)imod((int64_t)floor(pr_add(pool.eoz[lane], pr_mul(pool.edz[lane], t))), nz);
+          hit = 6 * nx * ny * nz + (i < 0 ? 0 : ny * nz) + wj * nz + wk;
         } else {
           const int row = i * ny + jj;
           const uint32_t word = __ldg(occ + row * wpr + (kk >> 5));
           if ((word >> (kk & 31)) & 1u) {
-            hit = face >= 0 ? __ldg(chunks[cur].cfp + ((int64_t)row * nz + kk) * 6 + face) : -1;
+            // hit code of a cell face: its cell_face_patch index
+            hit = face >= 0 ? (row * nz + kk) * 6 + face : -1;
           } else {
             double tn = tx;
             if (ty < tn) tn = ty;
@@ -558,7 +557,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const Wa
         }
       }
       if (hit != -2) {
-        chunks[cur].recv[q] = hit;
+        recv[q] = hit;  // no load on this path: the RLE pass maps codes to patches
         my_steps += it;
         my_fail += hit < 0;
         active = false;
@@ -572,7 +571,9 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const Wa
 // in shared memory (bitonic), run-length encode into (receiver, count) pairs at
 // out[(p - p0) * L ...], nnz[p - p0].
 struct RleChunk {
-  const int32_t* recv;  // receivers of the chunk (seed-major)
+  const int32_t* recv;  // hit codes of the chunk (seed-major)
+  const int32_t* ftab;  // face table of its case: hit code -> receiving patch
+  unsigned long long* fail;  // the chunk's failed-ray counter
   int64_t np;           // patches
   int64_t patch0;       // index of its first patch among the wave's patches
   int64_t ray0;         // offset of its rays (and stage entries) in the wave's buffers
@@ -600,10 +601,14 @@ __global__ void __launch_bounds__(512) k_patch_rle(const RleChunk* __restrict__ 
     }
     const int64_t p = gp - rc[c].patch0, np = rc[c].np;
     const int32_t* recv = rc[c].recv;
+    const int32_t* ftab = rc[c].ftab;
     for (int i = tid; i < Lpad; i += nt) {
       if (i < L) {
         const int sd = i / R;
-        key[i] = recv[((int64_t)sd * np + p) * R + (i - sd * R)];
+        const int32_t code = recv[((int64_t)sd * np + p) * R + (i - sd * R)];
+        const int32_t r = code >= 0 ? __ldg(ftab + code) : -1;
+        if (code >= 0 && r < 0) atomicAdd(rc[c].fail, 1ull);  // a face without a patch
+        key[i] = r;
       } else {
         key[i] = INT32_MAX;
       }
@@ -763,9 +768,9 @@ struct SeedTables {
 static Geom geom_of(const pr_case* c) {
   Geom g;
   g.occ = c->occ.ptr;
-  g.cfp = c->cfp.ptr;
-  g.hot = c->hot.ptr;
-  g.cold = c->cold.ptr;
+  g.cfp = c->cfp();
+  g.hot = c->hot();
+  g.cold = c->cold();
   g.nx = (int32_t)c->nx;
   g.ny = (int32_t)c->ny;
   g.nz = (int32_t)c->nz;
@@ -791,7 +796,7 @@ static int trace_grid() { return sm_count() * 8; }
 // Variants of the pooled traversal (minimum resident blocks per SM x DDA steps per burst).
 // Every variant writes the same receivers; the autotuner below picks the fastest per
 // problem class by timing them on the first chunk of the first call.
-using TraceKernel = void (*)(const WaveChunk*, int, int64_t, unsigned long long*, unsigned long long*);
+using TraceKernel = void (*)(const WaveChunk*, int, int64_t, int32_t*, unsigned long long*, unsigned long long*);
 struct TraceVariant {
   TraceKernel kernel;
   const char* name;
@@ -857,6 +862,7 @@ struct WaveLaunch {
   const WaveChunk* chunks;  // device table
   int n_chunks;
   int64_t total;            // global ray indices [0, total)
+  int32_t* recv;            // hit codes, by global ray index
   unsigned long long* work; // work-unit counter
   unsigned long long* ctr;  // 2 per chunk: DDA steps, failed rays
 };
@@ -864,7 +870,7 @@ struct WaveLaunch {
 static int launch_variant(int v, const WaveLaunch& w, cudaStream_t s) {
   PR_CUDA(cudaMemsetAsync(w.work, 0, sizeof(unsigned long long), s));
   ::pr::launch_mark(), kVariants[v].kernel<<<variant_grid(v), kWarps * 32, 0, s>>>(w.chunks, w.n_chunks, w.total,
-                                                                                  w.work, w.ctr);
+                                                                                  w.recv, w.work, w.ctr);
   PR_CUDA(cudaGetLastError());
   return PR_OK;
 }
@@ -1019,6 +1025,10 @@ int counts_batch(const pr_case* const* cases, int nc, int64_t R, const pr_pcg64*
   for (int c = 0; c < nc; ++c) {
     PR_ARG(cases[c] != nullptr, "case %d is NULL", c);
     PR_ARG(cases[c]->device == dev0, "case %d lives on another device", c);
+    if (6 * cases[c]->n_cells + 2 * cases[c]->ny * cases[c]->nz > (int64_t)INT32_MAX) {
+      set_error("case %d: %lld cells exceed the int32 hit codes of the traversal", c, (long long)cases[c]->n_cells);
+      return PR_ERR_LIMIT;
+    }
     PR_TRY(tables[c].build(seeds + (size_t)c * S, S, s));
     const int64_t P = cases[c]->n_patches;
     cc[c].k.reset(new pr_counts());
@@ -1059,7 +1069,8 @@ int counts_batch(const pr_case* const* cases, int nc, int64_t R, const pr_pcg64*
   DevBuf<WaveChunk> dchunks;
   DevBuf<RleChunk> drle;
   const int64_t max_wave_patches = wave_cap / L64 + (int64_t)chunks.size();
-  PR_TRY(recv.alloc(wave_cap, s));
+  // hit codes by wave-wide ray index: chunk starts are rounded up to whole work units
+  PR_TRY(recv.alloc(wave_cap + (int64_t)chunks.size() * kUnit, s));
   PR_TRY(st_col.alloc(wave_cap, s));
   PR_TRY(st_cnt.alloc(wave_cap, s));
   PR_TRY(nnz.alloc(max_wave_patches, s));
@@ -1096,15 +1107,11 @@ int counts_batch(const pr_case* const* cases, int nc, int64_t R, const pr_pcg64*
       const pr_case* c = cases[ch.c];
       WaveChunk& W = hw[k];
       W.occ = c->occ.ptr;
-      W.cfp = c->cfp.ptr;
-      W.hot = c->hot.ptr;
-      W.cold = c->cold.ptr;
       W.origin = c->origin.ptr;
       W.code = c->code.ptr;
       W.maps = tables[ch.c].maps.ptr;
       W.state = tables[ch.c].state.ptr;
       W.inc = tables[ch.c].inc.ptr;
-      W.recv = recv.ptr + ray0;
       W.n = ch.np * L64;
       W.np = ch.np;
       W.p0 = ch.p0;
@@ -1117,7 +1124,7 @@ int counts_batch(const pr_case* const* cases, int nc, int64_t R, const pr_pcg64*
       W.wpr = c->wpr;
       W.ny_d = (double)c->ny;
       W.nz_d = (double)c->nz;
-      hr[k] = RleChunk{recv.ptr + ray0, ch.np, patch0, ray0};
+      hr[k] = RleChunk{recv.ptr + start, c->ftab.ptr, ctr.ptr + 2 * (w0 + k) + 1, ch.np, patch0, ray0};
       start += (W.n + kUnit - 1) / kUnit * kUnit;
       ray0 += W.n;
       patch0 += ch.np;
@@ -1126,7 +1133,7 @@ int counts_batch(const pr_case* const* cases, int nc, int64_t R, const pr_pcg64*
     PR_CUDA(cudaMemcpyAsync(dchunks.ptr, hw.data(), nw * sizeof(WaveChunk), cudaMemcpyHostToDevice, s));
     PR_CUDA(cudaMemcpyAsync(drle.ptr, hr.data(), nw * sizeof(RleChunk), cudaMemcpyHostToDevice, s));
     unsigned long long* wave_ctr = ctr.ptr + 2 * w0;
-    WaveLaunch wl{dchunks.ptr, nw, total, work.ptr, wave_ctr};
+    WaveLaunch wl{dchunks.ptr, nw, total, recv.ptr, work.ptr, wave_ctr};
     if (!tuned) {
       const pr_case* c0 = cases[chunks[w0].c];
       PR_TRY(choose_variant(TuneKey{c0->nx, c0->ny, c0->nz, L64, nc}, wl, s, &variant));
