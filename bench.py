@@ -74,6 +74,8 @@ def parse_args():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain drop-in path measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of one baseline sample")
+    ap.add_argument("--rays", type=int, default=None,
+                    help="override rays per patch (small cases of the same kernels for profiling; not a bench line)")
     return ap.parse_args()
 
 
@@ -736,7 +738,10 @@ def run_reference(args, cfg):
 
 def main():
     args = parse_args()
-    cfg = WORKLOADS[args.workload]
+    cfg = dict(WORKLOADS[args.workload])
+    if args.rays is not None and "rays" in cfg:
+        cfg["rays"] = int(args.rays)
+        cfg["workload"] += f" [rays/patch overridden to {args.rays}: profiling case]"
     if args.impl == "reference":
         line = run_reference(args, cfg)
     elif args.workload == "c3":

@@ -51,6 +51,11 @@ void timer_end(int id, cudaStream_t s);
     }                                     \
   } while (0)
 
+// Keep freed stream-ordered allocations of the current device's default pool mapped (up to
+// PORERAD_POOL_RETAIN_BYTES, default a quarter of the device memory) instead of returning
+// them to the driver at every synchronisation; called before each allocation, acts once per device.
+void retain_pool_memory();
+
 // A device allocation owned by the library, released in stream order.
 template <typename T>
 struct DevBuf {
@@ -80,6 +85,7 @@ struct DevBuf {
     stream = s;
     n = count;
     if (count == 0) return PR_OK;
+    retain_pool_memory();
     cudaError_t e = cudaMallocAsync((void**)&ptr, count * sizeof(T), s);
     if (e != cudaSuccess) {
       ptr = nullptr;

@@ -1,8 +1,11 @@
-// Launch counter and optional per-kernel CUDA-event timers (benchmark instrumentation).
+// Launch counter, optional per-kernel CUDA-event timers (benchmark instrumentation) and the
+// retention setting of the stream-ordered memory pool.
 //
 // Timers record one event pair on the launching stream around each launch of the
 // instrumented kernels while enabled; pr_timers_read() waits for the pending events
 // and accumulates the elapsed times per kernel class.
+#include <atomic>
+#include <cstdlib>
 #include <mutex>
 #include <vector>
 
@@ -38,6 +41,23 @@ thread_local cudaEvent_t t_start[kTimerCount] = {nullptr};
 }  // namespace
 
 bool timers_on() { return g_on; }
+
+void retain_pool_memory() {
+  static std::atomic<bool> done[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || done[dev].load(std::memory_order_acquire)) return;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done[dev].load(std::memory_order_relaxed)) return;
+  cudaMemPool_t pool;
+  size_t free_b = 0, total_b = 0;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+    unsigned long long keep = total_b / 4;
+    if (const char* env = std::getenv("PORERAD_POOL_RETAIN_BYTES")) keep = std::strtoull(env, nullptr, 10);
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  done[dev].store(true, std::memory_order_release);
+}
 
 void timer_begin(int id, cudaStream_t s) {
   if (!g_on) return;

@@ -1175,8 +1175,7 @@ int counts_batch(const pr_case* const* cases, int nc, int64_t R, const pr_pcg64*
       PR_CUDA(cudaGetLastError());
       cc[ch.c].pieces.push_back(std::move(pc));
     }
-    // the compactions read the stage buffers: finish them before the next wave reuses them
-    PR_CUDA(cudaStreamSynchronize(s));
+    // the next wave's kernels reuse the stage buffers after these compactions in stream order
     w0 = w1;
   }
 
