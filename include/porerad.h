@@ -250,6 +250,16 @@ PR_API int pr_trace_variant_info(int* count, int* last_used, const char** name);
 /* Number of the library's own kernel launches so far (CUB primitives not counted). */
 PR_API long long pr_kernel_launches(void);
 
+/* ---- device memory (no counterpart in the reference) ------------------------------
+ * Library objects allocate through a per-device cache of freed blocks (size classes
+ * within 12.5 %, reuse ordered after the block's last use by an in-stream event wait),
+ * bounded by PORERAD_CACHE_BYTES (default a quarter of the device memory).  Stats: bytes
+ * cached, bytes live in library objects, driver allocations, allocations served from the
+ * cache.  release_cached returns every cached block of the device to the driver. */
+PR_API int pr_memory_stats(int device, long long* cached_bytes, long long* live_bytes, long long* device_mallocs,
+                           long long* cache_hits);
+PR_API int pr_memory_release_cached(int device);
+
 #ifdef __cplusplus
 }
 #endif

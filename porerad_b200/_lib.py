@@ -83,6 +83,9 @@ _SIGNATURES = {
     "pr_timers_read": (_i32, [_i32, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_f64)]),
     "pr_kernel_launches": (ctypes.c_longlong, []),
     "pr_trace_set_variant": (_i32, [_i32]),
+    "pr_memory_stats": (_i32, [_i32, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
+                               ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
+    "pr_memory_release_cached": (_i32, [_i32]),
     "pr_trace_variant_info": (_i32, [ctypes.POINTER(_i32), ctypes.POINTER(_i32), ctypes.POINTER(ctypes.c_char_p)]),
 }
 
@@ -209,6 +212,20 @@ class use_stream:
 
     def __exit__(self, *exc):
         _tls.stream = self.prev
+
+
+def memory_stats(device: int = 0) -> dict:
+    """Device-memory cache counters of libporerad on one device."""
+
+    v = [ctypes.c_longlong() for _ in range(4)]
+    check(load().pr_memory_stats(int(device), *[ctypes.byref(x) for x in v]))
+    return dict(zip(("cached_bytes", "live_bytes", "device_mallocs", "cache_hits"), (int(x.value) for x in v)))
+
+
+def release_cached_memory(device: int = 0) -> None:
+    """Return the library's cached device blocks to the driver (like emptying a caching allocator)."""
+
+    check(load().pr_memory_release_cached(int(device)))
 
 
 def trace_variant() -> tuple[int, str]:

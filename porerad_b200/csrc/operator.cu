@@ -476,38 +476,50 @@ __global__ void k_exp_scale(const double* __restrict__ y, int64_t n, double* __r
   }
 }
 
-// One balancing evaluation at y (d = e^y given):  s = S d;  f_new = y + log s - log A;
-// dF = f_new - f_old (when dF != nullptr);  closure |d s / A - 1|;  max |f_new|.
-// In multiplicative mode (mult = 1), also y_next = y + 0.5 (log A - log(d s)).
-template <int kMode>
-__global__ void __launch_bounds__(256) k_balance_eval(SymView S, double delta, const double* __restrict__ area,
-                                                      const double* __restrict__ y, const double* __restrict__ d,
-                                                      double* __restrict__ f, double* __restrict__ dF,
-                                                      double* __restrict__ sc, int mult, double* __restrict__ y_next) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  double mf = 0.0, mc = 0.0;
-  bool bad = false;
-  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < S.n; i += warps) {
+// One balancing evaluation at y (d = e^y given, the vector of the product):  s = S d;
+// f_new = y + log s - log A;  dF = f_new - f_old (when dF != nullptr);  closure
+// |d s / A - 1|;  max |f_new|.  In multiplicative mode (mult = 1), also
+// y_next = y + 0.5 (log A - log(d s)).
+struct BalanceEpi {
+  double delta;
+  const double* area;
+  const double* y;
+  const double* d;
+  double* f;
+  double* dF;
+  double* sc;
+  int mult;
+  double* y_next;
+  struct Red {
+    double mf = 0.0, mc = 0.0;
+    bool bad = false;
+  };
+  __device__ bool skip() const { return false; }
+  __device__ void row(int64_t i, double sp, Red& r) const {
     const double Ai = area[i];
-    const double s = sym_row<kMode>(S, i, d, lane) + delta * Ai * d[i];
-    if (lane == 0) {
-      if (!(s > 0.0 && isfinite(s))) bad = true;
-      const double fn = y[i] + log(s) - log(Ai);
-      if (dF) dF[i] = fn - f[i];
-      f[i] = fn;
-      const double row = d[i] * s;
-      mf = fmax(mf, fabs(fn));
-      mc = fmax(mc, fabs(row / Ai - 1.0));
-      if (mult) y_next[i] = y[i] + 0.5 * (log(Ai) - log(row));
+    const double s = sp + delta * Ai * d[i];
+    if (!(s > 0.0 && isfinite(s))) r.bad = true;
+    const double fn = y[i] + log(s) - log(Ai);
+    if (dF) dF[i] = fn - f[i];
+    f[i] = fn;
+    const double rowv = d[i] * s;
+    r.mf = fmax(r.mf, fabs(fn));
+    r.mc = fmax(r.mc, fabs(rowv / Ai - 1.0));
+    if (mult) y_next[i] = y[i] + 0.5 * (log(Ai) - log(rowv));
+  }
+  __device__ void finish(Red& r) const {
+    for (int o = 16; o > 0; o >>= 1) {
+      r.mf = fmax(r.mf, __shfl_xor_sync(PR_FULL, r.mf, o));
+      r.mc = fmax(r.mc, __shfl_xor_sync(PR_FULL, r.mc, o));
+    }
+    const bool bad = __any_sync(PR_FULL, r.bad);
+    if ((threadIdx.x & 31) == 0) {
+      atomic_max_nonneg(sc + 0, r.mf);
+      atomic_max_nonneg(sc + 1, r.mc);
+      if (bad) sc[2] = 1.0;
     }
   }
-  if (lane == 0) {
-    atomic_max_nonneg(sc + 0, mf);
-    atomic_max_nonneg(sc + 1, mc);
-    if (bad) sc[2] = 1.0;
-  }
-}
+};
 
 // y_next = y - beta f - sum_c gamma_c (dY_c - beta dF_c);  dY_slot = y_next - y.
 struct AAStep {
@@ -552,19 +564,22 @@ __global__ void __launch_bounds__(256) k_aa_dots(const double* __restrict__ dF, 
 
 // ------------------------------------------------------------------ products
 
-template <int kMode>
-__global__ void __launch_bounds__(256) k_sym_apply(SymView S, double delta, const double* __restrict__ area,
-                                                   const double* __restrict__ d, const double* __restrict__ x,
-                                                   int mode, double* __restrict__ u, double* __restrict__ y) {
-  // mode 0: y = S x;  mode 1: y = (d/A) S(u), u = d x;  mode 2: y = d S(u), u = d (x / A)
-  const int lane = threadIdx.x & 31;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  const double* v = mode == 0 ? x : u;
-  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < S.n; i += warps) {
-    const double s = sym_row<kMode>(S, i, v, lane) + delta * area[i] * v[i];
-    if (lane == 0) y[i] = mode == 0 ? s : (mode == 1 ? (d[i] / area[i]) * s : d[i] * s);
+// y = S v (mode 0), (d / A) S v with v = d x (mode 1), d S v with v = d (x / A) (mode 2).
+struct ApplyEpi {
+  double delta;
+  const double* area;
+  const double* d;
+  const double* v;
+  int mode;
+  double* y;
+  struct Red {};
+  __device__ bool skip() const { return false; }
+  __device__ void row(int64_t i, double sp, Red&) const {
+    const double s = sp + delta * area[i] * v[i];
+    y[i] = mode == 0 ? s : (mode == 1 ? (d[i] / area[i]) * s : d[i] * s);
   }
-}
+  __device__ void finish(Red&) const {}
+};
 
 __global__ void k_prep_u(const double* __restrict__ d, const double* __restrict__ area, const double* __restrict__ x,
                          int64_t n, int mode, double* __restrict__ u) {
@@ -714,14 +729,12 @@ static int balance_eval(pr_operator* op, BalanceWork& w, const double* y, double
   const int64_t n = w.n;
   PR_CUDA(cudaMemsetAsync(w.sc.ptr, 0, 4 * sizeof(double), s));
   ::pr::launch_mark(), k_exp_scale<<<grid_for(n, 256), 256, 0, s>>>(y, n, w.d.ptr, w.sc.ptr);
-  SymView S = sym_view(op->S);
-  dispatch_mode(op->S.mode, [&](auto u) {
-    ::pr::timer_begin(kTimerBalance, s);
-    ::pr::launch_mark(), k_balance_eval<decltype(u)::value><<<spmv_grid(n), 256, 0, s>>>(S, op->delta, op->area.ptr, y, w.d.ptr, w.f.ptr,
-                                                                     dF, w.sc.ptr, mult, y_next);
-    ::pr::timer_end(kTimerBalance, s);
-  });
-  PR_CUDA(cudaGetLastError());
+  const BalanceEpi epi{op->delta, op->area.ptr, y, w.d.ptr, w.f.ptr, dF, w.sc.ptr, mult, y_next};
+  int st = PR_OK;
+  ::pr::timer_begin(kTimerBalance, s);
+  dispatch_mode(op->S.mode, [&](auto u) { st = launch_spmv<decltype(u)::value, double>(op->S, w.d.ptr, epi, s); });
+  ::pr::timer_end(kTimerBalance, s);
+  PR_TRY(st);
   op->spmv_calls++;
   PR_CUDA(cudaMemcpyAsync(out, w.sc.ptr, sizeof(BalanceScalars), cudaMemcpyDeviceToHost, s));
   return PR_OK;
@@ -892,6 +905,81 @@ static int sym_union(const CountCsr& F, const CountCsr& T, pr_operator* op, cuda
   return PR_OK;
 }
 
+// CTA row boundaries of a blocked product: boundary c is the first row r whose cost
+// row_ptr[r] + r nnz / n reaches c / C of the total, so a CTA holds about 2 nnz / C
+// entries plus rows, and fewer than 2 n / C + 1 rows.
+__global__ void k_cta_rows(const int64_t* __restrict__ rp, int64_t n, int ctas, int64_t* __restrict__ out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > ctas) return;
+  if (c == 0 || c == ctas) {
+    out[c] = c == 0 ? 0 : n;
+    return;
+  }
+  const double avg = (double)rp[n] / (double)n;
+  const double target = (double)c * (2.0 * (double)rp[n] / (double)ctas);
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if ((double)rp[mid] + (double)mid * avg < target) lo = mid + 1;
+    else hi = mid;
+  }
+  out[c] = lo;
+}
+
+// seg[(b - 1) n + i] = first entry of row i with column >= b W, relative to row_ptr[i]
+// (b = 1 .. nb - 1); the words of a row ascend with the column in both union modes.
+__global__ void k_block_seg(const int64_t* __restrict__ rp, const uint32_t* __restrict__ words, int64_t n, int nb,
+                            int W, int bits, int32_t* __restrict__ seg) {
+  const int64_t total = n * (int64_t)(nb - 1);
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = t % n;
+    const int b = (int)(t / n) + 1;
+    const uint32_t key = (uint32_t)((uint64_t)b * (uint64_t)W) << bits;
+    int64_t lo = rp[i], hi = rp[i + 1];
+    const int64_t base = lo;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (words[mid] < key) lo = mid + 1;
+      else hi = mid;
+    }
+    seg[(int64_t)(b - 1) * n + i] = (int32_t)(lo - base);
+  }
+}
+
+// Column blocks for the shared-memory products of a union-stored S'.
+static int build_col_blocks(SymCsr& S, cudaStream_t s) {
+  ColBlocks& B = S.blk;
+  B.ready = false;
+  const int64_t n = S.n_rows;
+  if (n == 0 || S.mode == kValues) return PR_OK;
+  const int64_t kRowsCap = 6144;  // binary64 row sums of one CTA: 48 KB of shared memory
+  int64_t ctas = std::max<int64_t>(sm_count(), (2 * n + kRowsCap - 1) / kRowsCap);
+  if (ctas > n) ctas = std::max<int64_t>(1, n);
+  PR_TRY(B.cta_row.alloc(ctas + 1, s));
+  ::pr::launch_mark(), k_cta_rows<<<grid_for(ctas + 1, 256), 256, 0, s>>>(S.row_ptr.ptr, n, (int)ctas, B.cta_row.ptr);
+  PR_CUDA(cudaGetLastError());
+  std::vector<int64_t> h(ctas + 1);
+  PR_CUDA(cudaMemcpyAsync(h.data(), B.cta_row.ptr, (ctas + 1) * 8, cudaMemcpyDeviceToHost, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  int64_t rows_cap = 1;
+  for (int64_t c = 0; c < ctas; ++c) rows_cap = std::max(rows_cap, h[c + 1] - h[c]);
+  const int64_t stage_bytes = (int64_t)kBlkSmemMax - rows_cap * 8;
+  const int64_t W = stage_bytes / 8 / 64 * 64;
+  if (W < 1024) return PR_OK;  // rows too many for one CTA's row sums: warp-per-row products
+  B.W = (int)std::min<int64_t>(W, (n + 63) / 64 * 64);
+  B.nb = (int)((n + B.W - 1) / B.W);
+  B.ctas = (int)ctas;
+  B.rows_cap = (int)rows_cap;
+  if (B.nb > 1) {
+    PR_TRY(B.seg.alloc((size_t)(B.nb - 1) * n, s));
+    ::pr::launch_mark(), k_block_seg<<<grid_for(n * (B.nb - 1), 256), 256, 0, s>>>(
+        S.row_ptr.ptr, S.words.ptr, n, B.nb, B.W, S.mode == kPacked ? S.bits : 0, B.seg.ptr);
+    PR_CUDA(cudaGetLastError());
+  }
+  B.ready = true;
+  return PR_OK;
+}
+
 int apply(const pr_operator* op, int which, const double* x_dev, double* y_dev, cudaStream_t s);
 
 int operator_create(const pr_counts* k, const int64_t* rays, const double* area, double delta, double tol,
@@ -965,6 +1053,7 @@ int operator_create(const pr_counts* k, const int64_t* rays, const double* area,
     } else if (n > 0) {
       // equal areas and ray counts: S'_ij = factor (n_ij + n_ji) on the union of the patterns
       PR_TRY(sym_union(F, *T, op.get(), s));
+      PR_TRY(build_col_blocks(op->S, s));
     }
     op->FT = T;  // kept for raw_rmatvec
   }
@@ -1013,12 +1102,11 @@ int apply(const pr_operator* op, int which, const double* x, double* y, cudaStre
     ::pr::launch_mark(), k_prep_u<<<grid_for(n, 256), 256, 0, s>>>(op->scale.ptr, op->area.ptr, x, n, mode, u.ptr);
     PR_CUDA(cudaGetLastError());
   }
-  SymView S = sym_view(op->S);
-  dispatch_mode(op->S.mode, [&](auto un) {
-    ::pr::launch_mark(), k_sym_apply<decltype(un)::value><<<spmv_grid(n), 256, 0, s>>>(S, op->delta, op->area.ptr, op->scale.ptr, x,
-                                                                   mode, u.ptr, y);
-  });
-  PR_CUDA(cudaGetLastError());
+  const double* v = mode == 0 ? x : u.ptr;
+  const ApplyEpi epi{op->delta, op->area.ptr, op->scale.ptr, v, mode, y};
+  int st = PR_OK;
+  dispatch_mode(op->S.mode, [&](auto un) { st = launch_spmv<decltype(un)::value, double>(op->S, v, epi, s); });
+  PR_TRY(st);
   op->spmv_calls++;
   return PR_OK;
 }

@@ -56,12 +56,18 @@ void timer_end(int id, cudaStream_t s);
 // them to the driver at every synchronisation; called before each allocation, acts once per device.
 void retain_pool_memory();
 
-// A device allocation owned by the library, released in stream order.
+// The library's device-memory cache (arena.cu): allocate `bytes` for use on stream s (the
+// owning device is returned in *dev), and give a block back after its uses on stream s.
+int arena_alloc(size_t bytes, cudaStream_t s, void** out, int* dev);
+void arena_free(void* p, size_t bytes, cudaStream_t s, int dev);
+
+// A device allocation owned by the library, released in stream order (to the cache).
 template <typename T>
 struct DevBuf {
   T* ptr = nullptr;
   size_t n = 0;
   cudaStream_t stream = nullptr;
+  int dev = -1;
 
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
@@ -73,6 +79,7 @@ struct DevBuf {
       ptr = o.ptr;
       n = o.n;
       stream = o.stream;
+      dev = o.dev;
       o.ptr = nullptr;
       o.n = 0;
     }
@@ -85,18 +92,15 @@ struct DevBuf {
     stream = s;
     n = count;
     if (count == 0) return PR_OK;
-    retain_pool_memory();
-    cudaError_t e = cudaMallocAsync((void**)&ptr, count * sizeof(T), s);
-    if (e != cudaSuccess) {
+    const int st = arena_alloc(count * sizeof(T), s, (void**)&ptr, &dev);
+    if (st != PR_OK) {
       ptr = nullptr;
       n = 0;
-      set_error("device allocation of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
-      return e == cudaErrorMemoryAllocation ? PR_ERR_OOM : PR_ERR_CUDA;
     }
-    return PR_OK;
+    return st;
   }
   void release() {
-    if (ptr) cudaFreeAsync(ptr, stream);
+    if (ptr) arena_free(ptr, n * sizeof(T), stream, dev);
     ptr = nullptr;
     n = 0;
   }

@@ -30,14 +30,26 @@ struct CountCsr {
 };
 
 // Symmetric exchange matrix S' = 0.5 (A F + F^T A) without the support diagonal
-// (delta A, applied separately).  Row i holds row i of F followed by row i of F^T, so
-// S'_ij x_j is the sum over both segments; no union of the two patterns is formed.
-// Entry storage, by mode:
-//   kPacked:  one 32-bit word (col << bits) | n per entry, value factor * n
-//             (every patch with the same area and ray count, and col/count bits fit);
-//   kCounts:  col (int32) + n (int32), value factor * n (same uniform case, wide ids);
-//   kValues:  col (int32) + binary64 value 0.5 A n / R of the entry's origin patch.
+// (delta A, applied separately).  Entry storage, by mode:
+//   kPacked:  one 32-bit word (col << bits) | n per entry, value factor * n, n = n_ij + n_ji
+//             on the union of the patterns of F and F^T, columns ascending (every patch
+//             with the same area and ray count, and column/count bits fit in 32);
+//   kCounts:  col (int32) + n (int32) on the same union (same uniform case, wide ids);
+//   kValues:  col (int32) + binary64 value 0.5 A n / R of the entry's origin patch; row i
+//             holds row i of F followed by row i of F^T (two ascending runs).
 enum SymMode { kPacked = 0, kCounts = 1, kValues = 2 };
+
+// Column blocks of a union-stored S' for products that stage x in shared memory: block b
+// holds columns [b W, (b + 1) W); seg[(b - 1) n + i] (b = 1 .. nb - 1) is the offset of
+// block b's first entry in row i from row_ptr[i].  CTA c of a blocked product owns rows
+// [cta_row[c], cta_row[c + 1]), at most rows_cap of them, split so that every CTA has
+// about the same number of entries plus rows.
+struct ColBlocks {
+  bool ready = false;
+  int W = 0, nb = 0, ctas = 0, rows_cap = 0;
+  DevBuf<int32_t> seg;
+  DevBuf<int64_t> cta_row;
+};
 
 struct SymCsr {
   int64_t n_rows = 0, nnz = 0;
@@ -48,6 +60,7 @@ struct SymCsr {
   int mode = kPacked;
   int bits = 0;            // count bits of a packed word
   double factor = 0.0;     // 0.5 A / R in the uniform modes
+  ColBlocks blk;           // union modes
 };
 
 }  // namespace pr

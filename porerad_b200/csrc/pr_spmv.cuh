@@ -1,10 +1,16 @@
 // Sparse products over the symmetric exchange matrix and deterministic reductions.
 //
-// S x = S' x + delta A x, S' = 0.5 (A F + F^T A) (porerad/exchange.py:108-112), row i
-// stored as row i of F followed by row i of F^T.  One warp owns one row: lanes stride
-// over the row's entries (coalesced 32-bit word loads, gathers of x from L2) and the
-// partial sums meet in a fixed shuffle tree, so every product is bitwise reproducible.
+// S x = S' x + delta A x, S' = 0.5 (A F + F^T A) (porerad/exchange.py:108-112).  A product
+// is one kernel: the row sums of S' x followed by a per-row epilogue (the update of the
+// solver that consumes the product) and block reductions in a fixed order, so every
+// result is bitwise reproducible for a given operator.  Two row-sum schemes:
+//  * warp per row (k_spmv_rows): lanes stride over the row's entries (coalesced 32-bit
+//    word loads, gathers of x through L1/L2), partial sums meet in a fixed shuffle tree;
+//  * column-blocked (k_spmv_blk, union storage only): x is staged in shared memory one
+//    block of columns at a time, so the random gathers become shared-memory loads; each
+//    row's sum accumulates block by block in shared memory.
 #pragma once
+#include <mutex>
 #include <type_traits>
 
 #include "pr_objects.cuh"
@@ -37,42 +43,64 @@ inline SymView sym_view(const SymCsr& S) {
   return v;
 }
 
-// sum_j S'_ij x_j in binary64, the full sum on every lane of the warp.
-template <int kMode, typename Tx>
-__device__ __forceinline__ double sym_row(const SymView& S, int64_t i, const Tx* __restrict__ x, int lane) {
+// Coefficient and column of entry q (storage mode kMode).
+template <int kMode, typename Acc>
+__device__ __forceinline__ void sym_entry(const SymView& S, int64_t q, Acc& c, uint32_t& col) {
+  const uint32_t w = __ldg(S.words + q);
+  if constexpr (kMode == kPacked) {
+    c = (Acc)(w & S.mask);
+    col = w >> S.bits;
+  } else if constexpr (kMode == kCounts) {
+    c = (Acc)__ldg(S.cnt + q);
+    col = w;
+  } else {
+    c = (Acc)__ldg(S.val + q);
+    col = w;
+  }
+}
+
+// sum_j S'_ij x_j in precision Acc, the full sum on every lane of the warp.  Lane l adds
+// entries b + l, b + l + 32, ... in that order; four of them are loaded before the first
+// is added, so four word loads and four gathers are in flight per lane (the order of the
+// additions, and so the result, does not depend on the unrolling).
+template <int kMode, typename Acc, typename Tx>
+__device__ __forceinline__ Acc sym_row_acc(const SymView& S, int64_t i, const Tx* __restrict__ x, int lane) {
   const int64_t b = S.row_ptr[i], e = S.row_ptr[i + 1];
-  double acc = 0.0;
-  for (int64_t q = b + lane; q < e; q += 32) {
-    const uint32_t w = __ldg(S.words + q);
-    if constexpr (kMode == kPacked) {
-      acc = fma((double)(w & S.mask), (double)__ldg(x + (w >> S.bits)), acc);
-    } else if constexpr (kMode == kCounts) {
-      acc = fma((double)__ldg(S.cnt + q), (double)__ldg(x + w), acc);
-    } else {
-      acc = fma(__ldg(S.val + q), (double)__ldg(x + w), acc);
-    }
+  Acc acc = 0;
+  int64_t q = b + lane;
+  for (; q + 96 < e; q += 128) {
+    Acc c0, c1, c2, c3;
+    uint32_t j0, j1, j2, j3;
+    sym_entry<kMode>(S, q, c0, j0);
+    sym_entry<kMode>(S, q + 32, c1, j1);
+    sym_entry<kMode>(S, q + 64, c2, j2);
+    sym_entry<kMode>(S, q + 96, c3, j3);
+    const Acc x0 = (Acc)__ldg(x + j0), x1 = (Acc)__ldg(x + j1), x2 = (Acc)__ldg(x + j2), x3 = (Acc)__ldg(x + j3);
+    acc = fma(c0, x0, acc);
+    acc = fma(c1, x1, acc);
+    acc = fma(c2, x2, acc);
+    acc = fma(c3, x3, acc);
+  }
+  for (; q < e; q += 32) {
+    Acc c;
+    uint32_t j;
+    sym_entry<kMode>(S, q, c, j);
+    acc = fma(c, (Acc)__ldg(x + j), acc);
   }
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(PR_FULL, acc, o);
-  return kMode == kValues ? acc : acc * S.factor;
+  return kMode == kValues ? acc : acc * (Acc)S.factor;
+}
+
+// sum_j S'_ij x_j in binary64.
+template <int kMode, typename Tx>
+__device__ __forceinline__ double sym_row(const SymView& S, int64_t i, const Tx* __restrict__ x, int lane) {
+  return sym_row_acc<kMode, double>(S, i, x, lane);
 }
 
 // The same sum in binary32 (mixed-precision sweeps).
 template <int kMode>
 __device__ __forceinline__ float sym_row32(const SymView& S, int64_t i, const float* __restrict__ x, int lane) {
-  const int64_t b = S.row_ptr[i], e = S.row_ptr[i + 1];
-  float acc = 0.0f;
-  for (int64_t q = b + lane; q < e; q += 32) {
-    const uint32_t w = __ldg(S.words + q);
-    if constexpr (kMode == kPacked) {
-      acc = fmaf((float)(w & S.mask), __ldg(x + (w >> S.bits)), acc);
-    } else if constexpr (kMode == kCounts) {
-      acc = fmaf((float)__ldg(S.cnt + q), __ldg(x + w), acc);
-    } else {
-      acc = fmaf((float)__ldg(S.val + q), __ldg(x + w), acc);
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(PR_FULL, acc, o);
-  return kMode == kValues ? acc : acc * (float)S.factor;
+  return sym_row_acc<kMode, float>(S, i, x, lane);
 }
 
 // Calls fn(std::integral_constant<int, mode>) for the matrix's storage mode.
@@ -114,5 +142,160 @@ __device__ __forceinline__ void block_sum_store(double (&v)[K], double* __restri
 __global__ void k_sum_partials(const double* __restrict__ partial, int blocks, int K, double* __restrict__ out);
 
 int sum_partials(const double* partial, int blocks, int K, double* out, cudaStream_t s);
+
+
+// ------------------------------------------------------------------ generic products
+
+struct BlkView {
+  const int32_t* __restrict__ seg;
+  const int64_t* __restrict__ cta_row;
+  int W, nb;
+};
+
+inline BlkView blk_view(const SymCsr& S) { return BlkView{S.blk.seg.ptr, S.blk.cta_row.ptr, S.blk.W, S.blk.nb}; }
+
+// sum over entries [qb, qe) of a row of coefficient * xs[col - c0] (xs in shared memory) by
+// a group of G lanes (gl = lane within the group): lane gl adds entries qb + gl, qb + gl + G,
+// ... in that order, four loads ahead; the group's partials meet in a fixed shuffle tree
+// (every lane of the warp takes part, lanes of an idle group with qb = qe add zero).
+template <int kMode, int G, typename Acc, typename Tx>
+__device__ __forceinline__ Acc seg_sum(const SymView& S, int64_t qb, int64_t qe, const Tx* xs, uint32_t c0,
+                                       int gl) {
+  Acc acc = 0;
+  int64_t q = qb + gl;
+  for (; q + 3 * G < qe; q += 4 * G) {
+    Acc c0v, c1v, c2v, c3v;
+    uint32_t j0, j1, j2, j3;
+    sym_entry<kMode>(S, q, c0v, j0);
+    sym_entry<kMode>(S, q + G, c1v, j1);
+    sym_entry<kMode>(S, q + 2 * G, c2v, j2);
+    sym_entry<kMode>(S, q + 3 * G, c3v, j3);
+    const Acc x0 = (Acc)xs[j0 - c0], x1 = (Acc)xs[j1 - c0], x2 = (Acc)xs[j2 - c0], x3 = (Acc)xs[j3 - c0];
+    acc = fma(c0v, x0, acc);
+    acc = fma(c1v, x1, acc);
+    acc = fma(c2v, x2, acc);
+    acc = fma(c3v, x3, acc);
+  }
+  for (; q < qe; q += G) {
+    Acc c;
+    uint32_t j;
+    sym_entry<kMode>(S, q, c, j);
+    acc = fma(c, (Acc)xs[j - c0], acc);
+  }
+  for (int o = G / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(PR_FULL, acc, o);
+  return acc;
+}
+
+// An epilogue Epi provides: a Red type of per-thread reduction state (value-initialised),
+// bool skip() (the whole product is skipped, e.g. a converged solve), row(i, s, red) with
+// s = (S' x)_i, and finish(red), called by every thread of the block once its rows are done.
+
+template <int kMode, typename Acc, typename Tx, class Epi>
+__global__ void __launch_bounds__(256) k_spmv_rows(SymView S, const Tx* __restrict__ x, Epi epi) {
+  if (epi.skip()) return;
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  typename Epi::Red red{};
+  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < S.n; i += warps) {
+    const Acc sum = sym_row_acc<kMode, Acc>(S, i, x, lane);
+    if (lane == 0) epi.row(i, sum, red);
+  }
+  epi.finish(red);
+}
+
+constexpr int kBlkThreads = 1024;
+constexpr int kBlkSmemMax = 220 * 1024;  // dynamic shared memory of a blocked product
+
+// Stage g covers column blocks [g k, g k + k) (k = 2 for binary32 x, whose blocks are
+// half as many bytes), staged with 16-byte loads; groups of G lanes then take the CTA's
+// rows (32 / G rows in flight per warp: a row's segment of one stage is short).
+template <int kMode, typename Acc, typename Tx, class Epi>
+__global__ void __launch_bounds__(kBlkThreads, 1) k_spmv_blk(SymView S, BlkView B, const Tx* __restrict__ x, Epi epi) {
+  if (epi.skip()) return;
+  extern __shared__ __align__(16) unsigned char blk_smem[];
+  constexpr int k = sizeof(Tx) == 4 ? 2 : 1;
+  const int stage_cols = B.W * k;
+  Tx* xs = reinterpret_cast<Tx*>(blk_smem);
+  Acc* acc = reinterpret_cast<Acc*>(blk_smem + (size_t)stage_cols * sizeof(Tx));
+  constexpr int G = sizeof(Tx) == 4 ? 16 : 8;  // lanes per row segment
+  constexpr int kGroups = 32 / G;
+  const int64_t r0 = B.cta_row[blockIdx.x], r1 = B.cta_row[blockIdx.x + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int grp = lane / G, gl = lane % G;
+  const int stages = (B.nb + k - 1) / k;
+  for (int g = 0; g < stages; ++g) {
+    const int64_t c0 = (int64_t)g * stage_cols;
+    const int64_t cw = min((int64_t)stage_cols, S.n - c0);
+    {
+      // 16-byte loads when x + c0 is 16-byte aligned (W is a multiple of 64, so only the
+      // base of x decides), element loads otherwise
+      const int64_t vec = ((uintptr_t)(x + c0) & 15u) ? 0 : cw * (int64_t)sizeof(Tx) / 16;
+      const int4* src = reinterpret_cast<const int4*>(x + c0);
+      int4* dst = reinterpret_cast<int4*>(xs);
+      for (int64_t t = threadIdx.x; t < vec; t += blockDim.x) dst[t] = __ldg(src + t);
+      for (int64_t t = vec * 16 / (int64_t)sizeof(Tx) + threadIdx.x; t < cw; t += blockDim.x) xs[t] = __ldg(x + c0 + t);
+    }
+    __syncthreads();
+    const int b0 = g * k, b1 = min(B.nb, b0 + k);
+    for (int64_t base = r0 + (int64_t)warp * kGroups; base < r1; base += (int64_t)nwarps * kGroups) {
+      const int64_t i = base + grp;  // warp-uniform loop; a group past the end adds nothing
+      int64_t qb = 0, qe = 0;
+      if (i < r1) {
+        const int64_t rb = S.row_ptr[i];
+        qb = b0 == 0 ? rb : rb + B.seg[(int64_t)(b0 - 1) * S.n + i];
+        qe = b1 == B.nb ? S.row_ptr[i + 1] : rb + B.seg[(int64_t)(b1 - 1) * S.n + i];
+      }
+      const Acc part = seg_sum<kMode, G, Acc>(S, qb, qe, xs, (uint32_t)c0, gl);
+      if (gl == 0 && i < r1) acc[i - r0] = g == 0 ? part : acc[i - r0] + part;
+    }
+    __syncthreads();
+  }
+  typename Epi::Red red{};
+  for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+    const Acc a = acc[i - r0];
+    epi.row(i, kMode == kValues ? a : a * (Acc)S.factor, red);
+  }
+  epi.finish(red);
+}
+
+template <int kMode, typename Acc, typename Tx, class Epi>
+inline int allow_blk_smem() {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  PR_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev >= 0 && dev < 64 && done[dev]) return PR_OK;
+  PR_CUDA(cudaFuncSetAttribute(k_spmv_blk<kMode, Acc, Tx, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kBlkSmemMax));
+  if (dev >= 0 && dev < 64) done[dev] = true;
+  return PR_OK;
+}
+
+// Blocks of a product of S (the number of partial-sum slots its block reductions fill).
+inline int spmv_slots(const SymCsr& S) {
+  if (S.blk.ready) return S.blk.ctas;
+  return grid_for(S.n_rows * 32, 256, sm_count() * 8);
+}
+
+// One product of S with x (device vector of n entries) and the epilogue epi.
+template <int kMode, typename Acc, typename Tx, class Epi>
+inline int launch_spmv(const SymCsr& S, const Tx* x, const Epi& epi, cudaStream_t s) {
+  const SymView v = sym_view(S);
+  if (S.blk.ready && kMode != kValues) {
+    constexpr int k = sizeof(Tx) == 4 ? 2 : 1;
+    const size_t smem = (size_t)S.blk.W * k * sizeof(Tx) + (size_t)S.blk.rows_cap * sizeof(Acc);
+    if (smem > (size_t)kBlkSmemMax) {
+      set_error("blocked product needs %zu bytes of shared memory", smem);
+      return PR_ERR_LIMIT;
+    }
+    PR_TRY((allow_blk_smem<kMode, Acc, Tx, Epi>()));
+    ::pr::launch_mark(), k_spmv_blk<kMode, Acc, Tx, Epi><<<S.blk.ctas, kBlkThreads, smem, s>>>(v, blk_view(S), x, epi);
+  } else {
+    ::pr::launch_mark(), k_spmv_rows<kMode, Acc, Tx, Epi><<<spmv_slots(S), 256, 0, s>>>(v, x, epi);
+  }
+  PR_CUDA(cudaGetLastError());
+  return PR_OK;
+}
 
 }  // namespace pr

@@ -38,31 +38,35 @@ struct SeriesState {
   double tol_abs;   // rtol * max(sum|E|, tiny)
 };
 
-template <int kMode>
-__global__ void __launch_bounds__(256) k_series_step(SymView S, double delta, const double* __restrict__ area,
-                                                     const double* __restrict__ d, const double* __restrict__ eps,
-                                                     const double* __restrict__ v_in, double* __restrict__ v_out,
-                                                     double* __restrict__ absorbed, double* __restrict__ partial,
-                                                     const SeriesState* __restrict__ state) {
-  if (state->done) return;
-  const int lane = threadIdx.x & 31;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  double acc[2] = {0.0, 0.0};
-  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < S.n; i += warps) {
+// One reflection of the series on v = d (flight / A):  inc = d S v;  absorbed += eps inc;
+// flight = (1 - eps) inc;  v_out = d (flight / A);  block partials of |flight| and flight.
+struct SeriesEpi {
+  double delta;
+  const double* area;
+  const double* d;
+  const double* eps;
+  const double* v_in;
+  double* v_out;
+  double* absorbed;
+  double* partial;
+  const SeriesState* state;
+  struct Red {
+    double v[2] = {0.0, 0.0};
+  };
+  __device__ bool skip() const { return state->done != 0; }
+  __device__ void row(int64_t i, double sp, Red& r) const {
     const double Ai = area[i];
-    const double s = sym_row<kMode>(S, i, v_in, lane) + delta * Ai * v_in[i];
-    if (lane == 0) {
-      const double inc = d[i] * s;
-      const double e = eps[i];
-      absorbed[i] += e * inc;
-      const double fl = (1.0 - e) * inc;
-      v_out[i] = d[i] * (fl / Ai);
-      acc[0] += fabs(fl);
-      acc[1] += fl;
-    }
+    const double s = sp + delta * Ai * v_in[i];
+    const double inc = d[i] * s;
+    const double e = eps[i];
+    absorbed[i] += e * inc;
+    const double fl = (1.0 - e) * inc;
+    v_out[i] = d[i] * (fl / Ai);
+    r.v[0] += fabs(fl);
+    r.v[1] += fl;
   }
-  block_sum_store<2>(acc, partial);
-}
+  __device__ void finish(Red& r) const { block_sum_store<2>(r.v, partial); }
+};
 
 __global__ void k_series_finish(const double* __restrict__ partial, int blocks, long long max_it,
                                 SeriesState* __restrict__ state) {
@@ -108,14 +112,13 @@ __global__ void k_series_tol(const double* __restrict__ partial, int blocks, dou
 }
 
 static int red_blocks() { return sm_count() * 4; }
-static int spmv_blocks(int64_t rows) { return grid_for(rows * 32, 256, sm_count() * 8); }
 
 // FP64 reflection series on device vectors: emitted (n), eps (n) -> absorbed (n).
 int series_fp64(const pr_operator* op, const double* emitted, const double* eps, double rtol, int64_t max_it,
                 double* absorbed, double* residual, int64_t* iterations, cudaStream_t s) {
   const int64_t n = op->n;
   const int rb = red_blocks();
-  const int sb = spmv_blocks(n);
+  const int sb = spmv_slots(op->S);
   DevBuf<double> va, vb, partial;
   DevBuf<SeriesState> st;
   PR_TRY(va.alloc(n, s));
@@ -127,19 +130,18 @@ int series_fp64(const pr_operator* op, const double* emitted, const double* eps,
   PR_CUDA(cudaGetLastError());
   ::pr::launch_mark(), k_series_tol<<<1, 32, 0, s>>>(partial.ptr, rb, rtol, st.ptr);
   PR_CUDA(cudaGetLastError());
-  SymView S = sym_view(op->S);
   double* vin = va.ptr;
   double* vout = vb.ptr;
   SeriesState h;
   int batch = 4;
   for (int64_t launched = 0;;) {
     for (int b = 0; b < batch; ++b) {
+      const SeriesEpi epi{op->delta, op->area.ptr, op->scale.ptr, eps, vin, vout, absorbed, partial.ptr, st.ptr};
+      int rc = PR_OK;
       ::pr::timer_begin(kTimerSeries, s);
-      dispatch_mode(op->S.mode, [&](auto m) {
-        ::pr::launch_mark(), k_series_step<decltype(m)::value><<<sb, 256, 0, s>>>(
-            S, op->delta, op->area.ptr, op->scale.ptr, eps, vin, vout, absorbed, partial.ptr, st.ptr);
-      });
+      dispatch_mode(op->S.mode, [&](auto m) { rc = launch_spmv<decltype(m)::value, double>(op->S, vin, epi, s); });
       ::pr::timer_end(kTimerSeries, s);
+      PR_TRY(rc);
       ::pr::launch_mark(), k_series_finish<<<1, 32, 0, s>>>(partial.ptr, sb, (long long)max_it, st.ptr);
       std::swap(vin, vout);
     }
@@ -341,30 +343,33 @@ __global__ void __launch_bounds__(256) k_coarse(const int32_t* __restrict__ cfp,
 // One Chebyshev step on (I - om G) x = b in binary32 (Saad, Iterative Methods, Alg. 12.1):
 //   G d = scale * (S' u + delta A u), u = scale d / A;  x += d;  r -= (I - om G) d;
 //   d = c1 d + c2 r;  u_out = scale d / A.
-template <int kMode>
-__global__ void __launch_bounds__(256) k_cheb_step(SymView S, float delta, const float* __restrict__ scale,
-                                                   const float* __restrict__ area, const float* __restrict__ om,
-                                                   const float* __restrict__ u_in, float* __restrict__ u_out,
-                                                   float* __restrict__ x, float* __restrict__ r,
-                                                   float* __restrict__ d, float c1, float c2) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < S.n; i += warps) {
-    const float sum = sym_row32<kMode>(S, i, u_in, lane);
-    if (lane == 0) {
-      const float Ai = area[i], sc = scale[i];
-      const float gd = sc * (sum + delta * Ai * u_in[i]);
-      const float di = d[i];
-      const float ad = di - om[i] * gd;
-      x[i] += di;
-      const float ri = r[i] - ad;
-      r[i] = ri;
-      const float dn = c1 * di + c2 * ri;
-      d[i] = dn;
-      u_out[i] = sc * dn / Ai;
-    }
+struct ChebEpi {
+  float delta;
+  const float* scale;
+  const float* area;
+  const float* om;
+  const float* u_in;
+  float* u_out;
+  float* x;
+  float* r;
+  float* d;
+  float c1, c2;
+  struct Red {};
+  __device__ bool skip() const { return false; }
+  __device__ void row(int64_t i, float sum, Red&) const {
+    const float Ai = area[i], sc = scale[i];
+    const float gd = sc * (sum + delta * Ai * u_in[i]);
+    const float di = d[i];
+    const float ad = di - om[i] * gd;
+    x[i] += di;
+    const float ri = r[i] - ad;
+    r[i] = ri;
+    const float dn = c1 * di + c2 * ri;
+    d[i] = dn;
+    u_out[i] = sc * dn / Ai;
   }
-}
+  __device__ void finish(Red&) const {}
+};
 
 // J += x (when x != nullptr); u = scale J / A; also the binary32 copies of the coefficients.
 __global__ void k_refine_prep(double* __restrict__ J, const float* __restrict__ x, const double* __restrict__ scale,
@@ -381,35 +386,40 @@ __global__ void k_refine_prep(double* __restrict__ J, const float* __restrict__ 
 
 // Binary64 residual r = E - J + om G J, absorbed = eps G J; block partials of |r| and |E|;
 // binary32 start of the next correction solve: x = 0, r32 = d32 = r, u32 = scale r / A.
-template <int kMode>
-__global__ void __launch_bounds__(256) k_refine_residual(SymView S, double delta, const double* __restrict__ area,
-                                                         const double* __restrict__ scale,
-                                                         const double* __restrict__ eps, const double* __restrict__ E,
-                                                         const double* __restrict__ J, const double* __restrict__ u,
-                                                         double* __restrict__ absorbed, double* __restrict__ partial,
-                                                         float* __restrict__ x32, float* __restrict__ r32,
-                                                         float* __restrict__ d32, float* __restrict__ u32) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  double acc[2] = {0.0, 0.0};
-  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < S.n; i += warps) {
+struct RefineEpi {
+  double delta;
+  const double* area;
+  const double* scale;
+  const double* eps;
+  const double* E;
+  const double* J;
+  const double* u;
+  double* absorbed;
+  double* partial;
+  float* x32;
+  float* r32;
+  float* d32;
+  float* u32;
+  struct Red {
+    double v[2] = {0.0, 0.0};
+  };
+  __device__ bool skip() const { return false; }
+  __device__ void row(int64_t i, double sp, Red& red) const {
     const double Ai = area[i];
-    const double s = sym_row<kMode>(S, i, u, lane) + delta * Ai * u[i];
-    if (lane == 0) {
-      const double gj = scale[i] * s;
-      const double e = eps[i];
-      const double r = E[i] - J[i] + (1.0 - e) * gj;
-      absorbed[i] = e * gj;
-      acc[0] += fabs(r);
-      acc[1] += fabs(E[i]);
-      x32[i] = 0.0f;
-      r32[i] = (float)r;
-      d32[i] = (float)r;  // d0 = r0 / theta with theta = 1
-      u32[i] = (float)(scale[i] * (r / Ai));
-    }
+    const double s = sp + delta * Ai * u[i];
+    const double gj = scale[i] * s;
+    const double e = eps[i];
+    const double r = E[i] - J[i] + (1.0 - e) * gj;
+    absorbed[i] = e * gj;
+    red.v[0] += fabs(r);
+    red.v[1] += fabs(E[i]);
+    x32[i] = 0.0f;
+    r32[i] = (float)r;
+    d32[i] = (float)r;  // d0 = r0 / theta with theta = 1
+    u32[i] = (float)(scale[i] * (r / Ai));
   }
-  block_sum_store<2>(acc, partial);
-}
+  __device__ void finish(Red& red) const { block_sum_store<2>(red.v, partial); }
+};
 
 __global__ void k_to_f32(const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c,
                          int64_t n, float* __restrict__ fa, float* __restrict__ fb, float* __restrict__ fc) {
@@ -445,7 +455,7 @@ int series_mixed(const pr_operator* op, const double* emitted, const double* eps
   DevBuf<float> x32, r32, d32, ua, ub, sc32, ar32, om32;
   PR_TRY(J.alloc(n, s));
   PR_TRY(u.alloc(n, s));
-  const int sb = spmv_blocks(n);
+  const int sb = spmv_slots(op->S);
   PR_TRY(partial.alloc((size_t)2 * sb, s));
   PR_TRY(sums.alloc(2, s));
   PR_TRY(x32.alloc(n, s));
@@ -458,7 +468,6 @@ int series_mixed(const pr_operator* op, const double* emitted, const double* eps
   PR_TRY(om32.alloc(n, s));
   ::pr::launch_mark(), k_to_f32<<<grid_for(n, 256), 256, 0, s>>>(op->scale.ptr, op->area.ptr, eps, n, sc32.ptr, ar32.ptr, om32.ptr);
   PR_CUDA(cudaMemsetAsync(J.ptr, 0, n * 8, s));
-  SymView S = sym_view(op->S);
   const float c_delta = (float)op->delta;
   const double sigma1 = 1.0 / rho;  // theta / delta with theta = 1, delta = rho
   int outer = 0;
@@ -467,14 +476,15 @@ int series_mixed(const pr_operator* op, const double* emitted, const double* eps
   for (;;) {
     ::pr::launch_mark(), k_refine_prep<<<grid_for(n, 256), 256, 0, s>>>(J.ptr, outer > 0 ? x32.ptr : nullptr, op->scale.ptr,
                                                     op->area.ptr, n, u.ptr);
-    ::pr::timer_begin(kTimerRefine, s);
-    dispatch_mode(op->S.mode, [&](auto m) {
-      ::pr::launch_mark(), k_refine_residual<decltype(m)::value><<<sb, 256, 0, s>>>(
-          S, op->delta, op->area.ptr, op->scale.ptr, eps, emitted, J.ptr, u.ptr, absorbed, partial.ptr, x32.ptr,
-          r32.ptr, d32.ptr, ua.ptr);
-    });
-    ::pr::timer_end(kTimerRefine, s);
-    PR_CUDA(cudaGetLastError());
+    {
+      const RefineEpi epi{op->delta, op->area.ptr, op->scale.ptr, eps, emitted, J.ptr, u.ptr, absorbed,
+                          partial.ptr, x32.ptr, r32.ptr, d32.ptr, ua.ptr};
+      int rc = PR_OK;
+      ::pr::timer_begin(kTimerRefine, s);
+      dispatch_mode(op->S.mode, [&](auto m) { rc = launch_spmv<decltype(m)::value, double>(op->S, u.ptr, epi, s); });
+      ::pr::timer_end(kTimerRefine, s);
+      PR_TRY(rc);
+    }
     ++sp64;
     PR_TRY(sum_partials(partial.ptr, sb, 2, sums.ptr, s));
     double hs[2];
@@ -489,12 +499,12 @@ int series_mixed(const pr_operator* op, const double* emitted, const double* eps
     for (int k = 0; k < k_in; ++k) {
       const double rho_n = 1.0 / (2.0 * sigma1 - rho_k);
       const float c1 = (float)(rho_n * rho_k), c2 = (float)(2.0 * rho_n / rho);
+      const ChebEpi epi{c_delta, sc32.ptr, ar32.ptr, om32.ptr, uin, uout, x32.ptr, r32.ptr, d32.ptr, c1, c2};
+      int rc = PR_OK;
       ::pr::timer_begin(kTimerCheb, s);
-      dispatch_mode(op->S.mode, [&](auto m) {
-        ::pr::launch_mark(), k_cheb_step<decltype(m)::value><<<sb, 256, 0, s>>>(
-            S, c_delta, sc32.ptr, ar32.ptr, om32.ptr, uin, uout, x32.ptr, r32.ptr, d32.ptr, c1, c2);
-      });
+      dispatch_mode(op->S.mode, [&](auto m) { rc = launch_spmv<decltype(m)::value, float>(op->S, uin, epi, s); });
       ::pr::timer_end(kTimerCheb, s);
+      PR_TRY(rc);
       rho_k = rho_n;
       std::swap(uin, uout);
       ++sp32;
@@ -640,7 +650,7 @@ static int series_fp64_noalloc(const pr_operator* op, const double* emitted, con
     return PR_ERR_LIMIT;
   }
   const int rb = red_blocks();
-  const int sb = spmv_blocks(n);
+  const int sb = spmv_slots(op->S);
   if ((int64_t)2 * (sb > rb ? sb : rb) > kNoAllocPartials) {
     set_error("pr_reflection_series_noalloc: %d blocks exceed its partial-sum scratch", sb > rb ? sb : rb);
     return PR_ERR_LIMIT;
@@ -662,17 +672,16 @@ static int series_fp64_noalloc(const pr_operator* op, const double* emitted, con
   PR_CUDA(cudaGetLastError());
   ::pr::launch_mark(), k_series_tol<<<1, 32, 0, s>>>(partial, rb, rtol, st);
   PR_CUDA(cudaGetLastError());
-  SymView S = sym_view(op->S);
   double* vin = va;
   double* vout = vb;
   SeriesState h;
   int batch = 4;
   for (;;) {
     for (int b = 0; b < batch; ++b) {
-      dispatch_mode(op->S.mode, [&](auto m) {
-        ::pr::launch_mark(), k_series_step<decltype(m)::value><<<sb, 256, 0, s>>>(
-            S, op->delta, op->area.ptr, op->scale.ptr, eps, vin, vout, absorbed, partial, st);
-      });
+      const SeriesEpi epi{op->delta, op->area.ptr, op->scale.ptr, eps, vin, vout, absorbed, partial, st};
+      int rc = PR_OK;
+      dispatch_mode(op->S.mode, [&](auto m) { rc = launch_spmv<decltype(m)::value, double>(op->S, vin, epi, s); });
+      PR_TRY(rc);
       ::pr::launch_mark(), k_series_finish<<<1, 32, 0, s>>>(partial, sb, (long long)max_it, st);
       std::swap(vin, vout);
     }

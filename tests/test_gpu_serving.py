@@ -46,3 +46,27 @@ def test_results_same_alone_and_in_the_mix():
         assert m.closure_rel <= 1e-8
     slots_used = {f.result().slot for f in futs}
     assert len(slots_used) > 1
+
+
+def test_repeated_case_reuses_cached_device_memory():
+    """A repeated case takes every buffer from the library's cache and gives the same bits."""
+
+    import torch
+
+    from porerad_b200 import _lib, serving
+
+    req = _requests()[-1]
+    adm = serving.Admission(1 << 40)
+    first = serving.run_case(req, adm)
+    torch.cuda.synchronize()
+    before = _lib.memory_stats(torch.cuda.current_device())
+    again = serving.run_case(req, adm)
+    torch.cuda.synchronize()
+    after = _lib.memory_stats(torch.cuda.current_device())
+    assert after["device_mallocs"] == before["device_mallocs"]
+    assert after["cache_hits"] > before["cache_hits"]
+    assert after["live_bytes"] == before["live_bytes"]
+    assert (again.q_h, again.q_c, again.q_i) == (first.q_h, first.q_c, first.q_i)
+    assert np.array_equal(again.coarse_source, first.coarse_source)
+    _lib.release_cached_memory(torch.cuda.current_device())
+    assert _lib.memory_stats(torch.cuda.current_device())["cached_bytes"] == 0
