@@ -47,17 +47,16 @@ __global__ void k_cell_faces(const uint8_t* __restrict__ phases, int64_t nx, int
   }
 }
 
-// One 32-bit word per (row, w): bit b = solid[i, j, 32 w + b].
-__global__ void k_pack_occupancy(const uint8_t* __restrict__ solid, int64_t rows, int64_t nz, int wpr,
-                                 uint32_t* __restrict__ occ) {
-  const int64_t n = rows * wpr;
+// Bit c of the flat occupancy array = solid flag of cell c = (i ny + j) nz + k: word w holds
+// cells 32 w .. 32 w + 31, so a cell's occupancy bit and its cell_face_patch rows share the
+// one index.
+__global__ void k_pack_occupancy(const uint8_t* __restrict__ solid, int64_t n_cells, uint32_t* __restrict__ occ) {
+  const int64_t n = (n_cells + 31) / 32;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t row = t / wpr;
-    const int w = (int)(t % wpr);
     uint32_t word = 0;
     for (int b = 0; b < 32; ++b) {
-      const int64_t k = (int64_t)w * 32 + b;
-      if (k < nz && solid[row * nz + k]) word |= 1u << b;
+      const int64_t c = t * 32 + b;
+      if (c < n_cells && solid[c]) word |= 1u << b;
     }
     occ[t] = word;
   }
@@ -164,10 +163,8 @@ int case_build(pr_case* c, const uint8_t* phases, cudaStream_t s) {
   PR_TRY(off.alloc(n, s));
   ::pr::launch_mark(), k_cell_faces<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(ph.ptr, c->nx, c->ny, c->nz, c->solid.ptr, mask.ptr, nf.ptr);
   PR_CUDA(cudaGetLastError());
-  c->wpr = (int)((c->nz + 31) / 32);
-  const int64_t rows = c->nx * c->ny;
-  PR_TRY(c->occ.alloc(rows * c->wpr, s));
-  ::pr::launch_mark(), k_pack_occupancy<<<grid_for(rows * c->wpr, 256, 148 * 16), 256, 0, s>>>(c->solid.ptr, rows, c->nz, c->wpr, c->occ.ptr);
+  PR_TRY(c->occ.alloc((n + 31) / 32, s));
+  ::pr::launch_mark(), k_pack_occupancy<<<grid_for((n + 31) / 32, 256, 148 * 16), 256, 0, s>>>(c->solid.ptr, n, c->occ.ptr);
   PR_CUDA(cudaGetLastError());
 
   PR_TRY(nw.alloc(lat, s));

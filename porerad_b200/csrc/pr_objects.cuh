@@ -69,10 +69,9 @@ struct pr_case {
   int device = 0;
   int64_t nx = 0, ny = 0, nz = 0, n_cells = 0;
   int64_t n_patches = 0, n_wall = 0;
-  int wpr = 0;  // 32-bit occupancy words per (i, j) row
   double H = 0.0, area = 0.0;
   pr::DevBuf<uint8_t> solid;      // n_cells, 0/1
-  pr::DevBuf<uint32_t> occ;       // bit-packed solid flags, (nx*ny) rows of wpr words
+  pr::DevBuf<uint32_t> occ;       // bit-packed solid flags, bit c = cell c (flat)
   pr::DevBuf<int8_t> cls;         // patch class 0 hot, 1 cold, 2 internal
   pr::DevBuf<int8_t> face;        // patch face 0..5, -1 for walls
   pr::DevBuf<int8_t> code;        // emission normal: 0..5 as +x,-x,+y,-y,+z,-z

@@ -45,7 +45,7 @@ struct Geom {
   const int32_t* __restrict__ cfp;
   const int32_t* __restrict__ hot;
   const int32_t* __restrict__ cold;
-  int32_t nx, ny, nz, wpr;
+  int32_t nx, ny, nz;
   int64_t n_cells;
 };
 
@@ -183,8 +183,9 @@ __device__ int32_t dda_first_hit(const Geom& g, double ox, double oy, double oz,
       return i < 0 ? g.hot[wj * g.nz + wk] : g.cold[wj * g.nz + wk];
     }
     const int64_t row = i * g.ny + jj;
-    const uint32_t word = __ldg(g.occ + row * g.wpr + (kk >> 5));
-    if ((word >> (kk & 31)) & 1u) {
+    const int64_t cell = row * g.nz + kk;
+    const uint32_t word = __ldg(g.occ + (cell >> 5));
+    if ((word >> (cell & 31)) & 1u) {
       *steps = it + 1;
       return face >= 0 ? __ldg(g.cfp + (row * g.nz + kk) * 6 + face) : -1;
     }
@@ -287,7 +288,7 @@ struct WaveChunk {
   const pr_u128* state;  // per seed
   const pr_u128* inc;    // per seed
   int64_t n, np, p0, R, start, n_cells;
-  int32_t nx, ny, nz, wpr;
+  int32_t nx, ny, nz;
   double ny_d, nz_d;
 };
 
@@ -365,7 +366,7 @@ __device__ __forceinline__ int find_chunk(const WaveChunk* __restrict__ chunks, 
 // The pooled traversal over a table of chunks.  A warp works on one chunk at a time: when
 // its next work unit belongs to another chunk it stops generating, drains its lanes and
 // pool, flushes the chunk's step/failure counters (chunk_ctr[2 c], [2 c + 1]) and switches.
-template <int kMinBlocks, int kBurst>
+template <int kMinBlocks, int kBurst, int kLook>
 __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const WaveChunk* __restrict__ chunks,
                                                                         int n_chunks, int64_t total,
                                                                         int32_t* __restrict__ recv,
@@ -379,7 +380,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const Wa
   int64_t unit_next = 0, unit_end = 0;  // warp-uniform: the work unit being generated
   int unit_chunk = -1, cur = -1;        // warp-uniform: its chunk, and the chunk of the rays in flight
   const uint32_t* occ = nullptr;        // warp-uniform geometry of chunk cur
-  int nx = 0, ny = 0, nz = 0, wpr = 0;
+  int nx = 0, ny = 0, nz = 0;
   int head = 0, tail = 0;               // warp-uniform pool cursors
   bool more = true;                     // warp-uniform
   pr_u128 base_st{0, 0};
@@ -400,7 +401,6 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const Wa
       nx = chunks[cur].nx;
       ny = chunks[cur].ny;
       nz = chunks[cur].nz;
-      wpr = chunks[cur].wpr;
       base_s = -1;
     }
     // ---- generate one batch of 32 rays when the pool has room for it
@@ -508,59 +508,148 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const Wa
     head += min(__popc(idle), avail);
     __syncwarp();
     if (!more && head == tail && !__any_sync(PR_FULL, active)) break;
-    // ---- a burst of DDA steps (view_factors.py:225-255)
-#pragma unroll 1
-    for (int b = 0; b < kBurst; ++b) {
-      if (!active) continue;
-      int32_t hit = -2;
-      if (it >= cap) {
-        hit = -1;
-      } else {
-        ++it;
-        if ((unsigned)i >= (unsigned)nx) {
-          // hit code of a wall: 6 n_cells + (0 hot | ny nz cold) + j nz + k
-          const int wj = (int)imod((int64_t)floor(pr_add(pool.eoy[lane], pr_mul(pool.edy[lane], t))), ny);
-          const int wk = (int)imod((int64_t)floor(pr_add(pool.eoz[lane], pr_mul(pool.edz[lane], t))), nz);
-          hit = 6 * nx * ny * nz + (i < 0 ? 0 : ny * nz) + wj * nz + wk;
+    // ---- DDA steps (view_factors.py:225-255), kBurst rounds per refill
+    if constexpr (kLook == 0) {
+  #pragma unroll 1
+      for (int b = 0; b < kBurst; ++b) {
+        if (!active) continue;
+        int32_t hit = -2;
+        if (it >= cap) {
+          hit = -1;
         } else {
-          const int row = i * ny + jj;
-          const uint32_t word = __ldg(occ + row * wpr + (kk >> 5));
-          if ((word >> (kk & 31)) & 1u) {
-            // hit code of a cell face: its cell_face_patch index
-            hit = face >= 0 ? (row * nz + kk) * 6 + face : -1;
+          ++it;
+          if ((unsigned)i >= (unsigned)nx) {
+            // hit code of a wall: 6 n_cells + (0 hot | ny nz cold) + j nz + k
+            const int wj = (int)imod((int64_t)floor(pr_add(pool.eoy[lane], pr_mul(pool.edy[lane], t))), ny);
+            const int wk = (int)imod((int64_t)floor(pr_add(pool.eoz[lane], pr_mul(pool.edz[lane], t))), nz);
+            hit = 6 * nx * ny * nz + (i < 0 ? 0 : ny * nz) + wj * nz + wk;
           } else {
-            double tn = tx;
-            if (ty < tn) tn = ty;
-            if (tz < tn) tn = tz;
-            const bool cx = fabs(pr_sub(tx, tn)) <= PR_TIE;
-            const bool cy = fabs(pr_sub(ty, tn)) <= PR_TIE;
-            const bool cz = fabs(pr_sub(tz, tn)) <= PR_TIE;
-            if (cx) {
-              i += sx;
-              tx = pr_add(tx, ddx);
-              face = sx > 0 ? 1 : 0;
+            const int row = i * ny + jj;
+            const int cell = row * nz + kk;
+            const uint32_t word = __ldg(occ + (cell >> 5));
+            if ((word >> (cell & 31)) & 1u) {
+              // hit code of a cell face: its cell_face_patch index
+              hit = face >= 0 ? cell * 6 + face : -1;
+            } else {
+              double tn = tx;
+              if (ty < tn) tn = ty;
+              if (tz < tn) tn = tz;
+              const bool cx = fabs(pr_sub(tx, tn)) <= PR_TIE;
+              const bool cy = fabs(pr_sub(ty, tn)) <= PR_TIE;
+              const bool cz = fabs(pr_sub(tz, tn)) <= PR_TIE;
+              if (cx) {
+                i += sx;
+                tx = pr_add(tx, ddx);
+                face = sx > 0 ? 1 : 0;
+              }
+              if (cy) {
+                jj += sy;
+                jj = jj == ny ? 0 : (jj < 0 ? ny - 1 : jj);
+                ty = pr_add(ty, ddy);
+                if (!cx) face = sy > 0 ? 3 : 2;
+              }
+              if (cz) {
+                kk += sz;
+                kk = kk == nz ? 0 : (kk < 0 ? nz - 1 : kk);
+                tz = pr_add(tz, ddz);
+                if (!cx && !cy) face = sz > 0 ? 5 : 4;
+              }
+              t = tn;
             }
-            if (cy) {
-              jj += sy;
-              jj = jj == ny ? 0 : (jj < 0 ? ny - 1 : jj);
-              ty = pr_add(ty, ddy);
-              if (!cx) face = sy > 0 ? 3 : 2;
-            }
-            if (cz) {
-              kk += sz;
-              kk = kk == nz ? 0 : (kk < 0 ? nz - 1 : kk);
-              tz = pr_add(tz, ddz);
-              if (!cx && !cy) face = sz > 0 ? 5 : 4;
-            }
-            t = tn;
           }
         }
+        if (hit != -2) {
+          recv[q] = hit;  // no load on this path: the RLE pass maps codes to patches
+          my_steps += it;
+          my_fail += hit < 0;
+          active = false;
+        }
       }
-      if (hit != -2) {
-        recv[q] = hit;  // no load on this path: the RLE pass maps codes to patches
-        my_steps += it;
-        my_fail += hit < 0;
-        active = false;
+    } else {
+      // Lookahead rounds: the DDA state advances through up to kLook cells without waiting
+      // for their occupancy (the arithmetic does not depend on it), recording each cell's
+      // occupancy bit and hit code; the kLook occupancy words are then loaded together and
+      // the first solid cell decides.  A wall or the step cap ends the round early.  Step
+      // counts and hit codes are those of the one-cell-at-a-time loop: cells are visited in
+      // the same order with the same arithmetic, and the state past a solid cell is dropped.
+#pragma unroll 1
+      for (int b = 0; b < kBurst; ++b) {
+        if (!active) continue;
+        int32_t cell[kLook], code[kLook];  // each recorded cell and its hit code
+        int m = 0;      // cells recorded
+        int stop = 0;   // 0 none, 1 wall at position m, 2 step cap at position m
+        int32_t wall_code = -1;
+#pragma unroll
+        for (int p = 0; p < kLook; ++p) {
+          cell[p] = 0;
+          code[p] = -1;
+          if (stop == 0 && m == p) {
+            if (it + p >= cap) {
+              stop = 2;
+            } else if ((unsigned)i >= (unsigned)nx) {
+              const int wj = (int)imod((int64_t)floor(pr_add(pool.eoy[lane], pr_mul(pool.edy[lane], t))), ny);
+              const int wk = (int)imod((int64_t)floor(pr_add(pool.eoz[lane], pr_mul(pool.edz[lane], t))), nz);
+              wall_code = 6 * nx * ny * nz + (i < 0 ? 0 : ny * nz) + wj * nz + wk;
+              stop = 1;
+            } else {
+              cell[p] = (i * ny + jj) * nz + kk;
+              code[p] = face >= 0 ? cell[p] * 6 + face : -1;
+              m = p + 1;
+              double tn = tx;
+              if (ty < tn) tn = ty;
+              if (tz < tn) tn = tz;
+              const bool cx = fabs(pr_sub(tx, tn)) <= PR_TIE;
+              const bool cy = fabs(pr_sub(ty, tn)) <= PR_TIE;
+              const bool cz = fabs(pr_sub(tz, tn)) <= PR_TIE;
+              if (cx) {
+                i += sx;
+                tx = pr_add(tx, ddx);
+                face = sx > 0 ? 1 : 0;
+              }
+              if (cy) {
+                jj += sy;
+                jj = jj == ny ? 0 : (jj < 0 ? ny - 1 : jj);
+                ty = pr_add(ty, ddy);
+                if (!cx) face = sy > 0 ? 3 : 2;
+              }
+              if (cz) {
+                kk += sz;
+                kk = kk == nz ? 0 : (kk < 0 ? nz - 1 : kk);
+                tz = pr_add(tz, ddz);
+                if (!cx && !cy) face = sz > 0 ? 5 : 4;
+              }
+              t = tn;
+            }
+          }
+        }
+        uint32_t word[kLook];
+#pragma unroll
+        for (int p = 0; p < kLook; ++p) word[p] = p < m ? __ldg(occ + (cell[p] >> 5)) : 0u;
+        int32_t hit = -2;
+        int used = m;
+#pragma unroll
+        for (int p = kLook - 1; p >= 0; --p) {
+          if (p < m && ((word[p] >> (cell[p] & 31)) & 1u)) {
+            hit = code[p];  // the cell_face_patch index
+            used = p + 1;
+          }
+        }
+        if (hit == -2) {
+          if (stop == 1) {
+            hit = wall_code;
+            used = m + 1;
+          } else if (stop == 2) {
+            hit = -1;
+            used = m;
+          }
+        }
+        it += used;
+        if (hit != -2) {
+          recv[q] = hit;
+          my_steps += it;
+          my_fail += hit < 0;
+          active = false;
+        }
       }
     }
   }
@@ -774,7 +863,6 @@ static Geom geom_of(const pr_case* c) {
   g.nx = (int32_t)c->nx;
   g.ny = (int32_t)c->ny;
   g.nz = (int32_t)c->nz;
-  g.wpr = c->wpr;
   g.n_cells = c->n_cells;
   return g;
 }
@@ -793,21 +881,26 @@ static RaySrc src_of(const pr_case* c, const SeedTables& t) {
 
 static int trace_grid() { return sm_count() * 8; }
 
-// Variants of the pooled traversal (minimum resident blocks per SM x DDA steps per burst).
-// Every variant writes the same receivers; the autotuner below picks the fastest per
-// problem class by timing them on the first chunk of the first call.
+// Variants of the pooled traversal: minimum resident blocks per SM (the register budget),
+// rounds between lane refills, and cells of occupancy lookahead per round (lookN: N
+// occupancy loads in flight per lane; burst: one cell per round).  Every variant writes the
+// same receivers; the autotuner below picks the fastest per problem class by timing them
+// on the first wave of the first call.
 using TraceKernel = void (*)(const WaveChunk*, int, int64_t, int32_t*, unsigned long long*, unsigned long long*);
 struct TraceVariant {
   TraceKernel kernel;
   const char* name;
 };
 static const TraceVariant kVariants[] = {
-    {k_trace_pool<5, 4>, "5blk-burst4"},
-    {k_trace_pool<5, 8>, "5blk-burst8"},
-    {k_trace_pool<5, 2>, "5blk-burst2"},
-    {k_trace_pool<6, 4>, "6blk-burst4"},
-    {k_trace_pool<8, 4>, "8blk-burst4"},
-    {k_trace_pool<4, 4>, "4blk-burst4"},
+    {k_trace_pool<6, 4, 2>, "6blk-look2x4"},
+    {k_trace_pool<6, 2, 3>, "6blk-look3x2"},
+    {k_trace_pool<6, 2, 4>, "6blk-look4x2"},
+    {k_trace_pool<6, 6, 2>, "6blk-look2x6"},
+    {k_trace_pool<5, 4, 3>, "5blk-look3x4"},
+    {k_trace_pool<7, 4, 2>, "7blk-look2x4"},
+    {k_trace_pool<4, 4, 2>, "4blk-look2x4"},
+    {k_trace_pool<5, 8, 0>, "5blk-burst8"},
+    {k_trace_pool<6, 4, 0>, "6blk-burst4"},
 };
 static constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 
@@ -1025,6 +1118,7 @@ int counts_batch(const pr_case* const* cases, int nc, int64_t R, const pr_pcg64*
   for (int c = 0; c < nc; ++c) {
     PR_ARG(cases[c] != nullptr, "case %d is NULL", c);
     PR_ARG(cases[c]->device == dev0, "case %d lives on another device", c);
+    // int32 hit codes (and cell indices)
     if (6 * cases[c]->n_cells + 2 * cases[c]->ny * cases[c]->nz > (int64_t)INT32_MAX) {
       set_error("case %d: %lld cells exceed the int32 hit codes of the traversal", c, (long long)cases[c]->n_cells);
       return PR_ERR_LIMIT;
@@ -1121,7 +1215,6 @@ int counts_batch(const pr_case* const* cases, int nc, int64_t R, const pr_pcg64*
       W.nx = (int32_t)c->nx;
       W.ny = (int32_t)c->ny;
       W.nz = (int32_t)c->nz;
-      W.wpr = c->wpr;
       W.ny_d = (double)c->ny;
       W.nz_d = (double)c->nz;
       hr[k] = RleChunk{recv.ptr + start, c->ftab.ptr, ctr.ptr + 2 * (w0 + k) + 1, ch.np, patch0, ray0};
