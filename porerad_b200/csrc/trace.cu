@@ -753,6 +753,122 @@ __global__ void __launch_bounds__(512) k_patch_rle(const RleChunk* __restrict__ 
   }
 }
 
+// The same reduction with one warp per origin patch, for Lpad = 32 K <= 1024: the patch's
+// keys sit in registers, element e = r * 32 + lane in register r of lane `lane`, and are
+// sorted by the bitonic network (partners e ^ j: across lanes by shuffles for j < 32,
+// across registers for j >= 32); run heads and tails come from neighbour shuffles and
+// ballots, head positions go through the warp's shared row, and every tail writes its
+// (receiver, count).  Output layout as k_patch_rle.
+template <int K>
+__global__ void __launch_bounds__(128) k_patch_rle_warp(const RleChunk* __restrict__ rc, int n_chunks,
+                                                        int64_t total_patches, int L, int R,
+                                                        int32_t* __restrict__ st_col, int32_t* __restrict__ st_cnt,
+                                                        int32_t* __restrict__ nnz) {
+  constexpr int N = 32 * K;
+  __shared__ int32_t heads[4][N];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t gp = blockIdx.x * (int64_t)(blockDim.x >> 5) + wid; gp < total_patches; gp += warps) {
+    int c = 0;
+    {
+      int lo = 0, hi = n_chunks - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (rc[mid].patch0 <= gp) lo = mid;
+        else hi = mid - 1;
+      }
+      c = lo;
+    }
+    const int64_t p = gp - rc[c].patch0, np = rc[c].np;
+    const int32_t* recv = rc[c].recv;
+    const int32_t* ftab = rc[c].ftab;
+    int32_t x[K];
+    int bad = 0;
+#pragma unroll
+    for (int r = 0; r < K; ++r) {
+      const int e = r * 32 + lane;
+      int32_t v = INT32_MAX;
+      if (e < L) {
+        const int sd = e / R;
+        const int32_t code = recv[((int64_t)sd * np + p) * R + (e - sd * R)];
+        v = code >= 0 ? __ldg(ftab + code) : -1;
+        bad += code >= 0 && v < 0;  // a face without a patch
+      }
+      x[r] = v;
+    }
+    if (bad) atomicAdd(rc[c].fail, (unsigned long long)bad);
+    // bitonic sort, ascending
+#pragma unroll
+    for (int k = 2; k <= N; k <<= 1) {
+#pragma unroll
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        if (j >= 32) {
+          const int jr = j >> 5;
+#pragma unroll
+          for (int r = 0; r < K; ++r) {
+            if ((r & jr) == 0) {
+              const bool up = ((r * 32) & k) == 0;  // k >= 64 here: bit of r
+              const int32_t a = x[r], b = x[r | jr];
+              const bool sw = up ? (a > b) : (a < b);
+              x[r] = sw ? b : a;
+              x[r | jr] = sw ? a : b;
+            }
+          }
+        } else {
+          const bool lower = (lane & j) == 0;
+#pragma unroll
+          for (int r = 0; r < K; ++r) {
+            const bool up = (k < 32 ? (lane & k) : ((r * 32) & k)) == 0;
+            const int32_t y = __shfl_xor_sync(PR_FULL, x[r], j);
+            const int32_t lo_v = min(x[r], y), hi_v = max(x[r], y);
+            x[r] = (lower == up) ? lo_v : hi_v;
+          }
+        }
+      }
+    }
+    // run heads (key differs from its predecessor) and tails (differs from its successor)
+    int32_t* hrow = heads[wid];
+    int base = 0;
+#pragma unroll
+    for (int r = 0; r < K; ++r) {
+      const int e = r * 32 + lane;
+      int32_t prev = __shfl_up_sync(PR_FULL, x[r], 1);
+      const int32_t last_prev = __shfl_sync(PR_FULL, x[r > 0 ? r - 1 : 0], 31);
+      if (lane == 0) prev = last_prev;
+      const bool head = e < L && (e == 0 || x[r] != prev);
+      const unsigned hb = __ballot_sync(PR_FULL, head);
+      if (head) hrow[base + __popc(hb & lt)] = e;
+      base += __popc(hb);
+    }
+    __syncwarp();
+    int32_t* oc = st_col + rc[c].ray0 + p * L;
+    int32_t* on = st_cnt + rc[c].ray0 + p * L;
+    int runs = 0;  // heads at positions < e
+#pragma unroll
+    for (int r = 0; r < K; ++r) {
+      const int e = r * 32 + lane;
+      int32_t prev = __shfl_up_sync(PR_FULL, x[r], 1);
+      const int32_t last_prev = __shfl_sync(PR_FULL, x[r > 0 ? r - 1 : 0], 31);
+      if (lane == 0) prev = last_prev;
+      int32_t next = __shfl_down_sync(PR_FULL, x[r], 1);
+      const int32_t first_next = __shfl_sync(PR_FULL, x[r + 1 < K ? r + 1 : r], 0);
+      if (lane == 31) next = first_next;
+      const bool head = e < L && (e == 0 || x[r] != prev);
+      const bool tail = e < L && (e == L - 1 || x[r] != next);
+      const unsigned hb = __ballot_sync(PR_FULL, head);
+      const int run = runs + __popc(hb & lt) + (head ? 1 : 0) - 1;  // run index of element e
+      if (tail) {
+        oc[run] = x[r];
+        on[run] = e - hrow[run] + 1;
+      }
+      runs += __popc(hb);
+    }
+    if (lane == 0) nnz[gp] = base;
+    __syncwarp();
+  }
+}
+
 // Copy each row's unique pairs from the stage to its CSR position (warp per row).
 __global__ void k_compact_rows(const int32_t* __restrict__ st_col, const int32_t* __restrict__ st_cnt,
                                const int32_t* __restrict__ nnz, const int64_t* __restrict__ off, int64_t np,
@@ -1237,6 +1353,12 @@ int counts_batch(const pr_case* const* cases, int nc, int64_t R, const pr_pcg64*
     ::pr::timer_end(kTimerTrace, s);
     const int rle_grid = (int)std::min<int64_t>(patch0, (int64_t)sm_count() * 16);
     ::pr::timer_begin(kTimerRle, s);
+    if (Lpad <= 1024) {
+      const int wg = (int)std::min<int64_t>((patch0 + 3) / 4, (int64_t)sm_count() * 32);
+      auto kern = Lpad <= 64 ? k_patch_rle_warp<2> : Lpad <= 128 ? k_patch_rle_warp<4>
+                : Lpad <= 256 ? k_patch_rle_warp<8> : Lpad <= 512 ? k_patch_rle_warp<16> : k_patch_rle_warp<32>;
+      ::pr::launch_mark(), kern<<<wg, 128, 0, s>>>(drle.ptr, nw, patch0, L, (int)R, st_col.ptr, st_cnt.ptr, nnz.ptr);
+    } else
     ::pr::launch_mark(), k_patch_rle<<<rle_grid, rle_threads, smem, s>>>(drle.ptr, nw, patch0, L, (int)R, Lpad,
                                                                      st_col.ptr, st_cnt.ptr, nnz.ptr);
     ::pr::timer_end(kTimerRle, s);

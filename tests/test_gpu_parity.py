@@ -376,3 +376,19 @@ def test_batched_counts_equal_single_case_counts():
     for g, (h, st) in zip(got, want):
         assert g.sha256() == h
         assert g.dda_steps == st
+
+
+@pytest.mark.parametrize("R,seeds", [(20, [5]), (64, [6]), (100, [7]), (250, [8]), (700, [9]), (1000, [10]),
+                                     (300, [11, 12, 13]), (1100, [14])])
+def test_per_patch_reduction_against_oracle(oracle, R, seeds):
+    """Counts of every per-patch reduction width (32 to 1024 keys, several seeds, beyond 1024)."""
+
+    vf = _vf()
+    case = load_small("box12")
+    p = _patches(case)
+    po = oracle.build_surface_patches(case["phases"], float(case["H_m"]))
+    tables = [oracle.first_hit_counts(po, R, s) for s in seeds]
+    want = oracle.pool_counts(tables, po.n_patches) if len(seeds) > 1 else tables[0]
+    got = vf.first_hit_counts_pooled(p, R, seeds).to_numpy()
+    for g, w in zip(got, want):
+        assert np.array_equal(np.asarray(g), np.asarray(w))
