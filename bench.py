@@ -123,6 +123,8 @@ def served_step(phases, cfg, seeds, precision="mixed"):
     ch = coupled.prescribed_field_channels(op, p, cfg["T_m"], cfg["dT"], cfg["eps"], precision=precision)
     out["final"] = ch
     out["nnz_symmetric"] = op.nnz_symmetric
+    # products of every operator of the step: (entries of S', products made) for the roofline
+    out["products"] = [(o.nnz_symmetric, o.spmv_calls) for o in ops + [op]]
     out["balance"] = (op.balance_method, op.balance_iterations, op.row_sum_error)
     out["_keep"] = (geo, p, tables, pooled, op, ops)
     return out
@@ -392,12 +394,16 @@ def run_ours(args, cfg):
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
                 "share_of_step": t_tr / ms}
         spmv = {}
+        # entries of the operator of an average product: every operator of the step (sets A, B and
+        # the pooled one) is balanced and solved, each with its own number of entries
+        prods = last["products"]
+        nnz_avg = sum(z * c for z, c in prods) / max(sum(c for _, c in prods), 1)
         for name in ("balance", "series", "cheb", "refine"):
             n_k, t_k = timers[name]
             if n_k == 0:
                 continue
             # packed 4-byte words per entry, row offsets, and the P-vectors each kernel streams
-            bytes_per = nnz_s * 4 + P * (8 + 5 * (8 if name != "cheb" else 4))
+            bytes_per = nnz_avg * 4 + P * (8 + 5 * (8 if name != "cheb" else 4))
             spmv[name] = {"launches": n_k, "ms": t_k, "GB_per_s": bytes_per * n_k / (t_k * 1e-3) / 1e9}
         tot_b = sum(v["GB_per_s"] * v["ms"] for v in spmv.values())
         tot_t = sum(v["ms"] for v in spmv.values())
@@ -414,7 +420,8 @@ def run_ours(args, cfg):
             "vs_baseline": None, "dtype": "f64 (traversal), f32+f64 (radiosity)", "data": "synthetic",
             "config": {"workload": cfg["workload"], "archetype": cfg["arch"], "N": cfg["n"], "phi": cfg["phi"],
                        "rays_per_patch": cfg["rays"], "ray_sets": len(seeds), "n_patches": P,
-                       "pairs_pooled": last["nnz"], "nnz_symmetric": nnz_s, "parallelism": f"replicas x{world}",
+                       "pairs_pooled": last["nnz"], "nnz_symmetric": nnz_s,
+                       "nnz_symmetric_per_product": round(nnz_avg), "parallelism": f"replicas x{world}",
                        "l2": "256 MiB flush write before every timed step; CSR working set > L2"},
             "cases_per_s": world * args.steps / (t_max * 1e-3),
             "e2e": {"value": e2e_rays * world / e2e_s, "unit": "rays/s", "h2d_bytes_per_step": h2d,
