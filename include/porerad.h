@@ -78,6 +78,7 @@ typedef struct {
 typedef struct pr_case pr_case;         /* one x-oriented voxel geometry on one GPU */
 typedef struct pr_counts pr_counts;     /* pooled first-hit counts, CSR by origin   */
 typedef struct pr_operator pr_operator; /* projected view-factor operator F_p       */
+typedef struct pr_conduction pr_conduction; /* finite-volume conduction system A, b    */
 
 PR_API const char* pr_last_error(void);
 PR_API int pr_version(void);
@@ -232,6 +233,63 @@ PR_API int pr_cell_field_channels(const pr_case* c, const pr_operator* op, const
                                   double reference_temperature_K, int precision,
                                   double relative_tolerance, double* q, double* coarse, double* stats,
                                   void* stream);
+
+/* ---- conduction and the coupled solve (porerad/conduction.py, porerad/coupled.py) ---
+ * Replaces assemble_conduction(conductivity_x, H_m), conduction.py:53-92: the
+ * cell-centred finite-volume system of a conductivity field (nx*ny*nz f64, x-oriented).
+ * A is held as the conductance of every cell's +x, +y, +z face (harmonic mean x dx; y, z
+ * periodic; 0 on the last +x face), its diagonal and the wall responses 2 k dx. */
+PR_API int pr_conduction_create(const double* conductivity, int64_t nx, int64_t ny, int64_t nz, double H_m,
+                                void* stream, pr_conduction** out);
+PR_API void pr_conduction_destroy(pr_conduction* conduction);
+/* The stored arrays (any may be NULL): face conductances gx, gy, gz, diagonal, hot_rhs,
+ * cold_rhs (ConductionSystem.hot_rhs / cold_rhs, conduction.py:25-35). */
+PR_API int pr_conduction_arrays(const pr_conduction* conduction, double* gx, double* gy, double* gz, double* diag,
+                                double* hot_rhs, double* cold_rhs, void* stream);
+/* y = A x (ConductionSystem.matrix @ x). */
+PR_API int pr_conduction_apply(const pr_conduction* conduction, const double* x, double* y, void* stream);
+/* Replaces solve_conduction(system, T_hot_K, T_cold_K, rtol=), conduction.py:95-120:
+ * Jacobi-PCG from the linear profile; PR_ERR_SERIES ("conduction solve did not
+ * converge") unless ||A T - b|| <= 1e-9 ||b||. */
+PR_API int pr_conduction_solve(const pr_conduction* conduction, double T_hot_K, double T_cold_K, double rtol,
+                               double* T_out, int64_t* iterations, double* relative_residual, void* stream);
+/* Replaces ConductionSystem.wall_fluxes, conduction.py:43-50. */
+PR_API int pr_conduction_wall_fluxes(const pr_conduction* conduction, const double* T, double T_hot_K,
+                                     double T_cold_K, double* q_hot, double* q_cold, void* stream);
+
+#define PR_COUPLED_MAX_LINEAR 16
+enum {
+  PR_COUPLED_OK = 0,
+  PR_COUPLED_LINEAR = 1,       /* "linear solve did not converge" */
+  PR_COUPLED_LINE_SEARCH = 2,  /* "line search failed" */
+  PR_COUPLED_MAX_NEWTON = 3    /* "maximum Newton iterations reached" */
+};
+typedef struct {
+  int converged, gmres_iterations;
+  double rhs_l2_W, true_residual_l2_W, true_residual_relative;
+} pr_coupled_linear;
+/* CoupledResult (coupled.py:314-337) of the returned attempt and the quantities of
+ * wall_flux_metrics (coupled.py:443-472). */
+typedef struct {
+  int converged, newton_iterations, preconditioner_steps, failure, linear_residuals_pass, n_linear;
+  pr_coupled_linear linear[PR_COUPLED_MAX_LINEAR];
+  double final_residual_inf_W;
+  double q_cond_hot_W_m2, q_rad_hot_W_m2, q_total_hot_W_m2, q_cond_cold_W_m2, q_rad_cold_W_m2, q_total_cold_W_m2;
+  double radiative_fraction_hot, k_eff_apparent_W_mK, wall_flux_mismatch_rel, energy_residual_rel;
+  double global_energy_residual_W, residual_power_W, T_min_K, T_max_K;
+  int64_t temperature_bound_violations, series_iterations;
+} pr_coupled_result;
+/* Replaces solve_coupled(system, operator, patches, T_hot_K, T_cold_K, epsilon, T_initial),
+ * coupled.py:423-440 (preconditioner_steps = 0: 10 steps, then 20 from the same field when
+ * needed), or newton_krylov(..., preconditioner_steps), coupled.py:340-421, with
+ * preconditioner_steps > 0.  Outputs (any may be NULL): the cell field (nx*ny*nz), the
+ * final state's patch temperature, emitted and absorbed power (n_patches) and cell net
+ * power (nx*ny*nz). */
+PR_API int pr_coupled_solve(const pr_case* c, const pr_operator* op, const pr_conduction* conduction,
+                            double T_hot_K, double T_cold_K, double epsilon, const double* T_initial,
+                            int preconditioner_steps, double* T_out, double* patch_temperature,
+                            double* patch_emitted, double* patch_absorbed, double* cell_net_power,
+                            pr_coupled_result* result, void* stream);
 
 /* ---- instrumentation (no counterpart in the reference) ----------------------------
  * Kernel classes timed with CUDA events on their launching stream while enabled:

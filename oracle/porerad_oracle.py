@@ -5,7 +5,8 @@ used as the checker by ``tests/``, by ``__graft_entry__.smoke()`` and by the CPU
 leg of ``bench.py``.  The product (``porerad_b200``) never imports this module: its path
 runs on the GPU and fails loudly when the CUDA library is missing.
 
-Every function names the reference lines it restates.  The traversal itself is the C
+Every function names the reference lines it restates (porerad/view_factors.py,
+porerad/exchange.py, porerad/coupled.py, porerad/conduction.py).  The traversal itself is the C
 file ``oracle/dda.c`` (an OpenMP loop over rays, like the reference's Numba ``prange``);
 the rest is NumPy/SciPy.  Third-party arithmetic on the path is used exactly as the
 reference uses it: ``numpy.random.PCG64`` + ``Generator.random`` for the ray stream,
@@ -508,6 +509,280 @@ def ab_differences(set_a, set_b):  # coupled.py:201-213
 
 def append_required(channel_difference, source_difference):  # coupled.py:216-219
     return channel_difference > 0.01 or source_difference > 0.05
+
+
+# --------------------------------------------------------------------------- conduction (conduction.py)
+
+K_SOLID = 0.20  # porerad/constants.py:8
+K_GAS = 0.026   # porerad/constants.py:11
+
+
+def assemble_conduction(conductivity_x, H_m):
+    """conduction.py:53-92: face conductance 2 k1 k2 / (k1 + k2 + 1e-30) * dx^2 / dx between
+    neighbours (x open, y and z periodic), 2 k dx to the walls; A as a SciPy CSR matrix."""
+
+    from scipy.sparse import coo_matrix
+
+    k = np.ascontiguousarray(conductivity_x, dtype=np.float64)
+    nx, ny, nz = k.shape
+    dx = float(H_m) / nx
+    idx = np.arange(k.size, dtype=np.int64).reshape(k.shape)
+    diag = np.zeros(k.size)
+    rows, cols, vals = [], [], []
+    faces = [(idx[:-1], idx[1:], k[:-1], k[1:]),
+             (idx[:, :-1], idx[:, 1:], k[:, :-1], k[:, 1:]), (idx[:, -1], idx[:, 0], k[:, -1], k[:, 0]),
+             (idx[:, :, :-1], idx[:, :, 1:], k[:, :, :-1], k[:, :, 1:]),
+             (idx[:, :, -1], idx[:, :, 0], k[:, :, -1], k[:, :, 0])]
+    for lo, hi, klo, khi in faces:
+        g = (2.0 * klo * khi / (klo + khi + 1.0e-30) * (dx * dx) / dx).ravel()
+        lo, hi = lo.ravel(), hi.ravel()
+        diag[lo] += g
+        diag[hi] += g
+        rows += [lo, hi]
+        cols += [hi, lo]
+        vals += [-g, -g]
+    hot = np.zeros(k.size)
+    cold = np.zeros(k.size)
+    hot.reshape(k.shape)[0] = 2.0 * k[0] * (dx * dx / dx)
+    cold.reshape(k.shape)[-1] = 2.0 * k[-1] * (dx * dx / dx)
+    diag += hot + cold
+    rows.append(idx.ravel())
+    cols.append(idx.ravel())
+    vals.append(diag)
+    A = coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                   shape=(k.size, k.size)).tocsc().tocsr()
+    A.sum_duplicates()
+    A.sort_indices()
+    return types.SimpleNamespace(matrix=A, hot_rhs=hot, cold_rhs=cold, conductivity=k, H_m=float(H_m),
+                                 shape=k.shape)
+
+
+def boundary_rhs(system, T_hot_K, T_cold_K):  # conduction.py:37-40
+    return system.hot_rhs * float(T_hot_K) + system.cold_rhs * float(T_cold_K)
+
+
+def solve_conduction(system, T_hot_K, T_cold_K, *, rtol=1.0e-11):
+    """conduction.py:95-120: Jacobi-PCG (SciPy cg) from the linear wall-to-wall profile."""
+
+    from scipy.sparse.linalg import LinearOperator, cg
+
+    A = system.matrix
+    b = boundary_rhs(system, T_hot_K, T_cold_K)
+    nx = system.shape[0]
+    line = float(T_hot_K) + (float(T_cold_K) - float(T_hot_K)) * ((np.arange(nx) + 0.5) / nx)
+    x0 = np.broadcast_to(line[:, None, None], system.shape).reshape(-1).copy()
+    inv = 1.0 / A.diagonal()
+    M = LinearOperator(A.shape, matvec=lambda v: inv * v, dtype=np.float64)
+    T, info = cg(A, b, x0=x0, rtol=float(rtol), atol=0.0, maxiter=max(50000, 20 * nx), M=M)
+    rel = float(np.linalg.norm(A @ T - b) / np.linalg.norm(b))
+    if info != 0 or rel > 1.0e-9:
+        raise RuntimeError(f"conduction solve did not converge: info={info}, residual={rel:.3e}")
+    return T.reshape(system.shape)
+
+
+def wall_fluxes(system, T, T_hot_K, T_cold_K):  # conduction.py:43-50
+    k = system.conductivity
+    T = np.asarray(T, dtype=np.float64).reshape(system.shape)
+    dx = system.H_m / k.shape[0]
+    return (float(np.mean(2.0 * k[0] * (float(T_hot_K) - T[0]) / dx)),
+            float(np.mean(2.0 * k[-1] * (T[-1] - float(T_cold_K)) / dx)))
+
+
+# --------------------------------------------------------------------------- coupled solve (coupled.py:222-490)
+
+def emission_diagonal(patches, T_cells, epsilon):  # coupled.py:65-73
+    inner = patches.patch_class == INTERNAL
+    owner = patches.patch_cell[inner].astype(np.int64)
+    T = np.asarray(T_cells, dtype=np.float64).ravel()[owner]
+    d = np.zeros(patches.solid.size)
+    np.add.at(d, owner, 4.0 * float(epsilon) * SIGMA * patches.patch_area_m2[inner] * T**3)
+    return d
+
+
+def _radiation(operator, patches, T_cells, T_hot_K, T_cold_K, epsilon, rtol):  # coupled.py:86-105
+    Tp = patch_temperature(patches, T_cells, T_hot_K, T_cold_K)
+    eps = np.full(patches.n_patches, float(epsilon))
+    rad = net_patch_power(operator, Tp, eps, patches.patch_area_m2, relative_tolerance=rtol)
+    return types.SimpleNamespace(patch_temperature_K=Tp, patch_net_power_W=rad.net_power_W,
+                                 cell_net_power_W=cell_power(patches, rad.net_power_W), radiosity=rad)
+
+
+def _radiation_jvp(operator, patches, T_patch, dT_cells, epsilon, rtol):  # coupled.py:108-126
+    inner = patches.patch_class == INTERNAL
+    dTp = np.zeros(patches.n_patches)
+    dTp[inner] = np.asarray(dT_cells, dtype=np.float64).ravel()[patches.patch_cell[inner]]
+    eps = np.full(patches.n_patches, float(epsilon))
+    return cell_power(patches, net_patch_power_jvp(operator, T_patch, dTp, eps, patches.patch_area_m2,
+                                                   relative_tolerance=rtol))
+
+
+def flexible_gmres(matvec, rhs, precondition, *, restart, max_iterations, relative_tolerance, absolute_tolerance):
+    """coupled.py:230-290: right-preconditioned flexible GMRES, modified Gram-Schmidt with one
+    reorthogonalisation, least squares on the Hessenberg, confirmed by the true residual."""
+
+    b = np.asarray(rhs, dtype=np.float64)
+    x = np.zeros_like(b)
+    bn = max(float(np.linalg.norm(b)), _TINY)
+    thr = max(float(absolute_tolerance), float(relative_tolerance) * bn)
+    eps = np.finfo(np.float64).eps
+    done = 0
+    while done < max_iterations:
+        r = b - matvec(x)
+        beta = float(np.linalg.norm(r))
+        if beta <= thr:
+            return x, True, done, beta / bn
+        m = min(restart, max_iterations - done)
+        V = np.zeros((m + 1, b.size))
+        Z = np.zeros((m, b.size))
+        H = np.zeros((m + 1, m))
+        g = np.zeros(m + 1)
+        V[0] = r / beta
+        g[0] = beta
+        restart_x = None
+        for j in range(m):
+            Z[j] = precondition(V[j])
+            w = matvec(Z[j])
+            for _ in range(2):
+                for i in range(j + 1):
+                    h = float(np.dot(V[i], w))
+                    H[i, j] += h
+                    w -= h * V[i]
+            nn = float(np.linalg.norm(w))
+            H[j + 1, j] = nn
+            if nn > eps * beta:
+                V[j + 1] = w / nn
+            y = np.linalg.lstsq(H[: j + 2, : j + 1], g[: j + 2], rcond=None)[0]
+            est = float(np.linalg.norm(g[: j + 2] - H[: j + 2, : j + 1] @ y))
+            done += 1
+            if est <= thr or nn <= eps * beta:
+                cand = x + y @ Z[: j + 1]
+                tn = float(np.linalg.norm(b - matvec(cand)))
+                if tn <= thr:
+                    return cand, True, done, tn / bn
+                restart_x = cand
+                break
+        if restart_x is not None:
+            x = restart_x
+            continue
+        x = x + np.linalg.lstsq(H, g, rcond=None)[0] @ Z
+    tn = float(np.linalg.norm(b - matvec(x)))
+    return x, tn <= thr, done, tn / bn
+
+
+def _fixed_pcg(A, shift, steps):  # coupled.py:293-320: fixed Jacobi-PCG steps on A + diag(shift) from x = 0
+    inv = 1.0 / (A.diagonal() + shift)
+
+    def apply(rhs):
+        x = np.zeros_like(rhs)
+        r = rhs.copy()
+        z = inv * r
+        p = z.copy()
+        rz = r @ z
+        for step in range(steps):
+            Ap = A @ p + shift * p
+            a = rz / (p @ Ap)
+            x += a * p
+            r -= a * Ap
+            z = inv * r
+            if step + 1 < steps:
+                rzn = r @ z
+                p = z + (rzn / rz) * p
+                rz = rzn
+        return x
+
+    return apply
+
+
+def newton_krylov(system, operator, patches, T_hot_K, T_cold_K, epsilon, T_initial, preconditioner_steps):
+    """coupled.py:340-421."""
+
+    A = system.matrix
+    b = boundary_rhs(system, T_hot_K, T_cold_K)
+    lo, hi = float(T_cold_K), float(T_hot_K)
+    M = _fixed_pcg(A, emission_diagonal(patches, T_initial, epsilon), int(preconditioner_steps))
+    T = np.asarray(T_initial, dtype=np.float64).copy()
+    state = _radiation(operator, patches, T, T_hot_K, T_cold_K, epsilon, 1.0e-8)
+    R = A @ T.ravel() - b - state.cell_net_power_W.ravel()
+    last = 0.0 if max(float(np.linalg.norm(R, np.inf)), _TINY) <= 1.0e-13 else np.inf
+    out = types.SimpleNamespace(converged=False, newton_iterations=0, linear_solves=[],
+                                preconditioner_steps=int(preconditioner_steps), failure="")
+
+    def finish(ok, failure=""):
+        final = _radiation(operator, patches, T, T_hot_K, T_cold_K, epsilon, RADIOSITY_RTOL_FINAL)
+        out.temperature_K, out.state, out.converged, out.failure = T, final, ok, failure
+        out.final_residual_inf_W = float(np.linalg.norm(A @ T.ravel() - b - final.cell_net_power_W.ravel(), np.inf))
+        return out
+
+    for _ in range(8):
+        rn = float(np.linalg.norm(R, np.inf))
+        if rn <= 1.0e-13 and last <= 1.0e-10:
+            return finish(True)
+        Tp = state.patch_temperature_K.copy()
+
+        def J(v):
+            return A @ v - _radiation_jvp(operator, patches, Tp, v.reshape(system.shape), epsilon, 1.0e-8).ravel()
+
+        step, ok, its, rel = flexible_gmres(J, -R, M, restart=30, max_iterations=90, relative_tolerance=1.0e-8,
+                                            absolute_tolerance=1.0e-13)
+        out.linear_solves.append(dict(converged=ok, gmres_iterations=its, rhs_l2_W=float(np.linalg.norm(R)),
+                                      true_residual_l2_W=float(np.linalg.norm(J(step) + R)),
+                                      true_residual_relative=rel))
+        if not ok:
+            return finish(False, "linear solve did not converge")
+        if rn <= 1.0e-13 and float(np.max(np.abs(step))) <= 1.0e-10:
+            return finish(True)
+        alpha, accepted = 1.0, False
+        while alpha >= 2.0**-20:
+            cand = T.ravel() + alpha * step
+            if np.all(np.isfinite(cand)) and float(np.min(cand)) >= lo and float(np.max(cand)) <= hi:
+                trial = cand.reshape(system.shape)
+                ts = _radiation(operator, patches, trial, T_hot_K, T_cold_K, epsilon, 1.0e-8)
+                tr = A @ cand - b - ts.cell_net_power_W.ravel()
+                tn = float(np.linalg.norm(tr, np.inf))
+                if tn <= (1.0 - 1.0e-4 * alpha) * rn:
+                    accepted = True
+                    break
+            alpha *= 0.5
+        if not accepted:
+            return finish(False, "line search failed")
+        last = float(np.max(np.abs(trial - T)))
+        T, state, R = trial, ts, tr
+        out.newton_iterations += 1
+        if tn <= 1.0e-13 and last <= 1.0e-10:
+            return finish(True)
+    return finish(False, "maximum Newton iterations reached")
+
+
+def linear_residuals_pass(result):  # coupled.py:333-337
+    return bool(result.linear_solves) and all(
+        s["converged"] and s["true_residual_l2_W"] <= max(1.0e-13, 1.0e-8 * s["rhs_l2_W"]) for s in result.linear_solves)
+
+
+def solve_coupled(system, operator, patches, T_hot_K, T_cold_K, epsilon, T_initial):  # coupled.py:423-440
+    for steps in (10, 20):
+        res = newton_krylov(system, operator, patches, T_hot_K, T_cold_K, epsilon, T_initial, steps)
+        if res.converged and linear_residuals_pass(res):
+            break
+    return res
+
+
+def wall_flux_metrics(system, patches, result, T_hot_K, T_cold_K):  # coupled.py:443-472
+    qch, qcc = wall_fluxes(system, result.temperature_K, T_hot_K, T_cold_K)
+    area = cross_section_area(patches)
+    net = result.state.patch_net_power_W
+    qrh = -float(np.sum(net[patches.patch_class == HOT])) / area
+    qrc = float(np.sum(net[patches.patch_class == COLD])) / area
+    th, tc = qch + qrh, qcc + qrc
+    scale = max(abs(th), abs(tc), _TINY)
+    T = result.temperature_K
+    rad = result.state.radiosity
+    return {"q_cond_hot_W_m2": qch, "q_rad_hot_W_m2": qrh, "q_total_hot_W_m2": th, "q_cond_cold_W_m2": qcc,
+            "q_rad_cold_W_m2": qrc, "q_total_cold_W_m2": tc, "radiative_fraction_hot": qrh / th,
+            "k_eff_apparent_W_mK": th * patches.H_m / (float(T_hot_K) - float(T_cold_K)),
+            "wall_flux_mismatch_rel": abs(th - tc) / scale,
+            "energy_residual_rel": abs(float(np.sum(rad.net_power_W) + rad.residual_power_W)) / max(scale * area, _TINY),
+            "T_min_K": float(np.min(T)), "T_max_K": float(np.max(T)),
+            "temperature_bound_violations": int(np.count_nonzero((T < float(T_cold_K)) | (T > float(T_hot_K))))}
 
 
 def pcg64_state(seed: int):

@@ -47,6 +47,31 @@ _i64 = ctypes.c_int64
 _i32 = ctypes.c_int
 _f64 = ctypes.c_double
 
+COUPLED_MAX_LINEAR = 16
+COUPLED_FAILURES = {0: "", 1: "linear solve did not converge", 2: "line search failed",
+                    3: "maximum Newton iterations reached"}
+
+
+class CoupledLinear(ctypes.Structure):
+    """pr_coupled_linear: one Newton correction's linear solve."""
+
+    _fields_ = [("converged", _i32), ("gmres_iterations", _i32), ("rhs_l2_W", _f64),
+                ("true_residual_l2_W", _f64), ("true_residual_relative", _f64)]
+
+
+class CoupledResultC(ctypes.Structure):
+    """pr_coupled_result: the returned attempt of a coupled solve and its wall-flux metrics."""
+
+    _fields_ = [("converged", _i32), ("newton_iterations", _i32), ("preconditioner_steps", _i32),
+                ("failure", _i32), ("linear_residuals_pass", _i32), ("n_linear", _i32),
+                ("linear", CoupledLinear * COUPLED_MAX_LINEAR), ("final_residual_inf_W", _f64),
+                ("q_cond_hot_W_m2", _f64), ("q_rad_hot_W_m2", _f64), ("q_total_hot_W_m2", _f64),
+                ("q_cond_cold_W_m2", _f64), ("q_rad_cold_W_m2", _f64), ("q_total_cold_W_m2", _f64),
+                ("radiative_fraction_hot", _f64), ("k_eff_apparent_W_mK", _f64), ("wall_flux_mismatch_rel", _f64),
+                ("energy_residual_rel", _f64), ("global_energy_residual_W", _f64), ("residual_power_W", _f64),
+                ("T_min_K", _f64), ("T_max_K", _f64), ("temperature_bound_violations", _i64),
+                ("series_iterations", _i64)]
+
 _SIGNATURES = {
     "pr_last_error": (ctypes.c_char_p, []),
     "pr_version": (_i32, []),
@@ -78,6 +103,14 @@ _SIGNATURES = {
     "pr_net_patch_power_jvp": (_i32, [_vp, _vp, _vp, _vp, _vp, _f64, _vp, _vp]),
     "pr_prescribed_field_channels": (_i32, [_vp, _vp, _f64, _f64, _f64, _i32, _f64, _vp, _vp, _vp, _vp]),
     "pr_cell_field_channels": (_i32, [_vp, _vp, _vp, _f64, _f64, _f64, _i32, _f64, _i32, _f64, _vp, _vp, _vp, _vp]),
+    "pr_conduction_create": (_i32, [_vp, _i64, _i64, _i64, _f64, _vp, ctypes.POINTER(_vp)]),
+    "pr_conduction_destroy": (None, [_vp]),
+    "pr_conduction_arrays": (_i32, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "pr_conduction_apply": (_i32, [_vp, _vp, _vp, _vp]),
+    "pr_conduction_solve": (_i32, [_vp, _f64, _f64, _f64, _vp, ctypes.POINTER(_i64), ctypes.POINTER(_f64), _vp]),
+    "pr_conduction_wall_fluxes": (_i32, [_vp, _vp, _f64, _f64, ctypes.POINTER(_f64), ctypes.POINTER(_f64), _vp]),
+    "pr_coupled_solve": (_i32, [_vp, _vp, _vp, _f64, _f64, _f64, _vp, _i32, _vp, _vp, _vp, _vp, _vp,
+                                ctypes.POINTER(CoupledResultC), _vp]),
     "pr_timers_enable": (None, [_i32]),
     "pr_timers_reset": (None, []),
     "pr_timers_read": (_i32, [_i32, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_f64)]),

@@ -1,9 +1,12 @@
-"""Prescribed-field radiation channels on a B200: the callers of the radiosity path.
+"""Radiation channels and the strictly coupled radiation-conduction solve on a B200.
 
-Mirrors the prescribed-field part of ``porerad.coupled`` (porerad/coupled.py:45-219).
-:func:`prescribed_field_channels` runs on the GPU end to end (patch temperatures,
-emission, radiosity, per-class sums and the coarse source in libporerad); the small
-helpers keep the reference's host semantics for callers that use them directly.
+Mirrors ``porerad.coupled`` (porerad/coupled.py).  :func:`prescribed_field_channels` runs
+on the GPU end to end (patch temperatures, emission, radiosity, per-class sums and the
+coarse source in libporerad); :func:`solve_coupled` / :func:`newton_krylov` run the whole
+Newton-Krylov iteration on the device (conduction stencil, flexible GMRES, the radiosity
+JVP, the Jacobi-PCG preconditioner and the line search) with the conduction system of
+:mod:`porerad_b200.conduction`.  The small helpers keep the reference's host semantics for
+callers that use them directly.
 """
 
 from __future__ import annotations
@@ -248,3 +251,117 @@ def cell_field_channels(operator: ExchangeOperator, patches, T_cells, T_hot_K: f
     info = {"sweeps_or_reflections": int(stats[0]), "spmv": int(stats[1]), "residual": float(stats[2])}
     return PrescribedChannels(0.5 * (T_hot_K + T_cold_K), float(T_hot_K - T_cold_K), float(epsilon), float(q[0]),
                               float(q[1]), float(q[2]), float(q[3]), coarse, info)
+
+
+# Strictly coupled solve (coupled.py:222-490) on the device
+
+NEWTON_MAX_ITERATIONS = 8
+NEWTON_RESIDUAL_W = 1.0e-13
+NEWTON_STEP_K = 1.0e-10
+GMRES_RESTART = 30
+GMRES_MAX_ITERATIONS = 90
+GMRES_RTOL = 1.0e-8
+GMRES_ATOL = 1.0e-13
+PCG_STEPS = (10, 20)
+"""Preconditioner steps of the first attempt and of the restart from the same initial field."""
+
+
+@dataclass
+class CoupledResult:
+    """Converged coupled field, its radiation state and the iteration record (coupled.py:314-337)."""
+
+    temperature_K: np.ndarray
+    state: RadiationState
+    converged: bool
+    newton_iterations: int
+    linear_solves: list[dict] = field(default_factory=list)
+    final_residual_inf_W: float = float("nan")
+    preconditioner_steps: int = 0
+    failure: str = ""
+    metrics: dict = field(default_factory=dict, repr=False)
+
+    @property
+    def linear_residuals_pass(self) -> bool:
+        """Every linear solve met ||r||_2 <= max(1e-13, 1e-8 ||b||_2)."""
+
+        return bool(self.linear_solves) and all(
+            s["converged"] and s["true_residual_l2_W"] <= max(1.0e-13, 1.0e-8 * s["rhs_l2_W"])
+            for s in self.linear_solves
+        )
+
+
+def _coupled(system, operator: ExchangeOperator, patches, T_hot_K: float, T_cold_K: float, epsilon: float,
+             T_initial: np.ndarray, preconditioner_steps: int) -> CoupledResult:
+    dev = _device_of(patches)
+    shape = system.shape
+    if tuple(shape) != tuple(dev.shape):
+        raise ValueError("conduction grid and patch geometry differ")
+    n_cells = int(np.prod(shape))
+    T0 = np.ascontiguousarray(np.asarray(T_initial, dtype=np.float64).ravel())
+    T = np.empty(n_cells)
+    q = np.empty(n_cells)
+    P = dev.n_patches
+    Tp, E, ab = np.empty(P), np.empty(P), np.empty(P)
+    r = _lib.CoupledResultC()
+    _lib.check(_lib.load().pr_coupled_solve(dev.handle, operator.handle, system.handle, float(T_hot_K),
+                                            float(T_cold_K), float(epsilon), T0.ctypes.data,
+                                            int(preconditioner_steps), T.ctypes.data, Tp.ctypes.data, E.ctypes.data,
+                                            ab.ctypes.data, q.ctypes.data, ctypes.byref(r), _lib.stream()))
+    radiosity = RadiosityResult(E, ab, ab - E, float(r.residual_power_W), int(r.series_iterations))
+    state = RadiationState(Tp, radiosity.net_power_W, q.reshape(shape), radiosity)
+    linear = [{"converged": bool(L.converged), "gmres_iterations": int(L.gmres_iterations),
+               "rhs_l2_W": float(L.rhs_l2_W), "true_residual_l2_W": float(L.true_residual_l2_W),
+               "true_residual_relative": float(L.true_residual_relative)} for L in r.linear[:r.n_linear]]
+    metrics = {name: float(getattr(r, name)) for name in (
+        "q_cond_hot_W_m2", "q_rad_hot_W_m2", "q_total_hot_W_m2", "q_cond_cold_W_m2", "q_rad_cold_W_m2",
+        "q_total_cold_W_m2", "radiative_fraction_hot", "k_eff_apparent_W_mK", "wall_flux_mismatch_rel",
+        "energy_residual_rel", "T_min_K", "T_max_K")}
+    metrics["temperature_bound_violations"] = int(r.temperature_bound_violations)
+    return CoupledResult(T.reshape(shape), state, bool(r.converged), int(r.newton_iterations), linear,
+                         float(r.final_residual_inf_W), int(r.preconditioner_steps),
+                         _lib.COUPLED_FAILURES.get(int(r.failure), "unknown failure"), metrics)
+
+
+def newton_krylov(system, operator: ExchangeOperator, patches, T_hot_K: float, T_cold_K: float, epsilon: float,
+                  T_initial: np.ndarray, preconditioner_steps: int) -> CoupledResult:
+    """Newton-Krylov solve of A T - b - Q_rad(T) = 0 from T_initial (coupled.py:340-421), on the device.
+
+    Converged when ||R||_inf <= 1e-13 W and the last update is at most 1e-10 K; radiosity
+    is summed to 1e-8 inside the iteration and to 1e-13 for the returned state; trial
+    fields outside [T_c, T_h] are rejected by the line search.
+    """
+
+    if int(preconditioner_steps) <= 0:
+        raise ValueError("preconditioner_steps must be positive")
+    return _coupled(system, operator, patches, T_hot_K, T_cold_K, epsilon, T_initial, preconditioner_steps)
+
+
+def solve_coupled(system, operator: ExchangeOperator, patches, T_hot_K: float, T_cold_K: float, epsilon: float,
+                  T_initial: np.ndarray) -> CoupledResult:
+    """Coupled solve with 10 preconditioner steps, restarted from the same field with 20 if needed (coupled.py:423-440)."""
+
+    return _coupled(system, operator, patches, T_hot_K, T_cold_K, epsilon, T_initial, 0)
+
+
+def wall_flux_metrics(system, patches, result: CoupledResult, T_hot_K: float, T_cold_K: float) -> dict[str, float]:
+    """Conductive, radiative and total wall fluxes (W m^-2) and the acceptance quantities (coupled.py:443-472).
+
+    The device solve computes them from its final field and radiation state.
+    """
+
+    if not result.metrics:
+        raise ValueError("result does not come from newton_krylov / solve_coupled")
+    return dict(result.metrics)
+
+
+def acceptance_failures(result: CoupledResult, metrics: dict[str, float]) -> list[str]:
+    """Acceptance conditions of a coupled solution that are not met, empty when accepted (coupled.py:475-490)."""
+
+    checks = {
+        "Newton iteration converged": result.converged,
+        "linear residuals within max(1e-13, 1e-8 ||b||)": result.linear_residuals_pass,
+        "wall-flux mismatch <= 0.5 %": metrics["wall_flux_mismatch_rel"] <= 0.005,
+        "global energy residual <= 1e-3": metrics["energy_residual_rel"] <= 1.0e-3,
+        "temperature within the wall temperatures": metrics["temperature_bound_violations"] == 0,
+    }
+    return [name for name, ok in checks.items() if not ok]

@@ -16,19 +16,6 @@ void set_error(const char* fmt, ...) {
   g_error = buf;
 }
 
-// Keep freed device memory in the stream-ordered pool (serving reuses it).
-static void init_pool() {
-  static thread_local int done_dev = -1;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev == done_dev) return;
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-    uint64_t thr = UINT64_MAX;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-  }
-  done_dev = dev;
-}
-
 int case_build(pr_case* c, const uint8_t* phases, cudaStream_t s);
 int generate_rays(const pr_case* c, int64_t p0, int64_t p1, int64_t R, const pr_pcg64* seed, double* origins,
                   double* dirs, cudaStream_t s);
@@ -62,9 +49,7 @@ int cell_field_channels(const pr_case* c, const pr_operator* op, const double* T
 
 using namespace pr;
 
-#define PR_ENTRY_GUARD(obj)      \
-  DeviceGuard _guard((obj)->device); \
-  init_pool()
+#define PR_ENTRY_GUARD(obj) DeviceGuard _guard((obj)->device)
 
 #define PR_CHECK_NULL(p, name)                                  \
   do {                                                          \
@@ -88,7 +73,6 @@ int pr_case_create(const uint8_t* phases_x, int64_t nx, int64_t ny, int64_t nz, 
   PR_ARG(nx > 0 && ny > 0 && nz > 0, "grid dimensions must be positive");
   PR_ARG(nx < (1 << 30) && ny < (1 << 30) && nz < (1 << 30) && nx * ny * nz < ((int64_t)1 << 36),
          "grid too large");
-  init_pool();
   cudaStream_t s = (cudaStream_t)stream;
   pr_case* c = new (std::nothrow) pr_case();
   if (!c) {
@@ -274,7 +258,6 @@ int pr_counts_from_edges(const int32_t* origin, const int32_t* receiver, const i
   PR_CHECK_NULL(out, "out");
   *out = nullptr;
   PR_ARG(n_edges == 0 || (origin && receiver && count), "edge arrays must not be NULL");
-  init_pool();
   return counts_from_edges(origin, receiver, count, n_edges, n_patches, (cudaStream_t)stream, out);
 }
 

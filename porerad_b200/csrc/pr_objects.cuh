@@ -119,3 +119,14 @@ struct pr_operator {
   mutable std::shared_ptr<pr::CountCsr> FT;
   mutable cudaStream_t last_stream = nullptr;
 };
+
+// Cell-centred finite-volume conduction on an x-oriented grid (porerad/conduction.py): the
+// conductance of each cell's +x, +y and +z face (harmonic mean times dx, 0 on the +x face of
+// the last layer; y and z periodic), the diagonal of A, and the wall responses.
+struct pr_conduction {
+  int device = 0;
+  int64_t nx = 0, ny = 0, nz = 0, n = 0;
+  double H = 0.0, dx = 0.0;
+  pr::DevBuf<double> k, gx, gy, gz, diag, hot, cold;
+  cudaStream_t last_stream = nullptr;
+};

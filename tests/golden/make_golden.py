@@ -17,6 +17,11 @@ where the reference is not installed:
   for those microstructures (columns raw_count_sha256_A/B) with their seeds.
 * ``prescribed_field.json``: archived prescribed-field rows of
   results/prescribed_field.csv for the committed core microstructure, with its seeds.
+* ``coupled_<name>.npz``: the strictly coupled solve of each small case (conduction
+  system of K_SOLID/K_GAS, pure-conduction field, solve_coupled at two conditions: final
+  field, wall-flux metrics, Newton and GMRES iteration record).
+* ``coupled.json``: the archived rows of results/coupled.csv for the canonical
+  microstructures (groups canonical and thickness) with their case parameters.
 """
 
 from __future__ import annotations
@@ -105,6 +110,68 @@ def small_case(vf, ex, cp, name, spec):
     print(f"{name}: {n} patches, {pooled[2].size} pairs, {op.balance_method} {op.balance_iterations}")
 
 
+COUPLED_CONDITIONS = ((700.0, 20.0, 0.6), (500.0, 200.0, 0.3))  # (T_mean, delta_T, eps)
+
+
+def coupled_small(name, spec):
+    from porerad import conduction, coupled as cp, exchange as ex, view_factors as vf
+    from porerad.constants import K_GAS, K_SOLID
+
+    shape, phi, pseed, H, seeds, R = spec
+    ph = random_phases(shape, phi, pseed)
+    p = vf.build_surface_patches(ph, H)
+    o, r, c = vf.pool_counts([vf.first_hit_counts(p, R, s) for s in seeds], p.n_patches)
+    op = ex.ExchangeOperator(o, r, c, np.full(p.n_patches, R * len(seeds), np.int64), p.patch_area_m2)
+    system = conduction.assemble_conduction(np.where(ph == 1, K_SOLID, K_GAS), H)
+    out = dict(diag=system.matrix.diagonal(), hot_rhs=system.hot_rhs, cold_rhs=system.cold_rhs,
+               conditions=np.asarray(COUPLED_CONDITIONS))
+    names = ("q_cond_hot_W_m2", "q_rad_hot_W_m2", "q_total_hot_W_m2", "q_cond_cold_W_m2", "q_rad_cold_W_m2",
+             "q_total_cold_W_m2", "radiative_fraction_hot", "k_eff_apparent_W_mK", "wall_flux_mismatch_rel",
+             "energy_residual_rel", "T_min_K", "T_max_K")
+    out["metric_names"] = np.asarray(names)
+    metrics, record = [], []
+    for k, (Tm, dT, eps) in enumerate(COUPLED_CONDITIONS):
+        Th, Tc = Tm + dT / 2.0, Tm - dT / 2.0
+        T0 = conduction.solve_conduction(system, Th, Tc)
+        res = cp.solve_coupled(system, op, p, Th, Tc, eps, T0)
+        m = cp.wall_flux_metrics(system, p, res, Th, Tc)
+        assert not cp.acceptance_failures(res, m)
+        out[f"T_initial_{k}"] = T0
+        out[f"T_final_{k}"] = res.temperature_K
+        out[f"cell_power_{k}"] = res.state.cell_net_power_W
+        metrics.append([m[n] for n in names])
+        record.append([res.newton_iterations, res.preconditioner_steps, len(res.linear_solves)])
+        out[f"gmres_{k}"] = np.asarray([s["gmres_iterations"] for s in res.linear_solves], np.int64)
+    out["metrics"] = np.asarray(metrics)
+    out["record"] = np.asarray(record, np.int64)
+    np.savez_compressed(HERE / f"coupled_{name}.npz", **out)
+    print(f"coupled {name}: newton {[r[0] for r in record]}")
+
+
+def coupled_rows(ref):
+    cases = {r["case_id"]: r for r in csv.DictReader(open(ref / "data" / "cases_coupled.csv"))}
+    rows = []
+    for r in csv.DictReader(open(ref / "results" / "coupled.csv")):
+        c = cases[r["case_id"]]
+        if c["microstructure"] not in CANONICAL or c["group"] not in ("canonical", "thickness"):
+            continue
+        row = dict(case_id=r["case_id"], group=c["group"], microstructure=c["microstructure"],
+                   axis=c["transfer_axis"], repeats=int(c["repeats_along_axis"]), H_m=float(c["H_m"]),
+                   N_axis=int(c["N_axis"]), T_mean_K=float(c["T_mean_K"]), delta_T_K=float(c["delta_T_K"]),
+                   epsilon=float(c["epsilon"]), rays_per_patch=int(c["rays_per_patch_per_block"]),
+                   seeds_A=[int(s) for s in c["seeds_A"].split(";")],
+                   seeds_B=[int(s) for s in c["seeds_B"].split(";")], phase_sha256_x=c["phase_sha256_x"],
+                   newton_updates=int(r["newton_updates"]))
+        for k in ("q_cond_hot_W_m2", "q_rad_hot_W_m2", "q_total_hot_W_m2", "q_cond_cold_W_m2", "q_rad_cold_W_m2",
+                  "q_total_cold_W_m2", "radiative_fraction_hot", "k_eff_apparent_W_mK", "wall_flux_mismatch_rel",
+                  "energy_residual_rel", "T_min_K", "T_max_K"):
+            row[k] = float(r[k]) if r[k] != "" else None  # some archived rows leave the cold side empty
+        rows.append(row)
+    (HERE / "coupled.json").write_text(json.dumps(dict(rows=rows, source="data/cases_coupled.csv, "
+                                                                           "results/coupled.csv"), indent=1))
+    print("coupled rows:", len(rows))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -115,6 +182,8 @@ def main():
 
     for name, spec in SMALL_CASES.items():
         small_case(vf, ex, cp, name, spec)
+        coupled_small(name, spec)
+    coupled_rows(ref)
 
     rows = list(csv.DictReader(open(ref / "data" / "cases_coupled.csv")))
     hashes = {}

@@ -35,3 +35,14 @@ def prescribed_case() -> dict:
     return json.loads((GOLDEN / "prescribed_field.json").read_text())
 
 
+def load_coupled(name: str) -> dict:
+    """Coupled-solve golden of a small case (tests/golden/make_golden.py)."""
+
+    with np.load(GOLDEN / f"coupled_{name}.npz") as z:
+        return {k: z[k] for k in z.files}
+
+
+def coupled_rows() -> list[dict]:
+    """Archived results/coupled.csv rows of the canonical microstructures with their case parameters."""
+
+    return json.loads((GOLDEN / "coupled.json").read_text())["rows"]

@@ -1,0 +1,141 @@
+"""GPU parity of conduction and the strictly coupled Newton-Krylov solve.
+
+The conduction system's diagonal and wall responses must equal the reference's bit for
+bit (same face order of the sums).  Solves are compared with stated tolerances: the
+pure-conduction field stops at a relative residual of 1e-11 and the Newton iteration at
+1e-13 W; fields agree to about 1e-10 relative, the wall-flux metrics to 1e-8.  The
+archived rows of results/coupled.csv (canonical microstructures, counts from the stored
+seeds) are reproduced through the whole device path.
+"""
+
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+from tests.helpers import SMALL, coupled_rows, load_canonical, load_coupled, load_small
+
+pytestmark = pytest.mark.gpu
+
+FIELD_RTOL = 1e-9     # final temperature fields (Newton converged to 1e-13 W, step 1e-10 K)
+METRIC_RTOL = 1e-8    # wall fluxes, fractions, k_eff, T_min / T_max
+ARCHIVE_RTOL = 1e-7   # archived rows: also carry the balancing tolerance of the operator (d to 1e-8)
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.max(np.abs(a - b)) / max(float(np.max(np.abs(b))), 1e-300))
+
+
+def _small_setup(name):
+    from porerad_b200 import conduction, exchange, view_factors as vf
+    from porerad_b200.constants import K_GAS, K_SOLID
+
+    case = load_small(name)
+    ph = case["phases"]
+    H = float(case["H_m"])
+    n = case["patches_patch_class"].size
+    R = int(case["rays_per_patch"]) * len(case["seeds"])
+    op = exchange.ExchangeOperator(case["pooled_origin"], case["pooled_receiver"], case["pooled_count"],
+                                   np.full(n, R, np.int64), case["patches_patch_area_m2"])
+    p = vf.build_surface_patches(ph, H)
+    system = conduction.assemble_conduction(np.where(ph == 1, K_SOLID, K_GAS), H)
+    return case, op, p, system
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_conduction_system_bit_exact(name, oracle):
+    case, op, p, system = _small_setup(name)
+    g = load_coupled(name)
+    assert np.array_equal(system.matrix.diagonal(), g["diag"])
+    assert np.array_equal(system.hot_rhs, g["hot_rhs"]) and np.array_equal(system.cold_rhs, g["cold_rhs"])
+    ref = oracle.assemble_conduction(system.conductivity, system.H_m)
+    assert (system.matrix != ref.matrix).nnz == 0  # the materialised CSR is the reference's matrix
+    x = np.random.default_rng(3).standard_normal(system.conductivity.size)
+    assert _rel(system.apply(x), ref.matrix @ x) <= 1e-14
+    T = 600.0 + 50.0 * np.random.default_rng(4).random(system.conductivity.size)
+    got = system.wall_fluxes(T, 650.0, 550.0)
+    want = oracle.wall_fluxes(ref, T, 650.0, 550.0)
+    assert _rel(got, want) <= 1e-13
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_coupled_solve_against_reference(name):
+    from porerad_b200 import conduction, coupled
+
+    case, op, p, system = _small_setup(name)
+    g = load_coupled(name)
+    names = [str(x) for x in g["metric_names"]]
+    for k, (Tm, dT, eps) in enumerate(g["conditions"]):
+        Th, Tc = Tm + dT / 2.0, Tm - dT / 2.0
+        T0 = conduction.solve_conduction(system, Th, Tc)
+        assert _rel(T0, g[f"T_initial_{k}"]) <= 1e-10
+        res = coupled.solve_coupled(system, op, p, Th, Tc, eps, g[f"T_initial_{k}"])
+        m = coupled.wall_flux_metrics(system, p, res, Th, Tc)
+        assert not coupled.acceptance_failures(res, m), coupled.acceptance_failures(res, m)
+        assert res.newton_iterations == int(g["record"][k][0])
+        assert res.preconditioner_steps == int(g["record"][k][1])
+        assert _rel(res.temperature_K, g[f"T_final_{k}"]) <= FIELD_RTOL
+        assert _rel(res.state.cell_net_power_W, g[f"cell_power_{k}"]) <= 1e-7
+        for j, key in enumerate(names):
+            want = g["metrics"][k][j]
+            if key in ("wall_flux_mismatch_rel", "energy_residual_rel"):
+                assert m[key] <= max(100 * want, 1e-10), key
+            else:
+                assert abs(m[key] - want) <= METRIC_RTOL * max(abs(want), 1.0), key
+
+
+def test_newton_krylov_fixed_steps_and_errors():
+    from porerad_b200 import conduction, coupled
+
+    case, op, p, system = _small_setup("box12")
+    g = load_coupled("box12")
+    Tm, dT, eps = g["conditions"][0]
+    Th, Tc = Tm + dT / 2.0, Tm - dT / 2.0
+    res = coupled.newton_krylov(system, op, p, Th, Tc, eps, g["T_initial_0"], 20)
+    assert res.converged and res.preconditioner_steps == 20
+    assert res.linear_residuals_pass
+    assert _rel(res.temperature_K, g["T_final_0"]) <= FIELD_RTOL
+    with pytest.raises(ValueError):
+        coupled.newton_krylov(system, op, p, Th, Tc, eps, g["T_initial_0"], 0)
+    with pytest.raises(ValueError):
+        coupled.solve_coupled(system, op, p, Tc, Th, eps, g["T_initial_0"])  # walls swapped
+
+
+@pytest.mark.parametrize("case_id", [r["case_id"] for r in coupled_rows()])
+def test_archived_coupled_rows(case_id):
+    """results/coupled.csv through counts, operator, conduction and the coupled solve on the device."""
+
+    from porerad_b200 import conduction, coupled, exchange, view_factors as vf
+    from porerad_b200.constants import K_GAS, K_SOLID
+
+    row = next(r for r in coupled_rows() if r["case_id"] == case_id)
+    ph = vf.orient_along_x(load_canonical(row["microstructure"]), row["axis"])
+    ph = np.ascontiguousarray(np.concatenate([ph] * row["repeats"], axis=0))
+    assert ph.shape[0] == row["N_axis"]
+    assert hashlib.sha256(ph.tobytes()).hexdigest() == row["phase_sha256_x"]
+    H = row["H_m"]
+    Th, Tc = row["T_mean_K"] + row["delta_T_K"] / 2.0, row["T_mean_K"] - row["delta_T_K"] / 2.0
+    p = vf.build_surface_patches(ph, H)
+    seeds = row["seeds_A"] + row["seeds_B"]
+    table = vf.first_hit_counts_pooled(p, row["rays_per_patch"], seeds)
+    n = p.n_patches
+    op = exchange.ExchangeOperator(table, None, None, np.full(n, row["rays_per_patch"] * len(seeds), np.int64),
+                                   np.full(n, (H / ph.shape[0]) ** 2))
+    system = conduction.assemble_conduction(np.where(ph == 1, K_SOLID, K_GAS), H)
+    T0 = conduction.solve_conduction(system, Th, Tc)
+    res = coupled.solve_coupled(system, op, p, Th, Tc, row["epsilon"], T0)
+    m = coupled.wall_flux_metrics(system, p, res, Th, Tc)
+    assert not coupled.acceptance_failures(res, m), coupled.acceptance_failures(res, m)
+    assert res.newton_iterations == row["newton_updates"]
+    for key in ("q_cond_hot_W_m2", "q_rad_hot_W_m2", "q_total_hot_W_m2", "q_cond_cold_W_m2", "q_rad_cold_W_m2",
+                "q_total_cold_W_m2", "radiative_fraction_hot", "k_eff_apparent_W_mK", "T_min_K", "T_max_K"):
+        want = row[key]
+        if want is None:
+            continue
+        assert abs(m[key] - want) <= ARCHIVE_RTOL * abs(want), (key, m[key], want)
+    assert m["wall_flux_mismatch_rel"] <= 0.005 and m["energy_residual_rel"] <= 1e-3
+    op.close()
+    table.close()

@@ -12,7 +12,7 @@ import hashlib
 import numpy as np
 import pytest
 
-from tests.helpers import SMALL, count_hash_cases, load_canonical, load_small, prescribed_case
+from tests.helpers import SMALL, count_hash_cases, load_canonical, load_coupled, load_small, prescribed_case
 
 
 def _rel(a, b):
@@ -113,3 +113,38 @@ def test_oracle_errors(oracle):
     d[0] = (0.0, 0.0, 1.0)
     with pytest.raises(RuntimeError, match="1 rays did not resolve"):
         oracle.trace_first_hit(p, o, d)
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_oracle_conduction_and_coupled_solve(oracle, name):
+    """conduction.py and coupled.py:222-490 against the reference's outputs on the small cases."""
+
+    case = load_small(name)
+    g = load_coupled(name)
+    ph = case["phases"]
+    H = float(case["H_m"])
+    system = oracle.assemble_conduction(np.where(ph == 1, oracle.K_SOLID, oracle.K_GAS), H)
+    assert np.array_equal(system.matrix.diagonal(), g["diag"])
+    assert np.array_equal(system.hot_rhs, g["hot_rhs"]) and np.array_equal(system.cold_rhs, g["cold_rhs"])
+    n = case["patches_patch_class"].size
+    R = int(case["rays_per_patch"]) * len(case["seeds"])
+    op = oracle.ExchangeOperator(case["pooled_origin"], case["pooled_receiver"], case["pooled_count"],
+                                 np.full(n, R, np.int64), case["patches_patch_area_m2"])
+    p = oracle.build_surface_patches(ph, H)
+    names = [str(x) for x in g["metric_names"]]
+    for k, (Tm, dT, eps) in enumerate(g["conditions"]):
+        Th, Tc = Tm + dT / 2.0, Tm - dT / 2.0
+        T0 = oracle.solve_conduction(system, Th, Tc)
+        assert _rel(T0, g[f"T_initial_{k}"]) <= 1e-12
+        res = oracle.solve_coupled(system, op, p, Th, Tc, eps, T0)
+        assert res.converged and oracle.linear_residuals_pass(res)
+        assert [res.newton_iterations, res.preconditioner_steps, len(res.linear_solves)] == list(g["record"][k])
+        assert _rel(res.temperature_K, g[f"T_final_{k}"]) <= 1e-11
+        m = oracle.wall_flux_metrics(system, p, res, Th, Tc)
+        for j, key in enumerate(names):
+            want = g["metrics"][k][j]
+            if key in ("wall_flux_mismatch_rel", "energy_residual_rel"):
+                assert m[key] <= max(10 * want, 1e-11), key  # round-off quantities
+            else:
+                assert abs(m[key] - want) <= 1e-9 * max(abs(want), 1.0), key
+        assert m["temperature_bound_violations"] == 0
