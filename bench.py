@@ -58,6 +58,11 @@ WORKLOADS = {
                         "operator, FP32+FP64-refinement vs FP64 flux error per solve",
                archs=("TL", "FA"), n=192, phi=0.10, seed=0, rays=1000, sets=3, eps=0.6, T_m=700.0, dT=20.0, H=0.01,
                solves=20, sigma_K=5.0),
+    "coupled": dict(workload="strictly coupled radiation-conduction solve of the archived case "
+                             "coupled_OF_x_T700_eps0.6_N128 (canonical OF 128^3, 4 seed blocks x 64 rays/patch, eps 0.6, "
+                             "690->710 K along x): counts, balanced operator, conduction assembly + PCG, Newton-Krylov "
+                             "(flexible GMRES, radiosity JVP, Jacobi-PCG preconditioner, line search)",
+                    case_id="coupled_OF_x_T700_eps0.6_N128"),
     "c1": dict(workload="FI N=64^3 phi=0.10 (r=2, seed 0), 64 rays/patch x 1 set, eps 0.9, T 600->700 K along x, "
                         "FP64 radiosity",
                arch="FI", n=64, phi=0.10, seed=0, rays=64, sets=1, eps=0.9, T_m=650.0, dT=100.0, H=0.01),
@@ -641,6 +646,117 @@ def run_c3(args, cfg):
     }
 
 
+# --------------------------------------------------------------------------- coupled solve
+
+def _coupled_case(case_id):
+    golden = ROOT / "tests" / "golden"
+    row = next(r for r in json.loads((golden / "coupled.json").read_text())["rows"] if r["case_id"] == case_id)
+    with np.load(golden / f"canonical_{row['microstructure']}.npz") as z:
+        ph = np.unpackbits(z["bits"])[: int(np.prod(z["shape"]))].reshape(tuple(z["shape"])).astype(np.uint8)
+    ph = np.moveaxis(ph, "xyz".index(row["axis"]), 0)
+    ph = np.ascontiguousarray(np.concatenate([ph] * row["repeats"], axis=0))
+    return row, ph
+
+
+def coupled_step(row, ph):
+    """One archived coupled case from its phases: the run_coupled.py sequence on the device."""
+
+    import torch
+
+    from porerad_b200 import conduction, coupled, exchange, view_factors as vf
+    from porerad_b200.constants import K_GAS, K_SOLID
+
+    H = row["H_m"]
+    Th, Tc = row["T_mean_K"] + row["delta_T_K"] / 2.0, row["T_mean_K"] - row["delta_T_K"] / 2.0
+    marks = [time.perf_counter()]
+    p = vf.build_surface_patches(ph, H)
+    seeds = row["seeds_A"] + row["seeds_B"]
+    table = vf.first_hit_counts_pooled(p, row["rays_per_patch"], seeds)
+    torch.cuda.synchronize()
+    marks.append(time.perf_counter())
+    n = p.n_patches
+    op = exchange.ExchangeOperator(table, None, None, np.full(n, row["rays_per_patch"] * len(seeds), np.int64),
+                                   np.full(n, (H / ph.shape[0]) ** 2))
+    marks.append(time.perf_counter())
+    system = conduction.assemble_conduction(np.where(ph == 1, K_SOLID, K_GAS), H)
+    T0 = conduction.solve_conduction(system, Th, Tc)
+    marks.append(time.perf_counter())
+    res = coupled.solve_coupled(system, op, p, Th, Tc, row["epsilon"], T0)
+    m = coupled.wall_flux_metrics(system, p, res, Th, Tc)
+    marks.append(time.perf_counter())
+    out = dict(metrics=m, newton=res.newton_iterations, gmres=[s["gmres_iterations"] for s in res.linear_solves],
+               failures=coupled.acceptance_failures(res, m), n_patches=n, nnz=op.nnz_symmetric,
+               phases_ms={k: 1e3 * (marks[i + 1] - marks[i]) for i, k in
+                          enumerate(("patches_counts", "operator", "conduction", "newton_krylov"))})
+    op.close()
+    table.close()
+    system.close()
+    return out
+
+
+def run_coupled_bench(args, cfg):
+    import torch
+
+    from porerad_b200 import _lib
+
+    torch.cuda.set_device(0)
+    lib = _lib.load()
+    row, ph = _coupled_case(cfg["case_id"])
+    for _ in range(max(args.warmup, 1)):
+        coupled_step(row, ph)
+    torch.cuda.synchronize()
+    launches0 = lib.pr_kernel_launches()
+    outs = []
+    with ClockSampler(0) as clocks:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            outs.append(coupled_step(row, ph))
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+    last = outs[-1]
+    m = last["metrics"]
+    rel = {k: abs(m[k] - row[k]) / abs(row[k]) for k in ("q_total_hot_W_m2", "q_rad_hot_W_m2", "k_eff_apparent_W_mK")}
+    cpu = None
+    if not args.no_cpu:
+        cpu = coupled_cpu_sample(row, ph)
+    return {
+        "metric": "strictly coupled solves/s (whole archived case from its phases)", "value": args.steps / dt,
+        "unit": "cases/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "reference fixture",
+        "config": {"workload": cfg["workload"], "n_patches": last["n_patches"], "nnz_symmetric": last["nnz"],
+                   "cells": int(ph.size)},
+        "phases_ms": last["phases_ms"], "newton_updates": last["newton"], "gmres_iterations": last["gmres"],
+        "acceptance_failures": last["failures"], "rel_error_vs_archived": rel,
+        "archived_newton_updates": row["newton_updates"], "clocks": clocks.summary(),
+        "gpu_launches": int(lib.pr_kernel_launches() - launches0) // max(args.steps, 1), "cpu_baseline": cpu,
+    }
+
+
+def coupled_cpu_sample(row, ph):
+    """The oracle (NumPy/SciPy restatement of run_coupled.py's path) on the same case, timed on the host cores."""
+
+    from oracle import build as ob
+    from oracle import porerad_oracle as orc
+
+    ob.build()
+    cores = orc.set_threads()
+    H = row["H_m"]
+    Th, Tc = row["T_mean_K"] + row["delta_T_K"] / 2.0, row["T_mean_K"] - row["delta_T_K"] / 2.0
+    t0 = time.perf_counter()
+    p = orc.build_surface_patches(ph, H)
+    seeds = row["seeds_A"] + row["seeds_B"]
+    o, r, c = orc.pool_counts([orc.first_hit_counts(p, row["rays_per_patch"], s) for s in seeds], p.n_patches)
+    op = orc.ExchangeOperator(o, r, c, np.full(p.n_patches, row["rays_per_patch"] * len(seeds), np.int64),
+                              p.patch_area_m2)
+    system = orc.assemble_conduction(np.where(ph == 1, orc.K_SOLID, orc.K_GAS), H)
+    T0 = orc.solve_conduction(system, Th, Tc)
+    orc.solve_coupled(system, op, p, Th, Tc, row["epsilon"], T0)
+    dt = time.perf_counter() - t0
+    return {"value": 1.0 / dt, "unit": "cases/s", "cores": cores, "kind": "port",
+            "sample": f"the whole case once on the CPU ({dt:.1f} s): oracle patches, counts (OpenMP C traversal), "
+                      "SciPy-Anderson operator, SciPy CG conduction, NumPy/SciPy Newton-Krylov"}
+
+
 # --------------------------------------------------------------------------- coupled-size stress (c5)
 
 def run_c5(args, cfg):
@@ -722,6 +838,21 @@ def run_reference(args, cfg):
 
     if replicas.rank() != 0:
         return None  # the CPU reference runs once, on rank 0
+    if "case_id" in cfg:  # the coupled workload: the whole case on the host cores
+        row, ph = _coupled_case(cfg["case_id"])
+        vals, last = [], None
+        for _ in range(args.steps):
+            last = coupled_cpu_sample(row, ph)
+            vals.append(last["value"])
+        value = float(np.mean(vals))
+        return {"impl": "reference", "metric": "strictly coupled solves/s (whole archived case from its phases)",
+                "value": value, "unit": "cases/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": 0,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "reference fixture", "config": {"workload": cfg["workload"]},
+                "cpu_baseline": {**last, "value": value},
+                "e2e": {"value": value, "unit": "cases/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if "arch" not in cfg:
+        raise SystemExit("--impl reference times the CPU path of the c1, c2 and coupled workloads")
     seeds = ray_seeds(cfg)
     # warm-up runs of the sample, then K timed samples
     for _ in range(max(0, args.warmup)):
@@ -753,6 +884,8 @@ def main():
         line = run_reference(args, cfg)
     elif args.workload == "c3":
         line = run_c3(args, cfg)
+    elif args.workload == "coupled":
+        line = run_coupled_bench(args, cfg)
     elif args.workload == "c4":
         line = run_c4(args, cfg)
     elif args.workload == "c5":
