@@ -529,12 +529,54 @@ struct Reducer {
   }
 };
 
+// A CUDA graph captured on a private stream (capture is not allowed on the legacy default
+// stream) and launched on the caller's stream; rebuilt when its key changes.
+struct CapturedGraph {
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t cap = nullptr;
+  long long key = -1;
+  ~CapturedGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (cap) cudaStreamDestroy(cap);
+  }
+  template <class F>
+  int ensure(long long k, F&& record) {
+    if (exec && key == k) return PR_OK;
+    if (exec) {
+      cudaGraphExecDestroy(exec);
+      exec = nullptr;
+    }
+    if (!cap) PR_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    PR_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    const int st = record(cap);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(cap, &g);
+    if (st != PR_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    PR_CUDA(e);
+    const cudaError_t ei = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    PR_CUDA(ei);
+    key = k;
+    return PR_OK;
+  }
+  int launch(cudaStream_t s) {
+    PR_CUDA(cudaGraphLaunch(exec, s));
+    return PR_OK;
+  }
+};
+
 // Jacobi-preconditioned CG on (A + diag(shift)) x = rhs.  steps > 0: exactly that many steps
 // from x = 0, no convergence test (coupled.py:293-320).  steps == 0: from the given x until
-// ||r||_2 <= tol (checked on the device, polled by the host), at most max_it steps.
+// ||r||_2 <= tol (checked on the device, polled by the host), at most max_it steps.  Both run
+// as CUDA graphs of their fixed launch sequences (a preconditioner application is about 60
+// small launches).
 struct Pcg {
-  DevBuf<double> r, z, p, Ap, partial;
+  DevBuf<double> r, z, p, Ap, partial, gin, gout;
   DevBuf<PcgScalars> st;
+  CapturedGraph fixed_graph, batch_graph;
   int64_t n = 0;
   int init(int64_t n_, cudaStream_t s) {
     n = n_;
@@ -542,6 +584,8 @@ struct Pcg {
     PR_TRY(z.alloc(n, s));
     PR_TRY(p.alloc(n, s));
     PR_TRY(Ap.alloc(n, s));
+    PR_TRY(gin.alloc(n, s));
+    PR_TRY(gout.alloc(n, s));
     PR_TRY(partial.alloc((size_t)kRedBlocks * 2, s));
     PR_TRY(st.alloc(1, s));
     return PR_OK;
@@ -560,11 +604,21 @@ struct Pcg {
     PR_CUDA(cudaGetLastError());
     return PR_OK;
   }
-  int fixed(const CondView& A, const double* shift, const double* rhs, int steps, double* x, cudaStream_t s) {
+  int fixed_seq(const CondView& A, const double* shift, const double* rhs, int steps, double* x, cudaStream_t s) {
     ::pr::launch_mark(), k_pcg_start<<<kRedBlocks, 256, 0, s>>>(A, shift, rhs, x, 1, r.ptr, z.ptr, p.ptr, partial.ptr);
     ::pr::launch_mark(), k_pcg_init_scalars<<<1, 32, 0, s>>>(partial.ptr, kRedBlocks, 0.0, st.ptr);
     PR_CUDA(cudaGetLastError());
     for (int k = 0; k < steps; ++k) PR_TRY(step(A, shift, x, s, k + 1 < steps));
+    return PR_OK;
+  }
+  // x = (steps of PCG from 0)(rhs): the captured sequence between a copy in and a copy out
+  int fixed(const CondView& A, const double* shift, const double* rhs, int steps, double* x, cudaStream_t s) {
+    PR_TRY(fixed_graph.ensure(((long long)steps << 1) ^ (long long)(uintptr_t)shift, [&](cudaStream_t c) -> int {
+      return fixed_seq(A, shift, gin.ptr, steps, gout.ptr, c);
+    }));
+    PR_CUDA(cudaMemcpyAsync(gin.ptr, rhs, n * 8, cudaMemcpyDeviceToDevice, s));
+    PR_TRY(fixed_graph.launch(s));
+    PR_CUDA(cudaMemcpyAsync(x, gout.ptr, n * 8, cudaMemcpyDeviceToDevice, s));
     return PR_OK;
   }
   int solve(const CondView& A, const double* shift, const double* rhs, double tol, int64_t max_it, double* x,
@@ -572,15 +626,19 @@ struct Pcg {
     ::pr::launch_mark(), k_pcg_start<<<kRedBlocks, 256, 0, s>>>(A, shift, rhs, x, 0, r.ptr, z.ptr, p.ptr, partial.ptr);
     ::pr::launch_mark(), k_pcg_init_scalars<<<1, 32, 0, s>>>(partial.ptr, kRedBlocks, tol * tol, st.ptr);
     PR_CUDA(cudaGetLastError());
-    int batch = 16;
+    // graphs of 32 steps (steps after convergence return at once), polled every 1, 2, 4, 8 graphs
+    constexpr int kGraphSteps = 32;
+    PR_TRY(batch_graph.ensure((long long)(uintptr_t)x ^ ((long long)(uintptr_t)shift << 1), [&](cudaStream_t c) -> int {
+      for (int k = 0; k < kGraphSteps; ++k) PR_TRY(step(A, shift, x, c, true));
+      return PR_OK;
+    }));
+    int graphs = 1;
     for (int64_t done = 0; done < max_it;) {
-      const int64_t b = std::min<int64_t>(batch, max_it - done);
-      for (int64_t k = 0; k < b; ++k) PR_TRY(step(A, shift, x, s, true));
-      done += b;
+      for (int g = 0; g < graphs && done < max_it; ++g, done += kGraphSteps) PR_TRY(batch_graph.launch(s));
       PR_CUDA(cudaMemcpyAsync(out, st.ptr, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s));
       PR_CUDA(cudaStreamSynchronize(s));
       if (out->done) return PR_OK;
-      if (batch < 256) batch *= 2;
+      if (graphs < 8) graphs *= 2;
     }
     PR_CUDA(cudaMemcpyAsync(out, st.ptr, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s));
     PR_CUDA(cudaStreamSynchronize(s));
