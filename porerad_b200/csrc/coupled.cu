@@ -234,17 +234,24 @@ __global__ void __launch_bounds__(256) k_vstats(const double* __restrict__ x, co
   }
 }
 
+// one warp, fixed order (warp_sum_partials for the sums; min and max do not depend on it)
 __global__ void k_vstats_final(const double* __restrict__ partial, int blocks, double* __restrict__ out) {
-  if (threadIdx.x != 0) return;
-  double a = 0.0, b = 0.0, c = INFINITY, d = -INFINITY, e = 0.0;
-  for (int k = 0; k < blocks; ++k) {
+  const int lane = threadIdx.x & 31;
+  const double a = warp_sum_partials(partial, blocks, 5, 0, lane);
+  const double e = warp_sum_partials(partial, blocks, 5, 4, lane);
+  double b = 0.0, c = INFINITY, d = -INFINITY;
+  for (int k = lane; k < blocks; k += 32) {
     const double* p = partial + 5 * (int64_t)k;
-    a += p[0];
     b = fmax(b, p[1]);
     c = fmin(c, p[2]);
     d = fmax(d, p[3]);
-    e += p[4];
   }
+  for (int o = 16; o > 0; o >>= 1) {
+    b = fmax(b, __shfl_xor_sync(PR_FULL, b, o));
+    c = fmin(c, __shfl_xor_sync(PR_FULL, c, o));
+    d = fmax(d, __shfl_xor_sync(PR_FULL, d, o));
+  }
+  if (lane != 0) return;
   out[0] = a;
   out[1] = b;
   out[2] = c;
@@ -299,22 +306,20 @@ __global__ void __launch_bounds__(256) k_pcg_update(const double* __restrict__ d
   block_sum_store<2>(acc, partial);
 }
 
-// one thread: reduce the partials of p . Ap into st->pAp
+// one warp: reduce the partials of p . Ap into st->pAp
 __global__ void k_pcg_take_pAp(const double* __restrict__ partial, int blocks, PcgScalars* __restrict__ st) {
-  if (threadIdx.x != 0 || st->done) return;
-  double a = 0.0;
-  for (int b = 0; b < blocks; ++b) a += partial[b];
-  st->pAp = a;
+  if (st->done) return;
+  const double a = warp_sum_partials(partial, blocks, 1, 0, threadIdx.x & 31);
+  if (threadIdx.x == 0) st->pAp = a;
 }
 
-// one thread: r . z and r . r of the step; the convergence test (when tol2 > 0)
+// one warp: r . z and r . r of the step; the convergence test (when tol2 > 0)
 __global__ void k_pcg_take_rz(const double* __restrict__ partial, int blocks, PcgScalars* __restrict__ st) {
-  if (threadIdx.x != 0 || st->done) return;
-  double a = 0.0, b = 0.0;
-  for (int k = 0; k < blocks; ++k) {
-    a += partial[2 * k];
-    b += partial[2 * k + 1];
-  }
+  if (st->done) return;
+  const int lane = threadIdx.x & 31;
+  const double a = warp_sum_partials(partial, blocks, 2, 0, lane);
+  const double b = warp_sum_partials(partial, blocks, 2, 1, lane);
+  if (lane != 0) return;
   st->rz_new = a;
   st->rr = b;
   st->iterations += 1;
@@ -363,12 +368,10 @@ __global__ void __launch_bounds__(256) k_pcg_start(CondView A, const double* __r
 
 __global__ void k_pcg_init_scalars(const double* __restrict__ partial, int blocks, double tol2,
                                    PcgScalars* __restrict__ st) {
-  if (threadIdx.x != 0) return;
-  double a = 0.0, b = 0.0;
-  for (int k = 0; k < blocks; ++k) {
-    a += partial[2 * k];
-    b += partial[2 * k + 1];
-  }
+  const int lane = threadIdx.x & 31;
+  const double a = warp_sum_partials(partial, blocks, 2, 0, lane);
+  const double b = warp_sum_partials(partial, blocks, 2, 1, lane);
+  if (lane != 0) return;
   st->rz = a;
   st->rr = b;
   st->tol2 = tol2;

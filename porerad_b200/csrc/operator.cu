@@ -29,15 +29,13 @@
 namespace pr {
 
 __global__ void k_sum_partials(const double* __restrict__ partial, int blocks, int K, double* __restrict__ out) {
-  const int k = threadIdx.x;
-  if (k >= K) return;
-  double s = 0.0;
-  for (int b = 0; b < blocks; ++b) s += partial[(int64_t)b * K + k];
-  out[k] = s;
+  const int k = blockIdx.x;
+  const double s = warp_sum_partials(partial, blocks, K, k, threadIdx.x & 31);
+  if (threadIdx.x == 0) out[k] = s;
 }
 
 int sum_partials(const double* partial, int blocks, int K, double* out, cudaStream_t s) {
-  ::pr::launch_mark(), k_sum_partials<<<1, 32 * ((K + 31) / 32), 0, s>>>(partial, blocks, K, out);
+  ::pr::launch_mark(), k_sum_partials<<<K, 32, 0, s>>>(partial, blocks, K, out);
   PR_CUDA(cudaGetLastError());
   return PR_OK;
 }

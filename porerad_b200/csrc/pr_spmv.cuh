@@ -138,7 +138,17 @@ __device__ __forceinline__ void block_sum_store(double (&v)[K], double* __restri
   __syncthreads();
 }
 
-// out[k] = sum over blocks of partial[b * K + k], in block order (one thread per k).
+// Sum of a[b * stride + off] over b < count by one warp in a fixed order: lane l adds b = l,
+// l + 32, ... in turn, then the lanes meet in a fixed shuffle tree; every lane gets the sum.
+__device__ __forceinline__ double warp_sum_partials(const double* __restrict__ a, int count, int stride, int off,
+                                                    int lane) {
+  double s = 0.0;
+  for (int b = lane; b < count; b += 32) s += a[(int64_t)b * stride + off];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(PR_FULL, s, o);
+  return s;
+}
+
+// out[k] = sum over blocks of partial[b * K + k] (one warp per k, warp_sum_partials order).
 __global__ void k_sum_partials(const double* __restrict__ partial, int blocks, int K, double* __restrict__ out);
 
 int sum_partials(const double* partial, int blocks, int K, double* out, cudaStream_t s);

@@ -70,12 +70,11 @@ struct SeriesEpi {
 
 __global__ void k_series_finish(const double* __restrict__ partial, int blocks, long long max_it,
                                 SeriesState* __restrict__ state) {
-  if (threadIdx.x != 0 || state->done) return;
-  double a = 0.0, t = 0.0;
-  for (int b = 0; b < blocks; ++b) {
-    a += partial[2 * b];
-    t += partial[2 * b + 1];
-  }
+  if (state->done) return;  // one warp: the same value on every lane
+  const int lane = threadIdx.x & 31;
+  const double a = warp_sum_partials(partial, blocks, 2, 0, lane);
+  const double t = warp_sum_partials(partial, blocks, 2, 1, lane);
+  if (lane != 0) return;
   state->iters += 1;
   if (a <= state->tol_abs) {
     state->done = 1;
@@ -101,9 +100,8 @@ __global__ void __launch_bounds__(256) k_series_init(const double* __restrict__ 
 
 __global__ void k_series_tol(const double* __restrict__ partial, int blocks, double rtol,
                              SeriesState* __restrict__ state) {
+  const double a = warp_sum_partials(partial, blocks, 1, 0, threadIdx.x & 31);
   if (threadIdx.x != 0) return;
-  double a = 0.0;
-  for (int b = 0; b < blocks; ++b) a += partial[b];
   const double tiny = 2.2250738585072014e-308;
   state->done = 0;
   state->iters = 0;
