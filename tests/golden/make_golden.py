@@ -22,6 +22,10 @@ where the reference is not installed:
   field, wall-flux metrics, Newton and GMRES iteration record).
 * ``coupled.json``: the archived rows of results/coupled.csv for the canonical
   microstructures (groups canonical and thickness) with their case parameters.
+* ``prescribed_cases.json``: all 48 cases of data/cases_prescribed_field.csv (seeds, append
+  seeds and decision, conditions, phase hash) with their archived rows of
+  results/prescribed_field.csv (q_h, q_c, q_i and the A/B wall-channel difference); their
+  18 microstructures are stored like the canonical ones (``canonical_<name>.npz``).
 """
 
 from __future__ import annotations
@@ -172,6 +176,36 @@ def coupled_rows(ref):
     print("coupled rows:", len(rows))
 
 
+def prescribed_cases(ref):
+    cases = list(csv.DictReader(open(ref / "data" / "cases_prescribed_field.csv")))
+    res = list(csv.DictReader(open(ref / "results" / "prescribed_field.csv")))
+    out = []
+    for c in cases:
+        rows = [r for r in res if r["case_id"] == c["case_id"]]
+        out.append(dict(
+            case_id=c["case_id"], group=c["group"], structure=c["structure"], microstructure=c["microstructure"],
+            axis=c["transfer_axis"], H_m=float(c["H_m"]), rays_per_patch=int(c["rays_per_patch_per_block"]),
+            seeds_A=[int(x) for x in c["seeds_A"].split(";")], seeds_B=[int(x) for x in c["seeds_B"].split(";")],
+            append_seeds_A=[int(x) for x in c["append_seeds_A"].split(";")],
+            append_seeds_B=[int(x) for x in c["append_seeds_B"].split(";")],
+            append_used=c["append_used"] == "true",
+            conditions=[[float(a) for a in item.split("/")] for item in c["conditions"].split(";")],
+            phase_sha256_x=c["phase_sha256_x"], delta_T_K=float(rows[0]["delta_T_K"]),
+            ab_wall_channel_rel_difference=float(rows[0]["ab_wall_channel_rel_difference"]),
+            rows=[dict(T_mean_K=float(r["T_mean_K"]), epsilon=float(r["epsilon"]), q_h=float(r["q_h_W_m2"]),
+                       q_c=float(r["q_c_W_m2"]), q_i=float(r["q_i_W_m2"])) for r in rows]))
+    (HERE / "prescribed_cases.json").write_text(json.dumps(dict(
+        cases=out, source="data/cases_prescribed_field.csv, results/prescribed_field.csv"), indent=1))
+    names = sorted({c["microstructure"] for c in out})
+    for name in names:
+        ph = np.load(ref / "data" / "microstructures" / f"{name}.npz")["phases"]
+        assert ph.dtype == np.uint8 and set(np.unique(ph)) <= {0, 1}
+        np.savez_compressed(HERE / f"canonical_{name}.npz", bits=np.packbits(ph.ravel()),
+                            shape=np.asarray(ph.shape, np.int64),
+                            sha256=np.bytes_(hashlib.sha256(ph.tobytes()).hexdigest()))
+    print("prescribed-field cases:", len(out), "microstructures:", len(names))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -184,6 +218,7 @@ def main():
         small_case(vf, ex, cp, name, spec)
         coupled_small(name, spec)
     coupled_rows(ref)
+    prescribed_cases(ref)
 
     rows = list(csv.DictReader(open(ref / "data" / "cases_coupled.csv")))
     hashes = {}

@@ -46,3 +46,9 @@ def coupled_rows() -> list[dict]:
     """Archived results/coupled.csv rows of the canonical microstructures with their case parameters."""
 
     return json.loads((GOLDEN / "coupled.json").read_text())["rows"]
+
+
+def prescribed_cases() -> list[dict]:
+    """All 48 prescribed-field cases with their archived rows (tests/golden/make_golden.py)."""
+
+    return json.loads((GOLDEN / "prescribed_cases.json").read_text())["cases"]
