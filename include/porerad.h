@@ -291,6 +291,29 @@ PR_API int pr_coupled_solve(const pr_case* c, const pr_operator* op, const pr_co
                             double* patch_emitted, double* patch_absorbed, double* cell_net_power,
                             pr_coupled_result* result, void* stream);
 
+/* ---- multi-bounce ray statistics (porerad/properties.py, porerad/penetration.py) ----
+ * Rays enter the slab (the case's solid cells, x-oriented) through x = 0 at uniform
+ * transverse positions, at normal incidence (properties) or with Lambertian directions
+ * (penetration); at a solid surface a ray is absorbed with probability epsilon, else
+ * reflected diffusely, for at most max_bounces reflections.  Restart rule of a reflected ray
+ * (properties.py:14-22): */
+enum { PR_RESTART_ARTICLE = 0, PR_RESTART_HIT_POINT = 1 };
+typedef struct {
+  int64_t events, censored, interactions, scattered;
+  double event_length, censored_length, sum_mu, sum_mu2;
+} pr_properties_tally;
+/* Replaces the ray kernel of trace_properties(phases, axis, epsilon, n_rays=, seed=,
+ * max_bounces=, restart=), properties.py:53-279: first-segment interceptions (events) and
+ * right-censored crossings with their lengths in cells, surface interactions, reflections,
+ * and the sums of the cosine mu between incoming and reflected directions and of mu^2. */
+PR_API int pr_radiative_properties(const pr_case* c, double epsilon, int64_t n_rays, uint32_t seed, int restart,
+                                   int max_bounces, pr_properties_tally* out, void* stream);
+/* Replaces the ray kernel of trace_penetration(...), penetration.py:200-305: counts of rays
+ * reflected (left through x = 0), transmitted (x = N), absorbed, and stopped at the
+ * reflection or step limit (counts[0..3]). */
+PR_API int pr_penetration(const pr_case* c, double epsilon, int64_t n_rays, uint32_t seed, int restart,
+                          int max_bounces, int64_t* counts, void* stream);
+
 /* ---- instrumentation (no counterpart in the reference) ----------------------------
  * Kernel classes timed with CUDA events on their launching stream while enabled:
  * 0 fused ray generation + traversal, 1 per-patch count reduction, 2 balancing

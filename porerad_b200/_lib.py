@@ -52,6 +52,13 @@ COUPLED_FAILURES = {0: "", 1: "linear solve did not converge", 2: "line search f
                     3: "maximum Newton iterations reached"}
 
 
+class PropertiesTally(ctypes.Structure):
+    """pr_properties_tally: tallies of one properties run."""
+
+    _fields_ = [("events", _i64), ("censored", _i64), ("interactions", _i64), ("scattered", _i64),
+                ("event_length", _f64), ("censored_length", _f64), ("sum_mu", _f64), ("sum_mu2", _f64)]
+
+
 class CoupledLinear(ctypes.Structure):
     """pr_coupled_linear: one Newton correction's linear solve."""
 
@@ -111,6 +118,9 @@ _SIGNATURES = {
     "pr_conduction_wall_fluxes": (_i32, [_vp, _vp, _f64, _f64, ctypes.POINTER(_f64), ctypes.POINTER(_f64), _vp]),
     "pr_coupled_solve": (_i32, [_vp, _vp, _vp, _f64, _f64, _f64, _vp, _i32, _vp, _vp, _vp, _vp, _vp,
                                 ctypes.POINTER(CoupledResultC), _vp]),
+    "pr_radiative_properties": (_i32, [_vp, _f64, _i64, ctypes.c_uint32, _i32, _i32,
+                                       ctypes.POINTER(PropertiesTally), _vp]),
+    "pr_penetration": (_i32, [_vp, _f64, _i64, ctypes.c_uint32, _i32, _i32, _vp, _vp]),
     "pr_timers_enable": (None, [_i32]),
     "pr_timers_reset": (None, []),
     "pr_timers_read": (_i32, [_i32, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_f64)]),

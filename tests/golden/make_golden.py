@@ -26,6 +26,8 @@ where the reference is not installed:
   seeds and decision, conditions, phase hash) with their archived rows of
   results/prescribed_field.csv (q_h, q_c, q_i and the A/B wall-channel difference); their
   18 microstructures are stored like the canonical ones (``canonical_<name>.npz``).
+* ``multibounce.json``: the archived rows of results/radiative_properties.csv and
+  results/penetration_response.csv for the microstructures stored here.
 """
 
 from __future__ import annotations
@@ -206,6 +208,27 @@ def prescribed_cases(ref):
     print("prescribed-field cases:", len(out), "microstructures:", len(names))
 
 
+def multibounce_rows(ref):
+    have = {p.name[len("canonical_"):-4] for p in HERE.glob("canonical_*.npz")}
+    out = {}
+    for key, name in (("properties", "radiative_properties.csv"), ("penetration", "penetration_response.csv")):
+        rows = []
+        for r in csv.DictReader(open(ref / "results" / name)):
+            if r["microstructure"] not in have:
+                continue
+            row = {k: r[k] for k in ("microstructure", "structure", "transfer_axis")}
+            for k, v in r.items():
+                if k not in row and k != "retained":
+                    row[k] = float(v)
+            if "retained" in r:
+                row["retained"] = r["retained"] == "True"
+            rows.append(row)
+        out[key] = rows
+    out["source"] = "results/radiative_properties.csv, results/penetration_response.csv"
+    (HERE / "multibounce.json").write_text(json.dumps(out, indent=1))
+    print("multibounce rows:", {k: len(v) for k, v in out.items() if k != "source"})
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -219,6 +242,7 @@ def main():
         coupled_small(name, spec)
     coupled_rows(ref)
     prescribed_cases(ref)
+    multibounce_rows(ref)
 
     rows = list(csv.DictReader(open(ref / "data" / "cases_coupled.csv")))
     hashes = {}

@@ -52,3 +52,9 @@ def prescribed_cases() -> list[dict]:
     """All 48 prescribed-field cases with their archived rows (tests/golden/make_golden.py)."""
 
     return json.loads((GOLDEN / "prescribed_cases.json").read_text())["cases"]
+
+
+def multibounce_rows() -> dict:
+    """Archived properties and penetration rows of the stored microstructures (tests/golden/make_golden.py)."""
+
+    return json.loads((GOLDEN / "multibounce.json").read_text())
