@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the surface-radiation path on B200: first-hit rays/s and cases/s.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1|c3|c4|c5|coupled|descriptors] [--impl ours|reference]
 
 Workload c2 (default, the configuration the headline metric is quoted on): open-cell
 foam (OF) N=128^3, phi = 0.10, 64 Poisson seeds, geometry seed 1; 1000 rays per patch
@@ -63,6 +63,10 @@ WORKLOADS = {
                              "690->710 K along x): counts, balanced operator, conduction assembly + PCG, Newton-Krylov "
                              "(flexible GMRES, radiosity JVP, Jacobi-PCG preconditioner, line search)",
                     case_id="coupled_OF_x_T700_eps0.6_N128"),
+    "descriptors": dict(workload="morphology descriptors (scalar: phi_s, A_s, L_m, axial pore chords, 26-connected "
+                                 "pore percolation and largest cluster; directional: periodic chord histograms, "
+                                 "lineal path, interface normals) of the 22 stored 128^3 microstructures (OF/FI/FA/TL "
+                                 "core, canonical and matched pairs); L2 flushed before each step"),
     "c1": dict(workload="FI N=64^3 phi=0.10 (r=2, seed 0), 64 rays/patch x 1 set, eps 0.9, T 600->700 K along x, "
                         "FP64 radiosity",
                arch="FI", n=64, phi=0.10, seed=0, rays=64, sets=1, eps=0.9, T_m=650.0, dT=100.0, H=0.01),
@@ -833,11 +837,147 @@ def run_c5(args, cfg):
 
 # --------------------------------------------------------------------------- reference arm
 
+# --------------------------------------------------------------------------- morphology descriptors
+
+def _stored_microstructures():
+    golden = ROOT / "tests" / "golden"
+    out = []
+    for path in sorted(golden.glob("canonical_*.npz")):
+        with np.load(path) as z:
+            shape = tuple(int(v) for v in z["shape"])
+            out.append((path.name[len("canonical_"):-4],
+                        np.unpackbits(z["bits"])[: int(np.prod(shape))].reshape(shape).astype(np.uint8)))
+    return out
+
+
+def _descriptor_cpu_one(ph):
+    from oracle import morphology as om
+
+    return om.scalar_descriptors(ph), om.directional_descriptors(ph)
+
+
+def descriptors_cpu_sample(arrays, target_s: float):
+    """The oracle (NumPy/SciPy restatement of porerad.descriptors, scipy.ndimage.label for the clusters) on
+    the stored microstructures, one per process on every host core, until about target_s seconds of work."""
+
+    import multiprocessing as mp
+
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    done = 0
+    with mp.get_context("spawn").Pool(cores) as pool:
+        pool.map(_descriptor_cpu_one, [arrays[0]])  # start-up of the workers, untimed
+        t0 = time.perf_counter()
+        while True:
+            batch = [arrays[(done + i) % len(arrays)] for i in range(max(cores, len(arrays)))]
+            pool.map(_descriptor_cpu_one, batch, chunksize=1)
+            done += len(batch)
+            if time.perf_counter() - t0 >= target_s:
+                break
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": "microstructures/s", "cores": cores, "kind": "port",
+            "sample": f"{done} descriptor evaluations of the stored 128^3 microstructures in {dt:.1f} s "
+                      f"(scalar + directional, oracle, {cores} spawn workers)"}
+
+
+def run_descriptors_bench(args, cfg):
+    import torch
+
+    from porerad_b200 import _lib, descriptors as dm
+
+    torch.cuda.set_device(0)
+    lib = _lib.load()
+    named = _stored_microstructures()
+    host = [ph for _, ph in named]
+    dev = [torch.from_numpy(ph).cuda() for ph in host]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # 256 MB > L2
+    peaks, kind = measured_peaks()
+    cells = sum(int(ph.size) for ph in host)
+
+    def step(arrays):
+        return [dm.all_descriptors(a) for a in arrays]
+
+    for _ in range(max(args.warmup, 3)):
+        step(dev)
+    torch.cuda.synchronize()
+    lib.pr_timers_reset()
+    lib.pr_timers_enable(1)
+    launches0 = lib.pr_kernel_launches()
+    total_ms = 0.0
+    with ClockSampler(0) as clocks:
+        for _ in range(args.steps):
+            flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            out = step(dev)
+            e1.record()
+            torch.cuda.synchronize()
+            total_ms += e0.elapsed_time(e1)
+    lib.pr_timers_enable(0)
+    launches = lib.pr_kernel_launches() - launches0
+    timers = {}
+    for name, tid in (("morph", _lib.TIMER_MORPH), ("label", _lib.TIMER_LABEL)):
+        n, t = _lib.ctypes.c_longlong(), _lib.ctypes.c_double()
+        lib.pr_timers_read(tid, _lib.ctypes.byref(n), _lib.ctypes.byref(t))
+        timers[name] = (int(n.value), float(t.value))
+    value = args.steps * len(dev) / (total_ms * 1e-3)
+
+    # end to end from host arrays (pageable numpy, as a user passes them)
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        step(host)
+        torch.cuda.synchronize()
+        e2e_ms += 1e3 * (time.perf_counter() - t0)
+    e2e = args.steps * len(host) / (e2e_ms * 1e-3)
+
+    # roofline of the counts pass: one byte read per cell (the neighbours come from cache)
+    n_m, t_m = timers["morph"]
+    per_launch_bytes = cells / len(dev)
+    achieved = per_launch_bytes / (t_m / n_m * 1e-3) / 1e9 if n_m else None
+    n_l, t_l = timers["label"]
+    cpu = None if args.no_cpu else descriptors_cpu_sample(host, args.cpu_seconds)
+    check = out[0][0]
+    return {
+        "metric": "morphology descriptors (scalar + directional) per second", "value": value,
+        "unit": "microstructures/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8", "data": "reference microstructures (tests/golden)",
+        "config": {"workload": cfg["workload"], "microstructures": len(dev), "cells": cells,
+                   "l2": "flushed (256 MB write) before each step, outside the timed region"},
+        "e2e": {"value": e2e, "unit": "microstructures/s", "h2d_bytes_per_step": cells,
+                "d2h_bytes_per_step": int(sum(8 * (18 + sum(n + 1 for n in ph.shape)) for ph in host))},
+        "roofline": {"bound": "hbm", "kernel": "k_morph_counts", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"] if achieved else None,
+                     "peak_source": f"MEASURED_PEAKS.json ({kind})", "traffic": None,
+                     "bytes_per_launch": per_launch_bytes, "ms_per_launch": t_m / n_m if n_m else None},
+        "kernel_ms_per_microstructure": {"morph_counts": t_m / max(n_m, 1), "labelling": t_l / max(n_l, 1)},
+        "clocks": clocks.summary(), "gpu_launches": int(launches) // max(args.steps, 1), "cpu_baseline": cpu,
+        "first_result": {"phi_solid": check["phi_solid"], "mean_beam_length": check["mean_beam_length"]},
+    }
+
+
 def run_reference(args, cfg):
     from porerad_b200 import replicas
 
     if replicas.rank() != 0:
         return None  # the CPU reference runs once, on rank 0
+    if args.workload == "descriptors":
+        arrays = [ph for _, ph in _stored_microstructures()]
+        vals, last = [], None
+        for _ in range(args.steps):
+            last = descriptors_cpu_sample(arrays, max(1.0, args.cpu_seconds / 2))
+            vals.append(last["value"])
+        value = float(np.mean(vals))
+        return {"impl": "reference", "metric": "morphology descriptors (scalar + directional) per second",
+                "value": value, "unit": "microstructures/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": 0,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+                "data": "reference microstructures (tests/golden)", "config": {"workload": cfg["workload"]},
+                "cpu_baseline": {**last, "value": value},
+                "e2e": {"value": value, "unit": "microstructures/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if "case_id" in cfg:  # the coupled workload: the whole case on the host cores
         row, ph = _coupled_case(cfg["case_id"])
         vals, last = [], None
@@ -886,6 +1026,8 @@ def main():
         line = run_c3(args, cfg)
     elif args.workload == "coupled":
         line = run_coupled_bench(args, cfg)
+    elif args.workload == "descriptors":
+        line = run_descriptors_bench(args, cfg)
     elif args.workload == "c4":
         line = run_c4(args, cfg)
     elif args.workload == "c5":

@@ -314,11 +314,35 @@ PR_API int pr_radiative_properties(const pr_case* c, double epsilon, int64_t n_r
 PR_API int pr_penetration(const pr_case* c, double epsilon, int64_t n_rays, uint32_t seed, int restart,
                           int max_bounces, int64_t* counts, void* stream);
 
+/* ---- morphology descriptors ----------------------------------------------------
+ * Integer counts behind the scalar and directional descriptors of porerad/descriptors.py,
+ * for a uint8 phase array (nx, ny, nz) in C order (1 solid, 0 pore), on the host or the
+ * device.  Always: solid and pore cells; solid/non-solid faces inside the box per normal
+ * axis (interface_area, descriptors.py:38-43); pore/non-pore faces of the periodic cell
+ * (interface_face_counts, descriptors.py:120-123); pore runs per axis ending at the box
+ * faces (mean_pore_chords, descriptors.py:46-48: pore cells / runs).
+ * PR_MORPH_CHORDS: the periodic pore chords along each axis (periodic_chords,
+ * descriptors.py:82-109) as histograms chord_counts_a[0..n_a] of chord lengths (NULL skips
+ * the copy), and the all-pore lines.  PR_MORPH_CONNECTIVITY: 26-connected pore clusters
+ * (pore_connectivity, descriptors.py:51-60): their number, the largest, and percolation along
+ * each axis.  Fields not asked for are -1.  Arrays of 2^31 - 1 cells or more: PR_ERR_LIMIT. */
+enum { PR_MORPH_CHORDS = 1, PR_MORPH_CONNECTIVITY = 2 };
+typedef struct {
+  int64_t cells, solid_cells, pore_cells;
+  int64_t interface_faces[3], periodic_faces[3], pore_runs[3], all_pore_lines[3];
+  int64_t pore_clusters, largest_pore_cluster;
+  int32_t pore_percolates[3];
+} pr_morphology;
+PR_API int pr_morphology_counts(const uint8_t* phases, int64_t nx, int64_t ny, int64_t nz, int what,
+                                pr_morphology* out, int64_t* chord_counts_x, int64_t* chord_counts_y,
+                                int64_t* chord_counts_z, void* stream);
+
 /* ---- instrumentation (no counterpart in the reference) ----------------------------
  * Kernel classes timed with CUDA events on their launching stream while enabled:
  * 0 fused ray generation + traversal, 1 per-patch count reduction, 2 balancing
  * product, 3 reflection-series product, 4 binary32 Chebyshev sweep, 5 binary64
- * refinement residual. */
+ * refinement residual, 6 morphology counts (one pass over the phase array), 7 pore cluster
+ * labelling (union-find, sizes, summary). */
 PR_API void pr_timers_enable(int on);
 PR_API void pr_timers_reset(void);
 PR_API int pr_timers_read(int kernel_class, long long* launches, double* total_ms);

@@ -59,6 +59,14 @@ class PropertiesTally(ctypes.Structure):
                 ("event_length", _f64), ("censored_length", _f64), ("sum_mu", _f64), ("sum_mu2", _f64)]
 
 
+class Morphology(ctypes.Structure):
+    """pr_morphology: integer counts behind the morphology descriptors."""
+
+    _fields_ = [("cells", _i64), ("solid_cells", _i64), ("pore_cells", _i64), ("interface_faces", _i64 * 3),
+                ("periodic_faces", _i64 * 3), ("pore_runs", _i64 * 3), ("all_pore_lines", _i64 * 3),
+                ("pore_clusters", _i64), ("largest_pore_cluster", _i64), ("pore_percolates", _i32 * 3)]
+
+
 class CoupledLinear(ctypes.Structure):
     """pr_coupled_linear: one Newton correction's linear solve."""
 
@@ -121,6 +129,7 @@ _SIGNATURES = {
     "pr_radiative_properties": (_i32, [_vp, _f64, _i64, ctypes.c_uint32, _i32, _i32,
                                        ctypes.POINTER(PropertiesTally), _vp]),
     "pr_penetration": (_i32, [_vp, _f64, _i64, ctypes.c_uint32, _i32, _i32, _vp, _vp]),
+    "pr_morphology_counts": (_i32, [_vp, _i64, _i64, _i64, _i32, _vp, _vp, _vp, _vp, _vp]),
     "pr_timers_enable": (None, [_i32]),
     "pr_timers_reset": (None, []),
     "pr_timers_read": (_i32, [_i32, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_f64)]),
@@ -132,7 +141,7 @@ _SIGNATURES = {
     "pr_trace_variant_info": (_i32, [ctypes.POINTER(_i32), ctypes.POINTER(_i32), ctypes.POINTER(ctypes.c_char_p)]),
 }
 
-TIMER_TRACE, TIMER_RLE, TIMER_BALANCE, TIMER_SERIES, TIMER_CHEB, TIMER_REFINE = range(6)
+TIMER_TRACE, TIMER_RLE, TIMER_BALANCE, TIMER_SERIES, TIMER_CHEB, TIMER_REFINE, TIMER_MORPH, TIMER_LABEL = range(8)
 
 _lock = threading.Lock()
 _lib = None

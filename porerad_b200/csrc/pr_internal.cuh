@@ -22,7 +22,7 @@ inline void launch_mark() { g_launches.fetch_add(1, std::memory_order_relaxed); 
 
 // Optional CUDA-event timers around the hot kernels (see timers.cu).
 enum TimerId { kTimerTrace = 0, kTimerRle = 1, kTimerBalance = 2, kTimerSeries = 3, kTimerCheb = 4,
-               kTimerRefine = 5, kTimerCount = 6 };
+               kTimerRefine = 5, kTimerMorph = 6, kTimerLabel = 7, kTimerCount = 8 };
 bool timers_on();
 void timer_begin(int id, cudaStream_t s);
 void timer_end(int id, cudaStream_t s);
@@ -106,6 +106,16 @@ struct DevBuf {
   }
   size_t bytes() const { return n * sizeof(T); }
 };
+
+// True for device (or managed) memory; host and unregistered pointers give false.
+inline bool is_device_pointer(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
 
 inline int grid_for(int64_t n, int block, int cap = 148 * 32) {
   int64_t g = (n + block - 1) / block;

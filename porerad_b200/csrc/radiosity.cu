@@ -629,14 +629,6 @@ static int noalloc_scratch(double** out) {
   return PR_OK;
 }
 
-static bool is_device_pointer(const void* p) {
-  cudaPointerAttributes a;
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
 
 static int series_fp64_noalloc(const pr_operator* op, const double* emitted, const double* eps, double rtol,
                                int64_t max_it, double* absorbed, double* residual, int64_t* iterations,

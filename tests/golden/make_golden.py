@@ -28,6 +28,11 @@ where the reference is not installed:
   18 microstructures are stored like the canonical ones (``canonical_<name>.npz``).
 * ``multibounce.json``: the archived rows of results/radiative_properties.csv and
   results/penetration_response.csv for the microstructures stored here.
+* ``descriptors.json``: porerad.descriptors run on every microstructure stored here
+  (scalar and directional descriptors, chord histograms, lineal paths) with their archived
+  columns of data/microstructures.csv, and on seeded small and 128^3 phase arrays
+  (``random_phases``; sha256 of each recorded), edge cases included (uniform arrays,
+  thin boxes, all-pore lines, a non-cubic box).
 """
 
 from __future__ import annotations
@@ -229,6 +234,79 @@ def multibounce_rows(ref):
     print("multibounce rows:", {k: len(v) for k, v in out.items() if k != "source"})
 
 
+DESCRIPTOR_SMALL = {
+    # name: (shape, solid fraction, seed); directional descriptors need every axis >= 128
+    "d7x5x6": ((7, 5, 6), 0.40, 1),
+    "d9": ((9, 9, 9), 0.20, 2),
+    "d1x6x5": ((1, 6, 5), 0.50, 3),
+    "d12x3x1": ((12, 3, 1), 0.30, 4),
+    "d16": ((16, 16, 16), 0.60, 5),
+    "d10": ((10, 10, 10), 0.02, 6),
+    "d128_half": ((128, 128, 128), 0.50, 7),
+    "d128_sparse": ((128, 128, 128), 0.004, 8),
+    "d128_box": ((128, 136, 144), 0.30, 9),
+}
+
+
+def _plain(v):
+    if isinstance(v, np.ndarray):
+        return v.tolist()
+    if isinstance(v, (tuple, list)):
+        return [_plain(x) for x in v]
+    if isinstance(v, (np.bool_, bool)):
+        return bool(v)
+    if isinstance(v, (np.integer,)):
+        return int(v)
+    if isinstance(v, (np.floating,)):
+        return float(v)
+    return v
+
+
+def _descriptor_record(dm, ph, directional):
+    rec = {"shape": list(ph.shape), "sha256": hashlib.sha256(ph.tobytes()).hexdigest()}
+    try:
+        rec["scalar"] = {k: _plain(v) for k, v in dm.scalar_descriptors(ph).items()}
+    except Exception as e:  # noqa: BLE001 - the reference's own error is the expected outcome
+        rec["scalar_error"] = type(e).__name__
+    pore = ph == 0
+    rec["chords"] = []
+    for a in range(3):
+        chords, allp, M, N = dm.periodic_chords(pore, a)
+        rec["chords"].append({"hist": np.bincount(chords, minlength=N + 1).tolist(), "all_pore": int(allp),
+                              "lines": int(M), "N": int(N)})
+    rec["interface_face_counts"] = dm.interface_face_counts(~pore).tolist()
+    if directional:
+        rec["directional"] = [{k: _plain(v) for k, v in row.items()} for row in dm.directional_descriptors(ph)]
+    return rec
+
+
+def descriptor_rows(ref):
+    from porerad import descriptors as dm  # noqa: E402
+
+    table = {r["id"]: r for r in csv.DictReader(open(ref / "data" / "microstructures.csv"))}
+    stored = {}
+    for path in sorted(HERE.glob("canonical_*.npz")):
+        name = path.name[len("canonical_"):-4]
+        ph = np.load(ref / "data" / "microstructures" / f"{name}.npz")["phases"]
+        rec = _descriptor_record(dm, ph, True)
+        r = table[name]
+        rec["archived"] = {k: (float(r[k]) if k not in ("structure", "set", "medoid") else r[k]) for k in (
+            "structure", "set", "N", "target_phi", "realized_phi", "interfacial_area_density_per_cell",
+            "mean_beam_length_cells", "mean_pore_chord_x_cells", "mean_pore_chord_y_cells",
+            "mean_pore_chord_z_cells", "medoid")}
+        stored[name] = rec
+    small = {}
+    for name, (shape, phi, seed) in DESCRIPTOR_SMALL.items():
+        ph = random_phases(shape, phi, seed)
+        small[name] = dict(_descriptor_record(dm, ph, min(shape) >= 128), phi=phi, seed=seed)
+    for name, value in (("d_solid", 1), ("d_pore", 0)):
+        ph = np.full((4, 5, 6), value, np.uint8)
+        small[name] = dict(_descriptor_record(dm, ph, False), fill=value)
+    (HERE / "descriptors.json").write_text(json.dumps(dict(
+        stored=stored, small=small, source="porerad/descriptors.py; data/microstructures.csv"), indent=None))
+    print("descriptor records:", len(stored), "stored,", len(small), "small")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -243,6 +321,7 @@ def main():
     coupled_rows(ref)
     prescribed_cases(ref)
     multibounce_rows(ref)
+    descriptor_rows(ref)
 
     rows = list(csv.DictReader(open(ref / "data" / "cases_coupled.csv")))
     hashes = {}

@@ -58,3 +58,32 @@ def multibounce_rows() -> dict:
     """Archived properties and penetration rows of the stored microstructures (tests/golden/make_golden.py)."""
 
     return json.loads((GOLDEN / "multibounce.json").read_text())
+
+
+def descriptor_records() -> dict:
+    """porerad.descriptors outputs stored by make_golden.descriptor_rows."""
+
+    return json.loads((GOLDEN / "descriptors.json").read_text())
+
+
+def random_phases(shape, phi, seed) -> np.ndarray:
+    """The seeded phase arrays of make_golden.random_phases (same generator and threshold)."""
+
+    rng = np.random.default_rng(seed)
+    field = rng.random(shape)
+    field = (field + np.roll(field, 1, axis=0) + np.roll(field, 1, axis=2)) / 3.0
+    thr = np.quantile(field, phi)
+    return (field < thr).astype(np.uint8)
+
+
+def descriptor_phases(name: str, rec: dict) -> np.ndarray:
+    """Phase array of a descriptor record: a stored microstructure, a seeded array or a uniform one."""
+
+    if "fill" in rec:
+        ph = np.full(tuple(rec["shape"]), rec["fill"], np.uint8)
+    elif "seed" in rec:
+        ph = random_phases(tuple(rec["shape"]), rec["phi"], rec["seed"])
+    else:
+        ph = load_canonical(name)
+    assert hashlib.sha256(ph.tobytes()).hexdigest() == rec["sha256"]
+    return ph
