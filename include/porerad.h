@@ -337,6 +337,32 @@ PR_API int pr_morphology_counts(const uint8_t* phases, int64_t nx, int64_t ny, i
                                 pr_morphology* out, int64_t* chord_counts_x, int64_t* chord_counts_y,
                                 int64_t* chord_counts_z, void* stream);
 
+/* ---- microstructure rendering ------------------------------------------------------
+ * The grid work of porerad/geometry.py's generators; the random parameters, the foam graph
+ * and the fiber frames are drawn on the host as the reference draws them.
+ * pr_render_shapes replaces the union of shape_mask(N, center, radii, kind, R) calls
+ * (geometry.py:85-121) for ellipsoids and cylinders no longer than the cell, as render_foam
+ * (geometry.py:201-208) forms it: phases (device, N^3 bytes, C order) receives 1 inside any
+ * shape and 0 elsewhere, evaluated cell for cell as the reference's NumPy expression is
+ * (minimum-image offsets with NumPy's float remainder, R^T x as OpenBLAS's dgemm forms it).
+ * pr_stamp_fibers replaces _long_cylinder (geometry.py:59-82) for n_fibers fibers: fiber f
+ * marks (nodes[j] + offsets[k]) mod N for its nodes node_start[f] <= j < node_start[f+1] and
+ * disk offsets offset_start[f] <= k < offset_start[f+1] (int32 triples); clear = 1 zeroes the
+ * array first.  solid_cells (may be NULL) receives the solid cells of the result. */
+enum { PR_SHAPE_ELLIPSOID = 0, PR_SHAPE_CYLINDER = 1 };
+typedef struct {
+  int32_t kind;
+  int32_t pad;
+  double center[3];
+  double R[9];     /* rotation, row-major; local axis i is column i */
+  double radii[3]; /* r_x, r_y, r_z (a cylinder's half length) */
+} pr_shape;
+PR_API int pr_render_shapes(int64_t N, const pr_shape* shapes, int n_shapes, uint8_t* phases, int64_t* solid_cells,
+                            void* stream);
+PR_API int pr_stamp_fibers(int64_t N, const int32_t* nodes, const int64_t* node_start, const int32_t* offsets,
+                           const int64_t* offset_start, int n_fibers, int clear, uint8_t* phases,
+                           int64_t* solid_cells, void* stream);
+
 /* ---- instrumentation (no counterpart in the reference) ----------------------------
  * Kernel classes timed with CUDA events on their launching stream while enabled:
  * 0 fused ray generation + traversal, 1 per-patch count reduction, 2 balancing

@@ -67,6 +67,12 @@ class Morphology(ctypes.Structure):
                 ("pore_clusters", _i64), ("largest_pore_cluster", _i64), ("pore_percolates", _i32 * 3)]
 
 
+class Shape(ctypes.Structure):
+    """pr_shape: one ellipsoid or cylinder of a rendered microstructure."""
+
+    _fields_ = [("kind", _i32), ("pad", _i32), ("center", _f64 * 3), ("R", _f64 * 9), ("radii", _f64 * 3)]
+
+
 class CoupledLinear(ctypes.Structure):
     """pr_coupled_linear: one Newton correction's linear solve."""
 
@@ -130,6 +136,8 @@ _SIGNATURES = {
                                        ctypes.POINTER(PropertiesTally), _vp]),
     "pr_penetration": (_i32, [_vp, _f64, _i64, ctypes.c_uint32, _i32, _i32, _vp, _vp]),
     "pr_morphology_counts": (_i32, [_vp, _i64, _i64, _i64, _i32, _vp, _vp, _vp, _vp, _vp]),
+    "pr_render_shapes": (_i32, [_i64, _vp, _i32, _vp, _vp, _vp]),
+    "pr_stamp_fibers": (_i32, [_i64, _vp, _vp, _vp, _vp, _i32, _i32, _vp, _vp, _vp]),
     "pr_timers_enable": (None, [_i32]),
     "pr_timers_reset": (None, []),
     "pr_timers_read": (_i32, [_i32, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_f64)]),

@@ -136,3 +136,12 @@ def ray_set_seed(case_seed: int, set_index: int, block: int = 0) -> int:
     """Seed of ray block ``block`` of ray set ``set_index`` (0 = A, 1 = B, ...) of a case (below 2^63)."""
 
     return splitmix64(splitmix64(splitmix64(int(case_seed)) ^ int(set_index)) ^ int(block)) >> 1
+
+
+# The reference's own generators (porerad/geometry.py), rendered on the device: the module is a
+# drop-in for porerad.geometry as well as the home of the benchmark archetypes above.
+from .generators import (  # noqa: E402,F401
+    CORE_N, CORE_PHIS, FA_THETA_SIGMA, FIBER_LENGTH, FIBER_LINES, FOAM_NEIGHBOURS, FOAM_NODES, MATCHED_PAIRS,
+    MIN_PORE_CLUSTER, NODE_TO_STRUT, PHI_TOL, STRUCTURES, TL_BASE_N, TL_LAYERS, TL_NOISE, accepted, build, canonical,
+    core_realizations, fiber_lines, foam_graph, lamellar_field, matched, render_fibers, render_foam, shape_mask,
+    threshold)

@@ -28,6 +28,8 @@ where the reference is not installed:
   18 microstructures are stored like the canonical ones (``canonical_<name>.npz``).
 * ``multibounce.json``: the archived rows of results/radiative_properties.csv and
   results/penetration_response.csv for the microstructures stored here.
+* ``microstructures.json``: every row of data/microstructures.csv (id, structure, set, N,
+  target solid fraction, seed, archived phase_sha256) for the generator tests.
 * ``descriptors.json``: porerad.descriptors run on every microstructure stored here
   (scalar and directional descriptors, chord histograms, lineal paths) with their archived
   columns of data/microstructures.csv, and on seeded small and 128^3 phase arrays
@@ -307,6 +309,16 @@ def descriptor_rows(ref):
     print("descriptor records:", len(stored), "stored,", len(small), "small")
 
 
+def microstructure_rows(ref):
+    rows = []
+    for r in csv.DictReader(open(ref / "data" / "microstructures.csv")):
+        rows.append(dict(id=r["id"], structure=r["structure"], set=r["set"], N=int(r["N"]),
+                         target_phi=float(r["target_phi"]), seed=int(r["seed"]), phase_sha256=r["phase_sha256"]))
+    (HERE / "microstructures.json").write_text(json.dumps(dict(rows=rows, source="data/microstructures.csv"),
+                                                          indent=1))
+    print("microstructure rows:", len(rows))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -322,6 +334,7 @@ def main():
     prescribed_cases(ref)
     multibounce_rows(ref)
     descriptor_rows(ref)
+    microstructure_rows(ref)
 
     rows = list(csv.DictReader(open(ref / "data" / "cases_coupled.csv")))
     hashes = {}

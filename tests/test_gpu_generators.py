@@ -1,0 +1,71 @@
+"""The reference's microstructure generators on the device (porerad_b200.generators) against the
+archived phase_sha256 column of data/microstructures.csv: every core, canonical and matched
+array, bit for bit, and the core library's seed acceptance."""
+
+from __future__ import annotations
+
+import hashlib
+import json
+
+import numpy as np
+import pytest
+
+from tests.helpers import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+ROWS = json.loads((GOLDEN / "microstructures.json").read_text())["rows"]
+
+
+@pytest.fixture(scope="module")
+def gen():
+    from porerad_b200 import geometry
+
+    return geometry
+
+
+def _sha(ph) -> str:
+    return hashlib.sha256(np.ascontiguousarray(ph, dtype=np.uint8).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("row", ROWS, ids=[r["id"] for r in ROWS])
+def test_archived_microstructure(gen, row):
+    if row["set"] == "core":
+        ph = gen.build(row["structure"], row["N"], row["target_phi"], row["seed"])
+    elif row["set"] == "canonical":
+        ph = gen.canonical(row["structure"], row["N"])
+    else:
+        ph = gen.matched(row["structure"], int(row["id"][-1]))
+    assert ph.dtype == np.uint8 and ph.shape == (row["N"],) * 3
+    assert _sha(ph) == row["phase_sha256"]
+
+
+def test_core_realizations_with_rejections(gen):
+    """FA at phi 0.05 rejects seeds 1 and 3 (no x-aligned chord signature); the device
+    descriptors make the same decisions as the reference's."""
+
+    got = gen.core_realizations("FA", 0.05)
+    want = {r["seed"]: r["phase_sha256"] for r in ROWS
+            if r["set"] == "core" and r["structure"] == "FA" and r["target_phi"] == 0.05}
+    assert [s for s, _ in got] == sorted(want)
+    for s, ph in got:
+        assert _sha(ph) == want[s]
+
+
+def test_device_outputs_and_single_shapes(gen):
+    import torch
+
+    dev = gen.build("OF", 64, 0.10, 3, device=True)
+    assert isinstance(dev, torch.Tensor) and dev.is_cuda and dev.dtype == torch.uint8
+    assert np.array_equal(dev.cpu().numpy(), gen.build("OF", 64, 0.10, 3))
+    # an axis-aligned ellipsoid and cylinder against the closed-form test on the CPU
+    N, c = 24, (5.5, 20.25, 0.0)
+    half = N / 2.0
+    ax = [(np.arange(N) - c[a] + half) % float(N) - half for a in range(3)]
+    x, y, z = np.meshgrid(*ax, indexing="ij")
+    ell = gen.shape_mask(N, c, (3.0, 4.5, 2.0), "ellipsoid", np.eye(3))
+    assert np.array_equal(ell, (x / 3.0) ** 2 + (y / 4.5) ** 2 + (z / 2.0) ** 2 <= 1.0)
+    cyl = gen.shape_mask(N, c, (2.5, 2.5, 6.0), "cylinder", np.eye(3))
+    assert np.array_equal(cyl, ((x / 2.5) ** 2 + (y / 2.5) ** 2 <= 1.0) & (np.abs(z) <= 6.0))
+    with pytest.raises(ValueError):
+        gen.shape_mask(N, c, (1.0, 1.0, 1.0), "cone", np.eye(3))
