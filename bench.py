@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the surface-radiation path on B200: first-hit rays/s and cases/s.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1|c3|c4|c5|coupled|descriptors] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1|c3|c4|c5|coupled|descriptors|generators] [--impl ours|reference]
 
 Workload c2 (default, the configuration the headline metric is quoted on): open-cell
 foam (OF) N=128^3, phi = 0.10, 64 Poisson seeds, geometry seed 1; 1000 rays per patch
@@ -67,6 +67,9 @@ WORKLOADS = {
                                  "pore percolation and largest cluster; directional: periodic chord histograms, "
                                  "lineal path, interface normals) of the 22 stored 128^3 microstructures (OF/FI/FA/TL "
                                  "core, canonical and matched pairs); L2 flushed before each step"),
+    "generators": dict(workload="the reference's core microstructure library: OF/FI/FA/TL x phi {0.05,0.10,0.15}, "
+                                "N=128^3, seeds 0,1,... until 4 per cell pass the acceptance rules (scalar "
+                                "descriptors); 48 accepted arrays, bit-identical to data/microstructures.csv"),
     "c1": dict(workload="FI N=64^3 phi=0.10 (r=2, seed 0), 64 rays/patch x 1 set, eps 0.9, T 600->700 K along x, "
                         "FP64 radiosity",
                arch="FI", n=64, phi=0.10, seed=0, rays=64, sets=1, eps=0.9, T_m=650.0, dT=100.0, H=0.01),
@@ -960,11 +963,122 @@ def run_descriptors_bench(args, cfg):
     }
 
 
+# --------------------------------------------------------------------------- microstructure generators
+
+def _generator_cpu_one(job):
+    from oracle import generators as og
+    from oracle import morphology as om
+
+    structure, phi, seed = job
+    ph = og.build(structure, 128, phi, seed)
+    om.scalar_descriptors(ph)
+    return int(ph.sum())
+
+
+def generators_cpu_sample(target_s: float):
+    """The oracle (NumPy/SciPy restatement of porerad.geometry, the reference's CPU algorithm) building
+    and describing core-library arrays, one per process on every host core, until about target_s
+    seconds of work: the 16 trials at phi 0.10 (4 seeds per structure) per round."""
+
+    import multiprocessing as mp
+
+    cores = os.cpu_count() or 1
+    jobs = [(s, 0.10, k) for s in ("OF", "FI", "FA", "TL") for k in range(4)]
+    done = 0
+    with mp.get_context("spawn").Pool(min(cores, len(jobs))) as pool:
+        pool.map(_generator_cpu_one, [("TL", 0.10, 0)])  # worker start-up, untimed
+        t0 = time.perf_counter()
+        while True:
+            pool.map(_generator_cpu_one, jobs, chunksize=1)
+            done += len(jobs)
+            if time.perf_counter() - t0 >= target_s:
+                break
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": "microstructures/s", "cores": min(cores, len(jobs)), "kind": "port",
+            "sample": f"{done} core-library trials at phi 0.10 (4 seeds x OF/FI/FA/TL, build + scalar "
+                      f"descriptors) in {dt:.1f} s on {min(cores, len(jobs))} spawn workers"}
+
+
+def run_generators_bench(args, cfg):
+    import torch
+
+    from porerad_b200 import _lib, generators as gen
+
+    torch.cuda.set_device(0)
+    lib = _lib.load()
+
+    def step(device=True):
+        out = []
+        for s in gen.STRUCTURES:
+            for phi in gen.CORE_PHIS:
+                out += gen.core_realizations(s, phi, device=device)
+        return out
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    lib.pr_timers_reset()
+    lib.pr_timers_enable(1)
+    launches0 = lib.pr_kernel_launches()
+    total_ms = 0.0
+    with ClockSampler(0) as clocks:
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            out = step()
+            e1.record()
+            torch.cuda.synchronize()
+            total_ms += e0.elapsed_time(e1)
+    lib.pr_timers_enable(0)
+    launches = lib.pr_kernel_launches() - launches0
+    n_r, t_r = _lib.ctypes.c_longlong(), _lib.ctypes.c_double()
+    lib.pr_timers_read(_lib.TIMER_RENDER, _lib.ctypes.byref(n_r), _lib.ctypes.byref(t_r))
+    value = args.steps * len(out) / (total_ms * 1e-3)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        host = step(device=False)
+    e2e = args.steps * len(host) / (time.perf_counter() - t0)
+    ms_render = t_r.value / max(n_r.value, 1)
+    achieved = 128 ** 3 / (ms_render * 1e-3) / 1e9 if n_r.value else None
+    peaks, kind = measured_peaks()
+    cpu = None if args.no_cpu else generators_cpu_sample(args.cpu_seconds)
+    return {
+        "metric": "core-library microstructures per second (generation + acceptance)", "value": value,
+        "unit": "microstructures/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (shape tests), u8", "data": "the reference's generators (seeded)",
+        "config": {"workload": cfg["workload"], "accepted": len(out),
+                   "l2": "every trial writes a fresh 2 MiB array; outputs stay resident"},
+        "e2e": {"value": e2e, "unit": "microstructures/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(len(host) * 128 ** 3)},
+        "roofline": {"bound": "hbm", "kernel": "k_render_shapes / k_stamp", "achieved": achieved,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"] if achieved else None,
+                     "peak_source": f"MEASURED_PEAKS.json ({kind})", "traffic": None,
+                     "note": "algorithmic bytes = the 2 MiB array written per rendering; the shape tests are "
+                             "FP64 compute, so this fraction is low by construction"},
+        "renders_per_step": int(n_r.value) // max(args.steps, 1), "ms_per_render": ms_render,
+        "clocks": clocks.summary(), "gpu_launches": int(launches) // max(args.steps, 1), "cpu_baseline": cpu,
+    }
+
+
 def run_reference(args, cfg):
     from porerad_b200 import replicas
 
     if replicas.rank() != 0:
         return None  # the CPU reference runs once, on rank 0
+    if args.workload == "generators":
+        vals, last = [], None
+        for _ in range(args.steps):
+            last = generators_cpu_sample(max(1.0, args.cpu_seconds / 2))
+            vals.append(last["value"])
+        value = float(np.mean(vals))
+        return {"impl": "reference", "metric": "core-library microstructures per second (generation + acceptance)",
+                "value": value, "unit": "microstructures/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": 0,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 (shape tests), u8",
+                "data": "the reference's generators (seeded)", "config": {"workload": cfg["workload"]},
+                "cpu_baseline": {**last, "value": value},
+                "e2e": {"value": value, "unit": "microstructures/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if args.workload == "descriptors":
         arrays = [ph for _, ph in _stored_microstructures()]
         vals, last = [], None
@@ -1028,6 +1142,8 @@ def main():
         line = run_coupled_bench(args, cfg)
     elif args.workload == "descriptors":
         line = run_descriptors_bench(args, cfg)
+    elif args.workload == "generators":
+        line = run_generators_bench(args, cfg)
     elif args.workload == "c4":
         line = run_c4(args, cfg)
     elif args.workload == "c5":

@@ -368,7 +368,7 @@ PR_API int pr_stamp_fibers(int64_t N, const int32_t* nodes, const int64_t* node_
  * 0 fused ray generation + traversal, 1 per-patch count reduction, 2 balancing
  * product, 3 reflection-series product, 4 binary32 Chebyshev sweep, 5 binary64
  * refinement residual, 6 morphology counts (one pass over the phase array), 7 pore cluster
- * labelling (union-find, sizes, summary). */
+ * labelling (union-find, sizes, summary), 8 microstructure rendering (shapes or fibers). */
 PR_API void pr_timers_enable(int on);
 PR_API void pr_timers_reset(void);
 PR_API int pr_timers_read(int kernel_class, long long* launches, double* total_ms);

@@ -149,7 +149,7 @@ _SIGNATURES = {
     "pr_trace_variant_info": (_i32, [ctypes.POINTER(_i32), ctypes.POINTER(_i32), ctypes.POINTER(ctypes.c_char_p)]),
 }
 
-TIMER_TRACE, TIMER_RLE, TIMER_BALANCE, TIMER_SERIES, TIMER_CHEB, TIMER_REFINE, TIMER_MORPH, TIMER_LABEL = range(8)
+TIMER_TRACE, TIMER_RLE, TIMER_BALANCE, TIMER_SERIES, TIMER_CHEB, TIMER_REFINE, TIMER_MORPH, TIMER_LABEL, TIMER_RENDER = range(9)
 
 _lock = threading.Lock()
 _lib = None

@@ -191,8 +191,10 @@ PR_API int pr_render_shapes(int64_t N, const pr_shape* shapes, int n_shapes, uin
   delete[] host;
   PR_CUDA(e);
   const int64_t n = N * N * N;
+  timer_begin(kTimerRender, s);
   k_render_shapes<<<grid_for(n, 256, sm_count() * 16), 256, sizeof(GenShape) * (size_t)n_shapes, s>>>(
       (int)N, dev.ptr, n_shapes, phases);
+  timer_end(kTimerRender, s);
   launch_mark();
   PR_CUDA(cudaGetLastError());
   if (solid_cells) PR_TRY(count_solid(phases, n, solid_cells, s));
@@ -230,8 +232,10 @@ PR_API int pr_stamp_fibers(int64_t N, const int32_t* nodes, const int64_t* node_
       const int64_t w = (node_start[f + 1] - node_start[f]) * (offset_start[f + 1] - offset_start[f]);
       most = w > most ? w : most;
     }
+    timer_begin(kTimerRender, s);
     k_stamp<<<grid_for(most, 256, sm_count() * 8), 256, 0, s>>>((int)N, dn.ptr, dn0.ptr, dof.ptr, do0.ptr, n_fibers,
                                                                 phases);
+    timer_end(kTimerRender, s);
     launch_mark();
     PR_CUDA(cudaGetLastError());
     PR_CUDA(cudaStreamSynchronize(s));  // the host ranges may be freed by the caller on return

@@ -22,7 +22,7 @@ inline void launch_mark() { g_launches.fetch_add(1, std::memory_order_relaxed); 
 
 // Optional CUDA-event timers around the hot kernels (see timers.cu).
 enum TimerId { kTimerTrace = 0, kTimerRle = 1, kTimerBalance = 2, kTimerSeries = 3, kTimerCheb = 4,
-               kTimerRefine = 5, kTimerMorph = 6, kTimerLabel = 7, kTimerCount = 8 };
+               kTimerRefine = 5, kTimerMorph = 6, kTimerLabel = 7, kTimerRender = 8, kTimerCount = 9 };
 bool timers_on();
 void timer_begin(int id, cudaStream_t s);
 void timer_end(int id, cudaStream_t s);
