@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the surface-radiation path on B200: first-hit rays/s and cases/s.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1|c3|c4|c5|coupled|descriptors|generators] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1|c3|c4|c5|coupled|descriptors|generators|properties] [--impl ours|reference]
 
 Workload c2 (default, the configuration the headline metric is quoted on): open-cell
 foam (OF) N=128^3, phi = 0.10, 64 Poisson seeds, geometry seed 1; 1000 rays per patch
@@ -70,6 +70,10 @@ WORKLOADS = {
     "generators": dict(workload="the reference's core microstructure library: OF/FI/FA/TL x phi {0.05,0.10,0.15}, "
                                 "N=128^3, seeds 0,1,... until 4 per cell pass the acceptance rules (scalar "
                                 "descriptors); 48 accepted arrays, bit-identical to data/microstructures.csv"),
+    "properties": dict(workload="multi-bounce identifications of the archived set: 12 stored core 128^3 microstructures "
+                                "x axes x/y/z x eps {0.3,0.6,0.9}: radiative properties (2 seeds x 2e5 normal-incidence "
+                                "rays) and penetration response (2 seeds x 5e5 Lambertian rays), restart 'article', "
+                                "at most 1000 reflections"),
     "c1": dict(workload="FI N=64^3 phi=0.10 (r=2, seed 0), 64 rays/patch x 1 set, eps 0.9, T 600->700 K along x, "
                         "FP64 radiosity",
                arch="FI", n=64, phi=0.10, seed=0, rays=64, sets=1, eps=0.9, T_m=650.0, dT=100.0, H=0.01),
@@ -1062,11 +1066,148 @@ def run_generators_bench(args, cfg):
     }
 
 
+# --------------------------------------------------------------------------- multi-bounce statistics
+
+def _multibounce_jobs():
+    from tests.helpers import multibounce_rows
+
+    rows = multibounce_rows()
+    jobs = []
+    for kind in ("properties", "penetration"):
+        for r in rows[kind]:
+            jobs.append((kind, r["microstructure"], r["transfer_axis"], float(r["epsilon"])))
+    return jobs
+
+
+def _solid_x(name, axis):
+    from tests.helpers import load_canonical
+
+    ph = load_canonical(name)
+    return np.ascontiguousarray(np.moveaxis(ph == 1, "xyz".index(axis), 0)).astype(np.uint8)
+
+
+_MB_SEEDS = {"properties": ((123, 456), 200_000), "penetration": ((321, 654), 500_000)}
+
+
+def _multibounce_cpu_one(job):
+    from oracle import multibounce as om
+
+    kind, name, axis, eps = job
+    seeds, n = _MB_SEEDS[kind]
+    solid = _solid_x(name, axis)
+    for s in seeds:
+        om.run(solid, eps, n, s, penetration=kind == "penetration")
+    return len(seeds) * n
+
+
+def multibounce_cpu_sample(target_s: float):
+    """The oracle (C restatement of the reference's ray kernels, OpenMP over rays on every host core)
+    on identifications of the archived set in order until about target_s seconds."""
+
+    jobs = _multibounce_jobs()
+    rays, done = 0, 0
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < target_s and done < len(jobs):
+        rays += _multibounce_cpu_one(jobs[(done * 37) % len(jobs)])  # a spread over structures and kinds
+        done += 1
+    dt = time.perf_counter() - t0
+    return {"value": rays / dt, "unit": "rays/s", "cores": os.cpu_count() or 1, "kind": "port",
+            "sample": f"{done} identifications ({rays} source rays) of the archived set in {dt:.1f} s, "
+                      "oracle/multibounce.c with OpenMP"}
+
+
+def run_properties_bench(args, cfg):
+    import torch
+
+    from porerad_b200 import _lib, penetration, properties
+
+    torch.cuda.set_device(0)
+    lib = _lib.load()
+    jobs = _multibounce_jobs()
+    geos = {}
+    for kind, name, axis, eps in jobs:
+        if (name, axis) not in geos:
+            geos[(name, axis)] = properties._geometry(np.asarray(load_phases(name)), axis)
+    rays_per_step = sum(len(_MB_SEEDS[k][0]) * _MB_SEEDS[k][1] for k, *_ in jobs)
+
+    def step(resident=True):
+        if resident:  # every run of the set at once, RUN_STREAMS in flight
+            calls = []
+            for kind, name, axis, eps in jobs:
+                seeds, n = _MB_SEEDS[kind]
+                fn = properties.trace_properties if kind == "properties" else penetration.trace_penetration
+                calls += [(fn, (None, axis, eps), dict(n_rays=n, seed=s, _geo=geos[(name, axis)])) for s in seeds]
+            return properties.run_concurrently(calls)
+        out = []
+        for kind, name, axis, eps in jobs:
+            if kind == "properties":
+                out.append(properties.identify_properties(load_phases(name), axis, eps))
+            else:
+                out.append(penetration.penetration_response(load_phases(name), axis, eps))
+        return out
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    launches0 = lib.pr_kernel_launches()
+    total_ms = 0.0
+    with ClockSampler(0) as clocks:
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            step()
+            e1.record()
+            torch.cuda.synchronize()
+            total_ms += e0.elapsed_time(e1)
+    launches = lib.pr_kernel_launches() - launches0
+    value = args.steps * rays_per_step / (total_ms * 1e-3)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step(resident=False)
+    e2e = args.steps * rays_per_step / (time.perf_counter() - t0)
+    for g in geos.values():
+        g.close()
+    cpu = None if args.no_cpu else multibounce_cpu_sample(args.cpu_seconds)
+    return {
+        "metric": "multi-bounce source rays per second (archived identification set)", "value": value,
+        "unit": "rays/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "reference microstructures (tests/golden)",
+        "config": {"workload": cfg["workload"], "identifications": len(jobs), "rays_per_step": rays_per_step,
+                   "l2": "the 12 solid grids (2 MiB each) stay resident; rays carry no memory traffic"},
+        "e2e": {"value": e2e, "unit": "rays/s", "h2d_bytes_per_step": int(len(jobs) * 128 ** 3),
+                "d2h_bytes_per_step": int(len(jobs) * 2 * 64)},
+        "roofline": None,
+        "roofline_note": "one thread follows one ray through cell steps and reflections: issue- and "
+                         "divergence-bound integer/FP64 control work with no bandwidth or tensor bound",
+        "clocks": clocks.summary(), "gpu_launches": int(launches) // max(args.steps, 1), "cpu_baseline": cpu,
+    }
+
+
+def load_phases(name):
+    from tests.helpers import load_canonical
+
+    return load_canonical(name)
+
+
 def run_reference(args, cfg):
     from porerad_b200 import replicas
 
     if replicas.rank() != 0:
         return None  # the CPU reference runs once, on rank 0
+    if args.workload == "properties":
+        vals, last = [], None
+        for _ in range(args.steps):
+            last = multibounce_cpu_sample(max(1.0, args.cpu_seconds / 2))
+            vals.append(last["value"])
+        value = float(np.mean(vals))
+        return {"impl": "reference", "metric": "multi-bounce source rays per second (archived identification set)",
+                "value": value, "unit": "rays/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": 0,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "reference microstructures (tests/golden)", "config": {"workload": cfg["workload"]},
+                "cpu_baseline": {**last, "value": value},
+                "e2e": {"value": value, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if args.workload == "generators":
         vals, last = [], None
         for _ in range(args.steps):
@@ -1144,6 +1285,8 @@ def main():
         line = run_descriptors_bench(args, cfg)
     elif args.workload == "generators":
         line = run_generators_bench(args, cfg)
+    elif args.workload == "properties":
+        line = run_properties_bench(args, cfg)
     elif args.workload == "c4":
         line = run_c4(args, cfg)
     elif args.workload == "c5":

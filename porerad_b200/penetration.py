@@ -16,7 +16,7 @@ import numpy as np
 
 from . import _lib
 from .constants import SIGMA
-from .properties import RESTART_CODES, _geometry, seed_average, solid_along_x  # noqa: F401
+from .properties import RESTART_CODES, _geometry, run_concurrently, seed_average, solid_along_x  # noqa: F401
 
 SEEDS = (321, 654)
 N_RAYS = 500_000
@@ -67,8 +67,8 @@ def penetration_response(phases: np.ndarray, axis: str, epsilon: float, *, seeds
 
     geo = _geometry(phases, axis)
     try:
-        runs = [trace_penetration(phases, axis, epsilon, n_rays=n_rays, seed=s, restart=restart, _geo=geo)
-                for s in seeds]
+        runs = run_concurrently([(trace_penetration, (phases, axis, epsilon),
+                                  dict(n_rays=n_rays, seed=s, restart=restart, _geo=geo)) for s in seeds])
     finally:
         geo.close()
     out = {"n_rays": int(sum(r["n_rays"] for r in runs)), "terminated": int(sum(r["terminated"] for r in runs))}

@@ -14,6 +14,8 @@ from __future__ import annotations
 
 import ctypes
 import math
+import threading
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -46,6 +48,39 @@ def right_censored_mle(events: np.ndarray, censored: np.ndarray) -> tuple[float,
 
 def _geometry(phases, axis: str) -> DeviceGeometry:
     return DeviceGeometry(solid_along_x(phases, axis), 1.0)
+
+
+RUN_STREAMS = 8
+"""Runs (seeds, emissivities, axes) traced at once, each from its own host thread and stream: one
+run of 10^5 rays cannot fill the GPU by itself once its short rays have ended."""
+
+_pool = None
+_pool_lock = threading.Lock()
+_local = threading.local()
+
+
+def _in_own_stream(fn, args, kwargs):
+    import torch
+
+    if getattr(_local, "stream", None) is None:
+        _local.stream = torch.cuda.Stream()
+    with _lib.use_stream(_local.stream):
+        return fn(*args, **kwargs)
+
+
+def run_concurrently(calls):
+    """Results of calls [(fn, args, kwargs), ...] made on RUN_STREAMS worker threads, each with its
+    own CUDA stream (the library releases the GIL while it waits for the device); in order."""
+
+    global _pool
+    import torch
+
+    torch.cuda.synchronize()  # the geometries were built on the caller's stream
+    with _pool_lock:
+        if _pool is None:
+            _pool = ThreadPoolExecutor(RUN_STREAMS, thread_name_prefix="porerad-runs")
+    futs = [_pool.submit(_in_own_stream, fn, args, kwargs) for fn, args, kwargs in calls]
+    return [f.result() for f in futs]
 
 
 def trace_properties(phases: np.ndarray, axis: str, epsilon: float, *, n_rays: int = N_RAYS, seed: int = SEEDS[0],
@@ -91,8 +126,8 @@ def identify_properties(phases: np.ndarray, axis: str, epsilon: float, *, seeds=
 
     geo = _geometry(phases, axis)
     try:
-        runs = [trace_properties(phases, axis, epsilon, n_rays=n_rays, seed=s, restart=restart, _geo=geo)
-                for s in seeds]
+        runs = run_concurrently([(trace_properties, (phases, axis, epsilon),
+                                  dict(n_rays=n_rays, seed=s, restart=restart, _geo=geo)) for s in seeds])
     finally:
         geo.close()
     out = {"n_rays": int(sum(r["n_rays"] for r in runs))}

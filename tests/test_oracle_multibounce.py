@@ -1,0 +1,40 @@
+"""The multi-bounce oracle (oracle/multibounce.c) against archived rows of
+results/radiative_properties.csv and results/penetration_response.csv (CPU)."""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from oracle import multibounce as om
+from tests.helpers import load_canonical, multibounce_rows
+
+ROWS = multibounce_rows()
+NAME = "FI_core_phi0.05_s3"
+
+
+def _solid(name, axis):
+    ph = load_canonical(name)
+    return np.ascontiguousarray(np.moveaxis(ph == 1, "xyz".index(axis), 0)).astype(np.uint8)
+
+
+@pytest.mark.parametrize("row", [r for r in ROWS["penetration"] if r["microstructure"] == NAME][:3])
+def test_penetration_counts(row):
+    n = 500_000
+    counts = sum(om.run(_solid(NAME, row["transfer_axis"]), row["epsilon"], n, s, penetration=True) for s in (321, 654))
+    for k, key in enumerate(("reflectance", "transmittance", "absorptance")):
+        assert counts[k] / (2 * n) == pytest.approx(row[key], abs=1e-12)
+
+
+@pytest.mark.parametrize("row", [r for r in ROWS["properties"] if r["microstructure"] == NAME][:3])
+def test_property_estimates(row):
+    tal = [om.run(_solid(NAME, row["transfer_axis"]), row["epsilon"], 200_000, s, penetration=False)
+           for s in (123, 456)]
+    beta = np.mean([t[0] / (t[1] + t[3]) for t in tal])
+    omega = np.mean([t[5] / t[4] for t in tal])
+    g = np.mean([t[6] / t[5] for t in tal])
+    assert math.isclose(beta, row["beta_per_cell"], rel_tol=1e-12)
+    assert math.isclose(omega, row["omega"], rel_tol=1e-12)
+    assert math.isclose(g, row["g"], rel_tol=1e-10)
