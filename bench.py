@@ -527,6 +527,20 @@ def run_c4(args, cfg):
     launches = lib.pr_kernel_launches() - launches0
     served_rate = len(reqs) / t_sat
     rays = sum(r.rays for r in sat)
+    # the same requests carrying generator specs: each geometry is generated on the device by the
+    # worker that serves it (host generation leaves the served path)
+    spec_reqs = [serving.CaseRequest(serving.GeometrySpec(sp["arch"], sp["n"], sp["phi"], sp["seed"], sp["axis"]),
+                                     r.H_m, r.rays_per_patch, r.seeds, r.T_mean_K, r.delta_T_K, r.epsilon,
+                                     precision=r.precision, tag=r.tag) for sp, r in zip(specs, reqs)]
+    t0 = time.perf_counter()
+    with serving.Server(slots=cfg["slots"]) as srv:
+        spec_res = [f.result() for f in [srv.submit(r, t_submit=t0) for r in spec_reqs]]
+    t_spec = time.perf_counter() - t0
+    spec_same = all((a.q_h, a.q_c, a.q_i) == (b.q_h, b.q_c, b.q_i) for a, b in zip(spec_res, sat))
+    t0 = time.perf_counter()
+    for sp in specs:
+        _c4_geometry(sp)
+    host_gen_s = time.perf_counter() - t0
     # plain path, sequential, on the same requests
     plain_case(reqs[0])
     service = []
@@ -565,6 +579,10 @@ def run_c4(args, cfg):
         "rays_per_s_served": rays / t_sat,
         "plain": {"cases_per_s": plain_rate, "p50_s": serving.percentile(service, 50)},
         "served_over_plain": served_rate / plain_rate,
+        "served_from_specs": {"cases_per_s": len(spec_reqs) / t_spec, "results_identical": spec_same,
+                              "host_generation_s_per_case": host_gen_s / len(specs),
+                              "note": "requests carry (archetype, N, phi, seed, axis); the serving worker "
+                                      "generates the geometry on the device (geometry.make_device)"},
         "saturated_latency_s": {"p50": serving.percentile(sat_lat, 50), "p99": serving.percentile(sat_lat, 99)},
         "poisson": {"rate_per_s": lam, "served_p50_s": serving.percentile(lat, 50),
                     "served_p99_s": serving.percentile(lat, 99),

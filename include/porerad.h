@@ -363,6 +363,23 @@ PR_API int pr_stamp_fibers(int64_t N, const int32_t* nodes, const int64_t* node_
                            const int64_t* offset_start, int n_fibers, int clear, uint8_t* phases,
                            int64_t* solid_cells, void* stream);
 
+/* pr_stamp_fibers with any byte value (value 0 punches holes): the device work of the
+ * benchmark archetypes' segment and hole stamping as well. */
+PR_API int pr_stamp_cells(int64_t N, const int32_t* nodes, const int64_t* node_start, const int32_t* offsets,
+                          const int64_t* offset_start, int n_groups, int clear, int value, uint8_t* phases,
+                          int64_t* solid_cells, void* stream);
+
+/* ---- benchmark archetypes (no counterpart in the reference) -------------------------
+ * The grid work of porerad_b200.geometry's seeded archetypes, bit-identical to their host
+ * definitions.  pr_voronoi_edge_field: field (device, N^3 f64) = d3 - d1, the distances from
+ * each cell centre to its first and third nearest of n_seeds periodic points (seeds: n_seeds x 3
+ * f64, host or device), as SciPy's periodic k-d tree computes them.  pr_quantile_threshold:
+ * q = numpy.quantile(field, quantile) and phases = field <= q (below = 1) or field >= q; q_out
+ * and solid_cells may be NULL. */
+PR_API int pr_voronoi_edge_field(int64_t N, const double* seeds, int n_seeds, double* field, void* stream);
+PR_API int pr_quantile_threshold(const double* field, int64_t n, double quantile, int below, uint8_t* phases,
+                                 double* q_out, int64_t* solid_cells, void* stream);
+
 /* ---- instrumentation (no counterpart in the reference) ----------------------------
  * Kernel classes timed with CUDA events on their launching stream while enabled:
  * 0 fused ray generation + traversal, 1 per-patch count reduction, 2 balancing

@@ -138,6 +138,9 @@ _SIGNATURES = {
     "pr_morphology_counts": (_i32, [_vp, _i64, _i64, _i64, _i32, _vp, _vp, _vp, _vp, _vp]),
     "pr_render_shapes": (_i32, [_i64, _vp, _i32, _vp, _vp, _vp]),
     "pr_stamp_fibers": (_i32, [_i64, _vp, _vp, _vp, _vp, _i32, _i32, _vp, _vp, _vp]),
+    "pr_stamp_cells": (_i32, [_i64, _vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp, _vp]),
+    "pr_voronoi_edge_field": (_i32, [_i64, _vp, _i32, _vp, _vp]),
+    "pr_quantile_threshold": (_i32, [_vp, _i64, _f64, _i32, _vp, _vp, _vp, _vp]),
     "pr_timers_enable": (None, [_i32]),
     "pr_timers_reset": (None, []),
     "pr_timers_read": (_i32, [_i32, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_f64)]),

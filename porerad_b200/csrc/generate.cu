@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(256) k_render_shapes(int N, const GenShape* __
 // fiber f: nodes[node0[f] .. node0[f+1]) and disk offsets[off0[f] .. off0[f+1]), int32 triples
 __global__ void k_stamp(int N, const int* __restrict__ nodes, const int64_t* __restrict__ node0,
                         const int* __restrict__ offsets, const int64_t* __restrict__ off0, int n_fibers,
-                        uint8_t* __restrict__ phases) {
+                        uint8_t value, uint8_t* __restrict__ phases) {
   for (int f = 0; f < n_fibers; ++f) {
     const int64_t nn = node0[f + 1] - node0[f], no = off0[f + 1] - off0[f];
     const int* nd = nodes + 3 * node0[f];
@@ -92,7 +92,7 @@ __global__ void k_stamp(int N, const int* __restrict__ nodes, const int64_t* __r
         int v = (nd[3 * a + d] + od[3 * b + d]) % N;
         c[d] = v < 0 ? v + N : v;
       }
-      phases[((int64_t)c[0] * N + c[1]) * N + c[2]] = 1;
+      phases[((int64_t)c[0] * N + c[1]) * N + c[2]] = value;
     }
   }
 }
@@ -201,9 +201,10 @@ PR_API int pr_render_shapes(int64_t N, const pr_shape* shapes, int n_shapes, uin
   return PR_OK;
 }
 
-PR_API int pr_stamp_fibers(int64_t N, const int32_t* nodes, const int64_t* node_start, const int32_t* offsets,
-                           const int64_t* offset_start, int n_fibers, int clear, uint8_t* phases,
-                           int64_t* solid_cells, void* stream) {
+PR_API int pr_stamp_cells(int64_t N, const int32_t* nodes, const int64_t* node_start, const int32_t* offsets,
+                          const int64_t* offset_start, int n_fibers, int clear, int value, uint8_t* phases,
+                          int64_t* solid_cells, void* stream) {
+  PR_ARG(value >= 0 && value <= 255, "value must be a byte");
   PR_ARG(phases && node_start && offset_start, "phases, node_start and offset_start must not be NULL");
   PR_ARG(N > 0 && N <= 1290, "grid size N must be in 1..1290 (N^3 < 2^31)");
   PR_ARG(n_fibers >= 0, "n_fibers must not be negative");
@@ -234,7 +235,7 @@ PR_API int pr_stamp_fibers(int64_t N, const int32_t* nodes, const int64_t* node_
     }
     timer_begin(kTimerRender, s);
     k_stamp<<<grid_for(most, 256, sm_count() * 8), 256, 0, s>>>((int)N, dn.ptr, dn0.ptr, dof.ptr, do0.ptr, n_fibers,
-                                                                phases);
+                                                                (uint8_t)value, phases);
     timer_end(kTimerRender, s);
     launch_mark();
     PR_CUDA(cudaGetLastError());
@@ -242,6 +243,13 @@ PR_API int pr_stamp_fibers(int64_t N, const int32_t* nodes, const int64_t* node_
   }
   if (solid_cells) PR_TRY(count_solid(phases, n, solid_cells, s));
   return PR_OK;
+}
+
+PR_API int pr_stamp_fibers(int64_t N, const int32_t* nodes, const int64_t* node_start, const int32_t* offsets,
+                           const int64_t* offset_start, int n_fibers, int clear, uint8_t* phases,
+                           int64_t* solid_cells, void* stream) {
+  return pr_stamp_cells(N, nodes, node_start, offsets, offset_start, n_fibers, clear, 1, phases, solid_cells,
+                        stream);
 }
 
 }  // extern "C"

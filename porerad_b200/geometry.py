@@ -30,11 +30,15 @@ def _ball(radius: float) -> np.ndarray:
     return np.stack((dx[keep], dy[keep], dz[keep]), axis=1)
 
 
-def _stamp_segment(solid: np.ndarray, p0: np.ndarray, direction: np.ndarray, length: float, ball: np.ndarray) -> None:
-    n = np.asarray(solid.shape)
+def _segment_centres(p0: np.ndarray, direction: np.ndarray, length: float) -> np.ndarray:
     t = np.arange(-length / 2.0, length / 2.0 + 0.25, 0.25)
     centres = np.rint(p0[None, :] + t[:, None] * direction[None, :]).astype(np.int64)
-    centres = np.unique(centres, axis=0)
+    return np.unique(centres, axis=0)
+
+
+def _stamp_segment(solid: np.ndarray, p0: np.ndarray, direction: np.ndarray, length: float, ball: np.ndarray) -> None:
+    n = np.asarray(solid.shape)
+    centres = _segment_centres(p0, direction, length)
     pts = (centres[:, None, :] + ball[None, :, :]).reshape(-1, 3) % n
     solid[pts[:, 0], pts[:, 1], pts[:, 2]] = 1
 
@@ -48,14 +52,7 @@ def fibers(n: int, phi: float, seed: int, *, radius: float = 2.0, aligned: bool 
     target = phi * solid.size
     count = 0
     while count < target:
-        p0 = rng.random(3) * n
-        if aligned:
-            d = np.array([0.0, 0.0, 1.0])
-            length = float(n)
-        else:
-            v = rng.standard_normal(3)
-            d = v / np.linalg.norm(v)
-            length = float(n) * np.sqrt(3.0)
+        p0, d, length = _fiber_draws(n, rng, aligned)
         _stamp_segment(solid, p0, d, length, ball)
         count = int(solid.sum())
     return solid
@@ -107,6 +104,96 @@ def layers(n: int, phi: float, seed: int, *, thickness: int = 4, hole: int = 8) 
         for dz in range(thickness):
             solid[xy[:, 0], xy[:, 1], (z0 + dz) % n] = 0
     return solid
+
+
+def _fiber_draws(n: int, rng, aligned: bool):
+    p0 = rng.random(3) * n
+    if aligned:
+        return p0, np.array([0.0, 0.0, 1.0]), float(n)
+    v = rng.standard_normal(3)
+    return p0, v / np.linalg.norm(v), float(n) * np.sqrt(3.0)
+
+
+def _layer_sheets(n: int, phi: float, thickness: int, offset: int):
+    m = max(1, int(np.ceil(phi * n / thickness)))
+    return m, [(offset + (s * n) // m) % n for s in range(m)]
+
+
+def _hole_disk(hole: int) -> np.ndarray:
+    r = hole / 2.0
+    g = np.arange(-hole, hole + 1)
+    dx, dy = np.meshgrid(g, g, indexing="ij")
+    keep = dx * dx + dy * dy <= r * r
+    return np.stack((dx[keep], dy[keep]), axis=1)
+
+
+def make_device(archetype: str, n: int, phi: float, seed: int, *, stream=None):
+    """``make(archetype, n, phi, seed)`` generated on the device: a uint8 CUDA tensor equal to the
+    host array bit for bit.  The random draws stay on the host (the same NumPy generator calls);
+    the grid work runs in libporerad: segment and hole stamping with solid counts
+    (``pr_stamp_cells``), the foam's nearest-seed field (``pr_voronoi_edge_field``) and its quantile
+    threshold (``pr_quantile_threshold``)."""
+
+    import ctypes
+
+    import torch
+
+    from . import _lib
+
+    lib = _lib.load()
+    st = _lib.stream() if stream is None else _lib.stream_arg(stream)
+    n = int(n)
+    out = torch.empty((n, n, n), dtype=torch.uint8, device="cuda")
+    solid = ctypes.c_int64()
+    start = np.array([0, 1], np.int64)
+
+    def stamp(nodes, offsets, value, clear):
+        nd = np.ascontiguousarray(nodes, dtype=np.int32)
+        od = np.ascontiguousarray(offsets, dtype=np.int32)
+        ns = np.array([0, len(nd)], np.int64)
+        os_ = np.array([0, len(od)], np.int64)
+        _lib.check(lib.pr_stamp_cells(n, nd.ctypes.data, ns.ctypes.data, od.ctypes.data, os_.ctypes.data, 1,
+                                      int(clear), int(value), out.data_ptr(), ctypes.byref(solid), st))
+        return int(solid.value)
+
+    if archetype in ("FI", "FA"):
+        rng = np.random.default_rng(seed)
+        ball = _ball(2.0)
+        target = phi * n ** 3
+        count, first = 0, True
+        while count < target:
+            p0, d, length = _fiber_draws(n, rng, archetype == "FA")
+            count = stamp(_segment_centres(p0, d, length) % n, ball, 1, first)
+            first = False
+        if first:
+            out.zero_()
+            torch.cuda.current_stream().synchronize()
+        return out
+    if archetype == "OF":
+        rng = np.random.default_rng(seed)
+        pts = np.ascontiguousarray(rng.random((64, 3)) * n)
+        field = torch.empty((n, n, n), dtype=torch.float64, device="cuda")
+        _lib.check(lib.pr_voronoi_edge_field(n, pts.ctypes.data, 64, field.data_ptr(), st))
+        _lib.check(lib.pr_quantile_threshold(field.data_ptr(), n ** 3, float(phi), 1, out.data_ptr(), None, None, st))
+        return out
+    if archetype == "TL":
+        thickness, hole = 4, 8
+        rng = np.random.default_rng(seed)
+        offset = int(rng.integers(0, n))
+        m, sheet_z = _layer_sheets(n, phi, thickness, offset)
+        planes = np.array([(0, 0, (z0 + dz) % n) for z0 in sheet_z for dz in range(thickness)], np.int64)
+        g = np.arange(n)
+        plane_offsets = np.stack([a.ravel() for a in np.meshgrid(g, g, [0], indexing="ij")], axis=1)
+        count = stamp(planes, plane_offsets, 1, True)
+        disk = _hole_disk(hole)
+        hole_offsets = np.array([(dx, dy, dz) for dz in range(thickness) for dx, dy in disk], np.int64)
+        target = phi * n ** 3
+        while count > target:
+            z0 = sheet_z[int(rng.integers(0, m))]
+            c = rng.integers(0, n, size=2)
+            count = stamp(np.array([(c[0], c[1], z0)]), hole_offsets, 0, False)
+        return out
+    raise ValueError(f"unknown archetype {archetype!r}; expected one of {ARCHETYPES}")
 
 
 def make(archetype: str, n: int, phi: float, seed: int) -> np.ndarray:

@@ -29,10 +29,37 @@ _CHUNK_RAYS = 1 << 26  # rays per traversal chunk of libporerad (receiver + two 
 
 
 @dataclass
+class GeometrySpec:
+    """A seeded benchmark archetype (porerad_b200.geometry.make) generated on the device by the
+    worker that serves the request, oriented so that ``axis`` becomes x."""
+
+    archetype: str
+    n: int
+    phi: float
+    seed: int
+    axis: str = "x"
+
+    @property
+    def shape(self) -> tuple:
+        return (int(self.n),) * 3
+
+    def device_phases(self):
+        from . import geometry
+
+        import torch
+
+        ph = geometry.make_device(self.archetype, self.n, self.phi, self.seed)
+        if self.axis != "x":
+            ph = ph.movedim("xyz".index(self.axis), 0).contiguous()
+            torch.cuda.current_stream().synchronize()  # torch's copy, before the library's stream reads it
+        return ph
+
+
+@dataclass
 class CaseRequest:
     """One prescribed-field case (the inputs of porerad's run_prescribed_field for one condition)."""
 
-    phases: Any                 # uint8 (nx, ny, nz) x-oriented, NumPy array or CUDA tensor
+    phases: Any                 # uint8 (nx, ny, nz) x-oriented, NumPy array or CUDA tensor, or a GeometrySpec
     H_m: float
     rays_per_patch: int
     seeds: list
@@ -139,7 +166,9 @@ def run_case(req: CaseRequest, admission: Admission, on_admit: Callable[[int], N
     held = geo_bytes
     geo = table = op = None
     try:
-        geo = vf.DeviceGeometry(req.phases, req.H_m)
+        phases = req.phases.device_phases() if isinstance(req.phases, GeometrySpec) else req.phases
+        geo = vf.DeviceGeometry(phases, req.H_m)
+        del phases
         L = int(req.rays_per_patch) * len(req.seeds)
         need = footprint_bytes(geo.n_patches, L)
         admission.release(held)
