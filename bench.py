@@ -1029,12 +1029,8 @@ def run_generators_bench(args, cfg):
     torch.cuda.set_device(0)
     lib = _lib.load()
 
-    def step(device=True):
-        out = []
-        for s in gen.STRUCTURES:
-            for phi in gen.CORE_PHIS:
-                out += gen.core_realizations(s, phi, device=device)
-        return out
+    def step(device=True):  # the 12 cells at once (gen.core_library), TL's host fields overlapping
+        return [x for cell in gen.core_library(device=device).values() for x in cell]
 
     for _ in range(max(args.warmup, 3)):
         step()

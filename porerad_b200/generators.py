@@ -394,6 +394,19 @@ def core_realizations(structure, target_phi, n_accept=4, max_trials=80, *, devic
     return out
 
 
+def core_library(structures=STRUCTURES, phis=CORE_PHIS, n_accept=4, max_trials=80, *, device=False):
+    """Every cell of the core library, {(structure, phi): [(seed, phases), ...]}, as
+    ``core_realizations`` builds each; the cells run at once on worker threads with their own
+    streams, so TL's host fields overlap the device renderings of the other structures."""
+
+    from .streams import run_concurrently
+
+    cells = [(s, phi) for s in structures for phi in phis]
+    out = run_concurrently([(core_realizations, (s, phi, n_accept, max_trials), dict(device=device))
+                            for s, phi in cells])
+    return dict(zip(cells, out))
+
+
 def canonical(structure, N, *, device=False):
     """Canonical microstructure at phi_s = 0.10 and seed 0 on an N^3 grid (geometry.py:299-314);
     TL's field is drawn at N = 192 and resampled by periodic cubic splines on the host."""

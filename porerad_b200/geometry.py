@@ -230,5 +230,5 @@ def ray_set_seed(case_seed: int, set_index: int, block: int = 0) -> int:
 from .generators import (  # noqa: E402,F401
     CORE_N, CORE_PHIS, FA_THETA_SIGMA, FIBER_LENGTH, FIBER_LINES, FOAM_NEIGHBOURS, FOAM_NODES, MATCHED_PAIRS,
     MIN_PORE_CLUSTER, NODE_TO_STRUT, PHI_TOL, STRUCTURES, TL_BASE_N, TL_LAYERS, TL_NOISE, accepted, build, canonical,
-    core_realizations, fiber_lines, foam_graph, lamellar_field, matched, render_fibers, render_foam, shape_mask,
+    core_library, core_realizations, fiber_lines, foam_graph, lamellar_field, matched, render_fibers, render_foam, shape_mask,
     threshold)

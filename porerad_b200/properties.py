@@ -14,8 +14,6 @@ from __future__ import annotations
 
 import ctypes
 import math
-import threading
-from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -50,37 +48,7 @@ def _geometry(phases, axis: str) -> DeviceGeometry:
     return DeviceGeometry(solid_along_x(phases, axis), 1.0)
 
 
-RUN_STREAMS = 8
-"""Runs (seeds, emissivities, axes) traced at once, each from its own host thread and stream: one
-run of 10^5 rays cannot fill the GPU by itself once its short rays have ended."""
-
-_pool = None
-_pool_lock = threading.Lock()
-_local = threading.local()
-
-
-def _in_own_stream(fn, args, kwargs):
-    import torch
-
-    if getattr(_local, "stream", None) is None:
-        _local.stream = torch.cuda.Stream()
-    with _lib.use_stream(_local.stream):
-        return fn(*args, **kwargs)
-
-
-def run_concurrently(calls):
-    """Results of calls [(fn, args, kwargs), ...] made on RUN_STREAMS worker threads, each with its
-    own CUDA stream (the library releases the GIL while it waits for the device); in order."""
-
-    global _pool
-    import torch
-
-    torch.cuda.synchronize()  # the geometries were built on the caller's stream
-    with _pool_lock:
-        if _pool is None:
-            _pool = ThreadPoolExecutor(RUN_STREAMS, thread_name_prefix="porerad-runs")
-    futs = [_pool.submit(_in_own_stream, fn, args, kwargs) for fn, args, kwargs in calls]
-    return [f.result() for f in futs]
+from .streams import WORKERS as RUN_STREAMS, run_concurrently  # noqa: E402,F401
 
 
 def trace_properties(phases: np.ndarray, axis: str, epsilon: float, *, n_rays: int = N_RAYS, seed: int = SEEDS[0],

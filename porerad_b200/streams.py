@@ -1,0 +1,47 @@
+"""Independent calls on worker threads, each with its own CUDA stream.
+
+libporerad releases the GIL while it waits for the device, and every call orders its work on
+the calling thread's stream (``_lib.use_stream``); torch operations of a worker run on the same
+stream.  Calls that are independent (seeds of a ray statistic, cells of a microstructure
+library) then overlap on the GPU, and host work of one (NumPy fields, draws) overlaps the
+device work of the others.
+"""
+
+from __future__ import annotations
+
+import threading
+from concurrent.futures import ThreadPoolExecutor
+
+from . import _lib
+
+WORKERS = 8
+
+_pool = None
+_pool_lock = threading.Lock()
+_local = threading.local()
+
+
+def _in_own_stream(fn, args, kwargs):
+    import torch
+
+    if getattr(_local, "stream", None) is None:
+        _local.stream = torch.cuda.Stream()
+    with torch.cuda.stream(_local.stream), _lib.use_stream(_local.stream):
+        try:
+            return fn(*args, **kwargs)
+        finally:
+            _local.stream.synchronize()  # results leave the worker complete
+
+
+def run_concurrently(calls):
+    """Results of calls [(fn, args, kwargs), ...] made on WORKERS threads with their own streams, in order."""
+
+    global _pool
+    import torch
+
+    torch.cuda.synchronize()  # inputs were prepared on the caller's stream
+    with _pool_lock:
+        if _pool is None:
+            _pool = ThreadPoolExecutor(WORKERS, thread_name_prefix="porerad-worker")
+    futs = [_pool.submit(_in_own_stream, fn, args, kwargs) for fn, args, kwargs in calls]
+    return [f.result() for f in futs]

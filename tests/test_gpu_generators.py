@@ -69,3 +69,15 @@ def test_device_outputs_and_single_shapes(gen):
     assert np.array_equal(cyl, ((x / 2.5) ** 2 + (y / 2.5) ** 2 <= 1.0) & (np.abs(z) <= 6.0))
     with pytest.raises(ValueError):
         gen.shape_mask(N, c, (1.0, 1.0, 1.0), "cone", np.eye(3))
+
+
+def test_core_library_cells_at_once(gen):
+    """The cells of the core library built concurrently (own threads and streams) equal the
+    archived arrays and seeds."""
+
+    lib = gen.core_library(structures=("OF", "FA", "TL"), phis=(0.05, 0.15))
+    for (structure, phi), got in lib.items():
+        want = {r["seed"]: r["phase_sha256"] for r in ROWS
+                if r["set"] == "core" and r["structure"] == structure and r["target_phi"] == phi}
+        assert [s for s, _ in got] == sorted(want)
+        assert all(_sha(ph) == want[s] for s, ph in got)
