@@ -128,12 +128,18 @@ def served_step(phases, cfg, seeds, precision="mixed"):
     out["h2d"] = 32 * 130 * len(seeds) + n_ops * P * 16
     out["d2h"] = n_ops * (P * 8 + 8 * (4 + 512 + 4))
     ops = []
-    for t in tables if len(tables) > 1 else []:
+
+    def per_set(t):
         rays = np.full(geo.n_patches, cfg["rays"], np.int64)
         op = exchange.ExchangeOperator(t, None, None, rays, area)
-        ch = coupled.prescribed_field_channels(op, p, cfg["T_m"], cfg["dT"], cfg["eps"], precision=precision)
-        out["sets"].append(ch)
-        ops.append(op)
+        return op, coupled.prescribed_field_channels(op, p, cfg["T_m"], cfg["dT"], cfg["eps"], precision=precision)
+
+    if len(tables) > 1:  # the sets' operators and solves are independent: on worker streams at once
+        from porerad_b200 import streams
+
+        for op, ch in streams.run_concurrently([(per_set, (t,), {}) for t in tables]):
+            out["sets"].append(ch)
+            ops.append(op)
     rays = np.full(geo.n_patches, cfg["rays"] * len(seeds), np.int64)
     op = exchange.ExchangeOperator(pooled, None, None, rays, area)
     ch = coupled.prescribed_field_channels(op, p, cfg["T_m"], cfg["dT"], cfg["eps"], precision=precision)
