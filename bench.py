@@ -129,20 +129,20 @@ def served_step(phases, cfg, seeds, precision="mixed"):
     out["d2h"] = n_ops * (P * 8 + 8 * (4 + 512 + 4))
     ops = []
 
-    def per_set(t):
-        rays = np.full(geo.n_patches, cfg["rays"], np.int64)
+    def per_set(t, n_sets):
+        rays = np.full(geo.n_patches, cfg["rays"] * n_sets, np.int64)
         op = exchange.ExchangeOperator(t, None, None, rays, area)
         return op, coupled.prescribed_field_channels(op, p, cfg["T_m"], cfg["dT"], cfg["eps"], precision=precision)
 
-    if len(tables) > 1:  # the sets' operators and solves are independent: on worker streams at once
-        from porerad_b200 import streams
+    # the operators and solves of the sets and of their pool are independent: on worker streams at once
+    from porerad_b200 import streams
 
-        for op, ch in streams.run_concurrently([(per_set, (t,), {}) for t in tables]):
-            out["sets"].append(ch)
-            ops.append(op)
-    rays = np.full(geo.n_patches, cfg["rays"] * len(seeds), np.int64)
-    op = exchange.ExchangeOperator(pooled, None, None, rays, area)
-    ch = coupled.prescribed_field_channels(op, p, cfg["T_m"], cfg["dT"], cfg["eps"], precision=precision)
+    jobs = [(per_set, (t, 1), {}) for t in (tables if len(tables) > 1 else [])] + [(per_set, (pooled, len(seeds)), {})]
+    done = streams.run_concurrently(jobs)
+    for op, ch in done[:-1]:
+        out["sets"].append(ch)
+        ops.append(op)
+    op, ch = done[-1]
     out["final"] = ch
     out["nnz_symmetric"] = op.nnz_symmetric
     # products of every operator of the step: (entries of S', products made) for the roofline
