@@ -432,7 +432,10 @@ def run_ours(args, cfg):
         roof_spmv = {"bound": "hbm", "achieved": tot_b / tot_t if tot_t else None, "peak": peaks["hbm_gbs"],
                      "unit": "GB/s", "frac": (tot_b / tot_t) / peaks["hbm_gbs"] if tot_t else None,
                      "peak_source": f"MEASURED_PEAKS.json ({kind})", "kernels": spmv,
-                     "share_of_step": tot_t / ms}
+                     "share_of_step": tot_t / ms,
+                     "note": "the three operators' products run at once on three streams: a launch's "
+                             "event time includes the other streams' work, so this per-launch rate is a "
+                             "lower bound (one operator at a time it read 0.34 of the same peak)"}
         cpu = None if args.no_cpu else cpu_sample(cfg, seeds, args.cpu_seconds)
         line = {
             "metric": "first-hit rays/s (whole case: patches, counts A+B, 3 balanced operators, 3 mixed-precision "
