@@ -313,3 +313,12 @@ def all_descriptors(phases) -> tuple:
 
     c = morphology_counts(phases)
     return scalar_values(c), directional_rows(c)
+
+
+def all_descriptors_many(arrays) -> list:
+    """``all_descriptors`` of many phase arrays, on worker threads with their own streams (the host
+    arithmetic of one overlaps the device passes of the others); in order."""
+
+    from .streams import run_concurrently
+
+    return run_concurrently([(all_descriptors, (a,), {}) for a in arrays])

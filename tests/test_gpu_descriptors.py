@@ -100,3 +100,15 @@ def test_device_and_other_inputs(dm):
         dm.morphology_counts(np.zeros((4, 4), np.uint8))
     with pytest.raises(ValueError):
         dm.morphology_counts(np.zeros((4, 0, 4), np.uint8))
+
+
+def test_many_at_once_equals_one_by_one(dm):
+    arrays = [descriptor_phases(n, RECORDS["stored"][n]) for n in sorted(RECORDS["stored"])[:6]]
+    many = dm.all_descriptors_many(arrays)
+    for a, (sc, rows) in zip(arrays, many):
+        s1, r1 = dm.all_descriptors(a)
+        assert sc == s1
+        for x, y in zip(rows, r1):
+            assert {k: v for k, v in x.items() if k not in ("lineal_path", "chord_counts")} == \
+                   {k: v for k, v in y.items() if k not in ("lineal_path", "chord_counts")}
+            assert np.array_equal(x["chord_counts"], y["chord_counts"])
