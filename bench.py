@@ -1077,7 +1077,8 @@ def run_generators_bench(args, cfg):
         "dtype": "f64 (shape tests), u8", "data": "the reference's generators (seeded)",
         "config": {"workload": cfg["workload"], "accepted": len(out),
                    "l2": "every trial writes a fresh 2 MiB array; outputs stay resident"},
-        "e2e": {"value": e2e, "unit": "microstructures/s", "h2d_bytes_per_step": 0,
+        "e2e": {"value": e2e, "unit": "microstructures/s",
+                "h2d_bytes_per_step": int(12 * 8 * 128 ** 3),  # TL's normal draws, one N^3 f64 array per TL trial
                 "d2h_bytes_per_step": int(len(host) * 128 ** 3)},
         "roofline": {"bound": "hbm", "kernel": "k_render_shapes / k_stamp", "achieved": achieved,
                      "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"] if achieved else None,

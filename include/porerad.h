@@ -363,6 +363,15 @@ PR_API int pr_stamp_fibers(int64_t N, const int32_t* nodes, const int64_t* node_
                            const int64_t* offset_start, int n_fibers, int clear, uint8_t* phases,
                            int64_t* solid_cells, void* stream);
 
+/* Replaces the grid work of lamellar_field (geometry.py:223-239): field (device, N^3 f64) =
+ * base_x[i] + 0.35 sin(two_pi_layers (i + wav[j,k]) / N) + smoothed noise, wav[j,k] = waviness
+ * (0.65 sin_y[j] + 0.35 cos_z[k]); the 7-point periodic smoothing of noise (N^3 f64, host or
+ * device, the reference's normal draws) is summed in the reference's order and divided by 7;
+ * the sine is correctly rounded.  base_x, sin_y, cos_z: the N values the reference's cosine and
+ * sines take along each axis, computed on the host. */
+PR_API int pr_lamellar_field(int64_t N, const double* base_x, const double* sin_y, const double* cos_z,
+                             double waviness, double two_pi_layers, const double* noise, double* field,
+                             void* stream);
 /* pr_stamp_fibers with any byte value (value 0 punches holes): the device work of the
  * benchmark archetypes' segment and hole stamping as well. */
 PR_API int pr_stamp_cells(int64_t N, const int32_t* nodes, const int64_t* node_start, const int32_t* offsets,

@@ -12,10 +12,15 @@
 //    marks (node + offset) mod N.
 //  * k_count_solid: solid cells of the rendered array (the bisection on the radius,
 //    geometry.py:124-145, reads phi_s = solid / N^3).
+//  * k_lamellar: TL's continuous field (lamellar_field, geometry.py:223-239) from its host
+//    parts (the per-x cosine, the per-y sine and per-z cosine of the waviness, the normal noise):
+//    the wavy layer term with a correctly rounded sine, the 7-point periodic smoothing of the
+//    noise summed in NumPy's order; thresholded by pr_quantile_threshold.
 // Built with -fmad=false: every product and sum is rounded where NumPy rounds it.
 #include <new>
 
 #include "pr_internal.cuh"
+#include "pr_math.cuh"
 
 namespace pr {
 
@@ -118,6 +123,35 @@ __global__ void __launch_bounds__(256) k_count_solid(const uint8_t* __restrict__
     c += phases[t] == 1;
   for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
+__global__ void __launch_bounds__(256) k_lamellar(int N, const double* __restrict__ base,
+                                                  const double* __restrict__ sin_y, const double* __restrict__ cos_z,
+                                                  double waviness, double two_pi_layers,
+                                                  const double* __restrict__ noise, double* __restrict__ field) {
+  const int64_t n = (int64_t)N * N * N;
+  const int64_t plane = (int64_t)N * N;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t / plane), j = (int)((t / N) % N), k = (int)(t % N);
+    // wav = waviness * (0.65 sin(.)[y] + 0.35 cos(.)[z]);  arg = (2 pi n (x + wav)) / N
+    const double wav = waviness * (0.65 * sin_y[j] + 0.35 * cos_z[k]);
+    const double arg = (two_pi_layers * ((double)i + wav)) / (double)N;
+    double sv, cv;
+    pr_sincos(arg, &sv, &cv);
+    const double layer = base[i] + 0.35 * sv;
+    const int im = i ? i - 1 : N - 1, ip = i + 1 < N ? i + 1 : 0;
+    const int jm = j ? j - 1 : N - 1, jp = j + 1 < N ? j + 1 : 0;
+    const int km = k ? k - 1 : N - 1, kp = k + 1 < N ? k + 1 : 0;
+    const int64_t ci = (int64_t)i * plane, cj = (int64_t)j * N;
+    double w = noise[t];
+    w = w + noise[(int64_t)im * plane + cj + k];
+    w = w + noise[(int64_t)ip * plane + cj + k];
+    w = w + noise[ci + (int64_t)jm * N + k];
+    w = w + noise[ci + (int64_t)jp * N + k];
+    w = w + noise[ci + cj + km];
+    w = w + noise[ci + cj + kp];
+    field[t] = layer + w / 7.0;
+  }
 }
 
 int count_solid(const uint8_t* phases, int64_t n, int64_t* solid, cudaStream_t s) {
@@ -242,6 +276,35 @@ PR_API int pr_stamp_cells(int64_t N, const int32_t* nodes, const int64_t* node_s
     PR_CUDA(cudaStreamSynchronize(s));  // the host ranges may be freed by the caller on return
   }
   if (solid_cells) PR_TRY(count_solid(phases, n, solid_cells, s));
+  return PR_OK;
+}
+
+PR_API int pr_lamellar_field(int64_t N, const double* base_x, const double* sin_y, const double* cos_z,
+                             double waviness, double two_pi_layers, const double* noise, double* field,
+                             void* stream) {
+  PR_ARG(base_x && sin_y && cos_z && noise && field, "arrays must not be NULL");
+  PR_ARG(N > 0 && N <= 1290, "grid size N must be in 1..1290 (N^3 < 2^31)");
+  PR_ARG(is_device_pointer(field), "field must be device memory of N^3 doubles");
+  const cudaStream_t s = (cudaStream_t)stream;
+  const int64_t n = N * N * N;
+  DevBuf<double> axes, dn;
+  PR_TRY(axes.alloc((size_t)(3 * N), s));
+  PR_CUDA(cudaMemcpyAsync(axes.ptr, base_x, 8 * (size_t)N, cudaMemcpyDefault, s));
+  PR_CUDA(cudaMemcpyAsync(axes.ptr + N, sin_y, 8 * (size_t)N, cudaMemcpyDefault, s));
+  PR_CUDA(cudaMemcpyAsync(axes.ptr + 2 * N, cos_z, 8 * (size_t)N, cudaMemcpyDefault, s));
+  const double* nz = noise;
+  if (!is_device_pointer(noise)) {
+    PR_TRY(dn.alloc((size_t)n, s));
+    PR_CUDA(cudaMemcpyAsync(dn.ptr, noise, 8 * (size_t)n, cudaMemcpyHostToDevice, s));
+    nz = dn.ptr;
+  }
+  timer_begin(kTimerRender, s);
+  k_lamellar<<<grid_for(n, 256, sm_count() * 16), 256, 0, s>>>((int)N, axes.ptr, axes.ptr + N, axes.ptr + 2 * N,
+                                                               waviness, two_pi_layers, nz, field);
+  timer_end(kTimerRender, s);
+  launch_mark();
+  PR_CUDA(cudaGetLastError());
+  PR_CUDA(cudaStreamSynchronize(s));  // host inputs may be freed by the caller on return
   return PR_OK;
 }
 

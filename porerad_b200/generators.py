@@ -13,8 +13,11 @@ Where the work is:
   ``pr_render_shapes`` (cell for cell as the reference's shape test evaluates), fibers by
   ``pr_stamp_fibers`` (lattice nodes along the axis thickened by a one-cell disk); the solid
   count of each trial comes back for the bisection; acceptance uses the device descriptors;
-* TL is a NumPy field (sequential normal draws, glibc sine and cosine, a quantile threshold)
-  and stays on the host as the reference computes it.
+* TL's normal draws and its per-axis sines and cosines are host NumPy calls as in the
+  reference; the N^3 field (the wavy layers with a correctly rounded sine, the 7-point smoothing
+  of the noise) and its quantile threshold are device work (``pr_lamellar_field``,
+  ``pr_quantile_threshold``).  Where the canonical TL is resampled to N = 128 or 160 by SciPy's
+  periodic cubic splines, the field stays a host array.
 
 The arithmetic that must equal the reference's to reproduce its arrays bit for bit (frames,
 strut vectors, node rounding, disk offsets) follows geometry.py operation for operation.
@@ -327,6 +330,33 @@ def lamellar_field(N, seed, n_layers, waviness, noise_amp=TL_NOISE):
     return field + noise
 
 
+def _lamellar_device(N, seed, n_layers, waviness, noise_amp=TL_NOISE):
+    """lamellar_field's values in a device array: the draws and the per-axis sines and cosines on
+    the host as the reference makes them, the N^3 field on the device (``pr_lamellar_field``)."""
+
+    torch = _torch()
+    rng = np.random.default_rng(int(seed))
+    x = np.arange(N, dtype=float)
+    base = np.ascontiguousarray(np.cos(2.0 * np.pi * n_layers * x / float(N)))
+    ph1 = rng.uniform(0.0, 2 * np.pi)
+    ph2 = rng.uniform(0.0, 2 * np.pi)
+    sin_y = np.ascontiguousarray(np.sin(2 * np.pi * x / float(N) + ph1))
+    cos_z = np.ascontiguousarray(np.cos(4 * np.pi * x / float(N) + ph2))
+    noise = np.ascontiguousarray(rng.normal(scale=float(noise_amp), size=(N, N, N)))
+    field = torch.empty((N, N, N), dtype=torch.float64, device="cuda")
+    _lib.check(_lib.load().pr_lamellar_field(N, base.ctypes.data, sin_y.ctypes.data, cos_z.ctypes.data,
+                                             float(waviness), 2 * np.pi * n_layers, noise.ctypes.data,
+                                             field.data_ptr(), _lib.stream()))
+    return field
+
+
+def _threshold_device(field, target_phi):
+    out = _torch().empty(field.shape, dtype=_torch().uint8, device="cuda")
+    _lib.check(_lib.load().pr_quantile_threshold(field.data_ptr(), field.numel(), 1.0 - float(target_phi), 0,
+                                                 out.data_ptr(), None, None, _lib.stream()))
+    return out
+
+
 def threshold(field, target_phi):
     """Solid where the field reaches its (1 - phi_s) quantile (geometry.py:242-245)."""
 
@@ -348,8 +378,8 @@ def _build_device(structure, N, target_phi, seed, continuous_centers=False):
         render = _foam_renderer(N, points, edges)
         return _bisect_radius(lambda r: render(r, float(NODE_TO_STRUT * r)), target_phi, 0.2 * s, 4.0 * s)[1]
     if structure == "TL":
-        ph = threshold(lamellar_field(N, seed, TL_LAYERS[phi], 1.4 + 3.0 * float(target_phi)), target_phi)
-        return _torch().from_numpy(ph).cuda()
+        return _threshold_device(_lamellar_device(N, seed, TL_LAYERS[phi], 1.4 + 3.0 * float(target_phi)),
+                                 target_phi)
     raise ValueError(structure)
 
 
@@ -414,6 +444,9 @@ def canonical(structure, N, *, device=False):
     if structure == "TL":
         from scipy.ndimage import zoom
 
+        if N == TL_BASE_N:
+            out = _threshold_device(_lamellar_device(TL_BASE_N, 0, TL_LAYERS[0.10], 1.4 + 3.0 * 0.10), 0.10)
+            return out if device else _host(out)
         field = lamellar_field(TL_BASE_N, 0, TL_LAYERS[0.10], 1.4 + 3.0 * 0.10)
         if N != TL_BASE_N:
             field = zoom(field, float(N) / float(TL_BASE_N), order=3, mode="grid-wrap", grid_mode=True,
