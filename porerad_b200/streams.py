@@ -45,3 +45,14 @@ def run_concurrently(calls):
             _pool = ThreadPoolExecutor(WORKERS, thread_name_prefix="porerad-worker")
     futs = [_pool.submit(_in_own_stream, fn, args, kwargs) for fn, args, kwargs in calls]
     return [f.result() for f in futs]
+
+
+def submit(fn, *args, **kwargs):
+    """One call on a worker thread with its own stream; returns a Future.  Its inputs must be
+    complete on the device (library calls that return host results are)."""
+
+    global _pool
+    with _pool_lock:
+        if _pool is None:
+            _pool = ThreadPoolExecutor(WORKERS, thread_name_prefix="porerad-worker")
+    return _pool.submit(_in_own_stream, fn, args, kwargs)
