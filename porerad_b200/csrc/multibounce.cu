@@ -8,7 +8,8 @@
 // surface normals and step cap (properties.py:98-197), the same Lambertian sampling about the
 // surface normal (properties.py:200-226), and both restart rules of a reflected ray.  One
 // thread follows one ray; tallies accumulate per thread in ray order and meet in fixed-order
-// block reductions (the reference adds them with atomics in whatever order its threads run).
+// warp reductions, one partial per warp, then one fixed-order sum over the warps (the reference
+// adds them with atomics in whatever order its threads run).
 // Built with -fmad=false; the azimuth's sin and cos are correctly rounded (pr_sincos).
 #include "pr_math.cuh"
 #include "pr_spmv.cuh"
@@ -172,8 +173,10 @@ __device__ void mb_lambertian(uint32_t& state, double nx, double ny, double nz, 
 // Tallies of one thread: properties (0 events, 1 sum of event lengths, 2 censored, 3 sum of
 // censored lengths, 4 interactions, 5 scattered, 6 sum of mu, 7 sum of mu^2) or penetration
 // (0 reflected, 1 transmitted, 2 absorbed, 3 stopped at a cap).  Counts are exact in binary64.
+constexpr int kMbThreads = 64;  // small blocks: a block's registers return as soon as its two warps end
+
 template <bool kPenetration>
-__global__ void __launch_bounds__(256) k_multibounce(MbGrid g, int64_t n, uint32_t seed, double eps, int max_bounces,
+__global__ void __launch_bounds__(kMbThreads) k_multibounce(MbGrid g, int64_t n, uint32_t seed, double eps, int max_bounces,
                                                      int hit_point, double* __restrict__ partial) {
   double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   for (int64_t ray = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; ray < n; ray += (int64_t)gridDim.x * blockDim.x) {
@@ -254,7 +257,15 @@ __global__ void __launch_bounds__(256) k_multibounce(MbGrid g, int64_t n, uint32
       oz = pr_add(oz, pr_mul(dz, dist));
     }
   }
-  block_sum_store<8>(acc, partial);
+  // one partial per warp (no block barrier: a warp whose rays have ended does not wait for the others)
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+  if ((threadIdx.x & 31) == 0) {
+    const int64_t slot = (int64_t)blockIdx.x * (kMbThreads / 32) + (threadIdx.x >> 5);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) partial[slot * 8 + k] = acc[k];
+  }
 }
 
 }  // namespace
@@ -264,17 +275,18 @@ int sum_partials(const double* partial, int blocks, int K, double* out, cudaStre
 // One run of n rays of one seed: the 8 tallies (properties) or 4 counts (penetration).
 int multibounce(const pr_case* c, bool penetration, double eps, int64_t n, uint32_t seed, int max_bounces,
                 int hit_point, double* out8, cudaStream_t s) {
-  const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)sm_count() * 16);
+  const int blocks = (int)std::min<int64_t>((n + kMbThreads - 1) / kMbThreads, (int64_t)sm_count() * 64);
+  const int warps = blocks * (kMbThreads / 32);
   DevBuf<double> partial, out;
-  PR_TRY(partial.alloc((size_t)blocks * 8, s));
+  PR_TRY(partial.alloc((size_t)warps * 8, s));
   PR_TRY(out.alloc(8, s));
   const MbGrid g{c->occ.ptr, (int)c->nx, (int)c->ny, (int)c->nz};
   if (penetration)
-    ::pr::launch_mark(), k_multibounce<true><<<blocks, 256, 0, s>>>(g, n, seed, eps, max_bounces, hit_point, partial.ptr);
+    ::pr::launch_mark(), k_multibounce<true><<<blocks, kMbThreads, 0, s>>>(g, n, seed, eps, max_bounces, hit_point, partial.ptr);
   else
-    ::pr::launch_mark(), k_multibounce<false><<<blocks, 256, 0, s>>>(g, n, seed, eps, max_bounces, hit_point, partial.ptr);
+    ::pr::launch_mark(), k_multibounce<false><<<blocks, kMbThreads, 0, s>>>(g, n, seed, eps, max_bounces, hit_point, partial.ptr);
   PR_CUDA(cudaGetLastError());
-  PR_TRY(sum_partials(partial.ptr, blocks, 8, out.ptr, s));
+  PR_TRY(sum_partials(partial.ptr, warps, 8, out.ptr, s));
   PR_CUDA(cudaMemcpyAsync(out8, out.ptr, 64, cudaMemcpyDeviceToHost, s));
   PR_CUDA(cudaStreamSynchronize(s));
   return PR_OK;

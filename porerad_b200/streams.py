@@ -9,12 +9,14 @@ device work of the others.
 
 from __future__ import annotations
 
+import os
 import threading
 from concurrent.futures import ThreadPoolExecutor
 
 from . import _lib
 
-WORKERS = 8
+WORKERS = int(os.environ.get("PORERAD_WORKERS", "8"))
+"""Worker threads (and streams); PORERAD_WORKERS overrides the default of 8."""
 
 _pool = None
 _pool_lock = threading.Lock()
