@@ -15,7 +15,7 @@ import hashlib
 import numpy as np
 import pytest
 
-from tests.helpers import SMALL, coupled_rows, load_canonical, load_coupled, load_small
+from tests.helpers import SMALL, count_hash_cases, coupled_rows, load_canonical, load_coupled, load_small
 
 pytestmark = pytest.mark.gpu
 
@@ -139,3 +139,29 @@ def test_archived_coupled_rows(case_id):
     assert m["wall_flux_mismatch_rel"] <= 0.005 and m["energy_residual_rel"] <= 1e-3
     op.close()
     table.close()
+
+
+@pytest.mark.parametrize("case_id", ["coupled_TL_y_T700_eps0.6_N128", "coupled_FI_x_T400_eps0.6_N128"])
+def test_coupled_case_driver(case_id):
+    """cases.coupled_case (the run_coupled.py sequence) on archived rows: the stored count hashes
+    of sets A and B reproduced, the archived row, and the A/B comparison."""
+
+    from porerad_b200 import cases
+
+    row = next(r for r in coupled_rows() if r["case_id"] == case_id)
+    h = count_hash_cases()[f"{row['microstructure']}|{row['axis']}"]
+    case = dict(case_id=case_id, group=row["group"], microstructure=row["microstructure"], transfer_axis=row["axis"],
+                repeats_along_axis=row["repeats"], H_m=row["H_m"], N_axis=row["N_axis"], T_mean_K=row["T_mean_K"],
+                delta_T_K=row["delta_T_K"], epsilon=row["epsilon"], rays_per_patch_per_block=row["rays_per_patch"],
+                seeds_A=";".join(str(s) for s in row["seeds_A"]), seeds_B=row["seeds_B"],
+                phase_sha256_x=row["phase_sha256_x"], raw_count_sha256_A=h["sha256_A"], raw_count_sha256_B=h["sha256_B"])
+    out = cases.coupled_case(case, load_canonical(row["microstructure"]), ab=True)
+    assert out.count_hashes == {"A": True, "B": True}
+    assert out.row["newton_updates"] == row["newton_updates"]
+    assert set(out.row) <= set(cases.COUPLED_COLUMNS)
+    for key in ("q_total_hot_W_m2", "q_rad_hot_W_m2", "k_eff_apparent_W_mK", "T_min_K", "T_max_K"):
+        assert abs(out.row[key] - row[key]) <= ARCHIVE_RTOL * abs(row[key]), key
+    assert out.ab["max_temperature_difference_K"] >= 0.0 and out.ab["total_flux_rel_difference"] >= 0.0
+    bad = dict(case, phase_sha256_x="0" * 64)
+    with pytest.raises(ValueError):
+        cases.coupled_case(bad, load_canonical(row["microstructure"]))
