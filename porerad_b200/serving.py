@@ -25,7 +25,7 @@ from typing import Any, Callable
 
 import numpy as np
 
-_CHUNK_RAYS = 1 << 26  # rays per traversal chunk of libporerad (receiver + two stage buffers of int32)
+_WAVE_RAYS = 1 << 27  # rays per traversal wave of libporerad (receiver + two stage buffers of int32 per ray)
 
 
 @dataclass
@@ -107,7 +107,7 @@ def geometry_bytes(n_cells: int) -> int:
 def footprint_bytes(n_patches: int, rays_per_origin: int) -> int:
     """Upper bound of the device bytes of one case after its surface is built.
 
-    Traversal chunk buffers (three int32 per ray of a chunk), the pooled count table
+    Traversal wave buffers (three int32 per ray of a wave), the pooled count table
     (col + count per pair), its transpose and the symmetric matrix with the radix-sort
     scratch of the transpose (about 48 B per pair in all), and the P-vectors.  Pairs
     are bounded by P * min(rays per origin, P).
@@ -115,8 +115,8 @@ def footprint_bytes(n_patches: int, rays_per_origin: int) -> int:
 
     P, L = int(n_patches), int(rays_per_origin)
     pairs = P * min(L, P)
-    chunk = min(P * L, _CHUNK_RAYS)
-    return 12 * chunk + 48 * pairs + 400 * P + (64 << 20)
+    wave = min(P * L, _WAVE_RAYS)
+    return 12 * wave + 48 * pairs + 400 * P + (64 << 20)
 
 
 class Admission:
