@@ -347,8 +347,9 @@ PR_API int pr_morphology_counts(const uint8_t* phases, int64_t nx, int64_t ny, i
  * (minimum-image offsets with NumPy's float remainder, R^T x as OpenBLAS's dgemm forms it).
  * pr_stamp_fibers replaces _long_cylinder (geometry.py:59-82) for n_fibers fibers: fiber f
  * marks (nodes[j] + offsets[k]) mod N for its nodes node_start[f] <= j < node_start[f+1] and
- * disk offsets offset_start[f] <= k < offset_start[f+1] (int32 triples); clear = 1 zeroes the
- * array first.  solid_cells (may be NULL) receives the solid cells of the result. */
+ * disk offsets offset_start[f] <= k < offset_start[f+1] (int32 triples, host or device);
+ * node_start and offset_start (n_fibers + 1 entries each) are host arrays; clear = 1 zeroes
+ * the array first.  solid_cells (may be NULL) receives the solid cells of the result. */
 enum { PR_SHAPE_ELLIPSOID = 0, PR_SHAPE_CYLINDER = 1 };
 typedef struct {
   int32_t kind;
