@@ -179,10 +179,18 @@ def periodic_chords(pore, axis: int) -> tuple:
 def lineal_path(counts, n_all_pore, n_lines, N) -> np.ndarray:
     """L_a(l), l = 1..N, from the chord-count histogram of the periodic cell (descriptors.py:112-117)."""
 
+    # hits(l) = sum over chords of length L >= l of (L - l + 1) = T1(l) - (l - 1) T0(l), with the
+    # tail sums T0(l) = sum_{L >= l} c_L and T1(l) = sum_{L >= l} L c_L (exact integers)
     counts = np.asarray(counts, np.int64)
-    lengths = np.arange(len(counts), dtype=np.int64)
+    m = len(counts)
+    lengths = np.arange(m, dtype=np.int64)
+    t0 = np.zeros(m + 1, np.int64)
+    t1 = np.zeros(m + 1, np.int64)
+    t0[:m] = np.cumsum(counts[::-1])[::-1]
+    t1[:m] = np.cumsum((lengths * counts)[::-1])[::-1]
     seg = np.arange(1, N + 1, dtype=np.int64)
-    hits = (np.maximum(lengths[None, :] - seg[:, None] + 1, 0) * counts[None, :]).sum(axis=1)
+    at = np.minimum(seg, m)  # index m holds the empty tail
+    hits = t1[at] - (seg - 1) * t0[at]
     return (hits + n_all_pore * (seg - 1)) / (n_lines * N)
 
 
@@ -218,37 +226,33 @@ def histogram_quantiles(hist, quantiles=QUANTILES) -> np.ndarray:
     if n == 0:
         raise IndexError("quantiles of an empty sample")
     cum = np.cumsum(hist)
-
-    def value_at(pos: int) -> float:
-        return float(np.searchsorted(cum, pos, side="right"))
-
-    out = []
-    for q in quantiles:
-        v = float(n - 1) * float(q)
-        if v >= n - 1:
-            out.append(value_at(n - 1))
-            continue
-        lo = float(np.floor(v))
-        a, b = value_at(int(lo)), value_at(int(lo) + 1)
-        g = v - lo
-        d = b - a
-        out.append(b - d * (1.0 - g) if g >= 0.5 else a + d * g)
-    return np.asarray(out, dtype=np.float64)
+    q = np.asarray(quantiles, dtype=np.float64)
+    v = float(n - 1) * q
+    top = v >= n - 1
+    lo = np.where(top, float(n - 1), np.floor(v))
+    lo_i = lo.astype(np.int64)
+    a = np.searchsorted(cum, lo_i, side="right").astype(np.float64)
+    b = np.searchsorted(cum, np.where(top, lo_i, lo_i + 1), side="right").astype(np.float64)
+    g = v - lo
+    d = b - a
+    out = np.where(g >= 0.5, b - d * (1.0 - g), a + d * g)
+    return np.where(top, a, out)
 
 
 def _chord_stats(hist) -> tuple:
     """count, mean, std (population), max of the sample with histogram hist."""
 
-    hist = [int(v) for v in hist]
-    n = sum(hist)
+    hist = np.asarray(hist, np.int64)
+    n = int(hist.sum())
     if n == 0:
         return 0, float("nan"), float("nan"), float("nan")
-    s1 = sum(l * c for l, c in enumerate(hist))
-    s2 = sum(l * l * c for l, c in enumerate(hist))
+    lengths = np.arange(len(hist), dtype=np.int64)
+    s1 = int(np.dot(lengths, hist))  # exact: at most 1290 x 2^31
+    s2 = int(np.dot(lengths * lengths, hist))
     mean = float(s1) / float(n)
     var = Fraction(n * s2 - s1 * s1, n * n)
     std = float(np.sqrt(float(var)))
-    top = max(l for l, c in enumerate(hist) if c)
+    top = int(np.flatnonzero(hist)[-1])
     return n, mean, std, float(top)
 
 
