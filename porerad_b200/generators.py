@@ -277,20 +277,37 @@ def _strut_params(N, p0, p1):
     return center, 0.5 * L, _frame(vec / L, _EZ)
 
 
+# pr_shape as a NumPy record (int32 kind, int32 pad, f64 centre[3], f64 R[9], f64 radii[3]: 128 bytes)
+SHAPE_DTYPE = np.dtype([("kind", "<i4"), ("pad", "<i4"), ("center", "<f8", (3,)), ("R", "<f8", (9,)),
+                        ("radii", "<f8", (3,))])
+
+
 def _foam_renderer(N, points, edges):
     struts = [_strut_params(N, points[a], points[b]) for a, b in edges]
     out = _device_array(N)
-    eye = np.eye(3)
+    short = [(c, h, R) for c, h, R in struts if not float(2.0 * h) > float(N)]
+    longs = [_long_fiber(N, c, h, R) for c, h, R in struts if float(2.0 * h) > float(N)]
+    # the shape table once (nodes, then the struts no longer than the cell); a trial sets radii only
+    table = np.zeros(len(points) + len(short), dtype=SHAPE_DTYPE)
+    n_nodes = len(points)
+    table["kind"][:n_nodes] = 0
+    table["center"][:n_nodes] = np.asarray([tuple(p.tolist()) for p in points], dtype=float).reshape(-1, 3)
+    table["R"][:n_nodes] = np.eye(3).ravel()
+    table["kind"][n_nodes:] = 1
+    for q, (center, half, R) in enumerate(short):
+        table["center"][n_nodes + q] = center
+        table["R"][n_nodes + q] = np.asarray(R, dtype=float).ravel()
+        table["radii"][n_nodes + q, 2] = half
+    lib = _lib.load()
 
     def render(strut_radius, node_radius):
-        shapes = [_shape("ellipsoid", tuple(p.tolist()), (node_radius,) * 3, eye) for p in points]
-        longs = []
-        for center, half, R in struts:
-            if float(2.0 * half) > float(N):
-                longs.append(_long_fiber(N, center, half, R))
-            else:
-                shapes.append(_shape("cylinder", center, (strut_radius, strut_radius, half), R))
-        solid = _render_shapes(N, shapes, out)
+        table["radii"][:n_nodes] = float(node_radius)
+        table["radii"][n_nodes:, 0] = float(strut_radius)
+        table["radii"][n_nodes:, 1] = float(strut_radius)
+        solid = ctypes.c_int64()
+        _lib.check(lib.pr_render_shapes(N, table.ctypes.data, len(table), out.data_ptr(), ctypes.byref(solid),
+                                        _lib.stream()))
+        solid = int(solid.value)
         if longs:  # not reached for foams (struts are shorter than the cell); kept for generality
             extra = _device_array(N)
             _stamp(N, longs, strut_radius, extra)
