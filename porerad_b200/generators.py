@@ -86,6 +86,20 @@ def _device_array(N: int):
     return torch.empty((N, N, N), dtype=torch.uint8, device="cuda")
 
 
+_OFFSET_GRIDS: dict = {}
+
+
+def _offset_grid(pad: int):
+    """The lattice offsets -pad..pad per axis (ij order) and their float transpose, built once per pad."""
+
+    got = _OFFSET_GRIDS.get(pad)
+    if got is None:
+        g = np.arange(-pad, pad + 1, dtype=np.int64)
+        off = np.stack([a.ravel() for a in np.meshgrid(g, g, g, indexing="ij")], axis=1)
+        got = _OFFSET_GRIDS[pad] = (off, off.T.astype(float))  # the reference's layout for the product
+    return got
+
+
 class _Long:
     """A cylinder longer than the cell: its lattice nodes and, per radius, its disk offsets."""
 
@@ -102,10 +116,8 @@ class _Long:
     def disk(self, r):
         """Lattice offsets of the one-cell-thick disk of radius r normal to the axis (geometry.py:73-78)."""
 
-        pad = int(math.ceil(r)) + 2
-        g = np.arange(-pad, pad + 1, dtype=np.int64)
-        off = np.stack([a.ravel() for a in np.meshgrid(g, g, g, indexing="ij")], axis=1)
-        local = _matmul(self.Rq.T, off.T.astype(float)).T
+        off, off_t = _offset_grid(int(math.ceil(r)) + 2)
+        local = _matmul(self.Rq.T, off_t).T
         keep = (((local[:, 0] / r) ** 2 + (local[:, 1] / r) ** 2 <= 1.0 + 1e-12)
                 & (np.abs(local[:, 2]) <= 0.5 + 1e-12))
         return off[keep]
