@@ -404,24 +404,29 @@ __global__ void __launch_bounds__(256) k_label_merge(MorphGrid g, int tiles_y, i
   __syncthreads();
   const int tile = blockIdx.x;
   const int i0 = tile / (tiles_y * tiles_z) * kTX, j0 = (tile / tiles_z) % tiles_y * kTY, k0 = tile % tiles_z * kTZ;
+  const int lane = threadIdx.x & 31;
+  // uniform loops (kTile is a multiple of the block; 13 offsets for every lane) so that the lanes of
+  // a warp asking for the same pair of parents meet in one __match_any_sync: one of them goes on
   for (int l = threadIdx.x; l < kTile; l += blockDim.x) {
     const int li = l / (kTY * kTZ), lj = (l / kTZ) % kTY, lk = l % kTZ;
-    if (li != kTX - 1 && lj != 0 && lj != kTY - 1 && lk != 0 && lk != kTZ - 1) continue;
     const int i = i0 + li, j = j0 + lj, k = k0 + lk;
-    if (i >= g.nx || j >= g.ny || k >= g.nz) continue;
-    const int t = (i * g.ny + j) * g.nz + k;
-    if (g.ph[t] != 0) continue;
-    const int pt = __ldcg(parent + t);
+    const bool face = li == kTX - 1 || lj == 0 || lj == kTY - 1 || lk == 0 || lk == kTZ - 1;
+    const bool in = i < g.nx && j < g.ny && k < g.nz;
+    const int t = in ? (i * g.ny + j) * g.nz + k : 0;
+    const bool cand = face && in && g.ph[t] == 0;
+    const int pt = cand ? __ldcg(parent + t) : 0;
     for (int q = 14; q < 27; ++q) {
       int di, dj, dk;
       fwd_offset(q, di, dj, dk);
-      if (li + di < kTX && lj + dj >= 0 && lj + dj < kTY && lk + dk >= 0 && lk + dk < kTZ) continue;  // same tile
+      const bool other_tile = li + di >= kTX || lj + dj < 0 || lj + dj >= kTY || lk + dk < 0 || lk + dk >= kTZ;
       const int a = i + di, b = j + dj, c = k + dk;
-      if (a >= g.nx || b < 0 || b >= g.ny || c < 0 || c >= g.nz) continue;
-      const int u = (a * g.ny + b) * g.nz + c;
-      if (g.ph[u] != 0) continue;
-      const int pu = __ldcg(parent + u);
-      const unsigned long long key = ((unsigned long long)(unsigned int)pt << 32) | (unsigned int)pu;
+      bool ok = cand && other_tile && a < g.nx && b >= 0 && b < g.ny && c >= 0 && c < g.nz;
+      const int u = ok ? (a * g.ny + b) * g.nz + c : 0;
+      ok = ok && g.ph[u] == 0;
+      const int pu = ok ? __ldcg(parent + u) : 0;
+      const unsigned long long key = ok ? ((unsigned long long)(unsigned int)pt << 32) | (unsigned int)pu : ~0ull;
+      const unsigned int grp = __match_any_sync(0xffffffffu, key);
+      if (!ok || lane != __ffs(grp) - 1) continue;
       unsigned int h = (unsigned int)((key * 0x9E3779B97F4A7C15ull) >> 53) & (kPairSlots - 1);
       bool fresh = true;  // a full probe sequence unites without the check (correct, only slower)
       for (int probe = 0; probe < 64; ++probe) {
