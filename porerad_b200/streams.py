@@ -1,4 +1,4 @@
-"""Independent calls on worker threads, each with its own CUDA stream.
+"""Independent calls on worker threads, each with its own CUDA stream on the caller's device.
 
 libporerad releases the GIL while it waits for the device, and every call orders its work on
 the calling thread's stream (``_lib.use_stream``); torch operations of a worker run on the same
@@ -23,16 +23,21 @@ _pool_lock = threading.Lock()
 _local = threading.local()
 
 
-def _in_own_stream(fn, args, kwargs):
+def _in_own_stream(device, fn, args, kwargs):
     import torch
 
-    if getattr(_local, "stream", None) is None:
-        _local.stream = torch.cuda.Stream()
-    with torch.cuda.stream(_local.stream), _lib.use_stream(_local.stream):
+    torch.cuda.set_device(device)  # the current device is per thread: the caller's, not device 0
+    streams = getattr(_local, "streams", None)
+    if streams is None:
+        streams = _local.streams = {}
+    if device not in streams:
+        streams[device] = torch.cuda.Stream(device)
+    stream = streams[device]
+    with torch.cuda.stream(stream), _lib.use_stream(stream):
         try:
             return fn(*args, **kwargs)
         finally:
-            _local.stream.synchronize()  # results leave the worker complete
+            stream.synchronize()  # results leave the worker complete
 
 
 def run_concurrently(calls):
@@ -45,7 +50,8 @@ def run_concurrently(calls):
     with _pool_lock:
         if _pool is None:
             _pool = ThreadPoolExecutor(WORKERS, thread_name_prefix="porerad-worker")
-    futs = [_pool.submit(_in_own_stream, fn, args, kwargs) for fn, args, kwargs in calls]
+    device = torch.cuda.current_device()
+    futs = [_pool.submit(_in_own_stream, device, fn, args, kwargs) for fn, args, kwargs in calls]
     return [f.result() for f in futs]
 
 
@@ -54,7 +60,9 @@ def submit(fn, *args, **kwargs):
     complete on the device (library calls that return host results are)."""
 
     global _pool
+    import torch
+
     with _pool_lock:
         if _pool is None:
             _pool = ThreadPoolExecutor(WORKERS, thread_name_prefix="porerad-worker")
-    return _pool.submit(_in_own_stream, fn, args, kwargs)
+    return _pool.submit(_in_own_stream, torch.cuda.current_device(), fn, args, kwargs)
