@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the surface-radiation path on B200: first-hit rays/s and cases/s.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1|c3|c4|c5|coupled|descriptors|generators|properties] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1|c3|c4|c5|coupled|descriptors|generators|properties|archetypes] [--impl ours|reference]
 
 Workload c2 (default, the configuration the headline metric is quoted on): open-cell
 foam (OF) N=128^3, phi = 0.10, 64 Poisson seeds, geometry seed 1; 1000 rays per patch
@@ -74,6 +74,8 @@ WORKLOADS = {
                                 "x axes x/y/z x eps {0.3,0.6,0.9}: radiative properties (2 seeds x 2e5 normal-incidence "
                                 "rays) and penetration response (2 seeds x 5e5 Lambertian rays), restart 'article', "
                                 "at most 1000 reflections"),
+    "archetypes": dict(workload="benchmark archetypes generated on the device for serving: OF/FI/FA/TL at N = 128 and "
+                                "192, phi 0.10, seed 1 (geometry.make_device, bit-identical to the host definition)"),
     "c1": dict(workload="FI N=64^3 phi=0.10 (r=2, seed 0), 64 rays/patch x 1 set, eps 0.9, T 600->700 K along x, "
                         "FP64 radiosity",
                arch="FI", n=64, phi=0.10, seed=0, rays=64, sets=1, eps=0.9, T_m=650.0, dT=100.0, H=0.01),
@@ -1215,6 +1217,85 @@ def load_phases(name):
     return load_canonical(name)
 
 
+# --------------------------------------------------------------------------- archetype generation
+
+_ARCH_CASES = [(a, n) for n in (128, 192) for a in ("OF", "FI", "FA", "TL")]
+
+
+def archetypes_cpu_sample(target_s: float):
+    """The host definitions (geometry.make, NumPy/SciPy) of the same archetypes, one per process on
+    every host core, until about target_s seconds."""
+
+    import multiprocessing as mp
+
+    cores = os.cpu_count() or 1
+    done = 0
+    with mp.get_context("spawn").Pool(min(cores, len(_ARCH_CASES))) as pool:
+        pool.starmap(_arch_host_one, [("TL", 32)])  # worker start-up, untimed
+        t0 = time.perf_counter()
+        while True:
+            pool.starmap(_arch_host_one, _ARCH_CASES, chunksize=1)
+            done += len(_ARCH_CASES)
+            if time.perf_counter() - t0 >= target_s:
+                break
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": "microstructures/s", "cores": min(cores, len(_ARCH_CASES)), "kind": "port",
+            "sample": f"{done} host generations (OF/FI/FA/TL x N 128, 192) in {dt:.1f} s"}
+
+
+def _arch_host_one(arch, n):
+    from porerad_b200 import geometry
+
+    return int(geometry.make(arch, n, 0.10, 1).sum())
+
+
+def run_archetypes_bench(args, cfg):
+    import torch
+
+    from porerad_b200 import _lib, geometry
+
+    torch.cuda.set_device(0)
+    lib = _lib.load()
+    for _ in range(max(args.warmup, 3)):
+        for a, n in _ARCH_CASES:
+            geometry.make_device(a, n, 0.10, 1)
+    torch.cuda.synchronize()
+    per = {}
+    launches0 = lib.pr_kernel_launches()
+    with ClockSampler(0) as clocks:
+        total_ms = 0.0
+        for _ in range(args.steps):
+            for a, n in _ARCH_CASES:
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record()
+                geometry.make_device(a, n, 0.10, 1)
+                e1.record()
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1)
+                total_ms += ms
+                per.setdefault(f"{a}{n}", []).append(ms)
+    launches = lib.pr_kernel_launches() - launches0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for a, n in _ARCH_CASES:
+            geometry.make_device(a, n, 0.10, 1).cpu()
+    e2e = args.steps * len(_ARCH_CASES) / (time.perf_counter() - t0)
+    cpu = None if args.no_cpu else archetypes_cpu_sample(args.cpu_seconds)
+    return {
+        "metric": "benchmark archetypes generated per second (device, bit-identical to the host definition)",
+        "value": args.steps * len(_ARCH_CASES) / (total_ms * 1e-3), "unit": "microstructures/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 (fields), u8", "data": "synthetic (seeded)",
+        "config": {"workload": cfg["workload"], "l2": "each generation writes fresh arrays of 2-7 MiB"},
+        "ms_per_generation": {k: float(np.median(v)) for k, v in per.items()},
+        "e2e": {"value": e2e, "unit": "microstructures/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(sum(n ** 3 for _, n in _ARCH_CASES))},
+        "roofline": None, "clocks": clocks.summary(), "gpu_launches": int(launches) // max(args.steps, 1),
+        "cpu_baseline": cpu,
+    }
+
+
 def run_reference(args, cfg):
     from porerad_b200 import replicas
 
@@ -1311,6 +1392,8 @@ def main():
         line = run_generators_bench(args, cfg)
     elif args.workload == "properties":
         line = run_properties_bench(args, cfg)
+    elif args.workload == "archetypes":
+        line = run_archetypes_bench(args, cfg)
     elif args.workload == "c4":
         line = run_c4(args, cfg)
     elif args.workload == "c5":
