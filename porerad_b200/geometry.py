@@ -30,10 +30,15 @@ def _ball(radius: float) -> np.ndarray:
     return np.stack((dx[keep], dy[keep], dz[keep]), axis=1)
 
 
-def _segment_centres(p0: np.ndarray, direction: np.ndarray, length: float) -> np.ndarray:
+def _segment_points(p0: np.ndarray, direction: np.ndarray, length: float) -> np.ndarray:
+    """Lattice points along a segment every quarter cell (with repeats)."""
+
     t = np.arange(-length / 2.0, length / 2.0 + 0.25, 0.25)
-    centres = np.rint(p0[None, :] + t[:, None] * direction[None, :]).astype(np.int64)
-    return np.unique(centres, axis=0)
+    return np.rint(p0[None, :] + t[:, None] * direction[None, :]).astype(np.int64)
+
+
+def _segment_centres(p0: np.ndarray, direction: np.ndarray, length: float) -> np.ndarray:
+    return np.unique(_segment_points(p0, direction, length), axis=0)
 
 
 def _stamp_segment(solid: np.ndarray, p0: np.ndarray, direction: np.ndarray, length: float, ball: np.ndarray) -> None:
@@ -130,7 +135,8 @@ def _hole_disk(hole: int) -> np.ndarray:
 def make_device(archetype: str, n: int, phi: float, seed: int, *, stream=None):
     """``make(archetype, n, phi, seed)`` generated on the device: a uint8 CUDA tensor equal to the
     host array bit for bit.  The random draws stay on the host (the same NumPy generator calls);
-    the grid work runs in libporerad: segment and hole stamping with solid counts
+    the grid work runs in libporerad: fiber segments in batches, each cell keeping the first fiber
+    that covers it (``pr_stamp_first``, ``pr_first_threshold``), hole stamping with solid counts
     (``pr_stamp_cells``), the foam's nearest-seed field (``pr_voronoi_edge_field``) and its quantile
     threshold (``pr_quantile_threshold``)."""
 
@@ -147,6 +153,9 @@ def make_device(archetype: str, n: int, phi: float, seed: int, *, stream=None):
     solid = ctypes.c_int64()
     start = np.array([0, 1], np.int64)
 
+    def count_below(count, target):  # the host loop's condition `while count < target`
+        return count < target
+
     def stamp(nodes, offsets, value, clear):
         nd = np.ascontiguousarray(nodes, dtype=np.int32)
         od = np.ascontiguousarray(offsets, dtype=np.int32)
@@ -157,17 +166,35 @@ def make_device(archetype: str, n: int, phi: float, seed: int, *, stream=None):
         return int(solid.value)
 
     if archetype in ("FI", "FA"):
+        # the host loop adds one fiber until the solid reaches phi n^3; here batches of fibers are
+        # stamped at once, every cell keeping the first fiber that covers it, and the cells each
+        # fiber adds tell where the loop stops (the same union; draws past it are discarded)
         rng = np.random.default_rng(seed)
-        ball = _ball(2.0)
+        ball = np.ascontiguousarray(_ball(2.0), dtype=np.int32)
         target = phi * n ** 3
-        count, first = 0, True
-        while count < target:
-            p0, d, length = _fiber_draws(n, rng, archetype == "FA")
-            count = stamp(_segment_centres(p0, d, length) % n, ball, 1, first)
-            first = False
-        if first:
+        if not count_below(0, target):
             out.zero_()
             torch.cuda.current_stream().synchronize()
+            return out
+        first = torch.full((n, n, n), np.iinfo(np.int32).max, dtype=torch.int32, device="cuda")
+        torch.cuda.current_stream().synchronize()
+        batch, base, count, last = 64, 0, 0, -1
+        while last < 0:
+            # stamping is idempotent: the segment's lattice points need no deduplication here
+            nodes = [_segment_points(*_fiber_draws(n, rng, archetype == "FA")) % n for _ in range(batch)]
+            node_start = np.zeros(batch + 1, np.int64)
+            node_start[1:] = np.cumsum([len(a) for a in nodes])
+            nd = np.ascontiguousarray(np.concatenate(nodes), dtype=np.int32)
+            new = np.zeros(batch, np.int64)
+            _lib.check(lib.pr_stamp_first(n, nd.ctypes.data, node_start.ctypes.data, ball.ctypes.data, len(ball),
+                                          batch, base, first.data_ptr(), new.ctypes.data, st))
+            for f in range(batch):
+                count += int(new[f])
+                if not count_below(count, target):
+                    last = base + f
+                    break
+            base += batch
+        _lib.check(lib.pr_first_threshold(first.data_ptr(), n ** 3, last, out.data_ptr(), st))
         return out
     if archetype == "OF":
         rng = np.random.default_rng(seed)
