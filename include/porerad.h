@@ -387,17 +387,18 @@ PR_API int pr_stamp_cells(int64_t N, const int32_t* nodes, const int64_t* node_s
  * q = numpy.quantile(field, quantile) and phases = field <= q (below = 1) or field >= q; q_out
  * and solid_cells may be NULL. */
 PR_API int pr_voronoi_edge_field(int64_t N, const double* seeds, int n_seeds, double* field, void* stream);
-/* The fiber archetypes' loop "add a fiber until the solid fraction is reached" in batches:
- * pr_stamp_first stamps n_fibers (<= 1024) segments at once (fiber f: nodes[node_start[f] ..
- * node_start[f+1]), int32 triples, thickened by the shared offsets), keeping in first (device,
- * N^3 int32, initialised by the caller to INT32_MAX) the smallest index base + f of a fiber
- * covering each cell, and returns in new_cells[f] (host) the cells fiber base + f adds to the
- * union of all fibers before it.  pr_first_threshold writes phases = first <= last.
- * node_start and new_cells are host arrays. */
+/* The archetypes' loops "add a fiber until the solid fraction is reached" and "punch a hole
+ * until it falls to the target" in batches: pr_stamp_first stamps n_fibers (<= 1024) shapes at
+ * once (shape f: nodes[node_start[f] .. node_start[f+1]), int32 triples, thickened by the shared
+ * offsets), keeping in first (device, N^3 int32, initialised by the caller to INT32_MAX) the
+ * smallest index base + f of a shape covering each cell, and returns in new_cells[f] (host) the
+ * cells shape base + f covers first, counting only cells where mask (device, may be NULL) is 1.
+ * pr_first_threshold: mode 0 writes phases = first <= last, mode 1 clears the cells with
+ * first <= last.  node_start and new_cells are host arrays. */
 PR_API int pr_stamp_first(int64_t N, const int32_t* nodes, const int64_t* node_start, const int32_t* offsets,
-                          int64_t n_offsets, int n_fibers, int base, int32_t* first, int64_t* new_cells,
-                          void* stream);
-PR_API int pr_first_threshold(const int32_t* first, int64_t n, int last, uint8_t* phases, void* stream);
+                          int64_t n_offsets, int n_fibers, int base, int32_t* first, const uint8_t* mask,
+                          int64_t* new_cells, void* stream);
+PR_API int pr_first_threshold(const int32_t* first, int64_t n, int last, int mode, uint8_t* phases, void* stream);
 PR_API int pr_quantile_threshold(const double* field, int64_t n, double quantile, int below, uint8_t* phases,
                                  double* q_out, int64_t* solid_cells, void* stream);
 

@@ -141,8 +141,8 @@ _SIGNATURES = {
     "pr_stamp_cells": (_i32, [_i64, _vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp, _vp]),
     "pr_voronoi_edge_field": (_i32, [_i64, _vp, _i32, _vp, _vp]),
     "pr_lamellar_field": (_i32, [_i64, _vp, _vp, _vp, _f64, _f64, _vp, _vp, _vp]),
-    "pr_stamp_first": (_i32, [_i64, _vp, _vp, _vp, _i64, _i32, _i32, _vp, _vp, _vp]),
-    "pr_first_threshold": (_i32, [_vp, _i64, _i32, _vp, _vp]),
+    "pr_stamp_first": (_i32, [_i64, _vp, _vp, _vp, _i64, _i32, _i32, _vp, _vp, _vp, _vp]),
+    "pr_first_threshold": (_i32, [_vp, _i64, _i32, _i32, _vp, _vp]),
     "pr_quantile_threshold": (_i32, [_vp, _i64, _f64, _i32, _vp, _vp, _vp, _vp]),
     "pr_timers_enable": (None, [_i32]),
     "pr_timers_reset": (None, []),

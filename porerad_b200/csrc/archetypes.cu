@@ -6,11 +6,10 @@
 //    points.  Per axis the difference c - p is wrapped once into [-N/2, N/2] (below -N/2: + N,
 //    above N/2: - N), squares are summed x, y, z in that order and the square roots taken after
 //    ranking, the arithmetic of SciPy's periodic k-d tree query for these inputs.
-//  * k_stamp_first / k_first_hist / k_first_threshold: a batch of fibers stamped at once, each
-//    cell keeping the smallest index of a fiber that covers it; the cells each fiber adds are then
-//    a histogram, so the host finds where its one-fiber-at-a-time loop would stop (the first
-//    fiber after which the solid reaches its target) and the phases are "first index <= that
-//    fiber", the same union.
+//  * k_stamp_first / k_first_hist / k_first_threshold: a batch of fibers (or holes) stamped at
+//    once, each cell keeping the smallest index of one that covers it; the cells each adds (or,
+//    within a mask, removes) are then a histogram, so the host finds where its one-at-a-time loop
+//    would stop, and the phases follow from "first index <= that one" (the same union).
 //  * pr_quantile_threshold: NumPy's default quantile of a device array (the order statistics
 //    from a radix sort, the linear interpolation of numpy.quantile on the host) and the
 //    threshold field <= q (or >= q) into a phase array.
@@ -97,24 +96,31 @@ __global__ void k_stamp_first(int N, const int* __restrict__ nodes, const int64_
   }
 }
 
-// new[f] = cells whose first covering fiber is base + f (f < K <= 1024)
-__global__ void __launch_bounds__(256) k_first_hist(const int* __restrict__ first, int64_t n, int base, int K,
-                                                    unsigned long long* __restrict__ out) {
+// new[f] = cells whose first covering fiber is base + f (f < K <= 1024), among the cells where
+// mask is 1 when a mask is given
+__global__ void __launch_bounds__(256) k_first_hist(const int* __restrict__ first, const uint8_t* __restrict__ mask,
+                                                    int64_t n, int base, int K, unsigned long long* __restrict__ out) {
   __shared__ unsigned int h[1024];
   for (int q = threadIdx.x; q < K; q += blockDim.x) h[q] = 0;
   __syncthreads();
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
     const int v = first[t] - base;
-    if (v >= 0 && v < K) atomicAdd(h + v, 1u);
+    if (v >= 0 && v < K && (!mask || mask[t] == 1)) atomicAdd(h + v, 1u);
   }
   __syncthreads();
   for (int q = threadIdx.x; q < K; q += blockDim.x)
     if (h[q]) atomicAdd(out + q, (unsigned long long)h[q]);
 }
 
-__global__ void k_first_threshold(const int* __restrict__ first, int64_t n, int last, uint8_t* __restrict__ phases) {
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
-    phases[t] = first[t] <= last;
+// mode 0: phases = first <= last (the union of the fibers up to last); mode 1: cells covered by a
+// hole up to last are cleared
+__global__ void k_first_threshold(const int* __restrict__ first, int64_t n, int last, int mode,
+                                  uint8_t* __restrict__ phases) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    const bool covered = first[t] <= last;
+    if (mode == 0) phases[t] = covered;
+    else if (covered) phases[t] = 0;
+  }
 }
 
 // numpy.quantile(x, q) ("linear"): virtual index v = (n - 1) q between sorted values a and b
@@ -198,14 +204,15 @@ PR_API int pr_quantile_threshold(const double* field, int64_t n, double quantile
 }
 
 PR_API int pr_stamp_first(int64_t N, const int32_t* nodes, const int64_t* node_start, const int32_t* offsets,
-                          int64_t n_offsets, int n_fibers, int base, int32_t* first, int64_t* new_cells,
-                          void* stream) {
+                          int64_t n_offsets, int n_fibers, int base, int32_t* first, const uint8_t* mask,
+                          int64_t* new_cells, void* stream) {
   PR_ARG(node_start && first && new_cells, "node_start, first and new_cells must not be NULL");
   PR_ARG(N > 0 && N <= 1290, "grid size N must be in 1..1290 (N^3 < 2^31)");
   PR_ARG(n_fibers >= 0 && n_fibers <= 1024, "n_fibers must be in 0..1024");
   PR_ARG(base >= 0 && (int64_t)base + n_fibers < INT32_MAX, "fiber indices must stay below 2^31 - 1");
   PR_ARG(n_offsets >= 0 && n_offsets < INT32_MAX, "n_offsets out of range");
   PR_ARG(is_device_pointer(first), "first must be device memory of N^3 int32");
+  PR_ARG(!mask || is_device_pointer(mask), "mask must be device memory of N^3 bytes");
   const int64_t n_nodes = node_start[n_fibers];
   PR_ARG(node_start[0] == 0 && n_nodes >= 0, "fiber ranges must start at 0");
   for (int f = 0; f < n_fibers; ++f) PR_ARG(node_start[f + 1] >= node_start[f], "fiber ranges must not decrease");
@@ -230,7 +237,7 @@ PR_API int pr_stamp_first(int64_t N, const int32_t* nodes, const int64_t* node_s
                                                                      (int)n_offsets, n_fibers, base, first);
     launch_mark();
     PR_CUDA(cudaGetLastError());
-    k_first_hist<<<grid_for(n, 256, sm_count() * 4), 256, 0, s>>>(first, n, base, n_fibers, hist.ptr);
+    k_first_hist<<<grid_for(n, 256, sm_count() * 4), 256, 0, s>>>(first, mask, n, base, n_fibers, hist.ptr);
     launch_mark();
     PR_CUDA(cudaGetLastError());
   }
@@ -241,11 +248,12 @@ PR_API int pr_stamp_first(int64_t N, const int32_t* nodes, const int64_t* node_s
   return PR_OK;
 }
 
-PR_API int pr_first_threshold(const int32_t* first, int64_t n, int last, uint8_t* phases, void* stream) {
+PR_API int pr_first_threshold(const int32_t* first, int64_t n, int last, int mode, uint8_t* phases, void* stream) {
+  PR_ARG(mode == 0 || mode == 1, "mode must be 0 (union) or 1 (clear the covered cells)");
   PR_ARG(first && phases && n > 0, "first and phases must not be NULL; n must be positive");
   PR_ARG(is_device_pointer(first) && is_device_pointer(phases), "first and phases must be device memory");
   const cudaStream_t s = (cudaStream_t)stream;
-  k_first_threshold<<<grid_for(n, 256, sm_count() * 8), 256, 0, s>>>(first, n, last, phases);
+  k_first_threshold<<<grid_for(n, 256, sm_count() * 8), 256, 0, s>>>(first, n, last, mode, phases);
   launch_mark();
   PR_CUDA(cudaGetLastError());
   PR_CUDA(cudaStreamSynchronize(s));

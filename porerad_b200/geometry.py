@@ -187,14 +187,14 @@ def make_device(archetype: str, n: int, phi: float, seed: int, *, stream=None):
             nd = np.ascontiguousarray(np.concatenate(nodes), dtype=np.int32)
             new = np.zeros(batch, np.int64)
             _lib.check(lib.pr_stamp_first(n, nd.ctypes.data, node_start.ctypes.data, ball.ctypes.data, len(ball),
-                                          batch, base, first.data_ptr(), new.ctypes.data, st))
+                                          batch, base, first.data_ptr(), None, new.ctypes.data, st))
             for f in range(batch):
                 count += int(new[f])
                 if not count_below(count, target):
                     last = base + f
                     break
             base += batch
-        _lib.check(lib.pr_first_threshold(first.data_ptr(), n ** 3, last, out.data_ptr(), st))
+        _lib.check(lib.pr_first_threshold(first.data_ptr(), n ** 3, last, 0, out.data_ptr(), st))
         return out
     if archetype == "OF":
         rng = np.random.default_rng(seed)
@@ -213,12 +213,35 @@ def make_device(archetype: str, n: int, phi: float, seed: int, *, stream=None):
         plane_offsets = np.stack([a.ravel() for a in np.meshgrid(g, g, [0], indexing="ij")], axis=1)
         count = stamp(planes, plane_offsets, 1, True)
         disk = _hole_disk(hole)
-        hole_offsets = np.array([(dx, dy, dz) for dz in range(thickness) for dx, dy in disk], np.int64)
+        hole_offsets = np.ascontiguousarray([(dx, dy, dz) for dz in range(thickness) for dx, dy in disk],
+                                            dtype=np.int32)
         target = phi * n ** 3
-        while count > target:
-            z0 = sheet_z[int(rng.integers(0, m))]
-            c = rng.integers(0, n, size=2)
-            count = stamp(np.array([(c[0], c[1], z0)]), hole_offsets, 0, False)
+        if not count > target:  # the host loop's condition `while solid.sum() > target`
+            return out
+        # holes in batches: each cell keeps the first hole covering it, the solid cells each hole
+        # removes tell where the host loop stops, and the cells up to that hole are cleared
+        first = torch.full((n, n, n), np.iinfo(np.int32).max, dtype=torch.int32, device="cuda")
+        torch.cuda.current_stream().synchronize()
+        batch, base, last = 64, 0, -1
+        node_start = np.arange(batch + 1, dtype=np.int64)
+        while last < 0:
+            centres = []
+            for _ in range(batch):
+                z0 = sheet_z[int(rng.integers(0, m))]
+                c = rng.integers(0, n, size=2)
+                centres.append((c[0], c[1], z0))
+            nd = np.ascontiguousarray(centres, dtype=np.int32)
+            removed = np.zeros(batch, np.int64)
+            _lib.check(lib.pr_stamp_first(n, nd.ctypes.data, node_start.ctypes.data, hole_offsets.ctypes.data,
+                                          len(hole_offsets), batch, base, first.data_ptr(), out.data_ptr(),
+                                          removed.ctypes.data, st))
+            for f in range(batch):
+                count -= int(removed[f])
+                if not count > target:
+                    last = base + f
+                    break
+            base += batch
+        _lib.check(lib.pr_first_threshold(first.data_ptr(), n ** 3, last, 1, out.data_ptr(), st))
         return out
     raise ValueError(f"unknown archetype {archetype!r}; expected one of {ARCHETYPES}")
 
