@@ -72,6 +72,11 @@ def test_widened_entry_points_reject_bad_arguments():
     assert lib.pr_quantile_threshold(seeds, 6, 1.5, 1, ph, None, None, None) == ERR
     assert "quantile" in _lib.last_error()
     assert lib.pr_lamellar_field(8, None, seeds, seeds, 1.0, 1.0, seeds, seeds, None) == ERR
+    new = (ctypes.c_int64 * 2)()
+    assert lib.pr_stamp_first(8, None, starts, None, 0, 2000, 0, ph, None, new, None) == ERR
+    assert "n_fibers" in _lib.last_error()
+    assert lib.pr_first_threshold(ph, 8, 0, 2, ph, None) == ERR
+    assert "mode" in _lib.last_error()
     tally = _lib.PropertiesTally()
     assert lib.pr_radiative_properties(None, 0.5, 10, 1, 0, 10, ctypes.byref(tally), None) == ERR
     counts = (ctypes.c_int64 * 4)()
