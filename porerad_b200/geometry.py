@@ -1,8 +1,10 @@
 """Seeded synthetic voxel microstructures of the four benchmark archetypes (uint8, 1 = solid).
 
-These are the workload inputs of the benchmark and tests, generated on the host
-with NumPy from an integer seed.  They follow the archetype definitions of the
-benchmark configurations (not the reference's own generators, porerad/geometry.py):
+These are the workload inputs of the benchmark and tests, defined on the host with
+NumPy from an integer seed (``make``) and generated bit for bit on the device for
+serving (``make_device``).  They follow the archetype definitions of the benchmark
+configurations; the reference's own generators (porerad/geometry.py) are re-exported
+at the end of this module from ``porerad_b200.generators``:
 
 * FI: isotropic random-axis solid cylinders of radius r placed until the solid
   fraction reaches phi;
