@@ -1380,6 +1380,9 @@ def main():
     if args.rays is not None and "rays" in cfg:
         cfg["rays"] = int(args.rays)
         cfg["workload"] += f" [rays/patch overridden to {args.rays}: profiling case]"
+    if args.impl != "reference" and args.workload not in ("c1", "c2") and int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        # one process per GPU with independent replicas is the c1/c2 path; the others time one GPU
+        raise SystemExit(f"workload {args.workload} runs on one GPU; launch it without torchrun")
     if args.impl == "reference":
         line = run_reference(args, cfg)
     elif args.workload == "c3":
