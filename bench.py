@@ -1301,6 +1301,19 @@ def run_reference(args, cfg):
 
     if replicas.rank() != 0:
         return None  # the CPU reference runs once, on rank 0
+    if args.workload == "archetypes":
+        vals, last = [], None
+        for _ in range(args.steps):
+            last = archetypes_cpu_sample(max(1.0, args.cpu_seconds / 2))
+            vals.append(last["value"])
+        value = float(np.mean(vals))
+        return {"impl": "reference", "metric": "benchmark archetypes generated per second (device, bit-identical to "
+                                               "the host definition)",
+                "value": value, "unit": "microstructures/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": 0,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 (fields), u8",
+                "data": "synthetic (seeded)", "config": {"workload": cfg["workload"]},
+                "cpu_baseline": {**last, "value": value},
+                "e2e": {"value": value, "unit": "microstructures/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if args.workload == "properties":
         vals, last = [], None
         for _ in range(args.steps):
