@@ -113,3 +113,22 @@ def test_python_float_remainder(hm):
     want = np.remainder(a, 128.0)
     assert np.array_equal(out, want)
     assert np.array_equal(np.signbit(out), np.signbit(want))
+
+
+def test_sincos_correctly_rounded_on_the_layer_field_range(hm):
+    """The arguments of TL's wavy layers, 2 pi n (x + wav) / N, lie within about [-10, 60]: the
+    header's sine there is within one ulp of glibc's and, on every disagreement checked, the
+    correctly rounded one (the device TL field relies on it)."""
+
+    rng = np.random.default_rng(11)
+    x = rng.uniform(-10.0, 60.0, size=200_000)
+    s = np.empty_like(x)
+    c = np.empty_like(x)
+    hm.hm_sincos(x.ctypes.data, x.size, s.ctypes.data, c.ctypes.data)
+    gs = np.sin(x)
+    assert np.all(np.abs(s - gs) <= np.spacing(np.abs(gs)))
+    bad = np.flatnonzero(s != gs)
+    assert bad.size < 0.01 * x.size
+    for i in bad[:25]:
+        es, _ = _exact_sin_cos(float(x[i]))
+        assert abs(Decimal(float(s[i])) - es) <= abs(Decimal(float(gs[i])) - es)
