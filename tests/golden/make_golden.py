@@ -27,7 +27,8 @@ where the reference is not installed:
   results/prescribed_field.csv (q_h, q_c, q_i and the A/B wall-channel difference); their
   18 microstructures are stored like the canonical ones (``canonical_<name>.npz``).
 * ``multibounce.json``: the archived rows of results/radiative_properties.csv and
-  results/penetration_response.csv for the microstructures stored here.
+  results/penetration_response.csv (and of results/hit_point_restart/, the other restart rule)
+  for the microstructures stored here.
 * ``microstructures.json``: every row of data/microstructures.csv (id, structure, set, N,
   target solid fraction, seed, archived phase_sha256) for the generator tests.
 * ``descriptors.json``: porerad.descriptors run on every microstructure stored here
@@ -218,7 +219,9 @@ def prescribed_cases(ref):
 def multibounce_rows(ref):
     have = {p.name[len("canonical_"):-4] for p in HERE.glob("canonical_*.npz")}
     out = {}
-    for key, name in (("properties", "radiative_properties.csv"), ("penetration", "penetration_response.csv")):
+    for key, name in (("properties", "radiative_properties.csv"), ("penetration", "penetration_response.csv"),
+                      ("properties_hit_point", "hit_point_restart/radiative_properties.csv"),
+                      ("penetration_hit_point", "hit_point_restart/penetration_response.csv")):
         rows = []
         for r in csv.DictReader(open(ref / "results" / name)):
             if r["microstructure"] not in have:
@@ -231,7 +234,8 @@ def multibounce_rows(ref):
                 row["retained"] = r["retained"] == "True"
             rows.append(row)
         out[key] = rows
-    out["source"] = "results/radiative_properties.csv, results/penetration_response.csv"
+    out["source"] = ("results/radiative_properties.csv, results/penetration_response.csv and their "
+                     "hit_point_restart/ versions")
     (HERE / "multibounce.json").write_text(json.dumps(out, indent=1))
     print("multibounce rows:", {k: len(v) for k, v in out.items() if k != "source"})
 

@@ -63,3 +63,25 @@ def test_properties_every_microstructure(row):
     tal = [om.run(solid, row["epsilon"], 200_000, s, penetration=False) for s in (123, 456)]
     assert math.isclose(np.mean([t[0] / (t[1] + t[3]) for t in tal]), row["beta_per_cell"], rel_tol=1e-12)
     assert math.isclose(np.mean([t[5] / t[4] for t in tal]), row["omega"], rel_tol=1e-12)
+
+
+@pytest.mark.parametrize("row", [r for r in ROWS["penetration_hit_point"]][::9], ids=lambda r: r["microstructure"])
+def test_penetration_hit_point_restart(row):
+    """results/hit_point_restart/penetration_response.csv: the other restart rule."""
+
+    n = 500_000
+    solid = _solid(row["microstructure"], row["transfer_axis"])
+    counts = sum(om.run(solid, row["epsilon"], n, s, penetration=True, restart="hit_point") for s in (321, 654))
+    for k, key in enumerate(("reflectance", "transmittance", "absorptance")):
+        assert counts[k] / (2 * n) == pytest.approx(row[key], abs=1e-12)
+
+
+@pytest.mark.parametrize("row", [r for r in ROWS["properties_hit_point"]][::9], ids=lambda r: r["microstructure"])
+def test_properties_hit_point_restart(row):
+    """results/hit_point_restart/radiative_properties.csv: the other restart rule."""
+
+    solid = _solid(row["microstructure"], row["transfer_axis"])
+    tal = [om.run(solid, row["epsilon"], 200_000, s, penetration=False, restart="hit_point") for s in (123, 456)]
+    assert math.isclose(np.mean([t[0] / (t[1] + t[3]) for t in tal]), row["beta_per_cell"], rel_tol=1e-12)
+    assert math.isclose(np.mean([t[5] / t[4] for t in tal]), row["omega"], rel_tol=1e-12)
+    assert math.isclose(np.mean([t[6] / t[5] for t in tal]), row["g"], rel_tol=1e-10)
