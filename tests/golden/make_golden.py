@@ -29,6 +29,9 @@ where the reference is not installed:
 * ``multibounce.json``: the archived rows of results/radiative_properties.csv and
   results/penetration_response.csv (and of results/hit_point_restart/, the other restart rule)
   for the microstructures stored here.
+* ``ray_set_comparison.json``: the "A vs B" rows of results/coupled_ray_set_comparison.csv
+  (one emissivity, N = 128): largest temperature and relative total-flux differences of the
+  coupled solves with sets A and B on their own.
 * ``microstructures.json``: every row of data/microstructures.csv (id, structure, set, N,
   target solid fraction, seed, archived phase_sha256) for the generator tests.
 * ``descriptors.json``: porerad.descriptors run on every microstructure stored here
@@ -313,6 +316,19 @@ def descriptor_rows(ref):
     print("descriptor records:", len(stored), "stored,", len(small), "small")
 
 
+def ray_set_comparison_rows(ref):
+    rows = []
+    for r in csv.DictReader(open(ref / "results" / "coupled_ray_set_comparison.csv")):
+        if r["sets_compared"] == "A vs B" and ";" not in r["epsilon"] and r["N_axis"] == "128":
+            rows.append(dict(microstructure=r["microstructure"], axis=r["transfer_axis"], T_mean_K=float(r["T_mean_K"]),
+                             epsilon=float(r["epsilon"]),
+                             max_temperature_difference_K=float(r["max_temperature_difference_K"]),
+                             total_flux_rel_difference=float(r["total_flux_rel_difference"])))
+    (HERE / "ray_set_comparison.json").write_text(json.dumps(dict(
+        rows=rows, source="results/coupled_ray_set_comparison.csv (A vs B, one emissivity, N = 128)"), indent=1))
+    print("ray-set comparison rows:", len(rows))
+
+
 def microstructure_rows(ref):
     rows = []
     for r in csv.DictReader(open(ref / "data" / "microstructures.csv")):
@@ -339,6 +355,7 @@ def main():
     multibounce_rows(ref)
     descriptor_rows(ref)
     microstructure_rows(ref)
+    ray_set_comparison_rows(ref)
 
     rows = list(csv.DictReader(open(ref / "data" / "cases_coupled.csv")))
     hashes = {}

@@ -11,11 +11,12 @@ seeds) are reproduced through the whole device path.
 from __future__ import annotations
 
 import hashlib
+import json
 
 import numpy as np
 import pytest
 
-from tests.helpers import SMALL, count_hash_cases, coupled_rows, load_canonical, load_coupled, load_small
+from tests.helpers import GOLDEN, SMALL, count_hash_cases, coupled_rows, load_canonical, load_coupled, load_small
 
 pytestmark = pytest.mark.gpu
 
@@ -165,3 +166,26 @@ def test_coupled_case_driver(case_id):
     bad = dict(case, phase_sha256_x="0" * 64)
     with pytest.raises(ValueError):
         cases.coupled_case(bad, load_canonical(row["microstructure"]))
+
+
+RAYSET = json.loads((GOLDEN / "ray_set_comparison.json").read_text())["rows"]
+
+
+@pytest.mark.parametrize("ref", RAYSET, ids=lambda r: f"{r['microstructure']}-{r['axis']}")
+def test_ray_set_comparison_rows(ref):
+    """results/coupled_ray_set_comparison.csv (run_coupled.py --ab): the coupled solves with sets A
+    and B on their own differ by the archived largest temperature difference and relative
+    total-flux difference (the latter a difference of nearly equal fluxes: compared absolutely)."""
+
+    from porerad_b200 import cases
+
+    row = next(r for r in coupled_rows() if r["microstructure"] == ref["microstructure"] and r["axis"] == ref["axis"]
+               and r["T_mean_K"] == ref["T_mean_K"] and r["epsilon"] == ref["epsilon"] and r["repeats"] == 1)
+    case = dict(case_id=row["case_id"], transfer_axis=row["axis"], repeats_along_axis=row["repeats"], H_m=row["H_m"],
+                N_axis=row["N_axis"], T_mean_K=row["T_mean_K"], delta_T_K=row["delta_T_K"], epsilon=row["epsilon"],
+                rays_per_patch_per_block=row["rays_per_patch"], seeds_A=row["seeds_A"], seeds_B=row["seeds_B"],
+                phase_sha256_x=row["phase_sha256_x"])
+    out = cases.coupled_case(case, load_canonical(row["microstructure"]), ab=True)
+    dT, dq = out.ab["max_temperature_difference_K"], out.ab["total_flux_rel_difference"]
+    assert abs(dT - ref["max_temperature_difference_K"]) <= 1e-6 * ref["max_temperature_difference_K"] + 1e-9
+    assert abs(dq - ref["total_flux_rel_difference"]) <= 1e-6
