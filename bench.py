@@ -111,8 +111,13 @@ def make_phases(cfg):
 
 # --------------------------------------------------------------------------- our arm
 
-def served_step(phases, cfg, seeds, precision="mixed"):
-    """One case, device-resident; returns host scalars (the only device->host data)."""
+def served_step(phases, cfg, seeds, precision="mixed", serial=False, timers=False):
+    """One case, device-resident; returns host scalars (the only device->host data).
+
+    ``serial`` builds and solves the operators one after the other on the caller's stream
+    instead of on worker streams at once; ``timers`` (with ``serial``) records the library's
+    kernel timers of the operator stage alone in ``out["_timers"]``.
+    """
 
     from porerad_b200 import coupled, exchange, view_factors as vf
 
@@ -140,7 +145,23 @@ def served_step(phases, cfg, seeds, precision="mixed"):
     from porerad_b200 import streams
 
     jobs = [(per_set, (t, 1), {}) for t in (tables if len(tables) > 1 else [])] + [(per_set, (pooled, len(seeds)), {})]
-    done = streams.run_concurrently(jobs)
+    if serial:
+        from porerad_b200 import _lib
+
+        lib = _lib.load()
+        if timers:
+            import torch
+
+            torch.cuda.synchronize()
+            lib.pr_timers_reset()
+            lib.pr_timers_enable(1)
+        done = [f(*a, **kw) for f, a, kw in jobs]
+        if timers:
+            torch.cuda.synchronize()
+            lib.pr_timers_enable(0)
+            out["_timers"] = _timer_values(lib, ("balance", "series", "cheb", "refine"))
+    else:
+        done = streams.run_concurrently(jobs)
     for op, ch in done[:-1]:
         out["sets"].append(ch)
         ops.append(op)
@@ -163,21 +184,36 @@ def release(res):
     geo.close()
 
 
-def plain_step(phases_host, cfg, seeds):
-    """The reference case driver's call sequence through the drop-in NumPy API."""
+def plain_step(phases_host, cfg, seeds, stages=None):
+    """The reference case driver's call sequence through the drop-in NumPy API.
+
+    ``stages`` (a dict) receives the wall-clock seconds of each stage of the sequence.
+    """
 
     from porerad_b200 import coupled, exchange, view_factors as vf
 
+    st = stages if stages is not None else {}
+
+    def lap(name, t0):
+        st[name] = st.get(name, 0.0) + time.perf_counter() - t0
+        return time.perf_counter()
+
+    t = time.perf_counter()
     p = vf.build_surface_patches(phases_host, cfg["H"])
-    counts = {s: vf.first_hit_counts(p, cfg["rays"], s) for s in seeds}
     area = p.patch_area_m2
+    t = lap("patches", t)
+    counts = {s: vf.first_hit_counts(p, cfg["rays"], s) for s in seeds}
+    t = lap("first_hit_counts (device counts, arrays to host)", t)
     chs = []
     groups = [[s] for s in seeds] + ([seeds] if len(seeds) > 1 else [])
     for g in groups:
         o, r, c = vf.pool_counts([counts[s] for s in g], p.n_patches)
+        t = lap("pool_counts (host arrays to device and back)", t)
         op = exchange.ExchangeOperator(o, r, c, np.full(p.n_patches, cfg["rays"] * len(g), np.int64), area)
+        t = lap("ExchangeOperator (host arrays to device, balance)", t)
         chs.append(coupled.prescribed_field_channels(op, p, cfg["T_m"], cfg["dT"], cfg["eps"]))
         op.close()
+        t = lap("prescribed_field_channels (binary64)", t)
     return chs
 
 
@@ -263,52 +299,241 @@ def fp64_peak_tflops(torch) -> float:
     return best
 
 
-def ncu_traffic(kernel: str, workload: str):
-    """Per-ray DRAM traffic of a kernel from the committed ncu summary (profiles/), or None."""
+class CpuCounts:
+    """The oracle (the reference's CPU algorithm) timing first-hit counts of a bounded patch sample.
 
-    path = ROOT / "profiles" / f"{kernel}_{workload}.md"
-    if not path.is_file():
-        return None
-    for line in path.read_text().splitlines():
-        if line.startswith("dram_bytes_per_ray:"):
-            return float(line.split(":", 1)[1])
-    return None
+    The geometry and its patch table are built once.  A sample is ``blocks`` runs of consecutive
+    origin patches spread evenly over all patches, traced for every ray set with all host cores
+    (NumPy PCG64 rays, the OpenMP C traversal, np.unique per block as the reference does per chunk).
+    """
+
+    def __init__(self, cfg, seeds, blocks: int = 16):
+        from oracle import build as ob
+        from oracle import porerad_oracle as orc
+
+        ob.build()
+        self.orc = orc
+        self.cores = orc.set_threads()
+        self.cfg, self.seeds, self.blocks = cfg, seeds, blocks
+        self.patches = orc.build_surface_patches(make_phases(cfg), cfg["H"])
+        self.width = 64
+
+    def run(self, width: int):
+        P, R = self.patches.n_patches, self.cfg["rays"]
+        width = max(1, min(int(width), P // self.blocks))
+        starts = [int(b * P // self.blocks) for b in range(self.blocks)]
+        t0 = time.perf_counter()
+        for s in self.seeds:
+            for p0 in starts:
+                self.orc.first_hit_counts(self.patches, R, s, patch_start=p0, patch_end=p0 + width)
+        dt = time.perf_counter() - t0
+        return len(self.seeds) * self.blocks * width * R, dt, width
+
+    def calibrate(self, target_s: float):
+        rays, dt, w = self.run(self.width)
+        self.width = max(1, int(w * target_s / max(dt, 1e-3)))
+        return self.width
+
+    def describe(self, width: int, dt: float) -> str:
+        P = self.patches.n_patches
+        return (f"first-hit counts (NumPy PCG64 rays + OpenMP C traversal + np.unique) of {self.blocks} blocks of "
+                f"{width} consecutive origin patches spread evenly over {P} x {self.cfg['rays']} rays x "
+                f"{len(self.seeds)} sets ({self.blocks * width} patches, {dt:.1f} s); patch table built "
+                f"outside the timed sample")
 
 
 def cpu_sample(cfg, seeds, target_s: float):
-    """The oracle (the reference's CPU algorithm) on a bounded patch sample of the workload, all host cores."""
+    """One timed sample of about ``target_s`` seconds; the cpu_baseline object of a bench line."""
 
-    from oracle import build as ob
-    from oracle import porerad_oracle as orc
+    cc = CpuCounts(cfg, seeds)
+    cc.calibrate(min(2.0, target_s / 4))
+    rays, dt, width = cc.run(cc.calibrate(target_s))
+    return {"value": rays / dt, "unit": "rays/s", "cores": cc.cores, "kind": "port",
+            "sample": cc.describe(width, dt)}
 
-    ob.build()
-    cores = orc.set_threads()
-    phases = make_phases(cfg)
-    p = orc.build_surface_patches(phases, cfg["H"])
-    # calibrate on a small slice, then size the sample to about target_s seconds
-    t0 = time.perf_counter()
-    n0 = max(1, min(p.n_patches, 200_000 // cfg["rays"]))
-    o, d = orc.generate_rays(p, 0, n0, cfg["rays"], seeds[0])
-    orc.trace_first_hit(p, o, d)
-    rate = n0 * cfg["rays"] / (time.perf_counter() - t0)
-    n_patch = int(min(p.n_patches, max(1, target_s * rate / (cfg["rays"] * len(seeds)))))
-    t0 = time.perf_counter()
-    rays = 0
+
+def counts_step(phases, cfg, seeds, host_out=False):
+    """The count stage of one case: patch table, then per ray set fused generation + traversal + count rows.
+
+    ``phases`` is a device tensor (``host_out`` False: count tables stay in HBM) or pinned host
+    memory (``host_out`` True: the reference-facing calls ``build_surface_patches`` and
+    ``first_hit_counts``, whose (origin, receiver, count) arrays are copied to host NumPy).
+    """
+
+    from porerad_b200 import view_factors as vf
+
+    p = vf.build_surface_patches(phases, cfg["H"])
+    P = p.n_patches
+    out = {"rays": 0, "steps": 0, "pairs": [], "d2h": 0, "n_patches": P}
     for s in seeds:
-        orc.first_hit_counts(p, cfg["rays"], s, patch_end=n_patch)
-        rays += n_patch * cfg["rays"]
-    dt = time.perf_counter() - t0
-    return {"value": rays / dt, "unit": "rays/s", "cores": cores, "kind": "port",
-            "sample": f"first-hit counts (NumPy PCG64 rays + OpenMP C traversal + np.unique) of patches "
-                      f"0..{n_patch - 1} of {p.n_patches} x {cfg['rays']} rays x {len(seeds)} sets, {dt:.1f} s"}
+        if host_out:
+            o, r, c = vf.first_hit_counts(p, cfg["rays"], s)
+            out["pairs"].append(int(o.size))
+            out["d2h"] += o.nbytes + r.nbytes + c.nbytes
+            out["rays"] += P * cfg["rays"]
+            del o, r, c
+        else:
+            t = vf.first_hit_counts_pooled(p, cfg["rays"], [s])
+            out["rays"] += t.rays_traced
+            out["steps"] += t.dda_steps
+            out["pairs"].append(t.nnz)
+            t.close()
+    p.device().close()
+    # host->device per step: the phases (host form) and 130 PCG64 jump maps of 32 B per seed
+    out["h2d"] = 32 * 130 * len(seeds)
+    return out
+
+
+def _timer_values(lib, names):
+    """(launches, ms) of the library's CUDA-event timers, by name."""
+
+    from porerad_b200 import _lib
+
+    ids = {"trace": _lib.TIMER_TRACE, "rle": _lib.TIMER_RLE, "balance": _lib.TIMER_BALANCE,
+           "series": _lib.TIMER_SERIES, "cheb": _lib.TIMER_CHEB, "refine": _lib.TIMER_REFINE}
+    out = {}
+    for name in names:
+        n, t = _lib.ctypes.c_longlong(), _lib.ctypes.c_double()
+        lib.pr_timers_read(ids[name], _lib.ctypes.byref(n), _lib.ctypes.byref(t))
+        out[name] = (int(n.value), float(t.value))
+    return out
+
+
+def trace_profile(workload: str):
+    """Per-launch figures of the traversal kernel from the committed ncu summary (profiles/), or None."""
+
+    path = ROOT / "profiles" / f"trace_{workload}.md"
+    if not path.is_file():
+        return None
+    vals = {}
+    for line in path.read_text().splitlines():
+        for key in ("dram_bytes_per_ray", "warp_inst_per_step"):
+            if line.startswith(key + ":"):
+                vals[key] = float(line.split(":", 1)[1].split()[0])
+    return vals if "dram_bytes_per_ray" in vals else None
+
+
+def bench_config(cfg, seeds):
+    """The workload keys both arms print (the reference arm's line carries the same dict)."""
+
+    return {"workload": cfg["workload"], "archetype": cfg["arch"], "N": cfg["n"], "phi": cfg["phi"],
+            "geometry_seed": cfg["seed"], "rays_per_patch": cfg["rays"], "ray_sets": len(seeds),
+            "step": "first-hit counts of every ray set (ray generation, first-hit traversal, per-origin "
+                    "(receiver, count) rows); GPU steps also build the patch table",
+            "parallelism": "replicas", "l2": "256 MiB flush write before every timed GPU step; count tables > L2"}
+
+
+def whole_case(args, cfg, seeds, phases_dev, phases_host, pinned, lib, flush, rank):
+    """cases/s of the whole case (patches, counts, 3 balanced operators, 3 mixed-precision solves)."""
+
+    import torch
+
+    from porerad_b200 import replicas
+
+    k = max(1, min(args.steps, 10))
+    lib.pr_timers_reset()
+    lib.pr_timers_enable(1)
+    replicas.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    last = None
+    for _ in range(k):
+        flush.fill_(1)
+        last = served_step(phases_dev, cfg, seeds)
+        release(last)
+    e1.record()
+    torch.cuda.synchronize()
+    lib.pr_timers_enable(0)
+    ms = e0.elapsed_time(e1)
+    timers = _timer_values(lib, ("balance", "series", "cheb", "refine"))
+    t0 = time.perf_counter()
+    for _ in range(k):
+        res = served_step(pinned.numpy(), cfg, seeds)
+        release(res)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    ms, e2e_s = replicas.max_over_ranks([ms, e2e_s])
+    if rank != 0:
+        return None
+    # one operator at a time: the products of each operator alone, for a per-launch rate that no
+    # other stream's work inflates
+    solo = served_step(phases_dev, cfg, seeds, serial=True, timers=True)
+    solo_timers = solo.pop("_timers")
+    release(solo)
+    res64 = served_step(phases_dev, cfg, seeds, precision="fp64")
+    resm = served_step(phases_dev, cfg, seeds, precision="mixed")
+    f64, fm = res64["final"], resm["final"]
+    flux_err = max(abs(fm.q_h - f64.q_h) / abs(f64.q_h), abs(fm.q_c - f64.q_c) / abs(f64.q_c))
+    ab = None
+    if len(seeds) > 1:
+        from porerad_b200 import coupled
+
+        ab = coupled.ab_differences([resm["sets"][0]], [resm["sets"][1]])
+    release(res64)
+    release(resm)
+    plain = None
+    if not args.no_plain:
+        plain_step(phases_host, cfg, seeds)
+        torch.cuda.synchronize()
+        stages = {}
+        t0 = time.perf_counter()
+        plain_step(phases_host, cfg, seeds, stages=stages)
+        torch.cuda.synchronize()
+        plain_s = time.perf_counter() - t0
+        plain = {"cases_per_s": 1.0 / plain_s, "s_per_case": plain_s, "stages_s": stages,
+                 "path": "drop-in NumPy API: build_surface_patches, first_hit_counts per set, pool_counts, "
+                         "ExchangeOperator from host arrays, binary64 prescribed_field_channels"}
+    peaks, kind = measured_peaks()
+    P = last["n_patches"]
+
+    def spmv_rates(tm, prods):
+        nnz_avg = sum(z * c for z, c in prods) / max(sum(c for _, c in prods), 1)
+        out = {}
+        for name in ("balance", "series", "cheb", "refine"):
+            n_k, t_k = tm[name]
+            if n_k == 0:
+                continue
+            # packed 4-byte words per entry, row offsets, and the P-vectors each kernel streams
+            bytes_per = nnz_avg * 4 + P * (8 + 5 * (8 if name != "cheb" else 4))
+            out[name] = {"launches": n_k, "ms": t_k, "GB_per_s": bytes_per * n_k / (t_k * 1e-3) / 1e9,
+                         "frac": bytes_per * n_k / (t_k * 1e-3) / 1e9 / peaks["hbm_gbs"]}
+        tot_b = sum(v["GB_per_s"] * v["ms"] for v in out.values())
+        tot_t = sum(v["ms"] for v in out.values())
+        return out, (tot_b / tot_t if tot_t else None), tot_t, nnz_avg
+
+    kern, ach, tot_t, nnz_avg = spmv_rates(timers, last["products"])
+    kern_solo, ach_solo, _, _ = spmv_rates(solo_timers, solo["products"])
+    roof_spmv = {"bound": "hbm", "achieved": ach_solo, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                 "frac": ach_solo / peaks["hbm_gbs"] if ach_solo else None,
+                 "peak_source": f"MEASURED_PEAKS.json ({kind})", "kernels": kern_solo,
+                 "timing": "one operator at a time (the three operators of one case built and solved in turn)",
+                 "overlapped": {"achieved": ach, "kernels": kern, "share_of_step": tot_t / (ms / k),
+                                "note": "the three operators on three streams at once, as in the timed case: "
+                                        "a launch's event time includes the other streams' work (lower bound)"},
+                 "bytes": "4 B per packed S' entry + P x (8 + 5 x 8) B (f32 sweep: 5 x 4 B)",
+                 "nnz_symmetric_per_product": round(nnz_avg)}
+    return {
+        "cases_per_s": args.gpus * k / (ms * 1e-3), "ms_per_case": ms / k, "steps": k,
+        "e2e_cases_per_s": args.gpus * k / e2e_s,
+        "work": "patches, counts A+B, pooled A+B, 3 balanced operators, 3 mixed-precision channel solves",
+        "plain": plain, "served_over_plain": (args.gpus * k / e2e_s) / plain["cases_per_s"] if plain else None,
+        "mixed_vs_fp64_rel_flux_error": flux_err,
+        "mixed_vs_fp64_reference": "the device binary64 series on the same operator (pinned to the oracle's "
+                                   "binary64 series at 1e-9 by the parity tests)",
+        "ab_differences": {"wall_channel": ab[0], "coarse_source": ab[1]} if ab else None,
+        "q": {"q_h": f64.q_h, "q_c": f64.q_c, "q_i": f64.q_i},
+        "balance": {"method": last["balance"][0], "iterations": last["balance"][1],
+                    "row_sum_error": last["balance"][2]},
+        "nnz_symmetric": last["nnz_symmetric"], "pairs_pooled": last["nnz"],
+        "roofline_spmv": roof_spmv,
+    }
 
 
 def run_ours(args, cfg):
     import torch
 
-    from porerad_b200 import _lib
-
-    from porerad_b200 import replicas
+    from porerad_b200 import _lib, replicas
 
     world, rank, local = replicas.world_size(), replicas.rank(), replicas.local_rank()
     if world != args.gpus:
@@ -323,54 +548,43 @@ def run_ours(args, cfg):
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
 
     for _ in range(args.warmup):
-        release(served_step(phases_dev, cfg, seeds))
+        counts_step(phases_dev, cfg, seeds)
+    counts_step(pinned.numpy(), cfg, seeds, host_out=True)
     torch.cuda.synchronize()
 
-    barrier = replicas.barrier
-
-    # ---- timed region: device-resident inputs
+    # ---- timed region: device-resident inputs, count tables left in HBM
     lib.pr_timers_reset()
     lib.pr_timers_enable(1)
     launches0 = lib.pr_kernel_launches()
     rays = steps = 0
-    results = []
-    barrier()
+    last = None
+    replicas.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(args.steps):
             flush.fill_(1)  # 256 MiB write: L2 (126 MB) holds nothing of the previous step
-            res = served_step(phases_dev, cfg, seeds)
-            rays += res["rays"]
-            steps += res["steps"]
-            release(res)  # stream-ordered frees: the next step reuses the pool
-            results.append(res)
+            last = counts_step(phases_dev, cfg, seeds)
+            rays += last["rays"]
+            steps += last["steps"]
         e1.record()
         torch.cuda.synchronize()
-    barrier()
+    replicas.barrier()
     launches = lib.pr_kernel_launches() - launches0
     lib.pr_timers_enable(0)
     ms = e0.elapsed_time(e1)
-    timers = {}
-    for name, tid in (("trace", _lib.TIMER_TRACE), ("rle", _lib.TIMER_RLE), ("balance", _lib.TIMER_BALANCE),
-                      ("series", _lib.TIMER_SERIES), ("cheb", _lib.TIMER_CHEB), ("refine", _lib.TIMER_REFINE)):
-        n, t = _lib.ctypes.c_longlong(), _lib.ctypes.c_double()
-        lib.pr_timers_read(tid, _lib.ctypes.byref(n), _lib.ctypes.byref(t))
-        timers[name] = (int(n.value), float(t.value))
-    last = results[-1]
-    nnz_s = last["nnz_symmetric"]
-    P = last["n_patches"]
+    timers = _timer_values(lib, ("trace", "rle"))
 
-    # ---- end to end through the public API from pinned host memory
-    barrier()
+    # ---- end to end through the reference-facing API from pinned host memory, host arrays out
+    replicas.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e2e_rays = 0
     for _ in range(args.steps):
-        res = served_step(pinned.numpy(), cfg, seeds)
+        flush.fill_(1)
+        res = counts_step(pinned.numpy(), cfg, seeds, host_out=True)
         e2e_rays += res["rays"]
-        release(res)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     h2d = int(phases_host.nbytes) + int(res["h2d"])
@@ -378,92 +592,55 @@ def run_ours(args, cfg):
 
     t_max, e2e_s = replicas.max_over_ranks([ms, e2e_s])
     value = rays * world / (t_max * 1e-3)
+    case = whole_case(args, cfg, seeds, phases_dev, phases_host, pinned, lib, flush, rank)
     line = None
     if rank == 0:
-        # accuracy of the mixed solve against the binary64 series on the same operator
-        res64 = served_step(phases_dev, cfg, seeds, precision="fp64")
-        resm = served_step(phases_dev, cfg, seeds, precision="mixed")
-        f64, fm = res64["final"], resm["final"]
-        flux_err = max(abs(fm.q_h - f64.q_h) / abs(f64.q_h), abs(fm.q_c - f64.q_c) / abs(f64.q_c))
-        ab = None
-        if len(seeds) > 1:
-            from porerad_b200 import coupled
-
-            ab = coupled.ab_differences([resm["sets"][0]], [resm["sets"][1]])
-        release(res64)
-        release(resm)
-        plain = None
-        if not args.no_plain:
-            plain_step(phases_host, cfg, seeds)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            plain_step(phases_host, cfg, seeds)
-            torch.cuda.synchronize()
-            plain_s = time.perf_counter() - t0
-            plain = {"cases_per_s": 1.0 / plain_s, "s_per_case": plain_s,
-                     "path": "drop-in NumPy API: build_surface_patches, first_hit_counts per set, pool_counts, "
-                             "ExchangeOperator from host arrays, binary64 prescribed_field_channels"}
-        peaks, kind = measured_peaks()
         fp64 = fp64_peak_tflops(torch)
         n_tr, t_tr = timers["trace"]
         flops = 4.0 * steps + 30.0 * rays
         achieved = flops / (t_tr * 1e-3) / 1e12 if t_tr > 0 else None
-        per_ray_traffic = ncu_traffic("trace", args.workload)
+        prof = trace_profile(args.workload)
         roof = {"kernel": "k_trace_pool (fused PCG64 ray generation + FP64 DDA, pooled lanes)", "bound": "fp64",
                 "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
                 "frac": achieved / fp64 if achieved else None,
-                "traffic": per_ray_traffic * rays / max(n_tr, 1) if per_ray_traffic else None,
+                "traffic": prof["dram_bytes_per_ray"] * rays / max(n_tr, 1) if prof else None,
                 "launches": n_tr, "ms": t_tr,
                 "work": "4 FP64 ops per DDA step + 30 per ray (generation/setup); steps counted by the kernel",
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
                 "share_of_step": t_tr / ms}
-        spmv = {}
-        # entries of the operator of an average product: every operator of the step (sets A, B and
-        # the pooled one) is balanced and solved, each with its own number of entries
-        prods = last["products"]
-        nnz_avg = sum(z * c for z, c in prods) / max(sum(c for _, c in prods), 1)
-        for name in ("balance", "series", "cheb", "refine"):
-            n_k, t_k = timers[name]
-            if n_k == 0:
-                continue
-            # packed 4-byte words per entry, row offsets, and the P-vectors each kernel streams
-            bytes_per = nnz_avg * 4 + P * (8 + 5 * (8 if name != "cheb" else 4))
-            spmv[name] = {"launches": n_k, "ms": t_k, "GB_per_s": bytes_per * n_k / (t_k * 1e-3) / 1e9}
-        tot_b = sum(v["GB_per_s"] * v["ms"] for v in spmv.values())
-        tot_t = sum(v["ms"] for v in spmv.values())
-        roof_spmv = {"bound": "hbm", "achieved": tot_b / tot_t if tot_t else None, "peak": peaks["hbm_gbs"],
-                     "unit": "GB/s", "frac": (tot_b / tot_t) / peaks["hbm_gbs"] if tot_t else None,
-                     "peak_source": f"MEASURED_PEAKS.json ({kind})", "kernels": spmv,
-                     "share_of_step": tot_t / ms,
-                     "note": "the three operators' products run at once on three streams: a launch's "
-                             "event time includes the other streams' work, so this per-launch rate is a "
-                             "lower bound (one operator at a time it read 0.34 of the same peak)"}
+        if prof and "warp_inst_per_step" in prof and t_tr > 0:
+            # the bound that binds: warp instructions issued per second against one per cycle on each of
+            # the 4 schedulers of the 148 SMs (instructions per DDA step include the rays' generation)
+            inst = prof["warp_inst_per_step"] * steps
+            clk = (clocks.summary().get("sm_mhz") or 1965.0) * 1e6
+            peak_issue = 4 * 148 * clk
+            roof["issue"] = {"achieved_warp_inst_per_s": inst / (t_tr * 1e-3), "peak": peak_issue,
+                             "frac": inst / (t_tr * 1e-3) / peak_issue,
+                             "warp_inst_per_step": prof["warp_inst_per_step"],
+                             "source": f"profiles/trace_{args.workload}.md (ncu smsp__inst_executed.sum / "
+                                       "DDA steps of the captured launch)"}
         cpu = None if args.no_cpu else cpu_sample(cfg, seeds, args.cpu_seconds)
+        pairs = last["pairs"]
         line = {
-            "metric": "first-hit rays/s (whole case: patches, counts A+B, 3 balanced operators, 3 mixed-precision "
-                      "radiosity solves)",
+            "metric": "first-hit rays/s",
             "value": value, "unit": "rays/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64 (traversal), f32+f64 (radiosity)", "data": "synthetic",
-            "config": {"workload": cfg["workload"], "archetype": cfg["arch"], "N": cfg["n"], "phi": cfg["phi"],
-                       "rays_per_patch": cfg["rays"], "ray_sets": len(seeds), "n_patches": P,
-                       "pairs_pooled": last["nnz"], "nnz_symmetric": nnz_s,
-                       "nnz_symmetric_per_product": round(nnz_avg), "parallelism": f"replicas x{world}",
-                       "l2": "256 MiB flush write before every timed step; CSR working set > L2"},
-            "cases_per_s": world * args.steps / (t_max * 1e-3),
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": bench_config(cfg, seeds),
+            "case": {"n_patches": last["n_patches"], "pairs_per_set": pairs, "rays_per_step": rays / args.steps,
+                     "dda_steps_per_ray": steps / rays},
+            "timing": "value: CUDA events on the launching stream around the K steps (each step: 256 MiB L2 "
+                      "flush, patch table, counts of every set); e2e: wall clock around the same K steps through "
+                      "build_surface_patches + first_hit_counts from pinned host phases, NumPy arrays out",
             "e2e": {"value": e2e_rays * world / e2e_s, "unit": "rays/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "cases_per_s": world * args.steps / e2e_s},
-            "plain": plain,
-            "served_over_plain": (world * args.steps / e2e_s) / plain["cases_per_s"] if plain else None,
-            "mixed_vs_fp64_rel_flux_error": flux_err,
-            "ab_differences": {"wall_channel": ab[0], "coarse_source": ab[1]} if ab else None,
-            "q": {"q_h": f64.q_h, "q_c": f64.q_c, "q_i": f64.q_i},
-            "balance": {"method": last["balance"][0], "iterations": last["balance"][1],
-                        "row_sum_error": last["balance"][2]},
-            "rays_per_step": rays / args.steps, "dda_steps_per_ray": steps / rays,
-            "roofline": roof, "roofline_spmv": roof_spmv, "trace_variant": _lib.trace_variant()[1],
+                    "d2h_bytes_per_step": d2h,
+                    "d2h": "origin i32 + receiver i32 + count i64 per pair of every set (the reference's arrays)"},
+            "roofline": roof, "trace_variant": _lib.trace_variant()[1],
             "clocks": clocks.summary(), "gpu_launches": int(launches), "cpu_baseline": cpu,
+            "whole_case": case,
         }
+        if case is not None:
+            line["cases_per_s"] = case["cases_per_s"]
     replicas.finalize()
     return line
 
@@ -1367,22 +1544,25 @@ def run_reference(args, cfg):
     if "arch" not in cfg:
         raise SystemExit("--impl reference times the CPU path of the c1, c2 and coupled workloads")
     seeds = ray_seeds(cfg)
-    # warm-up runs of the sample, then K timed samples
+    cc = CpuCounts(cfg, seeds)
+    # each step is one bounded sample of the workload (about cpu_seconds / 3 of CPU work); warm-up
+    # steps run the calibration and the first samples untimed
+    width = cc.calibrate(0.5)
     for _ in range(max(0, args.warmup)):
-        cpu_sample(cfg, seeds, 1.0)
-    vals = []
-    last = None
+        width = cc.calibrate(max(0.5, args.cpu_seconds / 3))
+    rays = dt = 0.0
     for _ in range(args.steps):
-        last = cpu_sample(cfg, seeds, max(1.0, args.cpu_seconds / 2))
-        vals.append(last["value"])
-    value = float(np.mean(vals))
+        r, t, width = cc.run(width)
+        rays += r
+        dt += t
+    value = rays / dt
     return {
         "impl": "reference", "metric": "first-hit rays/s", "value": value, "unit": "rays/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": cfg["workload"], "archetype": cfg["arch"], "N": cfg["n"],
-                   "rays_per_patch": cfg["rays"], "ray_sets": len(seeds)},
-        "cpu_baseline": {**last, "value": value},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / max(args.steps, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": bench_config(cfg, seeds),
+        "cpu_baseline": {"value": value, "unit": "rays/s", "cores": cc.cores, "kind": "port",
+                         "sample": cc.describe(width, dt / max(args.steps, 1)) + " per step"},
         "e2e": {"value": value, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 

@@ -134,6 +134,12 @@ PR_API int pr_counts_info(const pr_counts* k, int64_t* nnz, int64_t* n_patches, 
 /* The sorted edge list (origin i32, receiver i32, count i64) and rays_per_origin (i64). */
 PR_API int pr_counts_copy(const pr_counts* k, int32_t* origin, int32_t* receiver, int64_t* count,
                    int64_t* rays_per_origin, void* stream);
+/* The pairs of origin rows [row_begin, row_end) only, in the same sorted order: the part of
+ * first_hit_counts' output (view_factors.py:273-287) whose origins lie in that patch range.
+ * *n_pairs receives their number; with origin, receiver and count all NULL nothing else is
+ * copied (size query).  PR_ERR_ARG for a range outside [0, n_patches]. */
+PR_API int pr_counts_rows(const pr_counts* k, int64_t row_begin, int64_t row_end, int64_t* n_pairs,
+                          int32_t* origin, int32_t* receiver, int64_t* count, void* stream);
 /* Replaces pool_counts(tables, n_patches), view_factors.py:290-300, and the re-pooling at
  * the top of ExchangeOperator.__init__ (exchange.py:59-67): sums the counts of equal
  * (origin, receiver) pairs of an arbitrary edge list into sorted CSR rows. */

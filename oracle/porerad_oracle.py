@@ -218,18 +218,20 @@ def trace_first_hit(patches, origins, directions, *, return_steps: bool = False)
 
 
 def first_hit_counts(patches, rays_per_patch: int, seed: int, *, patch_chunk: int = 16384, stats=None,
-                     patch_end: int | None = None):
+                     patch_start: int = 0, patch_end: int | None = None):
     """view_factors.py:273-287: per chunk of patches, unique (origin, receiver) pairs and counts.
 
-    ``patch_end`` (not in the reference) stops after the origins below it, for
-    timing a bounded sample; the pair keys still span all patches.
+    ``patch_start`` and ``patch_end`` (not in the reference) restrict the origins to
+    ``[patch_start, patch_end)``, for parity on a slice and for timing a bounded sample;
+    the rays of those origins are the ones a full pass draws (the stream is advanced by
+    ``start * R * 4``) and the pair keys still span all patches.
     """
 
     n = patches.n_patches
     R = int(rays_per_patch)
     last = n if patch_end is None else min(int(patch_end), n)
     parts = []
-    for start in range(0, last, int(patch_chunk)):
+    for start in range(max(0, int(patch_start)), last, int(patch_chunk)):
         end = min(start + int(patch_chunk), last)
         o, d = generate_rays(patches, start, end, R, seed)
         if stats is not None:

@@ -107,6 +107,7 @@ _SIGNATURES = {
     "pr_counts_info": (_i32, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64),
                               ctypes.POINTER(_i64)]),
     "pr_counts_copy": (_i32, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "pr_counts_rows": (_i32, [_vp, _i64, _i64, ctypes.POINTER(_i64), _vp, _vp, _vp, _vp]),
     "pr_counts_from_edges": (_i32, [_vp, _vp, _vp, _i64, _i64, _vp, ctypes.POINTER(_vp)]),
     "pr_counts_merge": (_i32, [_vp, _vp, _vp, ctypes.POINTER(_vp)]),
     "pr_counts_destroy": (None, [_vp]),

@@ -19,10 +19,16 @@ from . import _lib
 
 
 class ConductionSystem:
-    """Conduction matrix A and the wall responses of an x-oriented cell grid (conduction.py:24-50)."""
+    """Conduction matrix A and the wall responses of an x-oriented cell grid (conduction.py:24-50).
 
-    def __init__(self, conductivity_x: np.ndarray, H_m: float):
-        k = np.ascontiguousarray(conductivity_x, dtype=np.float64)
+    Constructed as the reference's dataclass is, ``ConductionSystem(matrix, hot_rhs, cold_rhs,
+    conductivity, H_m)``; :func:`assemble_conduction` passes ``None`` for the first three.  The
+    device system is always assembled from ``conductivity`` and ``H_m``; arrays that are given
+    must equal that assembly (``ValueError`` otherwise) and are then what the accessors return.
+    """
+
+    def __init__(self, matrix, hot_rhs, cold_rhs, conductivity: np.ndarray, H_m: float):
+        k = np.ascontiguousarray(conductivity, dtype=np.float64)
         if k.ndim != 3:
             raise ValueError("conductivity must be a 3-D array")
         nx, ny, nz = map(int, k.shape)
@@ -34,6 +40,23 @@ class ConductionSystem:
         self.H_m = float(H_m)
         self._arrays = None
         self._matrix = None
+        if hot_rhs is not None or cold_rhs is not None or matrix is not None:
+            self._adopt(matrix, hot_rhs, cold_rhs)
+
+    def _adopt(self, matrix, hot_rhs, cold_rhs) -> None:
+        """Keep caller-given arrays after checking them against the device assembly."""
+
+        for name, given in (("hot_rhs", hot_rhs), ("cold_rhs", cold_rhs)):
+            if given is not None and not np.array_equal(np.asarray(given, np.float64).ravel(),
+                                                        self._host_arrays()[name]):
+                raise ValueError(f"{name} does not match the conductivity field's assembly")
+        if matrix is not None:
+            from scipy.sparse import csr_matrix
+
+            given = csr_matrix(matrix)
+            if given.shape != self.matrix.shape or (given != self.matrix).nnz:
+                raise ValueError("matrix does not match the conductivity field's assembly")
+            self._matrix = given
 
     @property
     def handle(self) -> int:
@@ -117,7 +140,7 @@ class ConductionSystem:
 def assemble_conduction(conductivity_x: np.ndarray, H_m: float) -> ConductionSystem:
     """Assemble A and the wall responses for a conductivity field oriented along x (conduction.py:53-92)."""
 
-    return ConductionSystem(conductivity_x, H_m)
+    return ConductionSystem(None, None, None, conductivity_x, H_m)
 
 
 def solve_conduction(system: ConductionSystem, T_hot_K: float, T_cold_K: float, *,

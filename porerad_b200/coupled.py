@@ -17,8 +17,10 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
+from .conduction import ConductionSystem  # noqa: F401  (part of the module's namespace, coupled.py:23)
 from .constants import SIGMA
 from .exchange import ExchangeOperator, RadiosityResult, net_patch_power, net_patch_power_jvp
+from .krylov import FixedJacobiPCG, GMRESResult, flexible_gmres  # noqa: F401  (host helpers, coupled.py:225-320)
 from .view_factors import COLD, HOT, INTERNAL, SurfacePatches, _device_of
 
 _TINY = np.finfo(np.float64).tiny

@@ -218,14 +218,17 @@ int pr_counts_info(const pr_counts* k, int64_t* nnz, int64_t* n_patches, int64_t
   return PR_OK;
 }
 
-__global__ void k_expand_rows(const int64_t* __restrict__ rp, const int32_t* __restrict__ cnt, int64_t n,
-                              int32_t* __restrict__ origin, int64_t* __restrict__ count) {
+// Rows [r0, r1) of a count table as the reference's edge arrays: origin id and 64-bit count per
+// pair, written from position 0 (pair rp[r0] goes to index 0).  One warp per row.
+__global__ void k_expand_rows(const int64_t* __restrict__ rp, const int32_t* __restrict__ cnt, int64_t r0,
+                              int64_t r1, int32_t* __restrict__ origin, int64_t* __restrict__ count) {
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps)
+  const int64_t base = rp[r0];
+  for (int64_t i = r0 + blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < r1; i += warps)
     for (int64_t q = rp[i] + lane; q < rp[i + 1]; q += 32) {
-      if (origin) origin[q] = (int32_t)i;
-      if (count) count[q] = cnt[q];
+      if (origin) origin[q - base] = (int32_t)i;
+      if (count) count[q - base] = cnt[q];
     }
 }
 
@@ -241,14 +244,50 @@ int pr_counts_copy(const pr_counts* k, int32_t* origin, int32_t* receiver, int64
   if (m > 0 && (origin || count)) {
     if (origin) PR_TRY(o.alloc(m, s));
     if (count) PR_TRY(cn.alloc(m, s));
-    ::pr::launch_mark(), k_expand_rows<<<grid_for(n * 32, 256), 256, 0, s>>>(c.row_ptr.ptr, c.cnt.ptr, n, origin ? o.ptr : nullptr,
-                                                        count ? cn.ptr : nullptr);
+    ::pr::launch_mark(), k_expand_rows<<<grid_for(n * 32, 256), 256, 0, s>>>(c.row_ptr.ptr, c.cnt.ptr, 0, n,
+                                                                             origin ? o.ptr : nullptr,
+                                                                             count ? cn.ptr : nullptr);
     PR_CUDA(cudaGetLastError());
     if (origin) PR_CUDA(cudaMemcpyAsync(origin, o.ptr, m * 4, cudaMemcpyDefault, s));
     if (count) PR_CUDA(cudaMemcpyAsync(count, cn.ptr, m * 8, cudaMemcpyDefault, s));
   }
   if (receiver && m > 0) PR_CUDA(cudaMemcpyAsync(receiver, c.col.ptr, m * 4, cudaMemcpyDefault, s));
   if (rays_per_origin && n > 0) PR_CUDA(cudaMemcpyAsync(rays_per_origin, k->rays.ptr, n * 8, cudaMemcpyDefault, s));
+  PR_CUDA(cudaStreamSynchronize(s));
+  return PR_OK;
+}
+
+int pr_counts_rows(const pr_counts* k, int64_t row_begin, int64_t row_end, int64_t* n_pairs, int32_t* origin,
+                   int32_t* receiver, int64_t* count, void* stream) {
+  PR_CHECK_NULL(k, "counts");
+  PR_CHECK_NULL(n_pairs, "n_pairs");
+  PR_ENTRY_GUARD(k);
+  cudaStream_t s = (cudaStream_t)stream;
+  const CountCsr& c = *k->csr;
+  PR_ARG(0 <= row_begin && row_begin <= row_end && row_end <= c.n_rows, "row range outside the count table");
+  int64_t bounds[2] = {0, 0};
+  if (row_end > row_begin) {
+    PR_CUDA(cudaMemcpyAsync(&bounds[0], c.row_ptr.ptr + row_begin, 8, cudaMemcpyDeviceToHost, s));
+    PR_CUDA(cudaMemcpyAsync(&bounds[1], c.row_ptr.ptr + row_end, 8, cudaMemcpyDeviceToHost, s));
+    PR_CUDA(cudaStreamSynchronize(s));
+  }
+  const int64_t m = bounds[1] - bounds[0];
+  *n_pairs = m;
+  if (m == 0 || (!origin && !receiver && !count)) return PR_OK;
+  DevBuf<int32_t> o;
+  DevBuf<int64_t> cn;
+  if (origin) PR_TRY(o.alloc(m, s));
+  if (count) PR_TRY(cn.alloc(m, s));
+  if (origin || count) {
+    const int64_t rows = row_end - row_begin;
+    ::pr::launch_mark(), k_expand_rows<<<grid_for(rows * 32, 256), 256, 0, s>>>(c.row_ptr.ptr, c.cnt.ptr, row_begin,
+                                                                                row_end, origin ? o.ptr : nullptr,
+                                                                                count ? cn.ptr : nullptr);
+    PR_CUDA(cudaGetLastError());
+  }
+  if (origin) PR_CUDA(cudaMemcpyAsync(origin, o.ptr, m * 4, cudaMemcpyDefault, s));
+  if (count) PR_CUDA(cudaMemcpyAsync(count, cn.ptr, m * 8, cudaMemcpyDefault, s));
+  if (receiver) PR_CUDA(cudaMemcpyAsync(receiver, c.col.ptr + bounds[0], m * 4, cudaMemcpyDefault, s));
   PR_CUDA(cudaStreamSynchronize(s));
   return PR_OK;
 }

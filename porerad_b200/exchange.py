@@ -23,6 +23,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
+from .constants import SIGMA  # noqa: F401  (part of the module's namespace, exchange.py:28)
 from .view_factors import CountTable, pool_to_device
 
 SUPPORT_DIAGONAL_FRACTION = 1.0e-15

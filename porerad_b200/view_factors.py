@@ -261,6 +261,20 @@ class CountTable:
                                               _lib.ptr(rays), _lib.stream()))
         return (o, r, c, rays) if with_rays else (o, r, c)
 
+    def rows(self, patch_begin: int, patch_end: int):
+        """(origin int32, receiver int32, count int64) of the origins in [patch_begin, patch_end) only."""
+
+        lib = _lib.load()
+        m = ctypes.c_int64()
+        b, e = int(patch_begin), int(patch_end)
+        _lib.check(lib.pr_counts_rows(self.handle, b, e, ctypes.byref(m), None, None, None, _lib.stream()))
+        o = np.empty(m.value, np.int32)
+        r = np.empty(m.value, np.int32)
+        c = np.empty(m.value, np.int64)
+        _lib.check(lib.pr_counts_rows(self.handle, b, e, ctypes.byref(m), o.ctypes.data, r.ctypes.data, c.ctypes.data,
+                                      _lib.stream()))
+        return o, r, c
+
     def sha256(self) -> str:
         o, r, c, rays = self.to_numpy(with_rays=True)
         return count_sha256(o, r, c, rays)

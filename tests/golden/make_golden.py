@@ -1,6 +1,8 @@
 """Regenerate the golden fixtures of tests/golden from the reference implementation.
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <checkout of porerad> [--only part,part,...]
+
+(or set PORERAD_REFERENCE to the checkout instead of passing --reference.)
 
 Runs the unmodified reference package ``porerad`` (moxi000/pore-radiation-ijhmt2026)
 on small seeded inputs and stores its outputs, so that the GPU parity tests can run
@@ -12,16 +14,26 @@ where the reference is not installed:
   solve with and without a reference temperature, one JVP, and the prescribed-field
   channels (q_h, q_c, q_i, closure, coarse source) at two conditions.
 * ``canonical_<name>.npz``: the four canonical 128^3 microstructures of the
-  reference's data/microstructures (CC-BY 4.0, see README.md here), bit-packed.
-* ``count_hashes.json``: the stored first-hit count hashes of data/cases_coupled.csv
-  for those microstructures (columns raw_count_sha256_A/B) with their seeds.
+  reference's data/microstructures (CC-BY 4.0, credited in tests/golden/README.md), bit-packed.
+* ``count_hashes.json``: every stored first-hit count hash of data/cases_coupled.csv
+  (columns raw_count_sha256_A/B) with its seeds: the canonical 128^3 microstructures
+  stored here (``"array": "stored"``) and the N = 160 and 192 resolution microstructures,
+  which are not stored and are rebuilt by the generators from their archived phase hash
+  (``"array": "generated"``).
 * ``prescribed_field.json``: archived prescribed-field rows of
   results/prescribed_field.csv for the committed core microstructure, with its seeds.
 * ``coupled_<name>.npz``: the strictly coupled solve of each small case (conduction
   system of K_SOLID/K_GAS, pure-conduction field, solve_coupled at two conditions: final
   field, wall-flux metrics, Newton and GMRES iteration record).
-* ``coupled.json``: the archived rows of results/coupled.csv for the canonical
-  microstructures (groups canonical and thickness) with their case parameters.
+* ``coupled.json``: every archived row of results/coupled.csv with its case parameters
+  (groups canonical, thickness, resolution and matched; ``"array"`` says whether the
+  microstructure is stored here or rebuilt by the generators).
+* ``public_api.json``: the public names of porerad.view_factors, .exchange, .coupled and
+  .conduction (kind, call signature, class members, constant values).
+* ``fullpath.json``: the two ``first_hit_radiosity`` rows of results/fullpath_crosscheck.csv
+  (OF and TL canonical, x, 700 K, 20 K, eps 0.6) with the ray seeds of the coupled cases'
+  sets A + B and the reference's own channels recomputed from them, with the file's full-path
+  Monte Carlo rows of the same microstructures (channels and standard errors).
 * ``prescribed_cases.json``: all 48 cases of data/cases_prescribed_field.csv (seeds, append
   seeds and decision, conditions, phase hash) with their archived rows of
   results/prescribed_field.csv (q_h, q_c, q_i and the A/B wall-channel difference); their
@@ -63,6 +75,7 @@ SMALL_CASES = {
 CONDITIONS = [(700.0, 20.0, 0.6), (400.0, 100.0, 0.3)]
 CANONICAL = ["FA_canonical_phi0.10_N128", "FI_canonical_phi0.10_N128", "OF_canonical_phi0.10_N128",
              "TL_canonical_phi0.10_N128"]
+MATCHED = [f"{s}_matched_pair{k}" for s in ("FA", "FI") for k in (1, 2, 3)]
 CORE_CASE = "pf_OF_core_phi0.05_s3_x"
 
 
@@ -170,15 +183,14 @@ def coupled_rows(ref):
     rows = []
     for r in csv.DictReader(open(ref / "results" / "coupled.csv")):
         c = cases[r["case_id"]]
-        if c["microstructure"] not in CANONICAL or c["group"] not in ("canonical", "thickness"):
-            continue
+        stored = c["microstructure"] in CANONICAL or c["microstructure"] in MATCHED
         row = dict(case_id=r["case_id"], group=c["group"], microstructure=c["microstructure"],
                    axis=c["transfer_axis"], repeats=int(c["repeats_along_axis"]), H_m=float(c["H_m"]),
                    N_axis=int(c["N_axis"]), T_mean_K=float(c["T_mean_K"]), delta_T_K=float(c["delta_T_K"]),
                    epsilon=float(c["epsilon"]), rays_per_patch=int(c["rays_per_patch_per_block"]),
                    seeds_A=[int(s) for s in c["seeds_A"].split(";")],
                    seeds_B=[int(s) for s in c["seeds_B"].split(";")], phase_sha256_x=c["phase_sha256_x"],
-                   newton_updates=int(r["newton_updates"]))
+                   newton_updates=int(r["newton_updates"]), array="stored" if stored else "generated")
         for k in ("q_cond_hot_W_m2", "q_rad_hot_W_m2", "q_total_hot_W_m2", "q_cond_cold_W_m2", "q_rad_cold_W_m2",
                   "q_total_cold_W_m2", "radiative_fraction_hot", "k_eff_apparent_W_mK", "wall_flux_mismatch_rel",
                   "energy_residual_rel", "T_min_K", "T_max_K"):
@@ -339,36 +351,133 @@ def microstructure_rows(ref):
     print("microstructure rows:", len(rows))
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
-    args = ap.parse_args()
-    ref = Path(args.reference)
-    sys.path.insert(0, str(ref))
-    from porerad import coupled as cp, exchange as ex, view_factors as vf  # noqa: E402
-
-    for name, spec in SMALL_CASES.items():
-        small_case(vf, ex, cp, name, spec)
-        coupled_small(name, spec)
-    coupled_rows(ref)
-    prescribed_cases(ref)
-    multibounce_rows(ref)
-    descriptor_rows(ref)
-    microstructure_rows(ref)
-    ray_set_comparison_rows(ref)
-
-    rows = list(csv.DictReader(open(ref / "data" / "cases_coupled.csv")))
+def count_hash_rows(ref):
     hashes = {}
-    for r in rows:
-        if r["microstructure"] in CANONICAL and r["raw_count_sha256_A"]:
+    for r in csv.DictReader(open(ref / "data" / "cases_coupled.csv")):
+        if r["raw_count_sha256_A"]:
             key = f"{r['microstructure']}|{r['transfer_axis']}"
             hashes[key] = dict(microstructure=r["microstructure"], axis=r["transfer_axis"], H_m=float(r["H_m"]),
                                rays_per_patch=int(r["rays_per_patch_per_block"]),
                                seeds_A=[int(s) for s in r["seeds_A"].split(";")],
                                seeds_B=[int(s) for s in r["seeds_B"].split(";")],
                                phase_sha256_x=r["phase_sha256_x"], sha256_A=r["raw_count_sha256_A"],
-                               sha256_B=r["raw_count_sha256_B"], source="data/cases_coupled.csv")
+                               sha256_B=r["raw_count_sha256_B"], source="data/cases_coupled.csv",
+                               array="stored" if r["microstructure"] in CANONICAL else "generated")
     (HERE / "count_hashes.json").write_text(json.dumps(hashes, indent=1, sort_keys=True))
+    print("hash cases:", len(hashes))
+
+
+def fullpath_rows(ref):
+    """results/fullpath_crosscheck.csv first_hit_radiosity rows, with the reference's recomputation.
+
+    No script of the reference writes these rows and none records their rays.  Stored with them:
+    the prescribed-field channels the reference computes from the coupled case's sets A + B (2 + 2
+    blocks of 64 rays per patch) on the same microstructure, and the file's full-path Monte Carlo
+    rows of that microstructure.
+    """
+
+    from porerad import coupled as cp, exchange as ex, view_factors as vf
+
+    cases = {r["case_id"]: r for r in csv.DictReader(open(ref / "data" / "cases_coupled.csv"))}
+    rows = []
+    table = list(csv.DictReader(open(ref / "results" / "fullpath_crosscheck.csv")))
+    for r in table:
+        if r["method"] != "first_hit_radiosity":
+            continue
+        T, dT, eps = float(r["T_mean_K"]), float(r["delta_T_K"]), float(r["epsilon"])
+        c = cases[f"coupled_{r['structure']}_{r['transfer_axis']}_T{int(T)}_eps{eps:g}_N128"]
+        ph = vf.orient_along_x(np.load(ref / "data" / "microstructures" / f"{r['microstructure']}.npz")["phases"],
+                               r["transfer_axis"])
+        p = vf.build_surface_patches(ph, float(c["H_m"]))
+        seeds = [int(x) for k in ("seeds_A", "seeds_B") for x in c[k].split(";")]
+        R = int(c["rays_per_patch_per_block"])
+        o, rc, n = vf.pool_counts([vf.first_hit_counts(p, R, sd) for sd in seeds], p.n_patches)
+        op = ex.ExchangeOperator(o, rc, n, np.full(p.n_patches, R * len(seeds), np.int64), p.patch_area_m2)
+        ch = cp.prescribed_field_channels(op, p, T, dT, eps)
+        rows.append(dict(microstructure=r["microstructure"], axis=r["transfer_axis"], H_m=float(c["H_m"]),
+                         T_mean_K=T, delta_T_K=dT, epsilon=eps, rays_per_patch=R, seeds=seeds,
+                         phase_sha256_x=c["phase_sha256_x"], q_h=float(r["q_h_W_m2"]), q_c=float(r["q_c_W_m2"]),
+                         q_i=float(r["q_i_W_m2"]), recomputed=dict(q_h=ch.q_h, q_c=ch.q_c, q_i=ch.q_i),
+                         monte_carlo=[{k: float(m[k]) for k in ("q_h_W_m2", "q_c_W_m2", "q_i_W_m2", "q_h_se_W_m2",
+                                                                 "q_c_se_W_m2", "q_i_se_W_m2", "histories")}
+                                      for m in table if m["method"] == "full_path_monte_carlo"
+                                      and m["microstructure"] == r["microstructure"]]))
+        print("fullpath", r["microstructure"], ch.q_h, ch.q_c, ch.q_i, "archived", r["q_h_W_m2"], flush=True)
+    (HERE / "fullpath.json").write_text(json.dumps(dict(rows=rows, source="results/fullpath_crosscheck.csv, "
+                                                                            "data/cases_coupled.csv"), indent=1))
+
+
+def public_api(ref):
+    """Public names of the reference modules on the path, with call signatures.
+
+    A name is public when it does not start with an underscore and is not a module or a helper
+    imported from a third-party package or the standard library.
+    """
+
+    import importlib
+    import inspect
+    import types
+
+    out = {}
+    for mod_name in ("view_factors", "exchange", "coupled", "conduction"):
+        mod = importlib.import_module(f"porerad.{mod_name}")
+        names = {}
+        for name, obj in sorted(vars(mod).items()):
+            if name.startswith("_") or isinstance(obj, types.ModuleType) or name == "annotations":
+                continue
+            if not getattr(obj, "__module__", "porerad").startswith("porerad"):
+                continue  # helpers imported from NumPy, SciPy, Numba or the standard library
+            rec = {"kind": "class" if inspect.isclass(obj) else "function" if callable(obj) else "constant"}
+            if rec["kind"] == "constant":
+                rec["value"] = repr(obj)
+            else:
+                try:
+                    sig = inspect.signature(obj)
+                    rec["parameters"] = [[p.name, p.kind.name, None if p.default is p.empty else repr(p.default)]
+                                         for p in sig.parameters.values()]
+                except (TypeError, ValueError):
+                    pass
+                if rec["kind"] == "class":
+                    rec["members"] = sorted(n for n in vars(obj) if not n.startswith("_"))
+            names[name] = rec
+        out[mod_name] = names
+    (HERE / "public_api.json").write_text(json.dumps(out, indent=1, sort_keys=True))
+    print("public api:", {k: len(v) for k, v in out.items()})
+
+
+PARTS = ("small", "coupled_rows", "prescribed", "multibounce", "descriptors", "microstructures", "ray_sets",
+         "count_hashes", "stored_arrays", "fullpath", "public_api")
+
+
+def main():
+    import os
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=os.environ.get("PORERAD_REFERENCE"),
+                    help="checkout of moxi000/pore-radiation-ijhmt2026 (default: $PORERAD_REFERENCE)")
+    ap.add_argument("--only", default=",".join(PARTS), help="comma-separated parts: " + ", ".join(PARTS))
+    args = ap.parse_args()
+    if not args.reference:
+        ap.error("give --reference or set PORERAD_REFERENCE")
+    parts = set(args.only.split(","))
+    if parts - set(PARTS):
+        ap.error(f"unknown parts {sorted(parts - set(PARTS))}")
+    ref = Path(args.reference)
+    sys.path.insert(0, str(ref))
+    from porerad import coupled as cp, exchange as ex, view_factors as vf  # noqa: E402
+
+    if "small" in parts:
+        for name, spec in SMALL_CASES.items():
+            small_case(vf, ex, cp, name, spec)
+            coupled_small(name, spec)
+    steps = dict(coupled_rows=coupled_rows, prescribed=prescribed_cases, multibounce=multibounce_rows,
+                 descriptors=descriptor_rows, microstructures=microstructure_rows, ray_sets=ray_set_comparison_rows,
+                 count_hashes=count_hash_rows, fullpath=fullpath_rows, public_api=public_api)
+    for name, fn in steps.items():
+        if name in parts:
+            fn(ref)
+    if "stored_arrays" not in parts:
+        return
     for name in CANONICAL + ["OF_core_phi0.05_s3"]:
         ph = np.load(ref / "data" / "microstructures" / f"{name}.npz")["phases"]
         assert ph.dtype == np.uint8 and set(np.unique(ph)) <= {0, 1}
@@ -387,7 +496,6 @@ def main():
                          q_c=float(r["q_c_W_m2"]), q_i=float(r["q_i_W_m2"])) for r in res],
               source="data/cases_prescribed_field.csv, results/prescribed_field.csv")
     (HERE / "prescribed_field.json").write_text(json.dumps(pf, indent=1))
-    print("hash cases:", len(hashes))
 
 
 if __name__ == "__main__":

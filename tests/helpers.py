@@ -27,8 +27,25 @@ def load_canonical(name: str) -> np.ndarray:
     return ph
 
 
-def count_hash_cases() -> dict:
-    return json.loads((GOLDEN / "count_hashes.json").read_text())
+def count_hash_cases(array: str | None = None) -> dict:
+    """Stored count hashes of data/cases_coupled.csv; ``array`` selects "stored" or "generated" rows."""
+
+    rows = json.loads((GOLDEN / "count_hashes.json").read_text())
+    return {k: v for k, v in rows.items() if array is None or v.get("array", "stored") == array}
+
+
+def case_phases(name: str) -> np.ndarray:
+    """Phases of an archived microstructure: the stored fixture, or (N = 160 and 192 canonical arrays,
+    which are not stored) the device generators' rebuild; callers check the archived phase hash."""
+
+    if (GOLDEN / f"canonical_{name}.npz").is_file():
+        return load_canonical(name)
+    structure, kind, _, n = name.split("_")
+    if kind != "canonical" or not n.startswith("N"):
+        raise FileNotFoundError(f"no stored array and no generator rule for {name}")
+    from porerad_b200 import geometry
+
+    return geometry.canonical(structure, int(n[1:]))
 
 
 def prescribed_case() -> dict:

@@ -16,7 +16,8 @@ import json
 import numpy as np
 import pytest
 
-from tests.helpers import GOLDEN, SMALL, count_hash_cases, coupled_rows, load_canonical, load_coupled, load_small
+from tests.helpers import (GOLDEN, SMALL, case_phases, count_hash_cases, coupled_rows, load_canonical, load_coupled,
+                           load_small)
 
 pytestmark = pytest.mark.gpu
 
@@ -113,7 +114,7 @@ def test_archived_coupled_rows(case_id):
     from porerad_b200.constants import K_GAS, K_SOLID
 
     row = next(r for r in coupled_rows() if r["case_id"] == case_id)
-    ph = vf.orient_along_x(load_canonical(row["microstructure"]), row["axis"])
+    ph = vf.orient_along_x(case_phases(row["microstructure"]), row["axis"])
     ph = np.ascontiguousarray(np.concatenate([ph] * row["repeats"], axis=0))
     assert ph.shape[0] == row["N_axis"]
     assert hashlib.sha256(ph.tobytes()).hexdigest() == row["phase_sha256_x"]
@@ -189,3 +190,22 @@ def test_ray_set_comparison_rows(ref):
     dT, dq = out.ab["max_temperature_difference_K"], out.ab["total_flux_rel_difference"]
     assert abs(dT - ref["max_temperature_difference_K"]) <= 1e-6 * ref["max_temperature_difference_K"] + 1e-9
     assert abs(dq - ref["total_flux_rel_difference"]) <= 1e-6
+
+
+def test_conduction_system_from_reference_fields():
+    """ConductionSystem built as the reference's dataclass (matrix, hot_rhs, cold_rhs, conductivity,
+    H_m) from an assembled system's own arrays; arrays of another field are rejected."""
+
+    from porerad_b200 import conduction
+    from porerad_b200.constants import K_GAS, K_SOLID
+
+    case = load_small("slab16")
+    k = np.where(case["phases"] == 1, K_SOLID, K_GAS)
+    ref = conduction.assemble_conduction(k, float(case["H_m"]))
+    again = conduction.ConductionSystem(ref.matrix, ref.hot_rhs, ref.cold_rhs, k, float(case["H_m"]))
+    assert (again.matrix != ref.matrix).nnz == 0
+    assert np.array_equal(again.boundary_rhs(710.0, 690.0), ref.boundary_rhs(710.0, 690.0))
+    with pytest.raises(ValueError):
+        conduction.ConductionSystem(ref.matrix * 2.0, None, None, k, float(case["H_m"]))
+    with pytest.raises(ValueError):
+        conduction.ConductionSystem(None, ref.cold_rhs, None, k, float(case["H_m"]))

@@ -13,7 +13,7 @@ import hashlib
 import numpy as np
 import pytest
 
-from tests.helpers import SMALL, count_hash_cases, load_canonical, load_small, prescribed_case
+from tests.helpers import SMALL, case_phases, count_hash_cases, load_canonical, load_small, prescribed_case
 
 pytestmark = pytest.mark.gpu
 
@@ -176,7 +176,7 @@ def test_stored_count_hashes():
 
     vf = _vf()
     cache = {}
-    for key, c in sorted(count_hash_cases().items()):
+    for key, c in sorted(count_hash_cases("stored").items()):
         if c["microstructure"] not in cache:
             cache[c["microstructure"]] = load_canonical(c["microstructure"])
         ph = vf.orient_along_x(cache[c["microstructure"]], c["axis"])
@@ -186,6 +186,23 @@ def test_stored_count_hashes():
             table = vf.first_hit_counts_pooled(p, c["rays_per_patch"], c["seeds_" + s])
             assert table.sha256() == c["sha256_" + s], f"{key} set {s}"
             table.close()
+
+
+@pytest.mark.parametrize("key", sorted(count_hash_cases("generated")))
+def test_resolution_count_hashes(key):
+    """The stored raw_count_sha256_A/B of the N = 160 and 192 resolution cases (data/cases_coupled.csv):
+    the canonical arrays rebuilt by the generators (phase hash checked), 2 blocks of 64 rays per
+    patch per set, up to 1.4e8 rays per set."""
+
+    vf = _vf()
+    c = count_hash_cases("generated")[key]
+    ph = vf.orient_along_x(case_phases(c["microstructure"]), c["axis"])
+    assert hashlib.sha256(ph.tobytes()).hexdigest() == c["phase_sha256_x"]
+    p = vf.build_surface_patches(ph, c["H_m"])
+    for s in ("A", "B"):
+        table = vf.first_hit_counts_pooled(p, c["rays_per_patch"], c["seeds_" + s])
+        assert table.sha256() == c["sha256_" + s], f"{key} set {s}"
+        table.close()
 
 
 def test_archived_prescribed_field_rows():

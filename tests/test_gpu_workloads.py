@@ -1,0 +1,118 @@
+"""GPU parity on the benchmark workloads themselves, against the oracle on the same seeded inputs.
+
+* FI 64^3, phi 0.10, 64 rays per patch, one set (the small plain case): the whole case.  The
+  count hash equals the oracle's; the binary64 channels agree with the oracle's binary64
+  channels to 1e-9 and the mixed-precision channels (binary32 sweeps in binary64 refinement)
+  to 1e-8 relative.
+* OF 128^3, 1000 rays per patch, sets A and B (the headline case), and TL and FA 192^3, 1000
+  rays per patch, sets A, B and C (the coupled-size stress case): the full count tables of every
+  set are made on the device (up to 1.1e9 rays per set); the rows of three origin-patch slices
+  (first, middle and last patches) equal the oracle's counts of the same slices bit for bit.
+  The oracle draws the rays of a slice from the same PCG64 stream position as a full pass
+  (view_factors.py:149-151), so a slice checks the full-size tables without tracing them on the
+  CPU.  The slices of each workload hold 2-3 x 10^4 rays whose azimuth sine or cosine differs by
+  one ulp from glibc's; an equal count table shows that none of them changed a receiver.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FLUX_RTOL = 1e-9    # binary64 channels: both sides balance d to 1e-11 (d agrees to about 1e-8 relative)
+MIXED_RTOL = 1e-8   # mixed-precision channels against the oracle's binary64 channels
+
+C1 = dict(arch="FI", n=64, phi=0.10, seed=0, rays=64, sets=1, eps=0.9, T_m=650.0, dT=100.0, H=0.01)
+SLICED = {
+    "OF128-c2": (dict(arch="OF", n=128, phi=0.10, seed=1, rays=1000, sets=2, H=0.01), 4096),
+    "TL192-c5": (dict(arch="TL", n=192, phi=0.10, seed=0, rays=1000, sets=3, H=0.01), 2048),
+    "FA192-c5": (dict(arch="FA", n=192, phi=0.10, seed=0, ray_seed=7919, rays=1000, sets=3, H=0.01), 2048),
+}
+
+
+def _seeds(spec):
+    """The ray-set seeds the benchmark draws for a case (SplitMix64 of its case seed and set index)."""
+
+    from porerad_b200.geometry import ray_set_seed
+
+    return [ray_set_seed(spec.get("ray_seed", spec["seed"]), s) for s in range(spec["sets"])]
+
+
+def test_small_plain_case_whole_path_against_oracle(oracle):
+    from porerad_b200 import coupled, exchange, geometry, view_factors as vf
+
+    s = C1
+    ph = geometry.make(s["arch"], s["n"], s["phi"], s["seed"])
+    seeds = _seeds(s)
+    p = vf.build_surface_patches(ph, s["H"])
+    q = oracle.build_surface_patches(ph, s["H"])
+    assert p.n_patches == q.n_patches
+    table = vf.first_hit_counts_pooled(p, s["rays"], seeds)
+    pooled = oracle.pool_counts([oracle.first_hit_counts(q, s["rays"], sd) for sd in seeds], q.n_patches)
+    rays = np.full(q.n_patches, s["rays"] * len(seeds), np.int64)
+    assert table.rays_traced == int(rays.sum())
+    assert table.sha256() == oracle.count_sha256(*pooled, rays)
+
+    op = exchange.ExchangeOperator(table, None, None, rays, p.patch_area_m2)
+    ref_op = oracle.ExchangeOperator(*pooled, rays, q.patch_area_m2)
+    want = oracle.prescribed_field_channels(ref_op, q, s["T_m"], s["dT"], s["eps"])
+    got = coupled.prescribed_field_channels(op, p, s["T_m"], s["dT"], s["eps"])
+    mixed = coupled.prescribed_field_channels(op, p, s["T_m"], s["dT"], s["eps"], precision="mixed")
+    scale = max(abs(want.q_h), abs(want.q_c), abs(want.q_i))
+    for name in ("q_h", "q_c", "q_i"):
+        assert abs(getattr(got, name) - getattr(want, name)) <= FLUX_RTOL * scale, name
+    for name in ("q_h", "q_c"):
+        assert abs(getattr(mixed, name) - getattr(want, name)) <= MIXED_RTOL * abs(getattr(want, name)), name
+    assert abs(mixed.q_i - want.q_i) <= MIXED_RTOL * scale
+    assert float(np.sum(np.abs(got.coarse_source - want.coarse_source))) <= \
+        FLUX_RTOL * float(np.sum(np.abs(want.coarse_source)))
+    op.close()
+    table.close()
+
+
+@pytest.mark.parametrize("name", sorted(SLICED))
+def test_full_size_count_rows_on_patch_slices(oracle, name):
+    from porerad_b200 import geometry, view_factors as vf
+
+    s, width = SLICED[name]
+    ph = geometry.make(s["arch"], s["n"], s["phi"], s["seed"])
+    p = vf.build_surface_patches(ph, s["H"])
+    q = oracle.build_surface_patches(ph, s["H"])
+    P = p.n_patches
+    assert P == q.n_patches and P >= 3 * width
+    slices = [(0, width), (P // 2, P // 2 + width), (P - width, P)]
+    for sd in _seeds(s):
+        table = vf.first_hit_counts_pooled(p, s["rays"], [sd])
+        assert table.rays_traced == P * s["rays"]
+        for b, e in slices:
+            got = table.rows(b, e)
+            want = oracle.first_hit_counts(q, s["rays"], sd, patch_start=b, patch_end=e)
+            assert int(got[2].sum()) == (e - b) * s["rays"]
+            for g, w, field in zip(got, want, ("origin", "receiver", "count")):
+                assert g.dtype == w.dtype and np.array_equal(g, w), (name, sd, b, field)
+        table.close()
+
+
+def test_count_rows_edges_and_errors():
+    """Row ranges: empty, a single row, the whole table (equal to the full copy), out of range."""
+
+    from porerad_b200 import view_factors as vf
+    from tests.helpers import load_small
+
+    case = load_small("cube20")
+    p = vf.build_surface_patches(case["phases"], float(case["H_m"]))
+    table = vf.first_hit_counts_pooled(p, int(case["rays_per_patch"]), [int(x) for x in case["seeds"]])
+    full = table.to_numpy()
+    n = table.n_patches
+    for got, want in zip(table.rows(0, n), full):
+        assert np.array_equal(got, want)
+    assert all(a.size == 0 for a in table.rows(5, 5))
+    o, r, c = table.rows(7, 8)
+    sel = full[0] == 7
+    assert np.array_equal(o, full[0][sel]) and np.array_equal(r, full[1][sel]) and np.array_equal(c, full[2][sel])
+    for b, e in ((-1, 3), (3, n + 1), (4, 3)):
+        with pytest.raises(ValueError, match="row range"):
+            table.rows(b, e)
+    table.close()
