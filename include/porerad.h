@@ -189,9 +189,11 @@ PR_API int pr_reflection_series(const pr_operator* op, const double* emitted, co
  * code that must not take the allocator's implicit synchronisation in the middle of its
  * stream work.  It allocates nothing: its scratch (two vectors, block partial sums and
  * the convergence state) is one static device array held by every GPU that loads the
- * library until the process exits, sized for at most 262144 patches; larger operators
- * are rejected with PR_ERR_LIMIT.  emitted, emissivity and absorbed must be device
- * memory of the operator's device.  The first call on a device looks up the array's
+ * library until the process exits (4.2 MB), sized for at most 262144 patches and for the
+ * block partial sums of GPUs with up to 296 SMs (a B200 has 148); larger operators, or a
+ * GPU whose launches need more partial sums, are rejected with PR_ERR_LIMIT.  emitted,
+ * emissivity and absorbed must be device memory of the operator's device (PR_ERR_ARG for
+ * host memory or another GPU's memory).  The first call on a device looks up the array's
  * device address (cudaGetSymbolAddress) and should come before any stream capture.
  * Every call shares the one array: calls that overlap on the GPU (other streams, other
  * host threads) race and must be serialised by the caller. */

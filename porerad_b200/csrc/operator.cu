@@ -885,8 +885,9 @@ static int sym_union(const CountCsr& F, const CountCsr& T, pr_operator* op, cuda
   PR_CUDA(cudaMemcpyAsync(&nnz, S.row_ptr.ptr + n, 8, cudaMemcpyDeviceToHost, s));
   PR_CUDA(cudaStreamSynchronize(s));
   S.nnz = nnz;
-  PR_TRY(S.words.alloc(nnz > 0 ? nnz : 1, s));
-  PR_TRY(S.cnt.alloc(nnz > 0 ? nnz : 1, s));
+  // padded to a whole 16-byte quad: the blocked products read the entries four at a time
+  PR_TRY(S.words.alloc((size_t)(nnz + 4) / 4 * 4, s));
+  PR_TRY(S.cnt.alloc((size_t)(nnz + 4) / 4 * 4, s));
   ::pr::launch_mark(), k_merge_rank<<<grid_for(n * 32, 256), 256, 0, s>>>(
       F.row_ptr.ptr, F.col.ptr, F.cnt.ptr, T.row_ptr.ptr, T.col.ptr, T.cnt.ptr, n, S.row_ptr.ptr,
       (int32_t*)S.words.ptr, S.cnt.ptr, bad.ptr);

@@ -117,6 +117,16 @@ inline bool is_device_pointer(const void* p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+// Device memory (or managed memory) that belongs to the given device.
+inline bool is_device_pointer_of(const void* p, int device) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == device;
+}
+
 inline int grid_for(int64_t n, int block, int cap = 148 * 32) {
   int64_t g = (n + block - 1) / block;
   if (g < 1) g = 1;

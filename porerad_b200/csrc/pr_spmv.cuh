@@ -164,33 +164,60 @@ struct BlkView {
 
 inline BlkView blk_view(const SymCsr& S) { return BlkView{S.blk.seg.ptr, S.blk.cta_row.ptr, S.blk.W, S.blk.nb}; }
 
-// sum over entries [qb, qe) of a row of coefficient * xs[col - c0] (xs in shared memory) by
-// a group of G lanes (gl = lane within the group): lane gl adds entries qb + gl, qb + gl + G,
-// ... in that order, four loads ahead; the group's partials meet in a fixed shuffle tree
-// (every lane of the warp takes part, lanes of an idle group with qb = qe add zero).
+// Entries q .. q + 3 of one 16-byte quad of the word array (and of the count array in kCounts
+// mode): each entry inside [qb, qe) adds coefficient * xs[col - c0] to acc, in entry order.
+template <int kMode, typename Acc, typename Tx>
+__device__ __forceinline__ void quad_add(const SymView& S, const uint4& w, const int4& c, int64_t q, int64_t qb,
+                                         int64_t qe, const Tx* xs, uint32_t c0, Acc& acc) {
+  const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+  const int32_t cs[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    if (q + e >= qb && q + e < qe) {
+      Acc coef;
+      uint32_t col;
+      if constexpr (kMode == kPacked) {
+        coef = (Acc)(ws[e] & S.mask);
+        col = ws[e] >> S.bits;
+      } else {
+        coef = (Acc)cs[e];
+        col = ws[e];
+      }
+      acc = fma(coef, (Acc)xs[col - c0], acc);
+    }
+  }
+}
+
+// sum over entries [qb, qe) of a row of coefficient * xs[col - c0] (xs in shared memory) by a
+// group of G lanes (gl = lane within the group).  The group reads whole aligned 16-byte quads
+// of the word array (entries 4a .. 4a + 3 of quad a): lane gl takes quads a0 + gl, a0 + gl + G,
+// ..., U loads in flight per round (so the G lanes of a round read U x G x 16 contiguous
+// bytes), and adds the entries of each quad that lie in [qb, qe) in quad order.  The group's
+// partials meet in a fixed shuffle tree (every lane of the warp takes part; lanes of an idle
+// group, qb = qe, add zero).  Reads past the last entry stay inside the word array, whose
+// allocation is padded to a whole quad.
 template <int kMode, int G, typename Acc, typename Tx>
 __device__ __forceinline__ Acc seg_sum(const SymView& S, int64_t qb, int64_t qe, const Tx* xs, uint32_t c0,
                                        int gl) {
+  constexpr int U = kMode == kCounts ? 2 : 4;  // counts mode loads a second quad per entry quad
   Acc acc = 0;
-  int64_t q = qb + gl;
-  for (; q + 3 * G < qe; q += 4 * G) {
-    Acc c0v, c1v, c2v, c3v;
-    uint32_t j0, j1, j2, j3;
-    sym_entry<kMode>(S, q, c0v, j0);
-    sym_entry<kMode>(S, q + G, c1v, j1);
-    sym_entry<kMode>(S, q + 2 * G, c2v, j2);
-    sym_entry<kMode>(S, q + 3 * G, c3v, j3);
-    const Acc x0 = (Acc)xs[j0 - c0], x1 = (Acc)xs[j1 - c0], x2 = (Acc)xs[j2 - c0], x3 = (Acc)xs[j3 - c0];
-    acc = fma(c0v, x0, acc);
-    acc = fma(c1v, x1, acc);
-    acc = fma(c2v, x2, acc);
-    acc = fma(c3v, x3, acc);
-  }
-  for (; q < qe; q += G) {
-    Acc c;
-    uint32_t j;
-    sym_entry<kMode>(S, q, c, j);
-    acc = fma(c, (Acc)xs[j - c0], acc);
+  const int64_t a1 = (qe + 3) >> 2;
+  const uint4* __restrict__ w4 = reinterpret_cast<const uint4*>(S.words);
+  const int4* __restrict__ c4 = reinterpret_cast<const int4*>(S.cnt);
+  for (int64_t a = (qb >> 2) + gl; a < a1; a += U * G) {
+    uint4 w[U];
+    int4 c[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t au = a + (int64_t)u * G;
+      w[u] = au < a1 ? __ldg(w4 + au) : make_uint4(0u, 0u, 0u, 0u);
+      c[u] = make_int4(0, 0, 0, 0);
+      if constexpr (kMode == kCounts) {
+        if (au < a1) c[u] = __ldg(c4 + au);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) quad_add<kMode>(S, w[u], c[u], 4 * (a + (int64_t)u * G), qb, qe, xs, c0, acc);
   }
   for (int o = G / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(PR_FULL, acc, o);
   return acc;
@@ -294,6 +321,10 @@ inline int launch_spmv(const SymCsr& S, const Tx* x, const Epi& epi, cudaStream_
   const SymView v = sym_view(S);
   if (S.blk.ready && kMode != kValues) {
     constexpr int k = sizeof(Tx) == 4 ? 2 : 1;
+    if (((uintptr_t)S.words.ptr & 15u) || (kMode == kCounts && ((uintptr_t)S.cnt.ptr & 15u))) {
+      set_error("blocked product: the entry arrays are not 16-byte aligned");
+      return PR_ERR_CUDA;
+    }
     const size_t smem = (size_t)S.blk.W * k * sizeof(Tx) + (size_t)S.blk.rows_cap * sizeof(Acc);
     if (smem > (size_t)kBlkSmemMax) {
       set_error("blocked product needs %zu bytes of shared memory", smem);

@@ -604,7 +604,12 @@ int cell_field_channels(const pr_case* c, const pr_operator* op, const double* T
 namespace pr {
 
 static constexpr int64_t kNoAllocMaxPatches = 262144;  // 2 x 262144 x 8 B of vectors
-static constexpr int64_t kNoAllocPartials = 2 * 148 * 8 * 2;  // block partials, two values per block
+// Block partial sums, two values per block.  The series launches at most 8 blocks per SM (the
+// products of operators of at most kNoAllocMaxPatches rows: max(SMs, 86) blocked CTAs or 8 per SM
+// warp-per-row blocks; 4 per SM for the reductions), so 2 x 8 x 296 values cover GPUs of up to
+// 296 SMs (B200: 148).  A launch that would need more is rejected with PR_ERR_LIMIT below.
+static constexpr int64_t kNoAllocMaxSms = 296;
+static constexpr int64_t kNoAllocPartials = 2 * 8 * kNoAllocMaxSms;
 static constexpr int64_t kNoAllocDoubles = 2 * kNoAllocMaxPatches + kNoAllocPartials + 8;
 
 static __device__ __align__(256) double g_series_scratch[kNoAllocDoubles];
@@ -707,8 +712,10 @@ extern "C" PR_API int pr_reflection_series_noalloc(const pr_operator* op, const 
     return PR_ERR_ARG;
   }
   DeviceGuard guard(op->device);
-  if (!is_device_pointer(emitted) || !is_device_pointer(emissivity) || !is_device_pointer(absorbed)) {
-    set_error("pr_reflection_series_noalloc: emitted, emissivity and absorbed must be device memory");
+  if (!is_device_pointer_of(emitted, op->device) || !is_device_pointer_of(emissivity, op->device) ||
+      !is_device_pointer_of(absorbed, op->device)) {
+    set_error("pr_reflection_series_noalloc: emitted, emissivity and absorbed must be device memory of the "
+              "operator's device %d", op->device);
     return PR_ERR_ARG;
   }
   double res = 0.0;

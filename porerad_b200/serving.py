@@ -123,7 +123,9 @@ class Admission:
     """Device-memory budget shared by the workers: acquire blocks until the bytes fit.
 
     A request larger than the whole budget is admitted alone (when nothing else holds
-    memory) rather than never.
+    memory) rather than never.  ``grow`` enlarges a reservation in place: a worker whose
+    geometry is already resident keeps it counted while it waits for the rest of its
+    footprint.
     """
 
     def __init__(self, budget_bytes: int):
@@ -131,6 +133,35 @@ class Admission:
         self.reserved = 0
         self.peak = 0
         self._cv = threading.Condition()
+        self._waiting: dict[int, int] = {}  # ticket -> bytes held by a worker waiting in grow
+        self._tickets = 0
+
+    def grow(self, held: int, new: int, stop: Callable[[], bool] = lambda: False) -> bool:
+        """Turn a reservation of ``held`` bytes into one of ``new`` bytes, blocking until it fits.
+
+        While it waits the held bytes stay reserved.  If nothing is running (every reserved byte
+        belongs to waiting workers) the earliest waiter goes ahead even past the budget, so
+        waiters that each hold a resident geometry cannot block one another for ever.
+        """
+
+        with self._cv:
+            ticket = self._tickets
+            self._tickets += 1
+            self._waiting[ticket] = int(held)
+            try:
+                while self.reserved - held + new > self.budget:
+                    running = self.reserved - sum(self._waiting.values())
+                    if running <= 0 and ticket == min(self._waiting):
+                        break
+                    if stop():
+                        return False
+                    self._cv.wait(timeout=0.05)
+                self.reserved += int(new) - int(held)
+                self.peak = max(self.peak, self.reserved)
+                return True
+            finally:
+                del self._waiting[ticket]
+                self._cv.notify_all()
 
     def acquire(self, nbytes: int, stop: Callable[[], bool] = lambda: False) -> bool:
         with self._cv:
@@ -171,9 +202,8 @@ def run_case(req: CaseRequest, admission: Admission, on_admit: Callable[[int], N
         del phases
         L = int(req.rays_per_patch) * len(req.seeds)
         need = footprint_bytes(geo.n_patches, L)
-        admission.release(held)
-        held = 0
-        admission.acquire(geo.device_bytes + need)
+        # the geometry stays resident (and counted) while the worker waits for the rest
+        admission.grow(held, geo.device_bytes + need)
         held = geo.device_bytes + need
         t_admit = time.perf_counter()
         if on_admit:

@@ -76,3 +76,61 @@ def test_footprint_bounds_grow_with_work():
     assert 0 < a < b < c
     assert serving.footprint_bytes(10, 1000) < serving.footprint_bytes(10, 10_000) or True
     assert serving.percentile([1, 2, 3, 4], 50) == 2.5
+
+
+class GrowRunner:
+    """run_case's protocol: reserve the geometry, build it, then grow the reservation to the whole
+    footprint and run; records the bytes reserved while cases run."""
+
+    def __init__(self, geometry, rest, secs):
+        self.geometry, self.rest, self.secs = geometry, rest, secs
+        self.lock = threading.Lock()
+        self.max_reserved = 0
+        self.running = 0
+        self.max_running = 0
+
+    def __call__(self, req, admission):
+        admission.acquire(self.geometry)
+        held = self.geometry
+        try:
+            time.sleep(0.005)  # building the geometry
+            admission.grow(held, self.geometry + self.rest)
+            held = self.geometry + self.rest
+            with self.lock:
+                self.running += 1
+                self.max_running = max(self.max_running, self.running)
+                self.max_reserved = max(self.max_reserved, admission.reserved)
+            time.sleep(self.secs)
+            with self.lock:
+                self.running -= 1
+            return serving.CaseResult(req.tag["id"], 1.0, -1.0, 0.0, 0.0, None, t_admit=time.perf_counter())
+        finally:
+            admission.release(held)
+
+
+def test_waiting_geometry_stays_counted_and_waiters_do_not_deadlock():
+    """Budget 100, geometry 30 + rest 50.  Up to three geometries are admitted within the budget;
+    when all their workers wait to grow, the earliest goes ahead past the budget by at most its
+    remaining 50 bytes (so the reservation, which keeps counting the waiting geometries, stays
+    within 150), and only one case runs at a time."""
+
+    runner = GrowRunner(30, 50, 0.01)
+    with serving.Server(slots=4, hbm_budget_bytes=100, runner=runner, streams=False) as srv:
+        futs = [srv.submit(_req(i, 0, 0.0)) for i in range(16)]
+        results = [f.result(timeout=20) for f in futs]
+    assert sorted(r.tag for r in results) == list(range(16))
+    assert runner.max_running == 1
+    assert runner.max_reserved <= 150
+    assert srv.admission.reserved == 0 and srv.admission.peak <= 150
+
+
+def test_grow_within_budget_does_not_wait():
+    adm = serving.Admission(100)
+    assert adm.acquire(20)
+    assert adm.grow(20, 60)
+    assert adm.reserved == 60
+    assert adm.acquire(40)
+    assert adm.reserved == 100
+    adm.release(60)
+    adm.release(40)
+    assert adm.reserved == 0

@@ -44,6 +44,7 @@ def test_noalloc_series_matches_allocating_entry_point_twice():
                                    np.full(n, R, np.int64), area)
     fn = _entry(_lib.load())
     rng = np.random.default_rng(11)
+    dev = torch.cuda.current_device()
     for call in range(2):
         emitted = rng.standard_normal(n) * 1e-6
         eps = 0.3 + 0.6 * rng.random(n)
@@ -52,9 +53,16 @@ def test_noalloc_series_matches_allocating_entry_point_twice():
         d_eps = torch.tensor(eps, dtype=torch.float64, device="cuda")
         d_out = torch.full((n,), float("nan"), dtype=torch.float64, device="cuda")
         res, it = ctypes.c_double(), ctypes.c_int64()
+        torch.cuda.synchronize()
+        before = (_lib.memory_stats(dev), torch.cuda.memory_allocated(dev))
         status = fn(op.handle, d_e.data_ptr(), d_eps.data_ptr(), 1e-13, 10000, d_out.data_ptr(), ctypes.byref(res),
                     ctypes.byref(it), None)
         assert status == _lib.PR_OK, _lib.last_error()
+        torch.cuda.synchronize()
+        after = (_lib.memory_stats(dev), torch.cuda.memory_allocated(dev))
+        # nothing allocated: no driver allocation, no block taken from the library's cache, no
+        # torch allocation, and the library's live and cached bytes unchanged
+        assert after == before, (before, after)
         got = d_out.cpu().numpy()
         scale = float(np.max(np.abs(want.absorbed_power_W)))
         assert float(np.max(np.abs(got - want.absorbed_power_W))) <= RTOL * scale, f"call {call}"
