@@ -111,24 +111,29 @@ def cross_section_area(patches) -> float:
 
 
 def linear_cell_temperature(shape: tuple[int, int, int], T_mean_K: float, delta_T_K: float) -> np.ndarray:
-    """Linear field T_h + (T_c - T_h) s/H evaluated at the cell centres (coupled.py:138-143)."""
+    """The prescribed linear field at the cell centres: T_m + dT/2 at the hot wall (x = 0) falling
+    by dT over the N_x cells to T_m - dT/2 at the cold wall (coupled.py:138-143)."""
 
-    nx = int(shape[0])
-    axial = (T_mean_K + delta_T_K / 2.0) - (np.arange(nx, dtype=np.float64) + 0.5) * delta_T_K / nx
-    return np.broadcast_to(axial[:, None, None], tuple(int(n) for n in shape)).copy()
+    nx, ny, nz = (int(n) for n in shape)
+    T_hot = T_mean_K + delta_T_K / 2.0
+    centres = np.arange(nx, dtype=np.float64) + 0.5
+    out = np.empty((nx, ny, nz))
+    out[...] = (T_hot - centres * delta_T_K / nx)[:, None, None]
+    return out
 
 
 def coarse_source(cell_power_W: np.ndarray, bins: int = 8) -> np.ndarray:
-    """Cell power summed over a bins^3 grid of equal blocks (coupled.py:146-153)."""
+    """Cell power summed over blocks of a bins^3 grid (coupled.py:146-153).  Along an axis of n
+    cells there are min(bins, n) blocks; their sizes differ by at most one, the larger first."""
 
-    array = np.asarray(cell_power_W, dtype=np.float64)
-    parts = [np.array_split(np.arange(n), min(bins, n)) for n in array.shape]
-    return np.asarray(
-        [float(np.sum(array[np.ix_(xs, ys, zs)])) for xs in parts[0] for ys in parts[1] for zs in parts[2]]
-    ).reshape(tuple(len(p) for p in parts))
+    out = np.asarray(cell_power_W, dtype=np.float64)
+    for axis, n in enumerate(out.shape):
+        k = min(int(bins), n)
+        sizes = [n // k + (1 if b < n % k else 0) for b in range(k)]
+        out = np.add.reduceat(out, np.cumsum([0] + sizes[:-1]), axis=axis)
+    return out
 
 
-@dataclass
 class PrescribedChannels:
     """Radiation channels (W m^-2) under the prescribed linear field, q_h + q_c + q_i = 0 (coupled.py:156-167).
 
@@ -188,31 +193,39 @@ def prescribed_field_channels(operator: ExchangeOperator, patches, T_mean_K: flo
                               float(q[2]), float(q[3]), coarse, info)
 
 
-def relative_difference(a: float, b: float) -> float:
-    """coupled.py:197-198."""
+APPEND_CHANNEL_DIFFERENCE = 0.01
+APPEND_SOURCE_DIFFERENCE = 0.05
+"""A/B differences above which one more ray block is appended to each set (coupled.py:216-219)."""
 
-    return abs(float(a) - float(b)) / max(abs(float(a)), abs(float(b)), _TINY)
+
+def relative_difference(a: float, b: float) -> float:
+    """|a - b| relative to the larger magnitude (coupled.py:197-198)."""
+
+    a, b = float(a), float(b)
+    return abs(a - b) / max(abs(a), abs(b), _TINY)
+
+
+def _l1(x) -> float:
+    return float(np.sum(np.abs(x)))
 
 
 def ab_differences(set_a: list[PrescribedChannels], set_b: list[PrescribedChannels]) -> tuple[float, float]:
-    """Largest A/B relative difference of the wall channels and of the 8^3 coarse source, L1 (coupled.py:201-213)."""
+    """Disagreement of two ray sets over matching conditions (coupled.py:201-213): the largest
+    relative difference of a wall channel (q_h or q_c), and the largest L1 difference of the
+    8^3 coarse sources relative to the larger of their L1 norms."""
 
-    channel = max(
-        relative_difference(getattr(a, name), getattr(b, name))
-        for a, b in zip(set_a, set_b) for name in ("q_h", "q_c")
-    )
-    source = max(
-        float(np.sum(np.abs(a.coarse_source - b.coarse_source)))
-        / max(float(np.sum(np.abs(a.coarse_source))), float(np.sum(np.abs(b.coarse_source))), _TINY)
-        for a, b in zip(set_a, set_b)
-    )
-    return channel, source
+    walls, sources = [], []
+    for a, b in zip(set_a, set_b):
+        walls.extend((relative_difference(a.q_h, b.q_h), relative_difference(a.q_c, b.q_c)))
+        norm = max(_l1(a.coarse_source), _l1(b.coarse_source), _TINY)
+        sources.append(_l1(a.coarse_source - b.coarse_source) / norm)
+    return max(walls), max(sources)
 
 
 def append_required(channel_difference: float, source_difference: float) -> bool:
-    """One symmetric append of a further ray block to each set when the sets disagree (coupled.py:216-219)."""
+    """Whether the sets disagree enough to append one more ray block to each (coupled.py:216-219)."""
 
-    return channel_difference > 0.01 or source_difference > 0.05
+    return channel_difference > APPEND_CHANNEL_DIFFERENCE or source_difference > APPEND_SOURCE_DIFFERENCE
 
 
 def cell_field_channels(operator: ExchangeOperator, patches, T_cells, T_hot_K: float, T_cold_K: float,
@@ -356,14 +369,17 @@ def wall_flux_metrics(system, patches, result: CoupledResult, T_hot_K: float, T_
     return dict(result.metrics)
 
 
-def acceptance_failures(result: CoupledResult, metrics: dict[str, float]) -> list[str]:
-    """Acceptance conditions of a coupled solution that are not met, empty when accepted (coupled.py:475-490)."""
+_ACCEPTANCE = (
+    ("Newton iteration converged", lambda r, m: r.converged),
+    ("linear residuals within max(1e-13, 1e-8 ||b||)", lambda r, m: r.linear_residuals_pass),
+    ("wall-flux mismatch <= 0.5 %", lambda r, m: m["wall_flux_mismatch_rel"] <= 0.005),
+    ("global energy residual <= 1e-3", lambda r, m: m["energy_residual_rel"] <= 1.0e-3),
+    ("temperature within the wall temperatures", lambda r, m: m["temperature_bound_violations"] == 0),
+)
+"""Acceptance conditions of a coupled solution and their names (coupled.py:475-490)."""
 
-    checks = {
-        "Newton iteration converged": result.converged,
-        "linear residuals within max(1e-13, 1e-8 ||b||)": result.linear_residuals_pass,
-        "wall-flux mismatch <= 0.5 %": metrics["wall_flux_mismatch_rel"] <= 0.005,
-        "global energy residual <= 1e-3": metrics["energy_residual_rel"] <= 1.0e-3,
-        "temperature within the wall temperatures": metrics["temperature_bound_violations"] == 0,
-    }
-    return [name for name, ok in checks.items() if not ok]
+
+def acceptance_failures(result: CoupledResult, metrics: dict[str, float]) -> list[str]:
+    """Names of the acceptance conditions the solution does not meet; empty when it is accepted."""
+
+    return [name for name, holds in _ACCEPTANCE if not holds(result, metrics)]

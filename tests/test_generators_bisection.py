@@ -39,7 +39,7 @@ def test_bisection_matches_oracle(target, lo, hi, tol, max_iter):
         seen_oracle.append(r)
         return (field < r / 4.0).astype(np.uint8)
 
-    r, ph = gen._bisect_radius(render_ours, target, lo, hi, tol=tol, max_iter=max_iter)
+    r, ph = gen.bisect_radius(render_ours, target, lo, hi, tol=tol, max_iter=max_iter)
     want = og.bisect(render_oracle, target, lo, hi, tol=tol, max_iter=max_iter)
     assert seen_ours == seen_oracle
     assert np.array_equal(ph.a, want)

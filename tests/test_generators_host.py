@@ -44,25 +44,51 @@ def _bisect(render, target, lo, hi, tol, max_iter):
 def test_fiber_nodes_and_disks(row):
     N = row["N"]
     if row["set"] == "matched":
-        seed, n_lines = gen.MATCHED_PAIRS[int(row["id"][-1])][row["structure"]]
-        aligned = row["structure"] == "FA"
-        centers = [tuple(float(v) for v in c)
-                   for c in (np.random.default_rng(seed + 1000003).random((64, 3)) * N)[:n_lines]]
-        rng = np.random.default_rng(seed + (3000003 if aligned else 2000003))
-        rots = []
-        for _ in range(n_lines):
-            v = gen._fiber_axis(rng, aligned)
-            rots.append(gen._frame(v / np.linalg.norm(v), gen._EZ))
-        fibers = [gen._long_fiber(N, c, 0.5 * 9.0 * N, R) for c, R in zip(centers, rots)]
-        ph = _bisect(lambda r: _stamp(N, fibers, r), 0.1, 0.12, 7.0, 5e-4, 32)
+        draws = gen.draw_matched_fibers(N, int(row["id"][-1]), row["structure"])
+        half, target, lo, hi, tol, its = 0.5 * 9.0 * N, 0.1, 0.12, 7.0, 5e-4, 32
     else:
         phi = round(row["target_phi"], 2)
-        centers, rots = gen.fiber_lines(N, row["seed"], gen.FIBER_LINES[row["structure"]][phi],
+        draws = gen.draw_library_fibers(N, row["seed"], gen.FIBER_LINES[row["structure"]][phi],
                                         row["structure"] == "FA", row["set"] == "canonical")
         half = 0.5 * gen.FIBER_LENGTH[row["structure"]] * N
-        fibers = [gen._long_fiber(N, c, half, R) for c, R in zip(centers, rots)]
-        ph = _bisect(lambda r: _stamp(N, fibers, r), row["target_phi"], 0.1, 4.0, gen.PHI_TOL, 24)
+        target, lo, hi, tol, its = row["target_phi"], 0.1, 4.0, gen.PHI_TOL, 24
+    fibers = [gen.LatticeCylinder(N, c, half, f) for c, f in zip(draws.centres, draws.frames)]
+    ph = _bisect(lambda r: _stamp(N, fibers, r), target, lo, hi, tol, its)
     assert hashlib.sha256(ph.tobytes()).hexdigest() == row["phase_sha256"]
+
+
+def test_public_fiber_lines_and_foam_graph_forms():
+    """fiber_lines and foam_graph return the reference's forms (tuples of floats, 3 x 3 frames,
+    sorted (i, j) edges with i < j) built from the recorded draws."""
+
+    centres, frames = gen.fiber_lines(64, 3, 5, False)
+    d = gen.draw_library_fibers(64, 3, 5, False, False)
+    assert centres == [tuple(float(v) for v in c) for c in d.centres]
+    assert all(np.array_equal(a, b) for a, b in zip(frames, d.frames))
+    assert all(float(v).is_integer() for c in centres for v in c)
+    for f in frames:
+        assert np.allclose(f.T @ f, np.eye(3), atol=1e-14)
+    nodes, edges = gen.foam_graph(48, 2, 20)
+    assert nodes.shape == (20, 3) and edges == sorted(set(edges))
+    assert all(i < j for i, j in edges) and len(edges) >= 20 * gen.FOAM_NEIGHBOURS // 2
+
+
+def test_foam_edges_and_layer_field_against_oracle():
+    """The foam's draws (nodes, the periodic k-nearest-neighbour edges) and TL's host field equal
+    the oracle's restatement of the reference's generator, value for value."""
+
+    from scipy.spatial import cKDTree
+
+    from oracle import generators as og
+
+    for N, seed, n in ((128, 0, 32), (128, 5, 24), (160, 0, 32)):
+        foam = gen.draw_foam(N, seed, n)
+        pts = np.random.default_rng(seed).uniform(0, N, size=(n, 3))
+        _, nn = cKDTree(pts, boxsize=N).query(pts, k=4)
+        want = sorted({tuple(sorted((int(i), int(j)))) for i, row in enumerate(nn) for j in row[1:] if i != j})
+        assert np.array_equal(foam.nodes, pts) and [tuple(e) for e in foam.edges.tolist()] == want
+    for N, seed, layers, wav in ((48, 0, 7, 1.7), (40, 3, 9, 1.55)):
+        assert np.array_equal(gen.lamellar_field(N, seed, layers, wav), og.layered_field(N, seed, layers, wav))
 
 
 def test_acceptance_rules_on_stored_descriptors():
