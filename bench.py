@@ -47,7 +47,7 @@ WORKLOADS = {
     "c4": dict(workload="serving: Poisson stream of geometry-axis cases, N in {96,128,160,192}, archetypes OF/FI/FA/TL, "
                         "phi U(0.05,0.20), seeds 0-99, eps U(0.3,0.95), T_mean U(500,900) K with 100 K span, "
                         "250-1000 rays/patch; served = continuous batching, mixed precision",
-               requests=16, stream_seed=2026, slots=4, H=0.01),
+               requests=200, plain_requests=24, stream_seed=2026, slots=4, H=0.01),
     "c3": dict(workload="batched sweep: 48 geometries = OF/FI/FA/TL x phi {0.05,0.10,0.20} x seeds 0-3, N=128^3, "
                         "500 rays/patch, eps from {0.3,0.6,0.9} and axis from {x,y,z} (RNG seed 3); all first-hit "
                         "counts in shared persistent traversal launches, operators and mixed-precision solves "
@@ -669,113 +669,145 @@ def _c4_geometry(spec):
     return np.ascontiguousarray(np.moveaxis(ph, "xyz".index(spec["axis"]), 0))
 
 
-def plain_case(req):
-    """One request through the drop-in NumPy API (the reference driver's sequence, binary64 series)."""
+def plain_case(req, stages=None):
+    """One request through the drop-in NumPy API (the reference driver's sequence, binary64 series);
+    ``stages`` (a dict) receives the wall-clock seconds of each stage."""
 
     from porerad_b200 import coupled, exchange, view_factors as vf
 
+    st = stages if stages is not None else {}
+
+    def lap(name, t0):
+        st[name] = st.get(name, 0.0) + time.perf_counter() - t0
+        return time.perf_counter()
+
+    t = time.perf_counter()
     p = vf.build_surface_patches(req.phases, req.H_m)
+    t = lap("patches", t)
     tables = [vf.first_hit_counts(p, req.rays_per_patch, s) for s in req.seeds]
+    t = lap("first_hit_counts", t)
     o, r, c = vf.pool_counts(tables, p.n_patches)
+    t = lap("pool_counts", t)
     op = exchange.ExchangeOperator(o, r, c, np.full(p.n_patches, req.rays_per_patch * len(req.seeds), np.int64),
                                    p.patch_area_m2)
+    t = lap("ExchangeOperator", t)
     ch = coupled.prescribed_field_channels(op, p, req.T_mean_K, req.delta_T_K, req.epsilon)
     op.close()
+    lap("prescribed_field_channels", t)
     return ch
 
 
-def run_c4(args, cfg):
-    import multiprocessing
+def _replay(arrivals, submit):
+    """Submit request k at t0 + arrivals[k] (real time); returns t0."""
 
-    specs = c4_specs(cfg)
-    with multiprocessing.get_context("spawn").Pool(min(8, os.cpu_count() or 1)) as pool:
-        phases = pool.map(_c4_geometry, specs)
+    t0 = time.perf_counter()
+    for k, a in enumerate(arrivals):
+        delay = t0 + a - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        submit(k, t0 + a)
+    return t0
+
+
+def run_c4(args, cfg):
     import torch
 
-    from porerad_b200 import _lib, serving
+    from porerad_b200 import _lib, geometry, serving
     from porerad_b200.geometry import ray_set_seed
 
     torch.cuda.set_device(0)
-    reqs = [serving.CaseRequest(ph, cfg["H"], sp["rays"], [ray_set_seed(sp["seed"] * 131 + k, 0)], sp["T_mean"],
-                                100.0, sp["eps"], precision="mixed", tag=k)
-            for k, (sp, ph) in enumerate(zip(specs, phases))]
     lib = _lib.load()
-    # warm-up: one small case per slot count
-    with serving.Server(slots=1) as srv:
-        srv.submit(reqs[0]).result()
-    # saturated: every request arrives at t0
+    specs = c4_specs(cfg)
+
+    def request(k, sp, phases=None):
+        geo = phases if phases is not None else serving.GeometrySpec(sp["arch"], sp["n"], sp["phi"], sp["seed"],
+                                                                     sp["axis"])
+        return serving.CaseRequest(geo, cfg["H"], sp["rays"], [ray_set_seed(sp["seed"] * 131 + k, 0)],
+                                   sp["T_mean"], 100.0, sp["eps"], precision="mixed", tag=k)
+
+    reqs = [request(k, sp) for k, sp in enumerate(specs)]
+    with serving.Server(slots=cfg["slots"]) as srv:  # warm-up: pools, autotuning of the first classes
+        [f.result() for f in [srv.submit(r) for r in reqs[:8]]]
+
+    # ---- saturated: every request at t0
     launches0 = lib.pr_kernel_launches()
     with ClockSampler(0) as clocks:
         t0 = time.perf_counter()
         with serving.Server(slots=cfg["slots"]) as srv:
-            futs = [srv.submit(r, t_submit=t0) for r in reqs]
-            sat = [f.result() for f in futs]
+            sat = [f.result() for f in [srv.submit(r, t_submit=t0) for r in reqs]]
         t_sat = time.perf_counter() - t0
         peak_reserved = srv.admission.peak
     launches = lib.pr_kernel_launches() - launches0
     served_rate = len(reqs) / t_sat
     rays = sum(r.rays for r in sat)
-    # the same requests carrying generator specs: each geometry is generated on the device by the
-    # worker that serves it (host generation leaves the served path)
-    spec_reqs = [serving.CaseRequest(serving.GeometrySpec(sp["arch"], sp["n"], sp["phi"], sp["seed"], sp["axis"]),
-                                     r.H_m, r.rays_per_patch, r.seeds, r.T_mean_K, r.delta_T_K, r.epsilon,
-                                     precision=r.precision, tag=r.tag) for sp, r in zip(specs, reqs)]
-    t0 = time.perf_counter()
-    with serving.Server(slots=cfg["slots"]) as srv:
-        spec_res = [f.result() for f in [srv.submit(r, t_submit=t0) for r in spec_reqs]]
-    t_spec = time.perf_counter() - t0
-    spec_same = all((a.q_h, a.q_c, a.q_i) == (b.q_h, b.q_c, b.q_i) for a, b in zip(spec_res, sat))
-    t0 = time.perf_counter()
-    for sp in specs:
-        _c4_geometry(sp)
-    host_gen_s = time.perf_counter() - t0
-    # plain path, sequential, on the same requests
-    plain_case(reqs[0])
-    service = []
-    for r in reqs:
-        t = time.perf_counter()
-        plain_case(r)
-        service.append(time.perf_counter() - t)
-    plain_rate = len(reqs) / sum(service)
-    # Poisson arrivals at 0.8 x the plain rate, replayed in real time against the server
-    lam = 0.8 * plain_rate
-    arr = np.cumsum(np.random.default_rng(cfg["stream_seed"] + 1).exponential(1.0 / lam, size=len(reqs)))
+
+    # ---- Poisson arrivals at 0.8 x the saturated served rate, all requests, replayed in real time
+    rng = np.random.default_rng(cfg["stream_seed"] + 1)
+    lam = 0.8 * served_rate
+    arr = np.cumsum(rng.exponential(1.0 / lam, size=len(reqs)))
     arr -= arr[0]
-    t0 = time.perf_counter()
     with serving.Server(slots=cfg["slots"]) as srv:
         futs = []
-        for a, r in zip(arr, reqs):
-            delay = t0 + a - time.perf_counter()
-            if delay > 0:
-                time.sleep(delay)
-            futs.append(srv.submit(r, t_submit=t0 + a))
+        _replay(arr, lambda k, ts: futs.append(srv.submit(reqs[k], t_submit=ts)))
         pois = [f.result() for f in futs]
     lat = [r.latency_s for r in pois]
-    # the plain path under the same arrivals: one FIFO server with the measured service times
-    done, plain_lat = 0.0, []
-    for a, sv in zip(arr, service):
-        done = max(done, a) + sv
-        plain_lat.append(done - a)
-    sat_lat = [r.latency_s for r in sat]
+    same = all((a.q_h, a.q_c, a.q_i) == (b.q_h, b.q_c, b.q_i) for a, b in zip(pois, sat))
+
+    # ---- the plain per-case path on the first requests: host phases made before the clock starts,
+    # one FIFO server (each request runs to completion before the next), real-time arrivals
+    m = min(cfg["plain_requests"], len(specs))
+    host = []
+    for sp in specs[:m]:
+        ph = geometry.make_device(sp["arch"], sp["n"], sp["phi"], sp["seed"])
+        host.append(np.ascontiguousarray(np.moveaxis(ph.cpu().numpy(), "xyz".index(sp["axis"]), 0)))
+    plain_reqs = [request(k, sp, host[k]) for k, sp in enumerate(specs[:m])]
+    plain_case(plain_reqs[0])
+    stages, service = {}, []
+    for r in plain_reqs[:3]:
+        t = time.perf_counter()
+        plain_case(r, stages)
+        service.append(time.perf_counter() - t)
+    plain_rate = len(service) / sum(service)
+    lam_p = 0.8 * plain_rate
+    arr_p = np.cumsum(np.random.default_rng(cfg["stream_seed"] + 2).exponential(1.0 / lam_p, size=m))
+    arr_p -= arr_p[0]
+    plain_done = []
+    t0 = time.perf_counter()
+    for k, a in enumerate(arr_p):
+        delay = t0 + a - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        plain_case(plain_reqs[k], stages)
+        plain_done.append(time.perf_counter() - t0 - a)
+    plain_wall = time.perf_counter() - t0
+    # the served system under the same arrivals of the same requests
+    with serving.Server(slots=cfg["slots"]) as srv:
+        futs = []
+        _replay(arr_p, lambda k, ts: futs.append(srv.submit(reqs[k], t_submit=ts)))
+        served_at_plain = [f.result().latency_s for f in futs]
+    n_stage = len(service) + m
+    pct = serving.percentile
     return {
         "metric": "served cases/s (continuous batching, mixed precision), saturated request stream",
-        "value": served_rate, "unit": "cases/s", "n_gpus": 1, "steps": len(reqs), "warmup": 1,
+        "value": served_rate, "unit": "cases/s", "n_gpus": 1, "steps": len(reqs), "warmup": 8,
         "ms_per_step": 1e3 * t_sat / len(reqs), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 (traversal), f32+f64 (radiosity)", "data": "synthetic",
         "config": {"workload": cfg["workload"], "requests": len(reqs), "slots": cfg["slots"],
-                   "stream_seed": cfg["stream_seed"], "hbm_peak_reserved_GB": peak_reserved / 1e9},
+                   "stream_seed": cfg["stream_seed"], "hbm_peak_reserved_GB": peak_reserved / 1e9,
+                   "geometry": "requests carry generator specs; each worker generates its geometry on the device"},
         "rays_per_s_served": rays / t_sat,
-        "plain": {"cases_per_s": plain_rate, "p50_s": serving.percentile(service, 50)},
+        "saturated_latency_s": {"p50": pct([r.latency_s for r in sat], 50),
+                                "p99": pct([r.latency_s for r in sat], 99)},
+        "poisson": {"rate_per_s": lam, "requests": len(reqs), "served_p50_s": pct(lat, 50),
+                    "served_p99_s": pct(lat, 99), "results_equal_to_saturated_run": same},
+        "plain": {"cases_per_s": plain_rate, "service_s_first3": service, "requests": m,
+                  "stages_s_per_case": {k: v / n_stage for k, v in stages.items()},
+                  "poisson_rate_per_s": lam_p, "p50_s": pct(plain_done, 50), "p95_s": pct(plain_done, 95),
+                  "max_s": max(plain_done), "wall_s": plain_wall,
+                  "latency": "measured: one FIFO worker running the drop-in NumPy path on real-time arrivals"},
+        "served_at_plain_rate": {"p50_s": pct(served_at_plain, 50), "p95_s": pct(served_at_plain, 95),
+                                 "max_s": max(served_at_plain)},
         "served_over_plain": served_rate / plain_rate,
-        "served_from_specs": {"cases_per_s": len(spec_reqs) / t_spec, "results_identical": spec_same,
-                              "host_generation_s_per_case": host_gen_s / len(specs),
-                              "note": "requests carry (archetype, N, phi, seed, axis); the serving worker "
-                                      "generates the geometry on the device (geometry.make_device)"},
-        "saturated_latency_s": {"p50": serving.percentile(sat_lat, 50), "p99": serving.percentile(sat_lat, 99)},
-        "poisson": {"rate_per_s": lam, "served_p50_s": serving.percentile(lat, 50),
-                    "served_p99_s": serving.percentile(lat, 99),
-                    "plain_p50_s": serving.percentile(plain_lat, 50), "plain_p99_s": serving.percentile(plain_lat, 99),
-                    "plain_latency": "FIFO queue over the measured plain service times"},
         "clocks": clocks.summary(), "gpu_launches": int(launches),
     }
 
