@@ -25,7 +25,7 @@ INCLUDE = PKG.parent / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr", "-I", str(INCLUDE)]
-SOURCES = ["patches.cu", "trace.cu", "operator.cu", "radiosity.cu", "capi.cu", "timers.cu", "arena.cu", "coupled.cu", "multibounce.cu", "descriptors.cu", "generate.cu", "archetypes.cu"]
+SOURCES = ["patches.cu", "trace.cu", "operator.cu", "radiosity.cu", "capi.cu", "timers.cu", "arena.cu", "coupled.cu", "multibounce.cu", "descriptors.cu", "generate.cu", "archetypes.cu", "hostcopy.cu"]
 STRICT_FP = {"trace.cu", "patches.cu", "multibounce.cu", "generate.cu", "archetypes.cu"}
 
 

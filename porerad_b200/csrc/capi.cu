@@ -248,11 +248,11 @@ int pr_counts_copy(const pr_counts* k, int32_t* origin, int32_t* receiver, int64
                                                                              origin ? o.ptr : nullptr,
                                                                              count ? cn.ptr : nullptr);
     PR_CUDA(cudaGetLastError());
-    if (origin) PR_CUDA(cudaMemcpyAsync(origin, o.ptr, m * 4, cudaMemcpyDefault, s));
-    if (count) PR_CUDA(cudaMemcpyAsync(count, cn.ptr, m * 8, cudaMemcpyDefault, s));
+    if (origin) PR_TRY(copy_to_host(origin, o.ptr, m * 4, s));
+    if (count) PR_TRY(copy_to_host(count, cn.ptr, m * 8, s));
   }
-  if (receiver && m > 0) PR_CUDA(cudaMemcpyAsync(receiver, c.col.ptr, m * 4, cudaMemcpyDefault, s));
-  if (rays_per_origin && n > 0) PR_CUDA(cudaMemcpyAsync(rays_per_origin, k->rays.ptr, n * 8, cudaMemcpyDefault, s));
+  if (receiver && m > 0) PR_TRY(copy_to_host(receiver, c.col.ptr, m * 4, s));
+  if (rays_per_origin && n > 0) PR_TRY(copy_to_host(rays_per_origin, k->rays.ptr, n * 8, s));
   PR_CUDA(cudaStreamSynchronize(s));
   return PR_OK;
 }
@@ -285,9 +285,9 @@ int pr_counts_rows(const pr_counts* k, int64_t row_begin, int64_t row_end, int64
                                                                                 count ? cn.ptr : nullptr);
     PR_CUDA(cudaGetLastError());
   }
-  if (origin) PR_CUDA(cudaMemcpyAsync(origin, o.ptr, m * 4, cudaMemcpyDefault, s));
-  if (count) PR_CUDA(cudaMemcpyAsync(count, cn.ptr, m * 8, cudaMemcpyDefault, s));
-  if (receiver) PR_CUDA(cudaMemcpyAsync(receiver, c.col.ptr + bounds[0], m * 4, cudaMemcpyDefault, s));
+  if (origin) PR_TRY(copy_to_host(origin, o.ptr, m * 4, s));
+  if (count) PR_TRY(copy_to_host(count, cn.ptr, m * 8, s));
+  if (receiver) PR_TRY(copy_to_host(receiver, c.col.ptr + bounds[0], m * 4, s));
   PR_CUDA(cudaStreamSynchronize(s));
   return PR_OK;
 }

@@ -61,6 +61,12 @@ void retain_pool_memory();
 int arena_alloc(size_t bytes, cudaStream_t s, void** out, int* dev);
 void arena_free(void* p, size_t bytes, cudaStream_t s, int dev);
 
+// Copy bytes from the device to host memory after the work queued on stream s, and return
+// once they are there.  Large copies into pageable memory run through pinned staging buffers
+// and host threads (hostcopy.cu); everything else is one cudaMemcpyAsync (the caller then
+// synchronises the stream as before).
+int copy_to_host(void* dst, const void* src, size_t bytes, cudaStream_t s);
+
 // A device allocation owned by the library, released in stream order (to the cache).
 template <typename T>
 struct DevBuf {

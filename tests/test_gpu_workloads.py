@@ -116,3 +116,28 @@ def test_count_rows_edges_and_errors():
         with pytest.raises(ValueError, match="row range"):
             table.rows(b, e)
     table.close()
+
+
+def test_large_count_copies_to_pageable_and_pinned_memory_agree():
+    """Count arrays above 16 MB copied into pageable NumPy memory (pinned staging buffers, host
+    threads) equal the same arrays copied straight into pinned memory."""
+
+    import ctypes
+
+    import torch
+
+    from porerad_b200 import _lib, view_factors as vf
+    from tests.helpers import load_canonical
+
+    p = vf.build_surface_patches(load_canonical("FA_canonical_phi0.10_N128"), 0.01)
+    table = vf.first_hit_counts_pooled(p, 64, [11, 12])
+    o, r, c = table.to_numpy()
+    assert o.nbytes > (16 << 20) and o.size == table.nnz
+    pinned = [torch.empty(table.nnz, dtype=dt).pin_memory() for dt in (torch.int32, torch.int32, torch.int64)]
+    _lib.check(_lib.load().pr_counts_copy(table.handle, *[t.data_ptr() for t in pinned], None, _lib.stream()))
+    for got, want in zip((o, r, c), pinned):
+        assert np.array_equal(got, want.numpy())
+    b = table.n_patches // 3
+    for got, want in zip(table.rows(b, table.n_patches), (o, r, c)):
+        assert np.array_equal(got, want[o >= b])
+    table.close()
