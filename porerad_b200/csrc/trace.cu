@@ -575,16 +575,18 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const Wa
 #pragma unroll 1
       for (int b = 0; b < kBurst; ++b) {
         if (!active) continue;
-        int32_t cell[kLook], code[kLook];  // each recorded cell and its hit code
-        int m = 0;      // cells recorded
-        int stop = 0;   // 0 none, 1 wall at position m, 2 step cap at position m
+        int32_t cell[kLook];  // each recorded cell
+        int fc[kLook];        // and the face the ray entered it through (-1: its first cell)
+        int m = 0;            // cells recorded; while nothing stopped the round, m == p at step p
+        int stop = 0;         // 0 none, 1 wall at position m, 2 step cap at position m
         int32_t wall_code = -1;
+        const int left = cap - it;  // cells the step cap still allows
 #pragma unroll
         for (int p = 0; p < kLook; ++p) {
           cell[p] = 0;
-          code[p] = -1;
-          if (stop == 0 && m == p) {
-            if (it + p >= cap) {
+          fc[p] = -1;
+          if (stop == 0) {
+            if (p >= left) {
               stop = 2;
             } else if ((unsigned)i >= (unsigned)nx) {
               const int wj = (int)imod((int64_t)floor(pr_add(pool.eoy[lane], pr_mul(pool.edy[lane], t))), ny);
@@ -593,14 +595,14 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const Wa
               stop = 1;
             } else {
               cell[p] = (i * ny + jj) * nz + kk;
-              code[p] = face >= 0 ? cell[p] * 6 + face : -1;
+              fc[p] = face;
               m = p + 1;
-              double tn = tx;
-              if (ty < tn) tn = ty;
-              if (tz < tn) tn = tz;
-              const bool cx = fabs(pr_sub(tx, tn)) <= PR_TIE;
-              const bool cy = fabs(pr_sub(ty, tn)) <= PR_TIE;
-              const bool cz = fabs(pr_sub(tz, tn)) <= PR_TIE;
+              // t_next = min(tx, ty, tz); every axis within the tie tolerance of it is crossed.
+              // t_a >= t_next, so t_a - t_next is never negative and needs no absolute value.
+              const double tn = fmin(fmin(tx, ty), tz);
+              const bool cx = pr_sub(tx, tn) <= PR_TIE;
+              const bool cy = pr_sub(ty, tn) <= PR_TIE;
+              const bool cz = pr_sub(tz, tn) <= PR_TIE;
               if (cx) {
                 i += sx;
                 tx = pr_add(tx, ddx);
@@ -625,23 +627,27 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const Wa
         uint32_t word[kLook];
 #pragma unroll
         for (int p = 0; p < kLook; ++p) word[p] = p < m ? __ldg(occ + (cell[p] >> 5)) : 0u;
-        int32_t hit = -2;
-        int used = m;
+        // the first solid cell among the recorded ones decides; its hit code is its
+        // cell_face_patch index (cell * 6 + entry face), -1 for a ray starting inside solid
+        bool solid = false;
+        int hcell = 0, hface = -1, used = m;
 #pragma unroll
         for (int p = kLook - 1; p >= 0; --p) {
           if (p < m && ((word[p] >> (cell[p] & 31)) & 1u)) {
-            hit = code[p];  // the cell_face_patch index
+            solid = true;
+            hcell = cell[p];
+            hface = fc[p];
             used = p + 1;
           }
         }
-        if (hit == -2) {
-          if (stop == 1) {
-            hit = wall_code;
-            used = m + 1;
-          } else if (stop == 2) {
-            hit = -1;
-            used = m;
-          }
+        int32_t hit = -2;
+        if (solid) {
+          hit = hface >= 0 ? hcell * 6 + hface : -1;
+        } else if (stop == 1) {
+          hit = wall_code;
+          used = m + 1;
+        } else if (stop == 2) {
+          hit = -1;
         }
         it += used;
         if (hit != -2) {

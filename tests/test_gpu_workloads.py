@@ -122,8 +122,6 @@ def test_large_count_copies_to_pageable_and_pinned_memory_agree():
     """Count arrays above 16 MB copied into pageable NumPy memory (pinned staging buffers, host
     threads) equal the same arrays copied straight into pinned memory."""
 
-    import ctypes
-
     import torch
 
     from porerad_b200 import _lib, view_factors as vf
