@@ -153,6 +153,16 @@ __device__ __forceinline__ int64_t imod(int64_t a, int64_t n) {
   return m < 0 ? m + n : m;
 }
 
+// imod for a value given as a binary64 integer (a floor) and n < 2^31: 32-bit arithmetic when
+// the value fits in 32 bits (every wrap of a ray's coordinate in practice), else imod.
+__device__ __forceinline__ int imod_floor(double f, int n) {
+  if (fabs(f) < 2147483647.0) {
+    const int m = (int)f % n;
+    return m < 0 ? m + n : m;
+  }
+  return (int)imod((int64_t)f, (int64_t)n);
+}
+
 // First patch hit by the ray, or -1 when it resolves none (the reference's
 // failed flag); *steps counts the cells visited.
 __device__ int32_t dda_first_hit(const Geom& g, double ox, double oy, double oz, double dx, double dy,
@@ -437,9 +447,17 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const Wa
         base_m = m0;
         if (lane < cnt) {
           const int64_t gq = g0 + lane;
-          const int sq = (int)(gq / npR);
-          const int64_t rem = gq - (int64_t)sq * npR;
-          const int64_t p = C.p0 + rem / C.R;
+          // seed block and patch of ray gq without 64-bit divisions per lane: from the batch's
+          // (s0, rem0), at most a few seed blocks further (32 rays per batch)
+          int sq = s0;
+          int64_t rem = (g0 - (int64_t)s0 * npR) + lane;
+          while (rem >= npR) {
+            rem -= npR;
+            ++sq;
+          }
+          const int64_t p = C.p0 + (rem < (int64_t)UINT32_MAX && C.R < (int64_t)UINT32_MAX
+                                        ? (int64_t)((uint32_t)rem / (uint32_t)C.R)
+                                        : rem / C.R);
           pr_u128 st;
           if (sq == s0) {
             st = pr_u128_affine(maps0[kMapSmall + 2 * lane], maps0[kMapSmall + 2 * lane + 1], base_st);
@@ -459,8 +477,8 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const Wa
             axis_setup(oy, dy, j0, sj, b, db);
             axis_setup(oz, dz, k0, sk, e, de);
             ci = (int)max((int64_t)-1, min(i0, (int64_t)nx));
-            cj = (int)imod(j0, ny);
-            ck = (int)imod(k0, nz);
+            cj = imod_floor((double)j0, ny);
+            ck = imod_floor((double)k0, nz);
             double scale = pr_add(pr_mul(pr_mul(8.0, (double)nx),
                                          pr_add(1.0, pr_div(pr_add(fabs(dy), fabs(dz)), fabs(dx)))), 100.0);
             if (scale > 100000000.0) scale = 100000000.0;
@@ -520,8 +538,8 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const Wa
           ++it;
           if ((unsigned)i >= (unsigned)nx) {
             // hit code of a wall: 6 n_cells + (0 hot | ny nz cold) + j nz + k
-            const int wj = (int)imod((int64_t)floor(pr_add(pool.eoy[lane], pr_mul(pool.edy[lane], t))), ny);
-            const int wk = (int)imod((int64_t)floor(pr_add(pool.eoz[lane], pr_mul(pool.edz[lane], t))), nz);
+            const int wj = imod_floor(floor(pr_add(pool.eoy[lane], pr_mul(pool.edy[lane], t))), ny);
+            const int wk = imod_floor(floor(pr_add(pool.eoz[lane], pr_mul(pool.edz[lane], t))), nz);
             hit = 6 * nx * ny * nz + (i < 0 ? 0 : ny * nz) + wj * nz + wk;
           } else {
             const int row = i * ny + jj;
@@ -589,8 +607,8 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const Wa
             if (p >= left) {
               stop = 2;
             } else if ((unsigned)i >= (unsigned)nx) {
-              const int wj = (int)imod((int64_t)floor(pr_add(pool.eoy[lane], pr_mul(pool.edy[lane], t))), ny);
-              const int wk = (int)imod((int64_t)floor(pr_add(pool.eoz[lane], pr_mul(pool.edz[lane], t))), nz);
+              const int wj = imod_floor(floor(pr_add(pool.eoy[lane], pr_mul(pool.edy[lane], t))), ny);
+              const int wk = imod_floor(floor(pr_add(pool.eoz[lane], pr_mul(pool.edz[lane], t))), nz);
               wall_code = 6 * nx * ny * nz + (i < 0 ? 0 : ny * nz) + wj * nz + wk;
               stop = 1;
             } else {
