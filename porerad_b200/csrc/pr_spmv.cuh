@@ -274,16 +274,46 @@ __global__ void __launch_bounds__(kBlkThreads, 1) k_spmv_blk(SymView S, BlkView 
     }
     __syncthreads();
     const int b0 = g * k, b1 = min(B.nb, b0 + k);
-    for (int64_t base = r0 + (int64_t)warp * kGroups; base < r1; base += (int64_t)nwarps * kGroups) {
-      const int64_t i = base + grp;  // warp-uniform loop; a group past the end adds nothing
-      int64_t qb = 0, qe = 0;
+    // entries [qb, qe) of row i in this stage's column blocks (empty past the CTA's rows)
+    auto bounds = [&](int64_t i, int64_t& qb, int64_t& qe) {
+      qb = qe = 0;
       if (i < r1) {
         const int64_t rb = S.row_ptr[i];
         qb = b0 == 0 ? rb : rb + B.seg[(int64_t)(b0 - 1) * S.n + i];
         qe = b1 == B.nb ? S.row_ptr[i + 1] : rb + B.seg[(int64_t)(b1 - 1) * S.n + i];
       }
-      const Acc part = seg_sum<kMode, G, Acc>(S, qb, qe, xs, (uint32_t)c0, gl);
+    };
+    // The group's leader asks L2 for a row segment two iterations before the group sums it, so
+    // the sums read L2 instead of waiting on DRAM (a bulk prefetch of the segment's 16-byte
+    // quads; the entry arrays are padded to whole quads).
+    auto prefetch = [&](int64_t qb, int64_t qe) {
+      if (gl != 0 || qe <= qb) return;
+      const int64_t a0 = (qb >> 2) << 4, a1 = ((qe + 3) >> 2) << 4;  // byte range of the quads
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"((const char*)S.words + a0),
+                   "r"((unsigned)(a1 - a0))
+                   : "memory");
+      if constexpr (kMode == kCounts)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"((const char*)S.cnt + a0),
+                     "r"((unsigned)(a1 - a0))
+                     : "memory");
+    };
+    const int64_t stride = (int64_t)nwarps * kGroups;
+    int64_t i = r0 + (int64_t)warp * kGroups + grp;  // warp-uniform loop over base = i - grp
+    int64_t qb0, qe0, qb1, qe1;
+    bounds(i, qb0, qe0);
+    bounds(i + stride, qb1, qe1);
+    prefetch(qb0, qe0);
+    prefetch(qb1, qe1);
+    for (; i - grp < r1; i += stride) {
+      int64_t qb2, qe2;
+      bounds(i + 2 * stride, qb2, qe2);
+      const Acc part = seg_sum<kMode, G, Acc>(S, qb0, qe0, xs, (uint32_t)c0, gl);
       if (gl == 0 && i < r1) acc[i - r0] = g == 0 ? part : acc[i - r0] + part;
+      prefetch(qb2, qe2);
+      qb0 = qb1;
+      qe0 = qe1;
+      qb1 = qb2;
+      qe1 = qe2;
     }
     __syncthreads();
   }
