@@ -134,6 +134,7 @@ def coarse_source(cell_power_W: np.ndarray, bins: int = 8) -> np.ndarray:
     return out
 
 
+@dataclass
 class PrescribedChannels:
     """Radiation channels (W m^-2) under the prescribed linear field, q_h + q_c + q_i = 0 (coupled.py:156-167).
 
