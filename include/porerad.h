@@ -160,6 +160,15 @@ PR_API void pr_counts_destroy(pr_counts* k);
 PR_API int pr_operator_create(const pr_counts* counts, const int64_t* rays_per_origin,
                        const double* patch_area_m2, double support_diagonal_fraction,
                        double balance_tolerance, void* stream, pr_operator** out);
+/* pr_operator_create for n_ops count tables at once (batched sweeps): each operator is
+ * assembled as pr_operator_create does, then the balancing iterations of all of them run in
+ * lockstep, one launch making one product of every operator still iterating.  Each out[k]
+ * equals pr_operator_create of the same inputs bit for bit; out[k] is set only when every
+ * operator succeeds (the first failure's status is returned). */
+PR_API int pr_operator_create_batch(const pr_counts* const* counts, const int64_t* const* rays_per_origin,
+                                    const double* const* patch_area_m2, int n_ops,
+                                    double support_diagonal_fraction, double balance_tolerance,
+                                    void* stream, pr_operator** out);
 /* scale (P) f64 = ExchangeOperator.scale; the others as the attributes of the same names;
  * nnz_counts = pooled (origin, receiver) pairs, nnz_symmetric = entries of S on the union
  * pattern, spmv_calls = sparse products made with this operator so far. */

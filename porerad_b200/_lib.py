@@ -112,6 +112,7 @@ _SIGNATURES = {
     "pr_counts_merge": (_i32, [_vp, _vp, _vp, ctypes.POINTER(_vp)]),
     "pr_counts_destroy": (None, [_vp]),
     "pr_operator_create": (_i32, [_vp, _vp, _vp, _f64, _f64, _vp, ctypes.POINTER(_vp)]),
+    "pr_operator_create_batch": (_i32, [_vp, _vp, _vp, _i32, _f64, _f64, _vp, _vp]),
     "pr_operator_info": (_i32, [_vp, _vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32), ctypes.POINTER(_f64),
                                 ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     "pr_operator_apply": (_i32, [_vp, _i32, _vp, _vp, _vp]),

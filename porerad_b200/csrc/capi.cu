@@ -29,6 +29,8 @@ int counts_from_edges(const int32_t* origin, const int32_t* receiver, const int6
 int counts_merge(const pr_counts* A, const pr_counts* B, cudaStream_t s, pr_counts** out);
 int operator_create(const pr_counts* k, const int64_t* rays, const double* area, double delta, double tol,
                     cudaStream_t s, pr_operator** out);
+int operators_create_batch(const pr_counts* const* counts, const int64_t* const* rays, const double* const* area,
+                           int n_ops, double delta, double tol, cudaStream_t s, pr_operator** out);
 int apply(const pr_operator* op, int which, const double* x, double* y, cudaStream_t s);
 int reciprocity_error(const pr_operator* op, double* out, cudaStream_t s);
 int operator_edges(const pr_operator* op, int32_t* origin, int32_t* receiver, double* weight, cudaStream_t s);
@@ -326,6 +328,26 @@ int pr_operator_create(const pr_counts* counts, const int64_t* rays_per_origin, 
   PR_ENTRY_GUARD(counts);
   return operator_create(counts, rays_per_origin, patch_area_m2, support_diagonal_fraction, balance_tolerance,
                          (cudaStream_t)stream, out);
+}
+
+int pr_operator_create_batch(const pr_counts* const* counts, const int64_t* const* rays_per_origin,
+                             const double* const* patch_area_m2, int n_ops, double support_diagonal_fraction,
+                             double balance_tolerance, void* stream, pr_operator** out) {
+  PR_CHECK_NULL(out, "out");
+  PR_ARG(n_ops >= 0, "n_ops must not be negative");
+  if (n_ops == 0) return PR_OK;
+  PR_CHECK_NULL(counts, "counts");
+  PR_CHECK_NULL(rays_per_origin, "rays_per_origin");
+  PR_CHECK_NULL(patch_area_m2, "patch_area_m2");
+  for (int k = 0; k < n_ops; ++k) {
+    out[k] = nullptr;
+    PR_ARG(counts[k] && rays_per_origin[k] && patch_area_m2[k], "operator %d: counts, rays and areas must not be NULL",
+           k);
+    PR_ARG(counts[k]->device == counts[0]->device, "count tables live on different devices");
+  }
+  PR_ENTRY_GUARD(counts[0]);
+  return operators_create_batch(counts, rays_per_origin, patch_area_m2, n_ops, support_diagonal_fraction,
+                                balance_tolerance, (cudaStream_t)stream, out);
 }
 
 int pr_operator_info(const pr_operator* op, double* scale, int* balance_method, int* balance_iterations,

@@ -738,11 +738,10 @@ static int balance_eval(pr_operator* op, BalanceWork& w, const double* y, double
   return PR_OK;
 }
 
-static int balance(pr_operator* op, double tol, cudaStream_t s) {
-  const int64_t n = op->n;
+static int balance_multiplicative(pr_operator* op, BalanceWork& w, double tol, cudaStream_t s);
+
+static int balance_work(BalanceWork& w, int64_t n, cudaStream_t s) {
   const int M = 10;
-  const double beta = 0.5;
-  BalanceWork w;
   w.n = n;
   PR_TRY(w.y.alloc(n, s));
   PR_TRY(w.y2.alloc(n, s));
@@ -751,10 +750,19 @@ static int balance(pr_operator* op, double tol, cudaStream_t s) {
   PR_TRY(w.dY.alloc((size_t)M * n, s));
   PR_TRY(w.dF.alloc((size_t)M * n, s));
   PR_TRY(w.sc.alloc(4, s));
-  const int rg = red_grid();
-  PR_TRY(w.partial.alloc((size_t)rg * 20, s));
+  PR_TRY(w.partial.alloc((size_t)red_grid() * 20, s));
   PR_TRY(w.dots.alloc(20, s));
   PR_CUDA(cudaMemsetAsync(w.y.ptr, 0, n * sizeof(double), s));
+  return PR_OK;
+}
+
+static int balance(pr_operator* op, double tol, cudaStream_t s) {
+  const int64_t n = op->n;
+  const int M = 10;
+  const double beta = 0.5;
+  BalanceWork w;
+  PR_TRY(balance_work(w, n, s));
+  const int rg = red_grid();
   BalanceScalars sc;
   PR_TRY(balance_eval(op, w, w.y.ptr, nullptr, 0, nullptr, &sc, s));
   PR_CUDA(cudaStreamSynchronize(s));
@@ -827,7 +835,14 @@ static int balance(pr_operator* op, double tol, cudaStream_t s) {
     }
   }
   if (aa_ok) return PR_OK;
-  // ---- damped multiplicative iteration from y = 0 (exchange.py:185-196)
+  return balance_multiplicative(op, w, tol, s);
+}
+
+// Damped multiplicative iteration from y = 0 (exchange.py:185-196): the fallback when Anderson
+// acceleration does not reach the acceptance tolerance.
+static int balance_multiplicative(pr_operator* op, BalanceWork& w, double tol, cudaStream_t s) {
+  const int64_t n = op->n;
+  BalanceScalars sc;
   PR_CUDA(cudaMemsetAsync(w.y.ptr, 0, n * sizeof(double), s));
   double* y = w.y.ptr;
   double* y_next = w.y2.ptr;
@@ -849,6 +864,162 @@ static int balance(pr_operator* op, double tol, cudaStream_t s) {
   }
   set_error("diagonal balancing of the exchange matrix did not converge");
   return PR_ERR_BALANCE;
+}
+
+// Anderson balancing of several operators in lockstep (the iteration of balance(), operator by
+// operator the same steps): every iteration makes one product of each operator still iterating,
+// all in one launch of the batched blocked product, and takes one host round trip for all of
+// them.  A sweep of many small operators then fills the GPU with one grid per iteration instead
+// of one operator's grid per stream.  Operators that Anderson does not settle fall back to the
+// multiplicative iteration one at a time, as in balance().  Every operator must be blocked and of
+// storage mode kMode.
+template <int kMode>
+static int balance_batch(const std::vector<pr_operator*>& ops, double tol, cudaStream_t s) {
+  const int m = (int)ops.size();
+  if (m == 0) return PR_OK;
+  const int M = 10;
+  const double beta = 0.5, eps = 2.220446049250313e-16;
+  const double accept = fmin(fmax(10.0 * tol, 10.0 * eps), 1.0e-10);  // exchange.py:180
+  struct State {
+    BalanceWork w;
+    double G[10][10] = {{0}}, b[10] = {0};
+    int cols = 0, oldest = 0, iters = 0, slot = 0;
+    double* y = nullptr;
+    double* y_next = nullptr;
+    bool active = false, done = false;
+    BalanceScalars sc{};
+    double dots[20] = {0};
+  };
+  std::vector<State> st(m);
+  for (int k = 0; k < m; ++k) {
+    PR_TRY(balance_work(st[k].w, ops[k]->n, s));
+    st[k].y = st[k].w.y.ptr;
+    st[k].y_next = st[k].w.y2.ptr;
+  }
+  DevBuf<BlkItem<double, BalanceEpi>> items;
+  PR_TRY(items.alloc(m, s));
+  // one product of each listed operator at y[k] (differences into dF_out[k] when given)
+  auto products = [&](const std::vector<int>& which, const std::vector<double*>& ys,
+                      const std::vector<double*>& dF_out) -> int {
+    std::vector<const SymCsr*> mats;
+    std::vector<const double*> xs;
+    std::vector<BalanceEpi> epis;
+    for (size_t j = 0; j < which.size(); ++j) {
+      pr_operator* op = ops[which[j]];
+      BalanceWork& w = st[which[j]].w;
+      PR_CUDA(cudaMemsetAsync(w.sc.ptr, 0, 4 * sizeof(double), s));
+      ::pr::launch_mark(), k_exp_scale<<<grid_for(op->n, 256), 256, 0, s>>>(ys[j], op->n, w.d.ptr, w.sc.ptr);
+      mats.push_back(&op->S);
+      xs.push_back(w.d.ptr);
+      epis.push_back(BalanceEpi{op->delta, op->area.ptr, ys[j], w.d.ptr, w.f.ptr, dF_out[j], w.sc.ptr, 0, nullptr});
+      op->spmv_calls++;
+    }
+    PR_CUDA(cudaGetLastError());
+    ::pr::timer_begin(kTimerBalance, s);
+    const int rc = launch_spmv_batch<kMode, double>(mats, xs, epis, items.ptr, s);
+    ::pr::timer_end(kTimerBalance, s);
+    PR_TRY(rc);
+    for (int k : which) PR_CUDA(cudaMemcpyAsync(&st[k].sc, st[k].w.sc.ptr, sizeof(BalanceScalars),
+                                                cudaMemcpyDeviceToHost, s));
+    return PR_OK;
+  };
+  // y = 0 for every operator
+  {
+    std::vector<int> all(m);
+    std::vector<double*> ys(m), none(m, nullptr);
+    for (int k = 0; k < m; ++k) {
+      all[k] = k;
+      ys[k] = st[k].y;
+    }
+    PR_TRY(products(all, ys, none));
+    PR_CUDA(cudaStreamSynchronize(s));
+  }
+  for (int k = 0; k < m; ++k) {
+    pr_operator* op = ops[k];
+    if (!(st[k].sc.bad > 0) && st[k].sc.closure <= tol) {  // exchange.py:157-159
+      op->method = PR_BALANCE_NONE;
+      op->iterations = 0;
+      PR_CUDA(cudaMemcpyAsync(op->scale.ptr, st[k].w.d.ptr, op->n * 8, cudaMemcpyDeviceToDevice, s));
+      st[k].done = true;
+    } else {
+      st[k].active = !(st[k].sc.bad > 0) && st[k].sc.max_f > tol;
+    }
+  }
+  const int rg = red_grid();
+  for (int it = 0; it < 500; ++it) {  // scipy.optimize.anderson maxiter of exchange.py:177
+    std::vector<int> which;
+    std::vector<double*> ys, dFs;
+    for (int k = 0; k < m; ++k) {
+      State& q = st[k];
+      if (!q.active) continue;
+      const int64_t n = ops[k]->n;
+      AAStep step;
+      step.cols = q.cols;
+      step.beta = beta;
+      double gamma[10] = {0};
+      if (q.cols > 0) {
+        double Hf[100];
+        for (int i = 0; i < q.cols; ++i)
+          for (int j = 0; j < q.cols; ++j) Hf[i * q.cols + j] = q.G[i][j];
+        solve_gram(q.cols, Hf, q.b, gamma);
+      }
+      for (int c = 0; c < 10; ++c) step.gamma[c] = c < q.cols ? gamma[c] : 0.0;
+      if (q.cols < M) {
+        q.slot = q.cols;
+      } else {
+        q.slot = q.oldest;
+        q.oldest = (q.oldest + 1) % M;
+      }
+      step.slot = q.slot;
+      ::pr::launch_mark(), k_aa_update<<<grid_for(n, 256), 256, 0, s>>>(step, q.y, q.w.f.ptr, q.w.dY.ptr, q.w.dF.ptr, n,
+                                                                      q.y_next, q.w.dY.ptr);
+      which.push_back(k);
+      ys.push_back(q.y_next);
+      dFs.push_back(q.w.dF.ptr + (size_t)q.slot * n);
+    }
+    if (which.empty()) break;
+    PR_CUDA(cudaGetLastError());
+    PR_TRY(products(which, ys, dFs));
+    for (int k : which) {
+      State& q = st[k];
+      ++q.iters;
+      std::swap(q.y, q.y_next);
+      if (q.cols < M) ++q.cols;
+      ::pr::launch_mark(), k_aa_dots<<<rg, 256, 0, s>>>(q.w.dF.ptr, q.w.f.ptr, ops[k]->n, q.cols, q.slot,
+                                                        q.w.partial.ptr);
+      PR_TRY(sum_partials(q.w.partial.ptr, rg, 20, q.w.dots.ptr, s));
+      PR_CUDA(cudaMemcpyAsync(q.dots, q.w.dots.ptr, sizeof(q.dots), cudaMemcpyDeviceToHost, s));
+    }
+    PR_CUDA(cudaGetLastError());
+    PR_CUDA(cudaStreamSynchronize(s));
+    for (int k : which) {
+      State& q = st[k];
+      if (q.sc.bad > 0 || !std::isfinite(q.sc.max_f)) {
+        q.active = false;
+        continue;
+      }
+      for (int c = 0; c < q.cols; ++c) {
+        q.G[q.slot][c] = q.dots[c];
+        q.G[c][q.slot] = q.dots[c];
+        q.b[c] = q.dots[10 + c];
+      }
+      if (q.sc.max_f <= tol) q.active = false;
+    }
+  }
+  for (int k = 0; k < m; ++k) {
+    State& q = st[k];
+    if (q.done) continue;
+    pr_operator* op = ops[k];
+    if (q.y != q.w.y.ptr) PR_CUDA(cudaMemcpyAsync(q.w.y.ptr, q.y, op->n * 8, cudaMemcpyDeviceToDevice, s));
+    if (!(q.sc.bad > 0) && q.sc.max_f <= tol && q.sc.closure <= accept) {
+      PR_CUDA(cudaMemcpyAsync(op->scale.ptr, q.w.d.ptr, op->n * 8, cudaMemcpyDeviceToDevice, s));
+      op->method = PR_BALANCE_ANDERSON;
+      op->iterations = q.iters;
+    } else {
+      PR_TRY(balance_multiplicative(op, q.w, tol, s));
+    }
+  }
+  return PR_OK;
 }
 
 static bool all_equal_i64(const std::vector<int64_t>& v) {
@@ -981,10 +1152,11 @@ static int build_col_blocks(SymCsr& S, cudaStream_t s) {
 
 int apply(const pr_operator* op, int which, const double* x_dev, double* y_dev, cudaStream_t s);
 
-int operator_create(const pr_counts* k, const int64_t* rays, const double* area, double delta, double tol,
-                    cudaStream_t s, pr_operator** out) {
+// Everything of operator_create before the balancing: accounting, transpose, S', column blocks.
+static int operator_assemble(const pr_counts* k, const int64_t* rays, const double* area, double delta,
+                             cudaStream_t s, std::unique_ptr<pr_operator>& op) {
   const int64_t n = k->csr->n_rows;
-  std::unique_ptr<pr_operator> op(new pr_operator());
+  op.reset(new pr_operator());
   cudaGetDevice(&op->device);
   op->n = n;
   op->F = k->csr;
@@ -1056,15 +1228,19 @@ int operator_create(const pr_counts* k, const int64_t* rays, const double* area,
     }
     op->FT = T;  // kept for raw_rmatvec
   }
+  return PR_OK;
+}
+
+// Row closure of F_p (exchange.py:78-80) after the balancing.
+static int operator_closure(pr_operator* op, cudaStream_t s) {
+  const int64_t n = op->n;
   if (n > 0) {
-    PR_TRY(balance(op.get(), tol, s));
-    // row closure of F_p (exchange.py:78-80)
     DevBuf<double> ones, r;
     PR_TRY(ones.alloc(n, s));
     PR_TRY(r.alloc(n, s));
     std::vector<double> h1(n, 1.0);
     PR_CUDA(cudaMemcpyAsync(ones.ptr, h1.data(), n * 8, cudaMemcpyHostToDevice, s));
-    PR_TRY(apply(op.get(), PR_APPLY_MATVEC, ones.ptr, r.ptr, s));
+    PR_TRY(apply(op, PR_APPLY_MATVEC, ones.ptr, r.ptr, s));
     std::vector<double> hr(n);
     PR_CUDA(cudaMemcpyAsync(hr.data(), r.ptr, n * 8, cudaMemcpyDeviceToHost, s));
     PR_CUDA(cudaStreamSynchronize(s));
@@ -1077,7 +1253,38 @@ int operator_create(const pr_counts* k, const int64_t* rays, const double* area,
     }
   }
   PR_CUDA(cudaStreamSynchronize(s));
+  return PR_OK;
+}
+
+int operator_create(const pr_counts* k, const int64_t* rays, const double* area, double delta, double tol,
+                    cudaStream_t s, pr_operator** out) {
+  std::unique_ptr<pr_operator> op;
+  PR_TRY(operator_assemble(k, rays, area, delta, s, op));
+  if (op->n > 0) PR_TRY(balance(op.get(), tol, s));
+  PR_TRY(operator_closure(op.get(), s));
   *out = op.release();
+  return PR_OK;
+}
+
+// Several operators at once: each assembled as operator_create does, then the blocked operators
+// of each storage mode balanced together (balance_batch), the others one at a time; out[k] is
+// set only when every operator succeeds.
+int operators_create_batch(const pr_counts* const* counts, const int64_t* const* rays, const double* const* area,
+                           int n_ops, double delta, double tol, cudaStream_t s, pr_operator** out) {
+  std::vector<std::unique_ptr<pr_operator>> ops(n_ops);
+  for (int k = 0; k < n_ops; ++k) PR_TRY(operator_assemble(counts[k], rays[k], area[k], delta, s, ops[k]));
+  std::vector<pr_operator*> packed, counted;
+  for (int k = 0; k < n_ops; ++k) {
+    pr_operator* op = ops[k].get();
+    if (op->n == 0) continue;
+    if (op->S.blk.ready && op->S.mode == kPacked) packed.push_back(op);
+    else if (op->S.blk.ready && op->S.mode == kCounts) counted.push_back(op);
+    else PR_TRY(balance(op, tol, s));
+  }
+  PR_TRY(balance_batch<kPacked>(packed, tol, s));
+  PR_TRY(balance_batch<kCounts>(counted, tol, s));
+  for (int k = 0; k < n_ops; ++k) PR_TRY(operator_closure(ops[k].get(), s));
+  for (int k = 0; k < n_ops; ++k) out[k] = ops[k].release();
   return PR_OK;
 }
 

@@ -10,7 +10,9 @@
 //    block of columns at a time, so the random gathers become shared-memory loads; each
 //    row's sum accumulates block by block in shared memory.
 #pragma once
+#include <algorithm>
 #include <mutex>
+#include <vector>
 #include <type_traits>
 
 #include "pr_objects.cuh"
@@ -246,9 +248,10 @@ constexpr int kBlkSmemMax = 220 * 1024;  // dynamic shared memory of a blocked p
 // Stage g covers column blocks [g k, g k + k) (k = 2 for binary32 x, whose blocks are
 // half as many bytes), staged with 16-byte loads; groups of G lanes then take the CTA's
 // rows (32 / G rows in flight per warp: a row's segment of one stage is short).
+// The work of CTA `cta` of a blocked product (its row range B.cta_row[cta] .. B.cta_row[cta + 1]).
 template <int kMode, typename Acc, typename Tx, class Epi>
-__global__ void __launch_bounds__(kBlkThreads, 1) k_spmv_blk(SymView S, BlkView B, const Tx* __restrict__ x, Epi epi) {
-  if (epi.skip()) return;
+__device__ __forceinline__ void spmv_blk_cta(const SymView& S, const BlkView& B, const Tx* __restrict__ x,
+                                             const Epi& epi, int cta) {
   extern __shared__ __align__(16) unsigned char blk_smem[];
   constexpr int k = sizeof(Tx) == 4 ? 2 : 1;
   const int stage_cols = B.W * k;
@@ -256,7 +259,7 @@ __global__ void __launch_bounds__(kBlkThreads, 1) k_spmv_blk(SymView S, BlkView 
   Acc* acc = reinterpret_cast<Acc*>(blk_smem + (size_t)stage_cols * sizeof(Tx));
   constexpr int G = sizeof(Tx) == 4 ? 16 : 8;  // lanes per row segment
   constexpr int kGroups = 32 / G;
-  const int64_t r0 = B.cta_row[blockIdx.x], r1 = B.cta_row[blockIdx.x + 1];
+  const int64_t r0 = B.cta_row[cta], r1 = B.cta_row[cta + 1];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int grp = lane / G, gl = lane % G;
   const int stages = (B.nb + k - 1) / k;
@@ -326,6 +329,38 @@ __global__ void __launch_bounds__(kBlkThreads, 1) k_spmv_blk(SymView S, BlkView 
 }
 
 template <int kMode, typename Acc, typename Tx, class Epi>
+__global__ void __launch_bounds__(kBlkThreads, 1) k_spmv_blk(SymView S, BlkView B, const Tx* __restrict__ x, Epi epi) {
+  if (epi.skip()) return;
+  spmv_blk_cta<kMode, Acc>(S, B, x, epi, blockIdx.x);
+}
+
+// One product of each of several operators in one launch: item k owns the CTAs
+// [cta_begin_k, cta_begin_{k+1}) of the grid.  The epilogue must not index per-block storage by
+// blockIdx (BalanceEpi reduces with atomics only).
+template <typename Tx, class Epi>
+struct BlkItem {
+  SymView S;
+  BlkView B;
+  const Tx* x;
+  Epi epi;
+  int cta_begin;
+};
+
+template <int kMode, typename Acc, typename Tx, class Epi>
+__global__ void __launch_bounds__(kBlkThreads, 1) k_spmv_blk_batch(const BlkItem<Tx, Epi>* __restrict__ items,
+                                                                   int n_items) {
+  int lo = 0, hi = n_items - 1;  // the last item whose first CTA is at or before this one
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (items[mid].cta_begin <= (int)blockIdx.x) lo = mid;
+    else hi = mid - 1;
+  }
+  const BlkItem<Tx, Epi> it = items[lo];
+  if (it.epi.skip()) return;
+  spmv_blk_cta<kMode, Acc>(it.S, it.B, it.x, it.epi, (int)blockIdx.x - it.cta_begin);
+}
+
+template <int kMode, typename Acc, typename Tx, class Epi>
 inline int allow_blk_smem() {
   static std::mutex mu;
   static bool done[64] = {};
@@ -365,6 +400,56 @@ inline int launch_spmv(const SymCsr& S, const Tx* x, const Epi& epi, cudaStream_
   } else {
     ::pr::launch_mark(), k_spmv_rows<kMode, Acc, Tx, Epi><<<spmv_slots(S), 256, 0, s>>>(v, x, epi);
   }
+  PR_CUDA(cudaGetLastError());
+  return PR_OK;
+}
+
+template <int kMode, typename Acc, typename Tx, class Epi>
+inline int allow_blk_batch_smem() {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  PR_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev >= 0 && dev < 64 && done[dev]) return PR_OK;
+  PR_CUDA(cudaFuncSetAttribute(k_spmv_blk_batch<kMode, Acc, Tx, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kBlkSmemMax));
+  if (dev >= 0 && dev < 64) done[dev] = true;
+  return PR_OK;
+}
+
+// One product of each of the operators mats[k] (blocked, storage mode kMode) with xs[k] and
+// epilogue epis[k], all in one launch.  items is device scratch for mats.size() items.
+template <int kMode, typename Acc, typename Tx, class Epi>
+inline int launch_spmv_batch(const std::vector<const SymCsr*>& mats, const std::vector<const Tx*>& xs,
+                             const std::vector<Epi>& epis, BlkItem<Tx, Epi>* items, cudaStream_t s) {
+  const int n = (int)mats.size();
+  if (n == 0) return PR_OK;
+  constexpr int k = sizeof(Tx) == 4 ? 2 : 1;
+  std::vector<BlkItem<Tx, Epi>> h(n);
+  size_t smem = 0;
+  int ctas = 0;
+  for (int i = 0; i < n; ++i) {
+    const SymCsr& S = *mats[i];
+    if (!S.blk.ready || S.mode != kMode) {
+      set_error("batched product: operator %d is not a blocked operator of the batch's storage mode", i);
+      return PR_ERR_ARG;
+    }
+    if (((uintptr_t)S.words.ptr & 15u) || (kMode == kCounts && ((uintptr_t)S.cnt.ptr & 15u))) {
+      set_error("blocked product: the entry arrays are not 16-byte aligned");
+      return PR_ERR_CUDA;
+    }
+    h[i] = BlkItem<Tx, Epi>{sym_view(S), blk_view(S), xs[i], epis[i], ctas};
+    ctas += S.blk.ctas;
+    smem = std::max(smem, (size_t)S.blk.W * k * sizeof(Tx) + (size_t)S.blk.rows_cap * sizeof(Acc));
+  }
+  if (smem > (size_t)kBlkSmemMax) {
+    set_error("blocked product needs %zu bytes of shared memory", smem);
+    return PR_ERR_LIMIT;
+  }
+  PR_TRY((allow_blk_batch_smem<kMode, Acc, Tx, Epi>()));
+  PR_CUDA(cudaMemcpyAsync(items, h.data(), sizeof(BlkItem<Tx, Epi>) * n, cudaMemcpyHostToDevice, s));
+  ::pr::launch_mark(), k_spmv_blk_batch<kMode, Acc, Tx, Epi><<<ctas, kBlkThreads, smem, s>>>(items, n);
   PR_CUDA(cudaGetLastError());
   return PR_OK;
 }

@@ -66,7 +66,18 @@ class ExchangeOperator:
         finally:
             if own_table:
                 table.close()
-        self._h = _lib.Handle(out.value, "pr_operator_destroy")
+        self._adopt(out.value, area, support_diagonal_fraction, event_chunk_size)
+
+    @classmethod
+    def _from_handle(cls, handle: int, area: np.ndarray, support_diagonal_fraction: float,
+                     event_chunk_size: int = 4_000_000) -> "ExchangeOperator":
+        op = cls.__new__(cls)
+        op._adopt(handle, area, support_diagonal_fraction, event_chunk_size)
+        return op
+
+    def _adopt(self, handle: int, area: np.ndarray, support_diagonal_fraction: float, event_chunk_size: int) -> None:
+        n = int(area.size)
+        self._h = _lib.Handle(handle, "pr_operator_destroy")
         self.patch_area_m2 = area
         self.support_diagonal_fraction = float(support_diagonal_fraction)
         self.event_chunk_size = int(event_chunk_size)
@@ -91,6 +102,40 @@ class ExchangeOperator:
 
     def close(self) -> None:
         self._h.close()
+
+    @classmethod
+    def from_tables(cls, tables, rays_per_origin, patch_area_m2, *,
+                    support_diagonal_fraction: float = SUPPORT_DIAGONAL_FRACTION,
+                    balance_tolerance: float = 1.0e-11) -> list["ExchangeOperator"]:
+        """Operators of many device count tables built together (batched sweeps).
+
+        ``rays_per_origin`` and ``patch_area_m2`` hold one array per table.  The balancing
+        iterations of all operators run in lockstep with one product launch per iteration for all
+        of them; each operator equals ``ExchangeOperator(table, None, None, rays, area)`` bit for bit.
+        """
+
+        tables = list(tables)
+        m = len(tables)
+        rays = [np.ascontiguousarray(np.asarray(r, dtype=np.int64)) for r in rays_per_origin]
+        areas = [np.ascontiguousarray(np.asarray(a, dtype=np.float64).copy()) for a in patch_area_m2]
+        if not (len(rays) == len(areas) == m):
+            raise ValueError("one rays array and one area array per table")
+        for t, r, a in zip(tables, rays, areas):
+            if not isinstance(t, CountTable):
+                raise TypeError("from_tables takes device CountTables")
+            if not (t.n_patches == r.size == a.size):
+                raise ValueError("count table, rays_per_origin and patch_area_m2 disagree on the number of patches")
+        if m == 0:
+            return []
+        handles = (ctypes.c_void_p * m)(*[t.handle for t in tables])
+        rptr = (ctypes.c_void_p * m)(*[r.ctypes.data for r in rays])
+        aptr = (ctypes.c_void_p * m)(*[a.ctypes.data for a in areas])
+        out = (ctypes.c_void_p * m)()
+        _lib.check(_lib.load().pr_operator_create_batch(ctypes.addressof(handles), ctypes.addressof(rptr),
+                                                        ctypes.addressof(aptr), m, float(support_diagonal_fraction),
+                                                        float(balance_tolerance), _lib.stream(),
+                                                        ctypes.addressof(out)))
+        return [cls._from_handle(h, a, support_diagonal_fraction) for h, a in zip(out, areas)]
 
     @property
     def spmv_calls(self) -> int:

@@ -409,3 +409,40 @@ def test_per_patch_reduction_against_oracle(oracle, R, seeds):
     got = vf.first_hit_counts_pooled(p, R, seeds).to_numpy()
     for g, w in zip(got, want):
         assert np.array_equal(np.asarray(g), np.asarray(w))
+
+
+def test_operators_built_together_equal_operators_built_alone():
+    """ExchangeOperator.from_tables (operators assembled one by one, balancing iterations of all of
+    them in lockstep with one product launch per iteration) gives each operator bit for bit as
+    ExchangeOperator builds it alone: the four canonical 128^3 microstructures (blocked products)
+    and a small case (warp-per-row products, balanced on its own)."""
+
+    from porerad_b200 import exchange
+
+    vf = _vf()
+    tables, rays, areas = [], [], []
+    for name in ("FA", "FI", "OF", "TL"):
+        p = vf.build_surface_patches(load_canonical(f"{name}_canonical_phi0.10_N128"), 0.01)
+        tables.append(vf.first_hit_counts_pooled(p, 32, [101, 202]))
+        rays.append(np.full(p.n_patches, 64, np.int64))
+        areas.append(p.patch_area_m2)
+    case = load_small("cube20")
+    p = _patches(case)
+    R = int(case["rays_per_patch"])
+    tables.append(vf.first_hit_counts_pooled(p, R, [int(s) for s in case["seeds"]]))
+    rays.append(np.full(p.n_patches, R * len(case["seeds"]), np.int64))
+    areas.append(p.patch_area_m2)
+    together = exchange.ExchangeOperator.from_tables(tables, rays, areas)
+    for t, r, a, op in zip(tables, rays, areas, together):
+        alone = exchange.ExchangeOperator(t, None, None, r, a)
+        assert op.balance_method == alone.balance_method
+        assert op.balance_iterations == alone.balance_iterations
+        assert np.array_equal(op.scale, alone.scale)
+        assert op.row_sum_error == alone.row_sum_error
+        x = np.random.default_rng(3).random(op.n_patches)
+        assert np.array_equal(op.matvec(x), alone.matvec(x))
+        alone.close()
+        op.close()
+    with pytest.raises(ValueError):
+        exchange.ExchangeOperator.from_tables(tables[:2], rays[:1], areas[:2])
+    assert exchange.ExchangeOperator.from_tables([], [], []) == []
