@@ -50,8 +50,9 @@ WORKLOADS = {
                requests=200, plain_requests=24, stream_seed=2026, slots=4, H=0.01),
     "c3": dict(workload="batched sweep: 48 geometries = OF/FI/FA/TL x phi {0.05,0.10,0.20} x seeds 0-3, N=128^3, "
                         "500 rays/patch, eps from {0.3,0.6,0.9} and axis from {x,y,z} (RNG seed 3); all first-hit "
-                        "counts in shared persistent traversal launches, operators and mixed-precision solves "
-                        "overlapped on 4 streams",
+                        "counts in shared persistent traversal launches, all operators balanced together (one "
+                        "product launch per iteration for every operator), mixed-precision solves overlapped on "
+                        "4 streams",
                n=128, rays=500, phis=(0.05, 0.10, 0.20), seeds=4, H=0.01, T_m=700.0, dT=20.0, slots=4, pick_seed=3),
     "c5": dict(workload="coupled-size stress: TL and FA N=192^3 phi=0.10, 1000 rays/patch x sets A,B,C, eps 0.6, "
                         "T 690->710 K along x; then 20 solves at T_cell + N(0, 5 K) per voxel (seed 2) on the resident "
@@ -849,23 +850,26 @@ def run_c3(args, cfg):
     R, H = cfg["rays"], cfg["H"]
     streams = [torch.cuda.Stream() for _ in range(cfg["slots"])]
 
-    def solve(k, geo, table):
+    def solve(k, geo, op):
         with _lib.use_stream(streams[k % len(streams)]):
             p = vf.SurfacePatches(H_m=H, _device=geo)
-            op = exchange.ExchangeOperator(table, None, None, np.full(geo.n_patches, R, np.int64),
-                                           np.full(geo.n_patches, (H / cfg["n"]) ** 2))
             ch = coupled.prescribed_field_channels(op, p, cfg["T_m"], cfg["dT"], specs[k]["eps"], precision="mixed")
             op.close()
-            table.close()
             return ch
 
     def sweep():
         geos = [vf.DeviceGeometry(ph, H) for ph in dev_phases]
         pats = [vf.SurfacePatches(H_m=H, _device=g) for g in geos]
         tables = vf.first_hit_counts_batch(pats, R, seeds)
+        # the operators of all cases, their balancing iterations in shared product launches
+        ops = exchange.ExchangeOperator.from_tables(
+            tables, [np.full(g.n_patches, R, np.int64) for g in geos],
+            [np.full(g.n_patches, (H / cfg["n"]) ** 2) for g in geos])
+        for t in tables:
+            t.close()
         torch.cuda.synchronize()
         with concurrent.futures.ThreadPoolExecutor(cfg["slots"]) as ex:
-            chs = list(ex.map(lambda a: solve(*a), [(k, g, t) for k, (g, t) in enumerate(zip(geos, tables))]))
+            chs = list(ex.map(lambda a: solve(*a), [(k, g, o) for k, (g, o) in enumerate(zip(geos, ops))]))
         torch.cuda.synchronize()
         rays = sum(g.n_patches for g in geos) * R
         patches = [g.n_patches for g in geos]
