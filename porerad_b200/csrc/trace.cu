@@ -1041,6 +1041,7 @@ static const TraceVariant kVariants[] = {
     {k_trace_pool<4, 4, 2>, "4blk-look2x4"},
     {k_trace_pool<5, 8, 0>, "5blk-burst8"},
     {k_trace_pool<6, 4, 0>, "6blk-burst4"},
+    {k_trace_pool<7, 2, 3>, "7blk-look3x2"},
 };
 static constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 
