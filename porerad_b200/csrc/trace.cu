@@ -627,14 +627,14 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const Wa
                 face = sx > 0 ? 1 : 0;
               }
               if (cy) {
-                jj += sy;
-                jj = jj == ny ? 0 : (jj < 0 ? ny - 1 : jj);
+                jj += sy;  // periodic: ny -> 0 stepping up, -1 -> ny - 1 stepping down
+                if ((unsigned)jj >= (unsigned)ny) jj -= sy * ny;
                 ty = pr_add(ty, ddy);
                 if (!cx) face = sy > 0 ? 3 : 2;
               }
               if (cz) {
                 kk += sz;
-                kk = kk == nz ? 0 : (kk < 0 ? nz - 1 : kk);
+                if ((unsigned)kk >= (unsigned)nz) kk -= sz * nz;
                 tz = pr_add(tz, ddz);
                 if (!cx && !cy) face = sz > 0 ? 5 : 4;
               }
