@@ -166,16 +166,18 @@ struct BlkView {
 
 inline BlkView blk_view(const SymCsr& S) { return BlkView{S.blk.seg.ptr, S.blk.cta_row.ptr, S.blk.W, S.blk.nb}; }
 
-// Entries q .. q + 3 of one 16-byte quad of the word array (and of the count array in kCounts
-// mode): each entry inside [qb, qe) adds coefficient * xs[col - c0] to acc, in entry order.
+// Entries 0..3 of one 16-byte quad of the word array (and of the count array in kCounts mode):
+// entry e is summed when lo <= e < hi (the quad's part of the row segment), adding
+// coefficient * x[col] to acc in entry order.  xs0 points at x[0] of the staged block's
+// coordinates (the shared array shifted back by the block's first column), so x[col] is xs0[col].
 template <int kMode, typename Acc, typename Tx>
-__device__ __forceinline__ void quad_add(const SymView& S, const uint4& w, const int4& c, int64_t q, int64_t qb,
-                                         int64_t qe, const Tx* xs, uint32_t c0, Acc& acc) {
+__device__ __forceinline__ void quad_add(const SymView& S, const uint4& w, const int4& c, int lo, int hi,
+                                         const Tx* xs0, Acc& acc) {
   const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
   const int32_t cs[4] = {c.x, c.y, c.z, c.w};
 #pragma unroll
   for (int e = 0; e < 4; ++e) {
-    if (q + e >= qb && q + e < qe) {
+    if (e >= lo && e < hi) {
       Acc coef;
       uint32_t col;
       if constexpr (kMode == kPacked) {
@@ -185,41 +187,49 @@ __device__ __forceinline__ void quad_add(const SymView& S, const uint4& w, const
         coef = (Acc)cs[e];
         col = ws[e];
       }
-      acc = fma(coef, (Acc)xs[col - c0], acc);
+      acc = fma(coef, (Acc)xs0[col], acc);
     }
   }
 }
 
-// sum over entries [qb, qe) of a row of coefficient * xs[col - c0] (xs in shared memory) by a
-// group of G lanes (gl = lane within the group).  The group reads whole aligned 16-byte quads
-// of the word array (entries 4a .. 4a + 3 of quad a): lane gl takes quads a0 + gl, a0 + gl + G,
-// ..., U loads in flight per round (so the G lanes of a round read U x G x 16 contiguous
-// bytes), and adds the entries of each quad that lie in [qb, qe) in quad order.  The group's
-// partials meet in a fixed shuffle tree (every lane of the warp takes part; lanes of an idle
-// group, qb = qe, add zero).  Reads past the last entry stay inside the word array, whose
-// allocation is padded to a whole quad.
+// sum over entries [qb, qe) of a row of coefficient * x[col] (x staged in shared memory, xs0 as
+// in quad_add) by a group of G lanes (gl = lane within the group).  The group reads whole
+// aligned 16-byte quads of the word array (entries 4a .. 4a + 3 of quad a), from the quad
+// holding qb to the one holding qe - 1: lane gl takes quads gl, gl + G, ... of the segment,
+// U loads in flight per round (the G lanes of a round read U x G x 16 contiguous bytes), and
+// adds the entries of each quad that lie in [qb, qe) in quad order.  Indices relative to the
+// segment are 32-bit (a segment lies within one column block).  The group's partials meet in a
+// fixed shuffle tree (every lane of the warp takes part; lanes of an idle group, qb = qe, add
+// zero).  Reads past the last entry stay inside the word array, padded to a whole quad.
 template <int kMode, int G, typename Acc, typename Tx>
-__device__ __forceinline__ Acc seg_sum(const SymView& S, int64_t qb, int64_t qe, const Tx* xs, uint32_t c0,
-                                       int gl) {
+__device__ __forceinline__ Acc seg_sum(const SymView& S, int64_t qb, int64_t qe, const Tx* xs0, int gl) {
   constexpr int U = kMode == kCounts ? 2 : 4;  // counts mode loads a second quad per entry quad
   Acc acc = 0;
-  const int64_t a1 = (qe + 3) >> 2;
-  const uint4* __restrict__ w4 = reinterpret_cast<const uint4*>(S.words);
-  const int4* __restrict__ c4 = reinterpret_cast<const int4*>(S.cnt);
-  for (int64_t a = (qb >> 2) + gl; a < a1; a += U * G) {
-    uint4 w[U];
-    int4 c[U];
+  if (qe > qb) {
+    const int64_t a0 = qb >> 2;
+    const int nq = (int)(((qe + 3) >> 2) - a0);  // quads of the segment
+    const int lo0 = (int)(qb - 4 * a0);          // first entry of quad 0 in the segment (0..3)
+    const int hi0 = (int)(qe - 4 * a0);          // end of the segment, counted from quad 0
+    const uint4* __restrict__ w4 = reinterpret_cast<const uint4*>(S.words) + a0;
+    const int4* __restrict__ c4 = reinterpret_cast<const int4*>(S.cnt) + a0;
+    for (int k = gl; k < nq; k += U * G) {
+      uint4 w[U];
+      int4 c[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int64_t au = a + (int64_t)u * G;
-      w[u] = au < a1 ? __ldg(w4 + au) : make_uint4(0u, 0u, 0u, 0u);
-      c[u] = make_int4(0, 0, 0, 0);
-      if constexpr (kMode == kCounts) {
-        if (au < a1) c[u] = __ldg(c4 + au);
+      for (int u = 0; u < U; ++u) {
+        const int ku = k + u * G;
+        w[u] = ku < nq ? __ldg(w4 + ku) : make_uint4(0u, 0u, 0u, 0u);
+        c[u] = make_int4(0, 0, 0, 0);
+        if constexpr (kMode == kCounts) {
+          if (ku < nq) c[u] = __ldg(c4 + ku);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int q = 4 * (k + u * G);  // the quad's first entry, counted from quad 0
+        quad_add<kMode>(S, w[u], c[u], lo0 - q, hi0 - q, xs0, acc);
       }
     }
-#pragma unroll
-    for (int u = 0; u < U; ++u) quad_add<kMode>(S, w[u], c[u], 4 * (a + (int64_t)u * G), qb, qe, xs, c0, acc);
   }
   for (int o = G / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(PR_FULL, acc, o);
   return acc;
@@ -310,7 +320,7 @@ __device__ __forceinline__ void spmv_blk_cta(const SymView& S, const BlkView& B,
     for (; i - grp < r1; i += stride) {
       int64_t qb2, qe2;
       bounds(i + 2 * stride, qb2, qe2);
-      const Acc part = seg_sum<kMode, G, Acc>(S, qb0, qe0, xs, (uint32_t)c0, gl);
+      const Acc part = seg_sum<kMode, G, Acc>(S, qb0, qe0, xs - c0, gl);
       if (gl == 0 && i < r1) acc[i - r0] = g == 0 ? part : acc[i - r0] + part;
       prefetch(qb2, qe2);
       qb0 = qb1;
