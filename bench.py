@@ -640,6 +640,11 @@ def run_ours(args, cfg):
                     "d2h_bytes_per_step": d2h,
                     "d2h": "origin i32 + receiver i32 + count i64 per pair of every set (the reference's arrays)"},
             "roofline": roof, "trace_variant": _lib.trace_variant()[1],
+            "stage_ms_per_step": {"traversal": timers["trace"][1] / args.steps,
+                                  "per_origin_rows": timers["rle"][1] / args.steps,
+                                  "other": t_max / args.steps - (timers["trace"][1] + timers["rle"][1]) / args.steps,
+                                  "note": "device time of the traversal and row kernels from CUDA events; other = "
+                                          "the rest of the step (patch table, CSR assembly, flush, host gaps)"},
             "clocks": clocks.summary(), "gpu_launches": int(launches), "cpu_baseline": cpu,
             "whole_case": case,
         }

@@ -593,48 +593,46 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const Wa
 #pragma unroll 1
       for (int b = 0; b < kBurst; ++b) {
         if (!active) continue;
-        int32_t cell[kLook];  // each recorded cell
-        int fc[kLook];        // and the face the ray entered it through (-1: its first cell)
-        int m = 0;            // cells recorded; while nothing stopped the round, m == p at step p
-        int stop = 0;         // 0 none, 1 wall at position m, 2 step cap at position m
+        int32_t cell[kLook], code[kLook];  // each recorded cell and its hit code
+        int m = 0;      // cells recorded
+        int stop = 0;   // 0 none, 1 wall at position m, 2 step cap at position m
         int32_t wall_code = -1;
-        const int left = cap - it;  // cells the step cap still allows
 #pragma unroll
         for (int p = 0; p < kLook; ++p) {
           cell[p] = 0;
-          fc[p] = -1;
-          if (stop == 0) {
-            if (p >= left) {
+          code[p] = -1;
+          if (stop == 0 && m == p) {
+            if (it + p >= cap) {
               stop = 2;
             } else if ((unsigned)i >= (unsigned)nx) {
-              const int wj = imod_floor(floor(pr_add(pool.eoy[lane], pr_mul(pool.edy[lane], t))), ny);
-              const int wk = imod_floor(floor(pr_add(pool.eoz[lane], pr_mul(pool.edz[lane], t))), nz);
+              const int wj = (int)imod((int64_t)floor(pr_add(pool.eoy[lane], pr_mul(pool.edy[lane], t))), ny);
+              const int wk = (int)imod((int64_t)floor(pr_add(pool.eoz[lane], pr_mul(pool.edz[lane], t))), nz);
               wall_code = 6 * nx * ny * nz + (i < 0 ? 0 : ny * nz) + wj * nz + wk;
               stop = 1;
             } else {
               cell[p] = (i * ny + jj) * nz + kk;
-              fc[p] = face;
+              code[p] = face >= 0 ? cell[p] * 6 + face : -1;
               m = p + 1;
-              // t_next = min(tx, ty, tz); every axis within the tie tolerance of it is crossed.
-              // t_a >= t_next, so t_a - t_next is never negative and needs no absolute value.
-              const double tn = fmin(fmin(tx, ty), tz);
-              const bool cx = pr_sub(tx, tn) <= PR_TIE;
-              const bool cy = pr_sub(ty, tn) <= PR_TIE;
-              const bool cz = pr_sub(tz, tn) <= PR_TIE;
+              double tn = tx;
+              if (ty < tn) tn = ty;
+              if (tz < tn) tn = tz;
+              const bool cx = fabs(pr_sub(tx, tn)) <= PR_TIE;
+              const bool cy = fabs(pr_sub(ty, tn)) <= PR_TIE;
+              const bool cz = fabs(pr_sub(tz, tn)) <= PR_TIE;
               if (cx) {
                 i += sx;
                 tx = pr_add(tx, ddx);
                 face = sx > 0 ? 1 : 0;
               }
               if (cy) {
-                jj += sy;  // periodic: ny -> 0 stepping up, -1 -> ny - 1 stepping down
-                if ((unsigned)jj >= (unsigned)ny) jj -= sy * ny;
+                jj += sy;
+                jj = jj == ny ? 0 : (jj < 0 ? ny - 1 : jj);
                 ty = pr_add(ty, ddy);
                 if (!cx) face = sy > 0 ? 3 : 2;
               }
               if (cz) {
                 kk += sz;
-                if ((unsigned)kk >= (unsigned)nz) kk -= sz * nz;
+                kk = kk == nz ? 0 : (kk < 0 ? nz - 1 : kk);
                 tz = pr_add(tz, ddz);
                 if (!cx && !cy) face = sz > 0 ? 5 : 4;
               }
@@ -645,27 +643,23 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const Wa
         uint32_t word[kLook];
 #pragma unroll
         for (int p = 0; p < kLook; ++p) word[p] = p < m ? __ldg(occ + (cell[p] >> 5)) : 0u;
-        // the first solid cell among the recorded ones decides; its hit code is its
-        // cell_face_patch index (cell * 6 + entry face), -1 for a ray starting inside solid
-        bool solid = false;
-        int hcell = 0, hface = -1, used = m;
+        int32_t hit = -2;
+        int used = m;
 #pragma unroll
         for (int p = kLook - 1; p >= 0; --p) {
           if (p < m && ((word[p] >> (cell[p] & 31)) & 1u)) {
-            solid = true;
-            hcell = cell[p];
-            hface = fc[p];
+            hit = code[p];  // the cell_face_patch index
             used = p + 1;
           }
         }
-        int32_t hit = -2;
-        if (solid) {
-          hit = hface >= 0 ? hcell * 6 + hface : -1;
-        } else if (stop == 1) {
-          hit = wall_code;
-          used = m + 1;
-        } else if (stop == 2) {
-          hit = -1;
+        if (hit == -2) {
+          if (stop == 1) {
+            hit = wall_code;
+            used = m + 1;
+          } else if (stop == 2) {
+            hit = -1;
+            used = m;
+          }
         }
         it += used;
         if (hit != -2) {
