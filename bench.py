@@ -862,20 +862,29 @@ def run_c3(args, cfg):
             op.close()
             return ch
 
+    stage_s = {}
+
+    def lap(name, t0):
+        torch.cuda.synchronize()
+        stage_s[name] = time.perf_counter() - t0
+        return time.perf_counter()
+
     def sweep():
+        t = time.perf_counter()
         geos = [vf.DeviceGeometry(ph, H) for ph in dev_phases]
         pats = [vf.SurfacePatches(H_m=H, _device=g) for g in geos]
         tables = vf.first_hit_counts_batch(pats, R, seeds)
+        t = lap("patches_and_counts", t)
         # the operators of all cases, their balancing iterations in shared product launches
         ops = exchange.ExchangeOperator.from_tables(
             tables, [np.full(g.n_patches, R, np.int64) for g in geos],
             [np.full(g.n_patches, (H / cfg["n"]) ** 2) for g in geos])
-        for t in tables:
-            t.close()
-        torch.cuda.synchronize()
+        for tb in tables:
+            tb.close()
+        t = lap("operators", t)
         with concurrent.futures.ThreadPoolExecutor(cfg["slots"]) as ex:
             chs = list(ex.map(lambda a: solve(*a), [(k, g, o) for k, (g, o) in enumerate(zip(geos, ops))]))
-        torch.cuda.synchronize()
+        lap("solves", t)
         rays = sum(g.n_patches for g in geos) * R
         patches = [g.n_patches for g in geos]
         for g in geos:
@@ -901,7 +910,8 @@ def run_c3(args, cfg):
         "dtype": "f64 (traversal), f32+f64 (radiosity)", "data": "synthetic",
         "config": {"workload": cfg["workload"], "cases": len(specs), "patches_min": min(patches),
                    "patches_max": max(patches), "rays": rays},
-        "cases_per_s": len(specs) / dt, "trace_launches": int(n.value), "trace_ms": ms.value,
+        "cases_per_s": len(specs) / dt, "stages_s": dict(stage_s), "trace_launches": int(n.value),
+        "trace_ms": ms.value,
         "trace_variant": _lib.trace_variant()[1], "max_closure_rel": max(c.closure_rel for c in chs),
         "clocks": clocks.summary(), "gpu_launches": int(lib.pr_kernel_launches() - launches0),
     }
