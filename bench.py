@@ -858,6 +858,11 @@ def run_c3(args, cfg):
     def solve(k, geo, op):
         with _lib.use_stream(streams[k % len(streams)]):
             p = vf.SurfacePatches(H_m=H, _device=geo)
+            if not isinstance(op, exchange.ExchangeOperator):  # a count table: the operator built here alone
+                table = op
+                op = exchange.ExchangeOperator(table, None, None, np.full(geo.n_patches, R, np.int64),
+                                               np.full(geo.n_patches, (H / cfg["n"]) ** 2))
+                table.close()
             ch = coupled.prescribed_field_channels(op, p, cfg["T_m"], cfg["dT"], specs[k]["eps"], precision="mixed")
             op.close()
             return ch
@@ -869,22 +874,25 @@ def run_c3(args, cfg):
         stage_s[name] = time.perf_counter() - t0
         return time.perf_counter()
 
-    def sweep():
+    def sweep(batched=True):
         t = time.perf_counter()
         geos = [vf.DeviceGeometry(ph, H) for ph in dev_phases]
         pats = [vf.SurfacePatches(H_m=H, _device=g) for g in geos]
         tables = vf.first_hit_counts_batch(pats, R, seeds)
         t = lap("patches_and_counts", t)
-        # the operators of all cases, their balancing iterations in shared product launches
-        ops = exchange.ExchangeOperator.from_tables(
-            tables, [np.full(g.n_patches, R, np.int64) for g in geos],
-            [np.full(g.n_patches, (H / cfg["n"]) ** 2) for g in geos])
-        for tb in tables:
-            tb.close()
-        t = lap("operators", t)
+        if batched:
+            # the operators of all cases, their balancing iterations in shared product launches
+            ops = exchange.ExchangeOperator.from_tables(
+                tables, [np.full(g.n_patches, R, np.int64) for g in geos],
+                [np.full(g.n_patches, (H / cfg["n"]) ** 2) for g in geos])
+            for tb in tables:
+                tb.close()
+            t = lap("operators", t)
+        else:
+            ops = tables  # each operator built alone by its solve's worker (4 streams)
         with concurrent.futures.ThreadPoolExecutor(cfg["slots"]) as ex:
             chs = list(ex.map(lambda a: solve(*a), [(k, g, o) for k, (g, o) in enumerate(zip(geos, ops))]))
-        lap("solves", t)
+        lap("solves" if batched else "operators_and_solves", t)
         rays = sum(g.n_patches for g in geos) * R
         patches = [g.n_patches for g in geos]
         for g in geos:
@@ -903,6 +911,13 @@ def run_c3(args, cfg):
     lib.pr_timers_enable(0)
     n, ms = _lib.ctypes.c_longlong(), _lib.ctypes.c_double()
     lib.pr_timers_read(_lib.TIMER_TRACE, _lib.ctypes.byref(n), _lib.ctypes.byref(ms))
+    batched_stages = dict(stage_s)
+    # the same sweep with each case's operator built alone on one of the 4 worker streams
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sweep(batched=False)
+    dt_alone = time.perf_counter() - t0
+    alone_stages = {k: v for k, v in stage_s.items() if k in ("patches_and_counts", "operators_and_solves")}
     return {
         "metric": "first-hit rays/s and cases/s of the 48-case batched sweep (one count pass, overlapped solves)",
         "value": rays / dt, "unit": "rays/s", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": dt * 1e3,
@@ -910,7 +925,9 @@ def run_c3(args, cfg):
         "dtype": "f64 (traversal), f32+f64 (radiosity)", "data": "synthetic",
         "config": {"workload": cfg["workload"], "cases": len(specs), "patches_min": min(patches),
                    "patches_max": max(patches), "rays": rays},
-        "cases_per_s": len(specs) / dt, "stages_s": dict(stage_s), "trace_launches": int(n.value),
+        "cases_per_s": len(specs) / dt, "stages_s": batched_stages,
+        "operators_alone_on_4_streams": {"s": dt_alone, "cases_per_s": len(specs) / dt_alone, "stages_s": alone_stages},
+        "trace_launches": int(n.value),
         "trace_ms": ms.value,
         "trace_variant": _lib.trace_variant()[1], "max_closure_rel": max(c.closure_rel for c in chs),
         "clocks": clocks.summary(), "gpu_launches": int(lib.pr_kernel_launches() - launches0),
