@@ -234,6 +234,28 @@ __global__ void k_expand_rows(const int64_t* __restrict__ rp, const int32_t* __r
     }
 }
 
+// Rows [r0, r1) of a count table into pageable host arrays without expanding them on the device:
+// the row offsets come over (8 B per row), origins are filled on the host from them, and
+// the counts cross as the table's int32 values, widened to int64 on the host; 8 B per pair cross
+// the bus instead of 16.
+static int rows_to_pageable(const CountCsr& c, int64_t r0, int64_t r1, int64_t base, int64_t m, int32_t* origin,
+                            int32_t* receiver, int64_t* count, cudaStream_t s) {
+  if (origin) {
+    std::vector<int64_t> rp((size_t)(r1 - r0 + 1));
+    PR_CUDA(cudaMemcpyAsync(rp.data(), c.row_ptr.ptr + r0, rp.size() * 8, cudaMemcpyDeviceToHost, s));
+    PR_CUDA(cudaStreamSynchronize(s));
+    for (auto& v : rp) v -= base;
+    fill_rows_host(origin, rp.data(), r1 - r0, r0);
+  }
+  if (count) PR_TRY(copy_to_host_i64(count, c.cnt.ptr + base, m, s));
+  if (receiver) PR_TRY(copy_to_host(receiver, c.col.ptr + base, (size_t)m * 4, s));
+  return PR_OK;
+}
+
+static bool large_pageable(int64_t m, const void* a, const void* b) {
+  return m * 4 > ((int64_t)16 << 20) && (a || b) && (!a || is_pageable_host(a)) && (!b || is_pageable_host(b));
+}
+
 int pr_counts_copy(const pr_counts* k, int32_t* origin, int32_t* receiver, int64_t* count, int64_t* rays_per_origin,
                    void* stream) {
   PR_CHECK_NULL(k, "counts");
@@ -241,6 +263,12 @@ int pr_counts_copy(const pr_counts* k, int32_t* origin, int32_t* receiver, int64
   cudaStream_t s = (cudaStream_t)stream;
   const CountCsr& c = *k->csr;
   const int64_t m = c.nnz, n = c.n_rows;
+  if (large_pageable(m, origin, count)) {
+    PR_TRY(rows_to_pageable(c, 0, n, 0, m, origin, receiver, count, s));
+    if (rays_per_origin && n > 0) PR_TRY(copy_to_host(rays_per_origin, k->rays.ptr, n * 8, s));
+    PR_CUDA(cudaStreamSynchronize(s));
+    return PR_OK;
+  }
   DevBuf<int32_t> o;
   DevBuf<int64_t> cn;
   if (m > 0 && (origin || count)) {
@@ -276,6 +304,11 @@ int pr_counts_rows(const pr_counts* k, int64_t row_begin, int64_t row_end, int64
   const int64_t m = bounds[1] - bounds[0];
   *n_pairs = m;
   if (m == 0 || (!origin && !receiver && !count)) return PR_OK;
+  if (large_pageable(m, origin, count)) {
+    PR_TRY(rows_to_pageable(c, row_begin, row_end, bounds[0], m, origin, receiver, count, s));
+    PR_CUDA(cudaStreamSynchronize(s));
+    return PR_OK;
+  }
   DevBuf<int32_t> o;
   DevBuf<int64_t> cn;
   if (origin) PR_TRY(o.alloc(m, s));

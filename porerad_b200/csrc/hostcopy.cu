@@ -43,14 +43,15 @@ class CopyPool {
     cv_.notify_all();
     for (auto& w : workers_) w.join();
   }
-  // memcpy(dst, src, bytes) split over all threads, the caller's thread included; returns when done.
-  // Calls from several host threads take turns.
-  void copy(char* dst, const char* src, size_t bytes) {
+  // job(begin, end) over [0, total) split into one slice per thread (slices aligned to `align`
+  // items), the caller's thread included; returns when every slice is done.  Calls from several
+  // host threads take turns.
+  void run(size_t total, size_t align, const std::function<void(size_t, size_t)>& job) {
     std::lock_guard<std::mutex> turn(call_mu_);
     std::unique_lock<std::mutex> lk(mu_);
-    dst_ = dst;
-    src_ = src;
-    bytes_ = bytes;
+    job_ = &job;
+    total_ = total;
+    align_ = align == 0 ? 1 : align;
     pending_ = n_ - 1;
     ++generation_;
     lk.unlock();
@@ -59,14 +60,16 @@ class CopyPool {
     lk.lock();
     done_cv_.wait(lk, [this] { return pending_ == 0; });
   }
+  // memcpy split over the threads (4 KiB slices, so that threads fault in disjoint pages)
+  void copy(char* dst, const char* src, size_t bytes) {
+    run(bytes, 4096, [&](size_t b, size_t e) { memcpy(dst + b, src + b, e - b); });
+  }
 
  private:
   void part(unsigned t) {
-    // slices aligned to 4 KiB pages so that threads fault in disjoint pages
-    const size_t page = 4096;
-    const size_t per = ((bytes_ + n_ - 1) / n_ + page - 1) / page * page;
+    const size_t per = ((total_ + n_ - 1) / n_ + align_ - 1) / align_ * align_;
     const size_t b = (size_t)t * per;
-    if (b < bytes_) memcpy(dst_ + b, src_ + b, (bytes_ - b) < per ? (bytes_ - b) : per);
+    if (b < total_) (*job_)(b, (total_ - b) < per ? total_ : b + per);
   }
   void run(unsigned t) {
     unsigned long long seen = 0;
@@ -86,9 +89,8 @@ class CopyPool {
   std::vector<std::thread> workers_;
   std::mutex call_mu_, mu_;
   std::condition_variable cv_, done_cv_;
-  char* dst_ = nullptr;
-  const char* src_ = nullptr;
-  size_t bytes_ = 0;
+  const std::function<void(size_t, size_t)>* job_ = nullptr;
+  size_t total_ = 0, align_ = 1;
   unsigned pending_ = 0;
   unsigned long long generation_ = 0;
   bool quit_ = false;
@@ -138,19 +140,16 @@ bool pageable(const void* p) {
 
 }  // namespace
 
-int copy_to_host(void* dst, const void* src, size_t bytes, cudaStream_t s) {
-  if (bytes == 0) return PR_OK;
-  if (bytes <= kDirectMax || !pageable(dst)) {
-    PR_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s));
-    return PR_OK;
-  }
+// The pipeline: chunks of src (device) go through the staging buffers; for each chunk, on the
+// host, sink(staging, first byte of the chunk, its bytes) runs over the host threads.
+static int staged(const void* src, size_t bytes, cudaStream_t s,
+                  const std::function<void(const char*, size_t, size_t)>& sink) {
   int dev = 0;
   PR_CUDA(cudaGetDevice(&dev));
   Staging* st = nullptr;
   PR_TRY(staging_for(dev, &st));
   std::lock_guard<std::mutex> lk(st->mu);
   const char* s8 = static_cast<const char*>(src);
-  char* d8 = static_cast<char*>(dst);
   const size_t n = (bytes + kChunk - 1) / kChunk;
   auto issue = [&](size_t k) -> int {
     const size_t off = k * kChunk, len = (bytes - off) < kChunk ? (bytes - off) : kChunk;
@@ -160,13 +159,63 @@ int copy_to_host(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   };
   PR_TRY(issue(0));
   for (size_t k = 0; k < n; ++k) {
-    // the buffer of chunk k + 1 was emptied by the host copy of chunk k - 1 (finished below)
+    // the buffer of chunk k + 1 was emptied by the host work of chunk k - 1 (finished below)
     if (k + 1 < n) PR_TRY(issue(k + 1));
     PR_CUDA(cudaEventSynchronize(st->ready[k & 1]));
     const size_t off = k * kChunk, len = (bytes - off) < kChunk ? (bytes - off) : kChunk;
-    g_pool->copy(d8 + off, st->buf[k & 1], len);
+    sink(st->buf[k & 1], off, len);
   }
   return PR_OK;
 }
+
+int copy_to_host(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return PR_OK;
+  if (bytes <= kDirectMax || !pageable(dst)) {
+    PR_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s));
+    return PR_OK;
+  }
+  char* d8 = static_cast<char*>(dst);
+  return staged(src, bytes, s, [&](const char* buf, size_t off, size_t len) { g_pool->copy(d8 + off, buf, len); });
+}
+
+int copy_to_host_i64(int64_t* dst, const int32_t* src, int64_t n, cudaStream_t s) {
+  if (n <= 0) return PR_OK;
+  if ((size_t)n * 4 <= kDirectMax || !pageable(dst)) {
+    std::vector<int32_t> h((size_t)n);
+    PR_CUDA(cudaMemcpyAsync(h.data(), src, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+    PR_CUDA(cudaStreamSynchronize(s));
+    if (pageable(dst)) {
+      for (int64_t i = 0; i < n; ++i) dst[i] = h[i];
+    } else {
+      std::vector<int64_t> w(h.begin(), h.end());
+      PR_CUDA(cudaMemcpyAsync(dst, w.data(), (size_t)n * 8, cudaMemcpyDefault, s));
+      PR_CUDA(cudaStreamSynchronize(s));
+    }
+    return PR_OK;
+  }
+  return staged(src, (size_t)n * 4, s, [&](const char* buf, size_t off, size_t len) {
+    const int32_t* in = reinterpret_cast<const int32_t*>(buf);
+    int64_t* out = dst + off / 4;
+    g_pool->run(len / 4, 512, [&](size_t b, size_t e) {
+      for (size_t i = b; i < e; ++i) out[i] = in[i];
+    });
+  });
+}
+
+void fill_rows_host(int32_t* origin, const int64_t* row_ptr, int64_t n_rows, int64_t first_id) {
+  if (n_rows <= 0) return;
+  CopyPool* pool = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_pool) g_pool = new CopyPool();
+    pool = g_pool;
+  }
+  pool->run((size_t)n_rows, 64, [&](size_t b, size_t e) {
+    for (size_t i = b; i < e; ++i)
+      for (int64_t q = row_ptr[i]; q < row_ptr[i + 1]; ++q) origin[q] = (int32_t)(first_id + (int64_t)i);
+  });
+}
+
+bool is_pageable_host(const void* p) { return pageable(p); }
 
 }  // namespace pr

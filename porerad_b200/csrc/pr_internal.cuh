@@ -66,6 +66,13 @@ void arena_free(void* p, size_t bytes, cudaStream_t s, int dev);
 // and host threads (hostcopy.cu); everything else is one cudaMemcpyAsync (the caller then
 // synchronises the stream as before).
 int copy_to_host(void* dst, const void* src, size_t bytes, cudaStream_t s);
+// int32 device values into an int64 host array (widened on the host; same pipeline).
+int copy_to_host_i64(int64_t* dst, const int32_t* src, int64_t n, cudaStream_t s);
+// origin[q] = first_id + i for every q in [row_ptr[i], row_ptr[i + 1]) (host arrays), over the
+// host threads.
+void fill_rows_host(int32_t* origin, const int64_t* row_ptr, int64_t n_rows, int64_t first_id);
+// Host memory the GPU cannot reach directly (neither pinned nor managed).
+bool is_pageable_host(const void* p);
 
 // A device allocation owned by the library, released in stream order (to the cache).
 template <typename T>
