@@ -595,6 +595,8 @@ def run_ours(args, cfg):
     d2h = int(res["d2h"])
 
     t_max, e2e_s = replicas.max_over_ranks([ms, e2e_s])
+    # every replica traced the same seeded case: DDA steps and pairs per set agree on all ranks
+    agree = replicas.all_equal([steps, *last["pairs"]])
     value = rays * world / (t_max * 1e-3)
     case = whole_case(args, cfg, seeds, phases_dev, phases_host, pinned, lib, flush, rank)
     line = None
@@ -648,6 +650,8 @@ def run_ours(args, cfg):
             "clocks": clocks.summary(), "gpu_launches": int(launches), "cpu_baseline": cpu,
             "whole_case": case,
         }
+        if world > 1:
+            line["replicas_agree"] = agree
         if case is not None:
             line["cases_per_s"] = case["cases_per_s"]
     replicas.finalize()

@@ -170,14 +170,15 @@ inline BlkView blk_view(const SymCsr& S) { return BlkView{S.blk.seg.ptr, S.blk.c
 // entry e is summed when lo <= e < hi (the quad's part of the row segment), adding
 // coefficient * x[col] to acc in entry order.  xs0 points at x[0] of the staged block's
 // coordinates (the shared array shifted back by the block's first column), so x[col] is xs0[col].
-template <int kMode, typename Acc, typename Tx>
+// kWhole: the quad lies inside the segment (lo <= 0, hi >= 4), so no entry is tested.
+template <int kMode, bool kWhole, typename Acc, typename Tx>
 __device__ __forceinline__ void quad_add(const SymView& S, const uint4& w, const int4& c, int lo, int hi,
                                          const Tx* xs0, Acc& acc) {
   const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
   const int32_t cs[4] = {c.x, c.y, c.z, c.w};
 #pragma unroll
   for (int e = 0; e < 4; ++e) {
-    if (e >= lo && e < hi) {
+    if (kWhole || (e >= lo && e < hi)) {
       Acc coef;
       uint32_t col;
       if constexpr (kMode == kPacked) {
@@ -192,15 +193,39 @@ __device__ __forceinline__ void quad_add(const SymView& S, const uint4& w, const
   }
 }
 
+// V quads of a group lane, k, k + G, ..., k + (V - 1) G (all below the segment's quad count):
+// the loads first, then the entries in quad order.  Only the segment's first and last quads
+// are partial, so the per-entry tests run on those alone.
+template <int kMode, int G, int V, typename Acc, typename Tx>
+__device__ __forceinline__ void seg_quads(const SymView& S, const uint4* __restrict__ w4, const int4* __restrict__ c4,
+                                          int k, int lo0, int hi0, const Tx* xs0, Acc& acc) {
+  uint4 w[V];
+  int4 c[V];
+#pragma unroll
+  for (int u = 0; u < V; ++u) {
+    w[u] = __ldg(w4 + k + u * G);
+    c[u] = make_int4(0, 0, 0, 0);
+    if constexpr (kMode == kCounts) c[u] = __ldg(c4 + k + u * G);
+  }
+#pragma unroll
+  for (int u = 0; u < V; ++u) {
+    const int q = 4 * (k + u * G);  // the quad's first entry, counted from quad 0
+    const int lo = lo0 - q, hi = hi0 - q;
+    if (lo <= 0 && hi >= 4) quad_add<kMode, true>(S, w[u], c[u], lo, hi, xs0, acc);
+    else quad_add<kMode, false>(S, w[u], c[u], lo, hi, xs0, acc);
+  }
+}
+
 // sum over entries [qb, qe) of a row of coefficient * x[col] (x staged in shared memory, xs0 as
 // in quad_add) by a group of G lanes (gl = lane within the group).  The group reads whole
 // aligned 16-byte quads of the word array (entries 4a .. 4a + 3 of quad a), from the quad
-// holding qb to the one holding qe - 1: lane gl takes quads gl, gl + G, ... of the segment,
-// U loads in flight per round (the G lanes of a round read U x G x 16 contiguous bytes), and
-// adds the entries of each quad that lie in [qb, qe) in quad order.  Indices relative to the
-// segment are 32-bit (a segment lies within one column block).  The group's partials meet in a
-// fixed shuffle tree (every lane of the warp takes part; lanes of an idle group, qb = qe, add
-// zero).  Reads past the last entry stay inside the word array, padded to a whole quad.
+// holding qb to the one holding qe - 1: lane gl takes quads gl, gl + G, ... of the segment and
+// adds the entries of each quad that lie in [qb, qe) in quad order.  Loads go out U quads per
+// lane at a time while every lane of the group has U quads left, then two, then one, so no
+// lane issues work for quads past the segment.  Indices relative to the segment are 32-bit (a
+// segment lies within one column block).  The group's partials meet in a fixed shuffle tree
+// (every lane of the warp takes part; lanes of an idle group, qb = qe, add zero).  Reads stay
+// inside the word array, padded to a whole quad.
 template <int kMode, int G, typename Acc, typename Tx>
 __device__ __forceinline__ Acc seg_sum(const SymView& S, int64_t qb, int64_t qe, const Tx* xs0, int gl) {
   constexpr int U = kMode == kCounts ? 2 : 4;  // counts mode loads a second quad per entry quad
@@ -212,24 +237,15 @@ __device__ __forceinline__ Acc seg_sum(const SymView& S, int64_t qb, int64_t qe,
     const int hi0 = (int)(qe - 4 * a0);          // end of the segment, counted from quad 0
     const uint4* __restrict__ w4 = reinterpret_cast<const uint4*>(S.words) + a0;
     const int4* __restrict__ c4 = reinterpret_cast<const int4*>(S.cnt) + a0;
-    for (int k = gl; k < nq; k += U * G) {
-      uint4 w[U];
-      int4 c[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int ku = k + u * G;
-        w[u] = ku < nq ? __ldg(w4 + ku) : make_uint4(0u, 0u, 0u, 0u);
-        c[u] = make_int4(0, 0, 0, 0);
-        if constexpr (kMode == kCounts) {
-          if (ku < nq) c[u] = __ldg(c4 + ku);
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int q = 4 * (k + u * G);  // the quad's first entry, counted from quad 0
-        quad_add<kMode>(S, w[u], c[u], lo0 - q, hi0 - q, xs0, acc);
+    int k = gl;
+    for (; k + (U - 1) * G < nq; k += U * G) seg_quads<kMode, G, U>(S, w4, c4, k, lo0, hi0, xs0, acc);
+    if constexpr (U > 2) {
+      if (k + G < nq) {
+        seg_quads<kMode, G, 2>(S, w4, c4, k, lo0, hi0, xs0, acc);
+        k += 2 * G;
       }
     }
+    for (; k < nq; k += G) seg_quads<kMode, G, 1>(S, w4, c4, k, lo0, hi0, xs0, acc);
   }
   for (int o = G / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(PR_FULL, acc, o);
   return acc;

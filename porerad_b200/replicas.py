@@ -61,6 +61,26 @@ def max_over_ranks(values):
     return [float(v) for v in t.cpu()]
 
 
+def all_equal(values) -> bool:
+    """True when every rank passed the same list of integers (True with one rank).
+
+    Replicas of a seeded case must agree to the last integer (DDA steps, pairs per ray set);
+    the check takes the element-wise minimum and maximum over the ranks and compares them.
+    """
+
+    values = [int(v) for v in values]
+    if _dist is None:
+        return True
+    import torch
+
+    dev = "cuda" if _dist.get_backend() == "nccl" else "cpu"
+    lo = torch.tensor(values, dtype=torch.int64, device=dev)
+    hi = lo.clone()
+    _dist.all_reduce(lo, op=_dist.ReduceOp.MIN)
+    _dist.all_reduce(hi, op=_dist.ReduceOp.MAX)
+    return bool(torch.equal(lo.cpu(), hi.cpu()))
+
+
 def finalize() -> None:
     global _dist
     if _dist is not None:

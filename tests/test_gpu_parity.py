@@ -111,7 +111,9 @@ def test_exchange_operator(name):
     assert op.balance_method in ("anderson", "multiplicative")
     assert op.row_sum_error <= 1e-10
     assert _rel(op.scale, case["scale"]) <= SCALE_RTOL
+    # both sides form the same products of the same scale d; the defect stays at rounding level
     assert op.reciprocity_error() <= 1e-12
+    assert abs(op.reciprocity_error() - float(case["reciprocity_error"])) <= 4 * np.finfo(np.float64).eps
     assert np.array_equal(op.origin, case["pooled_origin"])
     assert np.array_equal(op.receiver, case["pooled_receiver"])
     assert np.array_equal(op.weight, case["pooled_count"] / np.float64(R))
