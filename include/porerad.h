@@ -140,11 +140,32 @@ PR_API int pr_counts_copy(const pr_counts* k, int32_t* origin, int32_t* receiver
  * copied (size query).  PR_ERR_ARG for a range outside [0, n_patches]. */
 PR_API int pr_counts_rows(const pr_counts* k, int64_t row_begin, int64_t row_end, int64_t* n_pairs,
                           int32_t* origin, int32_t* receiver, int64_t* count, void* stream);
+/* ---- pinned host blocks for results (no counterpart in the reference) ----------------
+ * first_hit_counts (view_factors.py:273-287) hands back gigabytes of NumPy arrays per call.
+ * Arrays placed in a pinned block of this pool receive pr_counts_copy / pr_counts_rows
+ * straight from the device at the link's rate; a released block is cached for the next
+ * request that it holds with at most twice the bytes (bounded by PORERAD_HOST_CACHE_BYTES, default 32 GiB),
+ * so pinning and page faults are paid once per size.  Blocks are page-aligned, rounded up
+ * to 2 MiB.  release: PR_ERR_ARG for a pointer that is not a live block of the pool.
+ * trim frees cached blocks, largest first, until at most keep_bytes stay cached. */
+PR_API int pr_host_block(long long bytes, void** out);
+PR_API int pr_host_block_release(void* block);
+PR_API int pr_host_blocks_trim(long long keep_bytes);
+PR_API int pr_host_blocks_stats(long long* live_bytes, long long* cached_bytes, long long* allocations,
+                                long long* reuses);
 /* Replaces pool_counts(tables, n_patches), view_factors.py:290-300, and the re-pooling at
  * the top of ExchangeOperator.__init__ (exchange.py:59-67): sums the counts of equal
  * (origin, receiver) pairs of an arbitrary edge list into sorted CSR rows. */
 PR_API int pr_counts_from_edges(const int32_t* origin, const int32_t* receiver, const int64_t* count,
                          int64_t n_edges, int64_t n_patches, void* stream, pr_counts** out);
+/* pool_counts(tables, n_patches) (view_factors.py:290-300) over a list of n_tables edge lists
+ * as the reference receives them: table t is origin[t], receiver[t], count[t] of n_edges[t]
+ * pairs, in host (pageable or pinned) or device memory.  The tables are copied one after the
+ * other into one device edge list (pageable ones above 16 MB through pinned staging buffers)
+ * and pooled there; ids outside [0, n_patches) give PR_ERR_ARG. */
+PR_API int pr_counts_from_tables(const int32_t* const* origin, const int32_t* const* receiver,
+                                 const int64_t* const* count, const int64_t* n_edges, int n_tables,
+                                 int64_t n_patches, void* stream, pr_counts** out);
 /* pool_counts (view_factors.py:290-300) of two device tables of the same patches, e.g. ray
  * sets A and B: rows merged, counts, rays per origin, rays traced and DDA steps summed. */
 PR_API int pr_counts_merge(const pr_counts* a, const pr_counts* b, void* stream, pr_counts** out);

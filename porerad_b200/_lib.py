@@ -108,7 +108,12 @@ _SIGNATURES = {
                               ctypes.POINTER(_i64)]),
     "pr_counts_copy": (_i32, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "pr_counts_rows": (_i32, [_vp, _i64, _i64, ctypes.POINTER(_i64), _vp, _vp, _vp, _vp]),
+    "pr_host_block": (_i32, [ctypes.c_longlong, ctypes.POINTER(_vp)]),
+    "pr_host_block_release": (_i32, [_vp]),
+    "pr_host_blocks_trim": (_i32, [ctypes.c_longlong]),
+    "pr_host_blocks_stats": (_i32, [ctypes.POINTER(ctypes.c_longlong)] * 4),
     "pr_counts_from_edges": (_i32, [_vp, _vp, _vp, _i64, _i64, _vp, ctypes.POINTER(_vp)]),
+    "pr_counts_from_tables": (_i32, [_vp, _vp, _vp, _vp, ctypes.c_int, _i64, _vp, ctypes.POINTER(_vp)]),
     "pr_counts_merge": (_i32, [_vp, _vp, _vp, ctypes.POINTER(_vp)]),
     "pr_counts_destroy": (None, [_vp]),
     "pr_operator_create": (_i32, [_vp, _vp, _vp, _f64, _f64, _vp, ctypes.POINTER(_vp)]),

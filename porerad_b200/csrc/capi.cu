@@ -26,6 +26,8 @@ int counts_batch(const pr_case* const* cases, int nc, int64_t R, const pr_pcg64*
                  pr_counts** out);
 int counts_from_edges(const int32_t* origin, const int32_t* receiver, const int64_t* count, int64_t m, int64_t n,
                       cudaStream_t s, pr_counts** out);
+int counts_from_tables(const int32_t* const* origin, const int32_t* const* receiver, const int64_t* const* count,
+                       const int64_t* n_edges, int n_tables, int64_t n, cudaStream_t s, pr_counts** out);
 int counts_merge(const pr_counts* A, const pr_counts* B, cudaStream_t s, pr_counts** out);
 int operator_create(const pr_counts* k, const int64_t* rays, const double* area, double delta, double tol,
                     cudaStream_t s, pr_operator** out);
@@ -287,6 +289,27 @@ int pr_counts_copy(const pr_counts* k, int32_t* origin, int32_t* receiver, int64
   return PR_OK;
 }
 
+int pr_host_block(long long bytes, void** out) {
+  PR_CHECK_NULL(out, "out");
+  PR_ARG(bytes > 0, "a host block needs a positive size");
+  return host_block_take((size_t)bytes, out);
+}
+
+int pr_host_block_release(void* block) {
+  PR_CHECK_NULL(block, "block");
+  return host_block_give(block);
+}
+
+int pr_host_blocks_trim(long long keep_bytes) {
+  PR_ARG(keep_bytes >= 0, "keep_bytes must not be negative");
+  return host_blocks_trim((size_t)keep_bytes);
+}
+
+int pr_host_blocks_stats(long long* live_bytes, long long* cached_bytes, long long* allocations, long long* reuses) {
+  host_blocks_stats(live_bytes, cached_bytes, allocations, reuses);
+  return PR_OK;
+}
+
 int pr_counts_rows(const pr_counts* k, int64_t row_begin, int64_t row_end, int64_t* n_pairs, int32_t* origin,
                    int32_t* receiver, int64_t* count, void* stream) {
   PR_CHECK_NULL(k, "counts");
@@ -333,6 +356,13 @@ int pr_counts_from_edges(const int32_t* origin, const int32_t* receiver, const i
   *out = nullptr;
   PR_ARG(n_edges == 0 || (origin && receiver && count), "edge arrays must not be NULL");
   return counts_from_edges(origin, receiver, count, n_edges, n_patches, (cudaStream_t)stream, out);
+}
+
+int pr_counts_from_tables(const int32_t* const* origin, const int32_t* const* receiver, const int64_t* const* count,
+                          const int64_t* n_edges, int n_tables, int64_t n_patches, void* stream, pr_counts** out) {
+  PR_CHECK_NULL(out, "out");
+  PR_ARG(n_tables == 0 || (origin && receiver && count && n_edges), "table arrays must not be NULL");
+  return counts_from_tables(origin, receiver, count, n_edges, n_tables, n_patches, (cudaStream_t)stream, out);
 }
 
 int pr_counts_merge(const pr_counts* a, const pr_counts* b, void* stream, pr_counts** out) {

@@ -13,10 +13,18 @@
 //   * a pool of host threads (one per hardware thread, at most 16), started on first use.
 //
 // Device memory, pinned or managed destinations and small copies take cudaMemcpyAsync.
+//
+// Results that leave the library as host arrays can instead live in pinned host blocks of the
+// library (pr_host_block): the device writes them straight into the caller's memory at the
+// link's rate, and a block the caller has released is kept for the next result of about its
+// size (pinning and first-touch faults are paid once, not per call).
+#include <cstdlib>
 #include <condition_variable>
 #include <functional>
+#include <map>
 #include <mutex>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "pr_internal.cuh"
@@ -178,6 +186,33 @@ int copy_to_host(void* dst, const void* src, size_t bytes, cudaStream_t s) {
   return staged(src, bytes, s, [&](const char* buf, size_t off, size_t len) { g_pool->copy(d8 + off, buf, len); });
 }
 
+int copy_from_host(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return PR_OK;
+  if (bytes <= kDirectMax || !pageable(src)) {
+    PR_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s));
+    return PR_OK;
+  }
+  int dev = 0;
+  PR_CUDA(cudaGetDevice(&dev));
+  Staging* st = nullptr;
+  PR_TRY(staging_for(dev, &st));
+  std::lock_guard<std::mutex> lk(st->mu);
+  const char* s8 = static_cast<const char*>(src);
+  char* d8 = static_cast<char*>(dst);
+  const size_t n = (bytes + kChunk - 1) / kChunk;
+  // host threads fill buffer k & 1 with chunk k while the DMA of chunk k - 1 runs from the other
+  for (size_t k = 0; k < n; ++k) {
+    const size_t off = k * kChunk, len = (bytes - off) < kChunk ? (bytes - off) : kChunk;
+    if (k >= 2) PR_CUDA(cudaEventSynchronize(st->ready[k & 1]));  // chunk k - 2 has left this buffer
+    g_pool->copy(st->buf[k & 1], s8 + off, len);
+    PR_CUDA(cudaMemcpyAsync(d8 + off, st->buf[k & 1], len, cudaMemcpyHostToDevice, s));
+    PR_CUDA(cudaEventRecord(st->ready[k & 1], s));
+  }
+  // the staging buffers are free again once their last DMAs are done
+  for (size_t k = n > 2 ? n - 2 : 0; k < n; ++k) PR_CUDA(cudaEventSynchronize(st->ready[k & 1]));
+  return PR_OK;
+}
+
 int copy_to_host_i64(int64_t* dst, const int32_t* src, int64_t n, cudaStream_t s) {
   if (n <= 0) return PR_OK;
   if ((size_t)n * 4 <= kDirectMax || !pageable(dst)) {
@@ -217,5 +252,130 @@ void fill_rows_host(int32_t* origin, const int64_t* row_ptr, int64_t n_rows, int
 }
 
 bool is_pageable_host(const void* p) { return pageable(p); }
+
+// ---- pinned host blocks handed to callers (sizes rounded up to 2 MiB)
+namespace {
+
+constexpr size_t kHostGrain = (size_t)2 << 20;
+
+struct HostBlocks {
+  std::mutex mu;
+  std::multimap<size_t, char*> free;      // capacity -> cached block
+  std::unordered_map<char*, size_t> cap;  // every block of the pool -> capacity
+  size_t cached = 0, live = 0;
+  long long allocs = 0, hits = 0;
+  size_t keep = 0;  // bound on cached bytes
+};
+
+HostBlocks& host_blocks() {
+  static HostBlocks* h = [] {
+    HostBlocks* b = new HostBlocks();
+    const char* env = std::getenv("PORERAD_HOST_CACHE_BYTES");
+    b->keep = env ? (size_t)std::strtoull(env, nullptr, 10) : ((size_t)32 << 30);
+    return b;
+  }();
+  return *h;
+}
+
+// Free cached blocks, largest first, until at most `keep` bytes stay cached (lock held by the
+// caller; the blocks to free are returned so that cudaFreeHost runs outside the lock).
+std::vector<char*> host_trim_locked(HostBlocks& H, size_t keep) {
+  std::vector<char*> out;
+  while (H.cached > keep && !H.free.empty()) {
+    auto it = std::prev(H.free.end());
+    H.cached -= it->first;
+    H.cap.erase(it->second);
+    out.push_back(it->second);
+    H.free.erase(it);
+  }
+  return out;
+}
+
+}  // namespace
+
+int host_block_take(size_t bytes, void** out) {
+  HostBlocks& H = host_blocks();
+  const size_t want = (bytes + kHostGrain - 1) / kHostGrain * kHostGrain;
+  {
+    std::lock_guard<std::mutex> lk(H.mu);
+    // the smallest cached block that holds the request, if it is at most twice its size
+    auto it = H.free.lower_bound(want);
+    if (it != H.free.end() && it->first <= 2 * want) {
+      *out = it->second;
+      H.cached -= it->first;
+      H.live += it->first;
+      ++H.hits;
+      H.free.erase(it);
+      return PR_OK;
+    }
+  }
+  char* p = nullptr;
+  if (cudaHostAlloc((void**)&p, want, cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    // cached blocks of other sizes may be what holds the memory: free them and try once more
+    std::vector<char*> drop;
+    {
+      std::lock_guard<std::mutex> lk(H.mu);
+      drop = host_trim_locked(H, 0);
+    }
+    for (char* d : drop) cudaFreeHost(d);
+    if (cudaHostAlloc((void**)&p, want, cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("a pinned host block of %zu bytes could not be allocated", want);
+      return PR_ERR_OOM;
+    }
+  }
+  std::lock_guard<std::mutex> lk(H.mu);
+  H.cap[p] = want;
+  H.live += want;
+  ++H.allocs;
+  *out = p;
+  return PR_OK;
+}
+
+int host_block_give(void* ptr) {
+  HostBlocks& H = host_blocks();
+  char* p = static_cast<char*>(ptr);
+  std::vector<char*> drop;
+  {
+    std::lock_guard<std::mutex> lk(H.mu);
+    auto c = H.cap.find(p);
+    if (c == H.cap.end()) {
+      set_error("not a host block of this library");
+      return PR_ERR_ARG;
+    }
+    for (auto it = H.free.equal_range(c->second).first; it != H.free.end() && it->first == c->second; ++it)
+      if (it->second == p) {
+        set_error("host block released twice");
+        return PR_ERR_ARG;
+      }
+    H.live -= c->second;
+    H.free.emplace(c->second, p);
+    H.cached += c->second;
+    drop = host_trim_locked(H, H.keep);
+  }
+  for (char* d : drop) cudaFreeHost(d);
+  return PR_OK;
+}
+
+int host_blocks_trim(size_t keep) {
+  HostBlocks& H = host_blocks();
+  std::vector<char*> drop;
+  {
+    std::lock_guard<std::mutex> lk(H.mu);
+    drop = host_trim_locked(H, keep);
+  }
+  for (char* d : drop) PR_CUDA(cudaFreeHost(d));
+  return PR_OK;
+}
+
+void host_blocks_stats(long long* live, long long* cached, long long* allocs, long long* hits) {
+  HostBlocks& H = host_blocks();
+  std::lock_guard<std::mutex> lk(H.mu);
+  if (live) *live = (long long)H.live;
+  if (cached) *cached = (long long)H.cached;
+  if (allocs) *allocs = H.allocs;
+  if (hits) *hits = H.hits;
+}
 
 }  // namespace pr

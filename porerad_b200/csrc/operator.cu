@@ -103,10 +103,16 @@ __global__ void k_row_sums(const int64_t* __restrict__ rp, const int32_t* __rest
   }
 }
 
-int counts_from_edges(const int32_t* origin, const int32_t* receiver, const int64_t* count, int64_t m, int64_t n,
-                      cudaStream_t s, pr_counts** out) {
+int counts_from_tables(const int32_t* const* origin, const int32_t* const* receiver, const int64_t* const* count,
+                       const int64_t* n_edges, int n_tables, int64_t n, cudaStream_t s, pr_counts** out) {
   PR_ARG(n >= 0 && n < INT32_MAX, "n_patches %lld outside the int32 patch ids", (long long)n);
-  PR_ARG(m >= 0, "negative edge count");
+  PR_ARG(n_tables >= 0, "negative number of tables");
+  int64_t m = 0;
+  for (int t = 0; t < n_tables; ++t) {
+    PR_ARG(n_edges[t] >= 0, "negative edge count");
+    PR_ARG(n_edges[t] == 0 || (origin[t] && receiver[t] && count[t]), "table %d has a NULL array", t);
+    m += n_edges[t];
+  }
   std::unique_ptr<pr_counts> k(new pr_counts());
   cudaGetDevice(&k->device);
   k->csr = std::make_shared<CountCsr>();
@@ -127,9 +133,15 @@ int counts_from_edges(const int32_t* origin, const int32_t* receiver, const int6
     PR_TRY(o.alloc(m, s));
     PR_TRY(r.alloc(m, s));
     PR_TRY(c.alloc(m, s));
-    PR_CUDA(cudaMemcpyAsync(o.ptr, origin, m * 4, cudaMemcpyDefault, s));
-    PR_CUDA(cudaMemcpyAsync(r.ptr, receiver, m * 4, cudaMemcpyDefault, s));
-    PR_CUDA(cudaMemcpyAsync(c.ptr, count, m * 8, cudaMemcpyDefault, s));
+    // the tables one after the other into one device edge list (ids are checked on the device)
+    int64_t at = 0;
+    for (int t = 0; t < n_tables; ++t) {
+      const int64_t mt = n_edges[t];
+      PR_TRY(copy_from_host(o.ptr + at, origin[t], (size_t)mt * 4, s));
+      PR_TRY(copy_from_host(r.ptr + at, receiver[t], (size_t)mt * 4, s));
+      PR_TRY(copy_from_host(c.ptr + at, count[t], (size_t)mt * 8, s));
+      at += mt;
+    }
     PR_TRY(key.alloc(m, s));
     PR_TRY(key_sorted.alloc(m, s));
     PR_TRY(c_sorted.alloc(m, s));
@@ -181,6 +193,11 @@ int counts_from_edges(const int32_t* origin, const int32_t* receiver, const int6
   k->last_stream = s;
   *out = k.release();
   return PR_OK;
+}
+
+int counts_from_edges(const int32_t* origin, const int32_t* receiver, const int64_t* count, int64_t m, int64_t n,
+                      cudaStream_t s, pr_counts** out) {
+  return counts_from_tables(&origin, &receiver, &count, &m, 1, n, s, out);
 }
 
 __global__ void k_merge_len(const int64_t* __restrict__ ap, const int32_t* __restrict__ ac,

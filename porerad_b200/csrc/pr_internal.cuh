@@ -66,6 +66,10 @@ void arena_free(void* p, size_t bytes, cudaStream_t s, int dev);
 // and host threads (hostcopy.cu); everything else is one cudaMemcpyAsync (the caller then
 // synchronises the stream as before).
 int copy_to_host(void* dst, const void* src, size_t bytes, cudaStream_t s);
+// Host (pageable or pinned) -> device copy; pageable sources above 16 MB go through the pinned
+// staging buffers, host threads filling one while the other's DMA runs.  Returns once the
+// source may be reused.
+int copy_from_host(void* dst, const void* src, size_t bytes, cudaStream_t s);
 // int32 device values into an int64 host array (widened on the host; same pipeline).
 int copy_to_host_i64(int64_t* dst, const int32_t* src, int64_t n, cudaStream_t s);
 // origin[q] = first_id + i for every q in [row_ptr[i], row_ptr[i + 1]) (host arrays), over the
@@ -73,6 +77,12 @@ int copy_to_host_i64(int64_t* dst, const int32_t* src, int64_t n, cudaStream_t s
 void fill_rows_host(int32_t* origin, const int64_t* row_ptr, int64_t n_rows, int64_t first_id);
 // Host memory the GPU cannot reach directly (neither pinned nor managed).
 bool is_pageable_host(const void* p);
+// Pinned host blocks handed to callers, reused after release (PORERAD_HOST_CACHE_BYTES bounds
+// the cached bytes, default 32 GiB).
+int host_block_take(size_t bytes, void** out);
+int host_block_give(void* p);
+int host_blocks_trim(size_t keep);
+void host_blocks_stats(long long* live, long long* cached, long long* allocs, long long* hits);
 
 // A device allocation owned by the library, released in stream order (to the cache).
 template <typename T>

@@ -272,8 +272,10 @@ constexpr int kBlkThreads = 1024;
 constexpr int kBlkSmemMax = 220 * 1024;  // dynamic shared memory of a blocked product
 
 // Stage g covers column blocks [g k, g k + k) (k = 2 for binary32 x, whose blocks are
-// half as many bytes), staged with 16-byte loads; groups of G lanes then take the CTA's
-// rows (32 / G rows in flight per warp: a row's segment of one stage is short).
+// half as many bytes), staged with 16-byte loads; groups of G = 8 lanes then take the CTA's
+// rows (4 rows in flight per warp: a row's segment of one stage is short).  Eight lanes per
+// segment measured faster than four for binary64 x and than sixteen for binary32 x on the
+// c2 operators.
 // The work of CTA `cta` of a blocked product (its row range B.cta_row[cta] .. B.cta_row[cta + 1]).
 template <int kMode, typename Acc, typename Tx, class Epi>
 __device__ __forceinline__ void spmv_blk_cta(const SymView& S, const BlkView& B, const Tx* __restrict__ x,
@@ -283,7 +285,7 @@ __device__ __forceinline__ void spmv_blk_cta(const SymView& S, const BlkView& B,
   const int stage_cols = B.W * k;
   Tx* xs = reinterpret_cast<Tx*>(blk_smem);
   Acc* acc = reinterpret_cast<Acc*>(blk_smem + (size_t)stage_cols * sizeof(Tx));
-  constexpr int G = sizeof(Tx) == 4 ? 16 : 8;  // lanes per row segment
+  constexpr int G = 8;  // lanes per row segment
   constexpr int kGroups = 32 / G;
   const int64_t r0 = B.cta_row[cta], r1 = B.cta_row[cta + 1];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;

@@ -230,6 +230,61 @@ def trace_first_hit(patches, origins: np.ndarray, directions: np.ndarray) -> np.
     return receiver
 
 
+PINNED_MIN_BYTES = 16 << 20  # edge lists above this size are handed back in pinned host blocks
+
+
+class _HostBlock:
+    """A pinned host block of the library; it goes back to the library's cache when the last
+    array over it is freed."""
+
+    __slots__ = ("ptr", "nbytes")
+
+    def __init__(self, nbytes: int):
+        out = ctypes.c_void_p()
+        _lib.check(_lib.load().pr_host_block(int(nbytes), ctypes.byref(out)))
+        self.ptr, self.nbytes = out.value, int(nbytes)
+
+    def __del__(self):
+        try:
+            _lib.load().pr_host_block_release(self.ptr)
+        except Exception:  # interpreter shutdown
+            pass
+
+
+def _edge_arrays(m: int):
+    """Empty (origin int32, receiver int32, count int64) arrays of m pairs.
+
+    Above PINNED_MIN_BYTES the three arrays are views of one pinned host block of the library
+    (count first, then origin, then receiver), so the device writes them directly; they are
+    ordinary writable NumPy arrays, and the block returns to the library's cache when all
+    three are freed.
+    """
+
+    if m * 16 <= PINNED_MIN_BYTES:
+        return np.empty(m, np.int32), np.empty(m, np.int32), np.empty(m, np.int64)
+    blk = _HostBlock(16 * m)
+    buf = (ctypes.c_char * (16 * m)).from_address(blk.ptr)
+    buf._block = blk  # the buffer (the arrays' base) keeps the block alive
+    c = np.frombuffer(buf, np.int64, m, 0)
+    o = np.frombuffer(buf, np.int32, m, 8 * m)
+    r = np.frombuffer(buf, np.int32, m, 12 * m)
+    return o, r, c
+
+
+def host_blocks_stats() -> dict:
+    """Bytes of the library's pinned host blocks held by arrays (live) and cached for reuse."""
+
+    v = [ctypes.c_longlong() for _ in range(4)]
+    _lib.check(_lib.load().pr_host_blocks_stats(*[ctypes.byref(x) for x in v]))
+    return dict(zip(("live_bytes", "cached_bytes", "allocations", "reuses"), (x.value for x in v)))
+
+
+def release_host_blocks(keep_bytes: int = 0) -> None:
+    """Free the library's cached pinned host blocks down to ``keep_bytes``."""
+
+    _lib.check(_lib.load().pr_host_blocks_trim(int(keep_bytes)))
+
+
 class CountTable:
     """Pooled first-hit counts resident on the GPU (a ``pr_counts``): CSR rows by origin patch."""
 
@@ -253,9 +308,7 @@ class CountTable:
     def to_numpy(self, with_rays: bool = False):
         """(origin int32, receiver int32, count int64) sorted by (origin, receiver) [+ rays_per_origin]."""
 
-        o = np.empty(self.nnz, np.int32)
-        r = np.empty(self.nnz, np.int32)
-        c = np.empty(self.nnz, np.int64)
+        o, r, c = _edge_arrays(self.nnz)
         rays = np.empty(self.n_patches, np.int64) if with_rays else None
         _lib.check(_lib.load().pr_counts_copy(self.handle, o.ctypes.data, r.ctypes.data, c.ctypes.data,
                                               _lib.ptr(rays), _lib.stream()))
@@ -268,9 +321,7 @@ class CountTable:
         m = ctypes.c_int64()
         b, e = int(patch_begin), int(patch_end)
         _lib.check(lib.pr_counts_rows(self.handle, b, e, ctypes.byref(m), None, None, None, _lib.stream()))
-        o = np.empty(m.value, np.int32)
-        r = np.empty(m.value, np.int32)
-        c = np.empty(m.value, np.int64)
+        o, r, c = _edge_arrays(m.value)
         _lib.check(lib.pr_counts_rows(self.handle, b, e, ctypes.byref(m), o.ctypes.data, r.ctypes.data, c.ctypes.data,
                                       _lib.stream()))
         return o, r, c
@@ -339,37 +390,58 @@ def first_hit_counts(patches, rays_per_patch: int, seed: int, *,
 def pool_counts(tables, n_patches: int) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
     """Sum integer edge counts of several ray blocks into one sorted edge list (view_factors.py:290-300)."""
 
-    n = int(n_patches)
-    o = np.ascontiguousarray(np.concatenate([np.asarray(t[0], np.int64) for t in tables]) if tables else
-                             np.empty(0, np.int64))
-    r = np.ascontiguousarray(np.concatenate([np.asarray(t[1], np.int64) for t in tables]) if tables else
-                             np.empty(0, np.int64))
-    c = np.ascontiguousarray(np.concatenate([np.asarray(t[2], np.int64) for t in tables]) if tables else
-                             np.empty(0, np.int64))
-    table = pool_to_device(o, r, c, n)
+    table = pool_tables_to_device(tables, n_patches)
     try:
         return table.to_numpy()
     finally:
         table.close()
 
 
+def _id_array(a, n: int) -> np.ndarray:
+    """Patch ids as a contiguous int32 array: int32 input as it is (its range is checked on the
+    device), other integer types checked here before they are narrowed."""
+
+    a = np.asarray(a)
+    if a.dtype == np.int32:
+        return np.ascontiguousarray(a)
+    if a.size and (a.min() < 0 or a.max() >= n):
+        raise IndexError(f"patch ids outside [0, {n})")
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def pool_tables_to_device(tables, n_patches: int) -> CountTable:
+    """Pool a list of (origin, receiver, count) edge lists into a device-resident CountTable.
+
+    The arrays go to the device as they are (no host concatenation): straight from pinned
+    memory such as ``first_hit_counts``' results, through the library's staging pipeline from
+    pageable memory; the ids are checked and the pairs pooled on the device.
+    """
+
+    n = int(n_patches)
+    keep = []
+    for t in tables:
+        o, r = _id_array(t[0], n), _id_array(t[1], n)
+        c = np.ascontiguousarray(np.asarray(t[2]), dtype=np.int64)
+        if not (o.size == r.size == c.size):
+            raise ValueError("origin, receiver and count must have the same length")
+        keep.append((o, r, c))
+    k = len(keep)
+    ptrs = [(ctypes.c_void_p * max(k, 1))(*[x[f].ctypes.data for x in keep]) for f in range(3)]
+    sizes = (ctypes.c_int64 * max(k, 1))(*[x[0].size for x in keep])
+    out = ctypes.c_void_p()
+    lib = _lib.load()
+    status = lib.pr_counts_from_tables(*[ctypes.addressof(a) for a in ptrs], ctypes.addressof(sizes), k, n,
+                                       _lib.stream(), ctypes.byref(out))
+    if status == _lib.PR_ERR_ARG and "patch ids outside" in _lib.last_error():
+        raise IndexError(f"patch ids outside [0, {n})")
+    _lib.check(status)
+    return CountTable(out.value)
+
+
 def pool_to_device(origin, receiver, count, n_patches: int) -> CountTable:
     """Pool an arbitrary (origin, receiver, count) edge list into a device-resident CountTable."""
 
-    o = np.asarray(origin)
-    r = np.asarray(receiver)
-    n = int(n_patches)
-    if o.size and (o.min() < 0 or o.max() >= n or r.min() < 0 or r.max() >= n):
-        raise IndexError(f"patch ids outside [0, {n})")
-    o32 = np.ascontiguousarray(o, dtype=np.int32)
-    r32 = np.ascontiguousarray(r, dtype=np.int32)
-    c64 = np.ascontiguousarray(np.asarray(count), dtype=np.int64)
-    if not (o32.size == r32.size == c64.size):
-        raise ValueError("origin, receiver and count must have the same length")
-    out = ctypes.c_void_p()
-    _lib.check(_lib.load().pr_counts_from_edges(o32.ctypes.data, r32.ctypes.data, c64.ctypes.data, int(o32.size), n,
-                                                _lib.stream(), ctypes.byref(out)))
-    return CountTable(out.value)
+    return pool_tables_to_device([(origin, receiver, count)], n_patches)
 
 
 def count_sha256(origin: np.ndarray, receiver: np.ndarray, count: np.ndarray, rays_per_origin: np.ndarray) -> str:

@@ -120,7 +120,8 @@ def test_count_rows_edges_and_errors():
 
 def test_large_count_copies_to_pageable_and_pinned_memory_agree():
     """Count arrays above 16 MB copied into pageable NumPy memory (pinned staging buffers, host
-    threads) equal the same arrays copied straight into pinned memory."""
+    threads), into the library's pinned host blocks (to_numpy) and into pinned torch memory are
+    equal; so are the row ranges."""
 
     import torch
 
@@ -129,13 +130,96 @@ def test_large_count_copies_to_pageable_and_pinned_memory_agree():
 
     p = vf.build_surface_patches(load_canonical("FA_canonical_phi0.10_N128"), 0.01)
     table = vf.first_hit_counts_pooled(p, 64, [11, 12])
+    m = table.nnz
+    assert m * 4 > (16 << 20)
     o, r, c = table.to_numpy()
-    assert o.nbytes > (16 << 20) and o.size == table.nnz
-    pinned = [torch.empty(table.nnz, dtype=dt).pin_memory() for dt in (torch.int32, torch.int32, torch.int64)]
-    _lib.check(_lib.load().pr_counts_copy(table.handle, *[t.data_ptr() for t in pinned], None, _lib.stream()))
-    for got, want in zip((o, r, c), pinned):
-        assert np.array_equal(got, want.numpy())
+    assert o.size == m and o.dtype == np.int32 and r.dtype == np.int32 and c.dtype == np.int64
+    assert o.flags.writeable and o.flags.c_contiguous and c.flags.aligned
+    assert vf.host_blocks_stats()["live_bytes"] >= 16 * m
+    lib = _lib.load()
+    pageable = [np.empty(m, np.int32), np.empty(m, np.int32), np.empty(m, np.int64)]
+    _lib.check(lib.pr_counts_copy(table.handle, *[a.ctypes.data for a in pageable], None, _lib.stream()))
+    pinned = [torch.empty(m, dtype=dt).pin_memory() for dt in (torch.int32, torch.int32, torch.int64)]
+    _lib.check(lib.pr_counts_copy(table.handle, *[t.data_ptr() for t in pinned], None, _lib.stream()))
+    for got, a, t in zip((o, r, c), pageable, pinned):
+        assert np.array_equal(got, a) and np.array_equal(got, t.numpy())
     b = table.n_patches // 3
+    sel = o >= b
     for got, want in zip(table.rows(b, table.n_patches), (o, r, c)):
-        assert np.array_equal(got, want[o >= b])
+        assert np.array_equal(got, want[sel])
+    rows_pageable = [np.empty(int(sel.sum()), dt) for dt in (np.int32, np.int32, np.int64)]
+    n = _lib.ctypes.c_int64()
+    _lib.check(lib.pr_counts_rows(table.handle, b, table.n_patches, _lib.ctypes.byref(n),
+                                  *[a.ctypes.data for a in rows_pageable], _lib.stream()))
+    for got, want in zip(rows_pageable, (o, r, c)):
+        assert np.array_equal(got, want[sel])
     table.close()
+
+
+def test_host_blocks_are_reused_and_checked():
+    """Released pinned blocks are cached and handed out again; foreign or released pointers are
+    refused; trimming frees the cache."""
+
+    import gc
+
+    from porerad_b200 import _lib, view_factors as vf
+
+    lib = _lib.load()
+    vf.release_host_blocks(0)
+    s0 = vf.host_blocks_stats()
+    o, r, c = vf._edge_arrays(3 << 20)  # 48 MiB: a pinned block
+    o[:] = 1
+    c[:] = -5
+    r[-1] = 7
+    assert int(o.sum()) == 3 << 20 and int(c[0]) == -5 and int(r[-1]) == 7
+    s1 = vf.host_blocks_stats()
+    assert s1["allocations"] == s0["allocations"] + 1 and s1["live_bytes"] >= 48 << 20
+    del o, r, c
+    gc.collect()
+    s2 = vf.host_blocks_stats()
+    assert s2["live_bytes"] == s0["live_bytes"] and s2["cached_bytes"] >= 48 << 20
+    o, r, c = vf._edge_arrays((3 << 20) - 1000)  # fits the cached block: reused, no new allocation
+    s3 = vf.host_blocks_stats()
+    assert s3["allocations"] == s1["allocations"] and s3["reuses"] == s2["reuses"] + 1
+    x = np.empty(16, np.int64)
+    assert lib.pr_host_block_release(_lib.ctypes.c_void_p(x.ctypes.data)) == _lib.PR_ERR_ARG
+    blk = _lib.ctypes.c_void_p()
+    _lib.check(lib.pr_host_block(1 << 20, _lib.ctypes.byref(blk)))
+    _lib.check(lib.pr_host_block_release(blk))
+    assert lib.pr_host_block_release(blk) == _lib.PR_ERR_ARG  # released twice
+    del o, r, c
+    gc.collect()
+    vf.release_host_blocks(0)
+    assert vf.host_blocks_stats()["cached_bytes"] == 0
+    small = vf._edge_arrays(1000)  # small edge lists stay ordinary NumPy memory
+    assert all(a.base is None for a in small)
+
+
+def test_pool_counts_of_large_tables_from_pinned_pageable_and_int64_inputs():
+    """pool_counts over per-set tables above 16 MB equals the device-pooled table whether the
+    tables sit in the library's pinned blocks (first_hit_counts' results), in pageable NumPy
+    memory (staged copies) or hold int64 ids; ids outside the patches raise IndexError."""
+
+    from porerad_b200 import view_factors as vf
+    from tests.helpers import load_canonical
+
+    p = vf.build_surface_patches(load_canonical("FA_canonical_phi0.10_N128"), 0.01)
+    P = p.n_patches
+    a = vf.first_hit_counts(p, 64, 11)
+    b = vf.first_hit_counts(p, 64, 12)
+    assert a[0].nbytes > (16 << 20) and a[0].base is not None  # pinned block views
+    want = vf.first_hit_counts_pooled(p, 64, [11, 12])
+    w = want.to_numpy()
+    want.close()
+    pageable = [tuple(np.array(x, copy=True) for x in t) for t in (a, b)]
+    wide = [(t[0].astype(np.int64), t[1].astype(np.int64), t[2]) for t in (a, b)]
+    for tables in ([a, b], pageable, wide, [pageable[0], b]):
+        got = vf.pool_counts(tables, P)
+        for g, x in zip(got, w):
+            assert g.dtype == x.dtype and np.array_equal(g, x)
+    for dt in (np.int32, np.int64):
+        bad = (pageable[0][0].astype(dt), pageable[0][1].astype(dt), pageable[0][2])
+        bad[1][12345] = P
+        with pytest.raises(IndexError):
+            vf.pool_counts([bad, b], P)
+    assert all(x.size == 0 for x in vf.pool_counts([], P))
