@@ -597,12 +597,13 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) k_trace_pool(const Wa
         int m = 0;      // cells recorded
         int stop = 0;   // 0 none, 1 wall at position m, 2 step cap at position m
         int32_t wall_code = -1;
+        const int left = cap - it;  // steps left before the ray's step cap
 #pragma unroll
         for (int p = 0; p < kLook; ++p) {
           cell[p] = 0;
           code[p] = -1;
-          if (stop == 0 && m == p) {
-            if (it + p >= cap) {
+          if (stop == 0) {  // while no stop is recorded, m == p
+            if (p >= left) {
               stop = 2;
             } else if ((unsigned)i >= (unsigned)nx) {
               stop = 1;  // the wall's hit code is formed after the round (i and t stay as they are)
