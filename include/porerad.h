@@ -149,6 +149,9 @@ PR_API int pr_counts_rows(const pr_counts* k, int64_t row_begin, int64_t row_end
  * to 2 MiB.  release: PR_ERR_ARG for a pointer that is not a live block of the pool.
  * trim frees cached blocks, largest first, until at most keep_bytes stay cached. */
 PR_API int pr_host_block(long long bytes, void** out);
+/* A cached block only: *out = NULL (and PR_OK) when no released block holds the request with at
+ * most twice its bytes; never pins new memory. */
+PR_API int pr_host_block_cached(long long bytes, void** out);
 PR_API int pr_host_block_release(void* block);
 PR_API int pr_host_blocks_trim(long long keep_bytes);
 PR_API int pr_host_blocks_stats(long long* live_bytes, long long* cached_bytes, long long* allocations,

@@ -292,7 +292,13 @@ int pr_counts_copy(const pr_counts* k, int32_t* origin, int32_t* receiver, int64
 int pr_host_block(long long bytes, void** out) {
   PR_CHECK_NULL(out, "out");
   PR_ARG(bytes > 0, "a host block needs a positive size");
-  return host_block_take((size_t)bytes, out);
+  return host_block_take((size_t)bytes, out, true);
+}
+
+int pr_host_block_cached(long long bytes, void** out) {
+  PR_CHECK_NULL(out, "out");
+  PR_ARG(bytes > 0, "a host block needs a positive size");
+  return host_block_take((size_t)bytes, out, false);
 }
 
 int pr_host_block_release(void* block) {

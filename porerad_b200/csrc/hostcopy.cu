@@ -293,9 +293,10 @@ std::vector<char*> host_trim_locked(HostBlocks& H, size_t keep) {
 
 }  // namespace
 
-int host_block_take(size_t bytes, void** out) {
+int host_block_take(size_t bytes, void** out, bool allocate) {
   HostBlocks& H = host_blocks();
   const size_t want = (bytes + kHostGrain - 1) / kHostGrain * kHostGrain;
+  *out = nullptr;
   {
     std::lock_guard<std::mutex> lk(H.mu);
     // the smallest cached block that holds the request, if it is at most twice its size
@@ -309,6 +310,7 @@ int host_block_take(size_t bytes, void** out) {
       return PR_OK;
     }
   }
+  if (!allocate) return PR_OK;  // no cached block fits: *out stays NULL
   char* p = nullptr;
   if (cudaHostAlloc((void**)&p, want, cudaHostAllocPortable) != cudaSuccess) {
     cudaGetLastError();

@@ -79,7 +79,9 @@ void fill_rows_host(int32_t* origin, const int64_t* row_ptr, int64_t n_rows, int
 bool is_pageable_host(const void* p);
 // Pinned host blocks handed to callers, reused after release (PORERAD_HOST_CACHE_BYTES bounds
 // the cached bytes, default 32 GiB).
-int host_block_take(size_t bytes, void** out);
+// A block of at least `bytes`: a cached one when one fits (at most twice the size), else a new
+// one if `allocate`, else *out = NULL.
+int host_block_take(size_t bytes, void** out, bool allocate);
 int host_block_give(void* p);
 int host_blocks_trim(size_t keep);
 void host_blocks_stats(long long* live, long long* cached, long long* allocs, long long* hits);
