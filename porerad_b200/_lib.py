@@ -109,7 +109,6 @@ _SIGNATURES = {
     "pr_counts_copy": (_i32, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "pr_counts_rows": (_i32, [_vp, _i64, _i64, ctypes.POINTER(_i64), _vp, _vp, _vp, _vp]),
     "pr_host_block": (_i32, [ctypes.c_longlong, ctypes.POINTER(_vp)]),
-    "pr_host_block_cached": (_i32, [ctypes.c_longlong, ctypes.POINTER(_vp)]),
     "pr_host_block_release": (_i32, [_vp]),
     "pr_host_blocks_trim": (_i32, [ctypes.c_longlong]),
     "pr_host_blocks_stats": (_i32, [ctypes.POINTER(ctypes.c_longlong)] * 4),

@@ -295,12 +295,6 @@ int pr_host_block(long long bytes, void** out) {
   return host_block_take((size_t)bytes, out, true);
 }
 
-int pr_host_block_cached(long long bytes, void** out) {
-  PR_CHECK_NULL(out, "out");
-  PR_ARG(bytes > 0, "a host block needs a positive size");
-  return host_block_take((size_t)bytes, out, false);
-}
-
 int pr_host_block_release(void* block) {
   PR_CHECK_NULL(block, "block");
   return host_block_give(block);

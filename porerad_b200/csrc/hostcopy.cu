@@ -18,6 +18,8 @@
 // library (pr_host_block): the device writes them straight into the caller's memory at the
 // link's rate, and a block the caller has released is kept for the next result of about its
 // size (pinning and first-touch faults are paid once, not per call).
+#include <sys/mman.h>
+
 #include <cstdlib>
 #include <condition_variable>
 #include <functional>
@@ -277,8 +279,40 @@ HostBlocks& host_blocks() {
   return *h;
 }
 
+CopyPool* copy_pool() {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_pool) g_pool = new CopyPool();
+  return g_pool;
+}
+
+// Pinned memory of `bytes` (a multiple of kHostGrain): page-aligned memory with huge pages
+// advised, its pages faulted in by the copy threads in parallel (one write per 4 KiB page;
+// the kernel zero-fills them), then registered with the driver.  Pinning this way costs
+// about the parallel first-touch of the pages, where cudaHostAlloc faults them in on one
+// thread.
+char* pin_new(size_t bytes) {
+  void* p = nullptr;
+  if (posix_memalign(&p, kHostGrain, bytes) != 0) return nullptr;
+  madvise(p, bytes, MADV_HUGEPAGE);  // advice only: ignored where huge pages are off
+  char* c = static_cast<char*>(p);
+  copy_pool()->run(bytes, kHostGrain, [&](size_t b, size_t e) {
+    for (size_t q = b; q < e; q += 4096) reinterpret_cast<volatile char*>(c)[q] = 0;
+  });
+  if (cudaHostRegister(p, bytes, cudaHostRegisterPortable) != cudaSuccess) {
+    cudaGetLastError();
+    free(p);
+    return nullptr;
+  }
+  return c;
+}
+
+void unpin(char* p) {
+  cudaHostUnregister(p);
+  free(p);
+}
+
 // Free cached blocks, largest first, until at most `keep` bytes stay cached (lock held by the
-// caller; the blocks to free are returned so that cudaFreeHost runs outside the lock).
+// caller; the blocks to free are returned so that they are unpinned outside the lock).
 std::vector<char*> host_trim_locked(HostBlocks& H, size_t keep) {
   std::vector<char*> out;
   while (H.cached > keep && !H.free.empty()) {
@@ -311,18 +345,17 @@ int host_block_take(size_t bytes, void** out, bool allocate) {
     }
   }
   if (!allocate) return PR_OK;  // no cached block fits: *out stays NULL
-  char* p = nullptr;
-  if (cudaHostAlloc((void**)&p, want, cudaHostAllocPortable) != cudaSuccess) {
-    cudaGetLastError();
+  char* p = pin_new(want);
+  if (!p) {
     // cached blocks of other sizes may be what holds the memory: free them and try once more
     std::vector<char*> drop;
     {
       std::lock_guard<std::mutex> lk(H.mu);
       drop = host_trim_locked(H, 0);
     }
-    for (char* d : drop) cudaFreeHost(d);
-    if (cudaHostAlloc((void**)&p, want, cudaHostAllocPortable) != cudaSuccess) {
-      cudaGetLastError();
+    for (char* d : drop) unpin(d);
+    p = pin_new(want);
+    if (!p) {
       set_error("a pinned host block of %zu bytes could not be allocated", want);
       return PR_ERR_OOM;
     }
@@ -356,7 +389,7 @@ int host_block_give(void* ptr) {
     H.cached += c->second;
     drop = host_trim_locked(H, H.keep);
   }
-  for (char* d : drop) cudaFreeHost(d);
+  for (char* d : drop) unpin(d);
   return PR_OK;
 }
 
@@ -367,7 +400,7 @@ int host_blocks_trim(size_t keep) {
     std::lock_guard<std::mutex> lk(H.mu);
     drop = host_trim_locked(H, keep);
   }
-  for (char* d : drop) PR_CUDA(cudaFreeHost(d));
+  for (char* d : drop) unpin(d);
   return PR_OK;
 }
 

@@ -13,11 +13,8 @@ blocks in one device pass and returns a device-resident :class:`CountTable` that
 
 from __future__ import annotations
 
-import collections
 import ctypes
 import hashlib
-import math
-import threading
 
 import numpy as np
 
@@ -252,56 +249,27 @@ class _HostBlock:
             pass
 
 
-_SEEN_SIZES: "collections.OrderedDict[int, None]" = collections.OrderedDict()  # recent size classes
-_SEEN_MAX = 64
-_SEEN_LOCK = threading.Lock()
+def _pinned_block(nbytes: int) -> "_HostBlock":
+    """A pinned host block for a result of ``nbytes``: a released block of about that size from
+    the library's cache, else a newly pinned one."""
 
-
-def _size_class(nbytes: int) -> int:
-    """Size classes a quarter of a binary order wide (a cached block serves requests within a
-    factor 2 of its size, so neighbouring classes share blocks)."""
-
-    return int(4 * math.log2(max(nbytes, 1)))
-
-
-def _pinned_block(nbytes: int):
-    """A pinned host block for a result of ``nbytes``, or None for pageable memory.
-
-    A released block of about that size is reused.  A new block is pinned only for a size class
-    seen before: pinning costs more than one staged copy into pageable memory, so it pays only
-    for sizes that come back (repeated cases, the steps of a run), not for a one-off.
-    """
-
-    lib = _lib.load()
     out = ctypes.c_void_p()
-    _lib.check(lib.pr_host_block_cached(int(nbytes), ctypes.byref(out)))
-    if out.value is None:
-        cls = _size_class(nbytes)
-        with _SEEN_LOCK:
-            seen = cls in _SEEN_SIZES
-            _SEEN_SIZES[cls] = None
-            _SEEN_SIZES.move_to_end(cls)
-            while len(_SEEN_SIZES) > _SEEN_MAX:
-                _SEEN_SIZES.popitem(last=False)
-        if not seen:
-            return None
-        _lib.check(lib.pr_host_block(int(nbytes), ctypes.byref(out)))
+    _lib.check(_lib.load().pr_host_block(int(nbytes), ctypes.byref(out)))
     return _HostBlock(out.value, nbytes)
 
 
 def _edge_arrays(m: int):
     """Empty (origin int32, receiver int32, count int64) arrays of m pairs.
 
-    Above PINNED_MIN_BYTES the three arrays are, when ``_pinned_block`` gives one, views of one
-    pinned host block of the library (count first, then origin, then receiver), so the device
-    writes them directly; they are ordinary writable NumPy arrays, and the block returns to the
-    library's cache when all three are freed.  Otherwise they are pageable NumPy arrays, filled
-    through the library's staging pipeline.
+    Above PINNED_MIN_BYTES the three arrays are views of one pinned host block of the library
+    (count first, then origin, then receiver), so the device writes them directly; they are
+    ordinary writable NumPy arrays, and the block returns to the library's cache when all three
+    are freed.
     """
 
-    blk = _pinned_block(16 * m) if m * 16 > PINNED_MIN_BYTES else None
-    if blk is None:
+    if m * 16 <= PINNED_MIN_BYTES:
         return np.empty(m, np.int32), np.empty(m, np.int32), np.empty(m, np.int64)
+    blk = _pinned_block(16 * m)
     buf = (ctypes.c_char * (16 * m)).from_address(blk.ptr)
     buf._block = blk  # the buffer (the arrays' base) keeps the block alive
     c = np.frombuffer(buf, np.int64, m, 0)
