@@ -146,8 +146,7 @@ PR_API int pr_counts_rows(const pr_counts* k, int64_t row_begin, int64_t row_end
  * straight from the device at the link's rate; a released block is cached for the next
  * request that it holds with at most twice the bytes (bounded by PORERAD_HOST_CACHE_BYTES, default 32 GiB),
  * so pinning and page faults are paid once per size.  Blocks are page-aligned, rounded up
- * to 2 MiB; a new block is host memory whose pages the library's copy threads fault in
- * together, then registered with the driver.  release: PR_ERR_ARG for a pointer that is not a live block of the pool.
+ * to 2 MiB.  release: PR_ERR_ARG for a pointer that is not a live block of the pool.
  * trim frees cached blocks, largest first, until at most keep_bytes stay cached. */
 PR_API int pr_host_block(long long bytes, void** out);
 PR_API int pr_host_block_release(void* block);

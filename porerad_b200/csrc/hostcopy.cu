@@ -18,8 +18,6 @@
 // library (pr_host_block): the device writes them straight into the caller's memory at the
 // link's rate, and a block the caller has released is kept for the next result of about its
 // size (pinning and first-touch faults are paid once, not per call).
-#include <sys/mman.h>
-
 #include <cstdlib>
 #include <condition_variable>
 #include <functional>
@@ -279,37 +277,19 @@ HostBlocks& host_blocks() {
   return *h;
 }
 
-CopyPool* copy_pool() {
-  std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_pool) g_pool = new CopyPool();
-  return g_pool;
-}
-
-// Pinned memory of `bytes` (a multiple of kHostGrain): page-aligned memory with huge pages
-// advised, its pages faulted in by the copy threads in parallel (one write per 4 KiB page;
-// the kernel zero-fills them), then registered with the driver.  Pinning this way costs
-// about the parallel first-touch of the pages, where cudaHostAlloc faults them in on one
-// thread.
+// Pinned memory of `bytes` from the driver, or nullptr.  (Registering host memory whose pages
+// the copy threads had faulted in together pinned faster, but the c2 count step then showed
+// 40 ms more host time per step and the serving rate fell by a quarter: not kept.)
 char* pin_new(size_t bytes) {
-  void* p = nullptr;
-  if (posix_memalign(&p, kHostGrain, bytes) != 0) return nullptr;
-  madvise(p, bytes, MADV_HUGEPAGE);  // advice only: ignored where huge pages are off
-  char* c = static_cast<char*>(p);
-  copy_pool()->run(bytes, kHostGrain, [&](size_t b, size_t e) {
-    for (size_t q = b; q < e; q += 4096) reinterpret_cast<volatile char*>(c)[q] = 0;
-  });
-  if (cudaHostRegister(p, bytes, cudaHostRegisterPortable) != cudaSuccess) {
+  char* p = nullptr;
+  if (cudaHostAlloc((void**)&p, bytes, cudaHostAllocPortable) != cudaSuccess) {
     cudaGetLastError();
-    free(p);
     return nullptr;
   }
-  return c;
+  return p;
 }
 
-void unpin(char* p) {
-  cudaHostUnregister(p);
-  free(p);
-}
+void unpin(char* p) { cudaFreeHost(p); }
 
 // Free cached blocks, largest first, until at most `keep` bytes stay cached (lock held by the
 // caller; the blocks to free are returned so that they are unpinned outside the lock).
