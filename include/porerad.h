@@ -122,6 +122,15 @@ PR_API int pr_trace_first_hit(const pr_case* c, const double* origins, const dou
  * patch reduced into one sorted CSR row.  rays_per_origin = R * n_seeds. */
 PR_API int pr_first_hit_counts(const pr_case* c, int64_t rays_per_patch, const pr_pcg64* seeds,
                         int n_seeds, void* stream, pr_counts** out);
+/* first_hit_counts (view_factors.py:273-287) straight into host memory: the sorted edge list
+ * of pr_first_hit_counts + pr_counts_copy, written into origin / receiver / count chunk by
+ * chunk (64 M rays each) on a copy stream of its own while the next chunks trace, so that
+ * with pinned arrays the copies overlap the traversal.  capacity = pairs the arrays hold
+ * (n_patches * rays_per_patch * n_seeds always suffices; PR_ERR_LIMIT if exceeded); *n_pairs
+ * receives the list's length.  No device table is kept. */
+PR_API int pr_first_hit_counts_host(const pr_case* c, int64_t rays_per_patch, const pr_pcg64* seeds,
+                                    int n_seeds, void* stream, int32_t* origin, int32_t* receiver,
+                                    int64_t* count, int64_t capacity, int64_t* n_pairs);
 /* pr_first_hit_counts for n_cases geometries at once (batched sweeps, serving): the rays of
  * all cases share persistent launches of the traversal, waves of up to 2^27 rays that mix
  * chunks of cases of different sizes.  seeds holds n_seeds per case (case-major); out

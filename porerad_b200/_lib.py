@@ -108,6 +108,8 @@ _SIGNATURES = {
                               ctypes.POINTER(_i64)]),
     "pr_counts_copy": (_i32, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "pr_counts_rows": (_i32, [_vp, _i64, _i64, ctypes.POINTER(_i64), _vp, _vp, _vp, _vp]),
+    "pr_first_hit_counts_host": (_i32, [_vp, _i64, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _i64,
+                                        ctypes.POINTER(_i64)]),
     "pr_host_block": (_i32, [ctypes.c_longlong, ctypes.POINTER(_vp)]),
     "pr_host_block_release": (_i32, [_vp]),
     "pr_host_blocks_trim": (_i32, [ctypes.c_longlong]),

@@ -22,8 +22,11 @@ int generate_rays(const pr_case* c, int64_t p0, int64_t p1, int64_t R, const pr_
 int trace_given(const pr_case* c, const double* origins, const double* dirs, int64_t n, int32_t* receiver,
                 int64_t* n_failed, cudaStream_t s);
 int first_hit_counts(const pr_case* c, int64_t R, const pr_pcg64* seeds, int S, cudaStream_t s, pr_counts** out);
+struct HostSink;
 int counts_batch(const pr_case* const* cases, int nc, int64_t R, const pr_pcg64* seeds, int S, cudaStream_t s,
-                 pr_counts** out);
+                 pr_counts** out, HostSink* sink);
+int first_hit_counts_host(const pr_case* c, int64_t R, const pr_pcg64* seeds, int S, cudaStream_t s,
+                          int32_t* origin, int32_t* receiver, int64_t* count, int64_t capacity, int64_t* n_pairs);
 int counts_from_edges(const int32_t* origin, const int32_t* receiver, const int64_t* count, int64_t m, int64_t n,
                       cudaStream_t s, pr_counts** out);
 int counts_from_tables(const int32_t* const* origin, const int32_t* const* receiver, const int64_t* const* count,
@@ -201,6 +204,20 @@ int pr_first_hit_counts(const pr_case* c, int64_t rays_per_patch, const pr_pcg64
   return first_hit_counts(c, rays_per_patch, seeds, n_seeds, (cudaStream_t)stream, out);
 }
 
+int pr_first_hit_counts_host(const pr_case* c, int64_t rays_per_patch, const pr_pcg64* seeds, int n_seeds,
+                             void* stream, int32_t* origin, int32_t* receiver, int64_t* count, int64_t capacity,
+                             int64_t* n_pairs) {
+  PR_CHECK_NULL(c, "case");
+  PR_CHECK_NULL(n_pairs, "n_pairs");
+  *n_pairs = 0;
+  PR_ARG(seeds_ok(seeds), "seeds must not be NULL");
+  PR_ARG(origin && receiver && count, "origin, receiver and count must not be NULL");
+  PR_ARG(capacity >= 0, "negative capacity");
+  PR_ENTRY_GUARD(c);
+  return first_hit_counts_host(c, rays_per_patch, seeds, n_seeds, (cudaStream_t)stream, origin, receiver, count,
+                               capacity, n_pairs);
+}
+
 int pr_first_hit_counts_batch(const pr_case* const* cases, int n_cases, int64_t rays_per_patch,
                               const pr_pcg64* seeds, int n_seeds, void* stream, pr_counts** out) {
   PR_CHECK_NULL(cases, "cases");
@@ -210,7 +227,7 @@ int pr_first_hit_counts_batch(const pr_case* const* cases, int n_cases, int64_t 
   for (int c = 0; c < n_cases; ++c) out[c] = nullptr;
   PR_CHECK_NULL(cases[0], "cases[0]");
   PR_ENTRY_GUARD(cases[0]);
-  return counts_batch(cases, n_cases, rays_per_patch, seeds, n_seeds, (cudaStream_t)stream, out);
+  return counts_batch(cases, n_cases, rays_per_patch, seeds, n_seeds, (cudaStream_t)stream, out, nullptr);
 }
 
 int pr_counts_info(const pr_counts* k, int64_t* nnz, int64_t* n_patches, int64_t* rays, int64_t* dda_steps) {

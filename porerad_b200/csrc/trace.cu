@@ -908,6 +908,26 @@ __global__ void k_compact_rows(const int32_t* __restrict__ st_col, const int32_t
   }
 }
 
+// One chunk's rows in the layout first_hit_counts hands back (view_factors.py:273-287): the
+// origin patch id of every pair, its receiver and its count widened to int64, at the chunk's
+// exclusive row offsets (one warp per row).
+__global__ void k_compact_host(const int32_t* __restrict__ st_col, const int32_t* __restrict__ st_cnt,
+                               const int32_t* __restrict__ nnz, const int64_t* __restrict__ off, int64_t np,
+                               int L, int64_t first_id, int32_t* __restrict__ origin, int32_t* __restrict__ col,
+                               int64_t* __restrict__ cnt) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t p = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); p < np; p += warps) {
+    const int m = nnz[p];
+    const int64_t dst = off[p];
+    for (int e = lane; e < m; e += 32) {
+      origin[dst + e] = (int32_t)(first_id + p);
+      col[dst + e] = st_col[p * L + e];
+      cnt[dst + e] = st_cnt[p * L + e];
+    }
+  }
+}
+
 __global__ void k_i32_to_i64(const int32_t* __restrict__ in, int64_t* __restrict__ out, int64_t n) {
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
     out[t] = in[t];
@@ -1235,12 +1255,48 @@ struct CaseCounts {
   std::vector<Piece> pieces;  // compacted chunks in patch order
 };
 
+// A count pass of one case that hands its edge list to host memory while it runs: each
+// chunk's rows, once compacted, are laid out as first_hit_counts returns them and copied on a
+// stream of their own into origin / receiver / count at their place in the sorted list, while
+// the next chunks trace; no device table is kept.
+struct HostSink {
+  int32_t* origin;
+  int32_t* receiver;
+  int64_t* count;
+  int64_t capacity;  // pairs the arrays hold
+  int64_t written = 0;
+};
+
+namespace {
+// The copy stream of a host pass and what its copies read, released in this order: the stream
+// is drained before the device buffers go back to the cache.
+struct HostPass {
+  struct Piece {
+    DevBuf<int32_t> o, r;
+    DevBuf<int64_t> c;
+  };
+  std::vector<Piece> pieces;
+  std::vector<cudaEvent_t> events;
+  cudaStream_t copy = nullptr;
+  ~HostPass() {
+    if (copy) {
+      cudaStreamSynchronize(copy);
+      cudaStreamDestroy(copy);
+    }
+    for (cudaEvent_t e : events) cudaEventDestroy(e);
+    pieces.clear();
+  }
+};
+}  // namespace
+
 // first_hit_counts for n_cases geometries at once (view_factors.py:273-300 per case): every
 // case traces rays_per_patch rays per patch for each of its S seeds (seeds[c * S + s]);
-// chunks of all cases share persistent launches of the pooled traversal.
+// chunks of all cases share persistent launches of the pooled traversal.  With `sink` (one
+// case), the edge list goes to host memory as the chunks finish and `out` is not used.
 int counts_batch(const pr_case* const* cases, int nc, int64_t R, const pr_pcg64* seeds, int S, cudaStream_t s,
-                 pr_counts** out) {
+                 pr_counts** out, HostSink* sink) {
   PR_ARG(nc > 0, "no cases");
+  PR_ARG(!sink || nc == 1, "a host pass takes one case");
   PR_ARG(R > 0 && S > 0, "rays_per_patch and the number of seeds must be positive");
   const int64_t L64 = R * S;
   if (L64 > kMaxSegment) {
@@ -1299,6 +1355,13 @@ int counts_batch(const pr_case* const* cases, int nc, int64_t R, const pr_pcg64*
                         for (const Chunk& ch : chunks) t += ch.np * L64;
                         return t;
                       }()));
+  if (sink) {
+    // one chunk per wave, so that every chunk's copy overlaps the next chunk's traversal
+    wave_cap = 0;
+    for (const Chunk& ch : chunks) wave_cap = std::max(wave_cap, ch.np * L64);
+  }
+  HostPass hp;
+  if (sink) PR_CUDA(cudaStreamCreateWithFlags(&hp.copy, cudaStreamNonBlocking));
   DevBuf<int32_t> recv, st_col, st_cnt, nnz;
   DevBuf<int64_t> off;
   DevBuf<unsigned long long> work, ctr;
@@ -1403,7 +1466,37 @@ int counts_batch(const pr_case* const* cases, int nc, int64_t R, const pr_pcg64*
       PR_CUDA(cudaMemcpyAsync(&totals[k], o + ch.np, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     }
     PR_CUDA(cudaStreamSynchronize(s));
-    for (int k = 0; k < nw; ++k) {
+    for (int k = 0; k < nw && sink; ++k) {
+      const Chunk& ch = chunks[w0 + k];
+      const RleChunk& rc = hr[k];
+      const int64_t n = totals[k];
+      if (sink->written + n > sink->capacity) {
+        set_error("the edge list exceeds the %lld pairs the host arrays hold", (long long)sink->capacity);
+        return PR_ERR_LIMIT;
+      }
+      HostPass::Piece pc;
+      PR_TRY(pc.o.alloc(n > 0 ? n : 1, s));
+      PR_TRY(pc.r.alloc(n > 0 ? n : 1, s));
+      PR_TRY(pc.c.alloc(n > 0 ? n : 1, s));
+      ::pr::launch_mark(), k_compact_host<<<grid_for(ch.np * 32, 256), 256, 0, s>>>(
+          st_col.ptr + rc.ray0, st_cnt.ptr + rc.ray0, nnz.ptr + rc.patch0, off.ptr + rc.patch0 + k, ch.np, L, ch.p0,
+          pc.o.ptr, pc.r.ptr, pc.c.ptr);
+      PR_CUDA(cudaGetLastError());
+      cudaEvent_t ev = nullptr;
+      PR_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      hp.events.push_back(ev);
+      PR_CUDA(cudaEventRecord(ev, s));
+      PR_CUDA(cudaStreamWaitEvent(hp.copy, ev, 0));
+      if (n > 0) {
+        const int64_t at = sink->written;
+        PR_CUDA(cudaMemcpyAsync(sink->origin + at, pc.o.ptr, (size_t)n * 4, cudaMemcpyDeviceToHost, hp.copy));
+        PR_CUDA(cudaMemcpyAsync(sink->receiver + at, pc.r.ptr, (size_t)n * 4, cudaMemcpyDeviceToHost, hp.copy));
+        PR_CUDA(cudaMemcpyAsync(sink->count + at, pc.c.ptr, (size_t)n * 8, cudaMemcpyDeviceToHost, hp.copy));
+      }
+      sink->written += n;
+      hp.pieces.push_back(std::move(pc));
+    }
+    for (int k = 0; k < nw && !sink; ++k) {
       const Chunk& ch = chunks[w0 + k];
       const RleChunk& rc = hr[k];
       CaseCounts::Piece pc;
@@ -1429,6 +1522,18 @@ int counts_batch(const pr_case* const* cases, int nc, int64_t R, const pr_pcg64*
   for (size_t k = 0; k < chunks.size(); ++k) {
     steps[chunks[k].c] += (int64_t)hctr[2 * k];
     fails[chunks[k].c] += (int64_t)hctr[2 * k + 1];
+  }
+  if (sink) {
+    PR_CUDA(cudaStreamSynchronize(hp.copy));
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      g_last_variant = variant;
+    }
+    if (fails[0]) {
+      set_error("%lld rays did not resolve a receiving patch", (long long)fails[0]);
+      return PR_ERR_UNRESOLVED;
+    }
+    return PR_OK;
   }
   for (int c = 0; c < nc; ++c) {
     CountCsr& csr = *cc[c].k->csr;
@@ -1474,7 +1579,16 @@ int counts_batch(const pr_case* const* cases, int nc, int64_t R, const pr_pcg64*
 }
 
 int first_hit_counts(const pr_case* c, int64_t R, const pr_pcg64* seeds, int S, cudaStream_t s, pr_counts** out) {
-  return counts_batch(&c, 1, R, seeds, S, s, out);
+  return counts_batch(&c, 1, R, seeds, S, s, out, nullptr);
+}
+
+int first_hit_counts_host(const pr_case* c, int64_t R, const pr_pcg64* seeds, int S, cudaStream_t s,
+                          int32_t* origin, int32_t* receiver, int64_t* count, int64_t capacity, int64_t* n_pairs) {
+  HostSink sink{origin, receiver, count, capacity, 0};
+  *n_pairs = 0;
+  PR_TRY(counts_batch(&c, 1, R, seeds, S, s, nullptr, &sink));
+  *n_pairs = sink.written;
+  return PR_OK;
 }
 
 }  // namespace pr

@@ -231,6 +231,7 @@ def trace_first_hit(patches, origins: np.ndarray, directions: np.ndarray) -> np.
 
 
 PINNED_MIN_BYTES = 16 << 20  # edge lists above this size are handed back in pinned host blocks
+HOST_PASS_MAX_BYTES = 16 << 30  # first_hit_counts writes straight to host up to this upper bound
 
 
 class _HostBlock:
@@ -387,11 +388,29 @@ def first_hit_counts(patches, rays_per_patch: int, seed: int, *,
 
     if int(patch_chunk) <= 0:
         raise ValueError("patch_chunk must be positive")
-    table = first_hit_counts_pooled(patches, rays_per_patch, [seed])
-    try:
-        return table.to_numpy()
-    finally:
-        table.close()
+    dev = _device_of(patches)
+    cap = int(dev.n_patches) * int(rays_per_patch)  # pairs never exceed rays
+    if 16 * cap <= PINNED_MIN_BYTES or 16 * cap > HOST_PASS_MAX_BYTES:
+        table = first_hit_counts_pooled(patches, rays_per_patch, [seed])
+        try:
+            return table.to_numpy()
+        finally:
+            table.close()
+    # The pass writes the sorted list into a pinned block sized for one pair per ray, chunk by
+    # chunk while the next chunks trace; the arrays returned are views of its first pairs.
+    blk = _pinned_block(16 * cap)
+    buf = (ctypes.c_char * (16 * cap)).from_address(blk.ptr)
+    buf._block = blk
+    c = np.frombuffer(buf, np.int64, cap, 0)
+    o = np.frombuffer(buf, np.int32, cap, 8 * cap)
+    r = np.frombuffer(buf, np.int32, cap, 12 * cap)
+    arr = _lib.seeds_struct([_lib.pcg64_state(int(seed))])
+    n = ctypes.c_int64()
+    _lib.check(_lib.load().pr_first_hit_counts_host(dev.handle, int(rays_per_patch), ctypes.addressof(arr), 1,
+                                                    _lib.stream(), o.ctypes.data, r.ctypes.data, c.ctypes.data,
+                                                    cap, ctypes.byref(n)))
+    m = int(n.value)
+    return o[:m], r[:m], c[:m]
 
 
 def pool_counts(tables, n_patches: int) -> tuple[np.ndarray, np.ndarray, np.ndarray]:

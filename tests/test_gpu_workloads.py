@@ -230,3 +230,26 @@ def test_pool_counts_of_large_tables_from_pinned_pageable_and_int64_inputs():
         with pytest.raises(IndexError):
             vf.pool_counts([bad, b], P)
     assert all(x.size == 0 for x in vf.pool_counts([], P))
+
+
+def test_first_hit_counts_host_pass_equals_the_device_table():
+    """Above 16 MB first_hit_counts writes the sorted list into a pinned host block chunk by
+    chunk (64 M rays each) while later chunks trace; the arrays equal the device table's copy,
+    with one chunk (64 rays per patch) and with three (1000 rays per patch: 1.96e8 rays)."""
+
+    from porerad_b200 import view_factors as vf
+    from tests.helpers import load_canonical
+
+    p = vf.build_surface_patches(load_canonical("FA_canonical_phi0.10_N128"), 0.01)
+    P = p.n_patches
+    for R in (64, 1000):
+        got = vf.first_hit_counts(p, R, 11)
+        assert got[0].base is not None  # views of the pass's pinned block
+        t = vf.first_hit_counts_pooled(p, R, [11])
+        want = t.to_numpy()
+        t.close()
+        for g, w in zip(got, want):
+            assert g.dtype == w.dtype and g.flags.c_contiguous and np.array_equal(g, w)
+        assert int(got[2].sum()) == P * R
+        if R == 1000:
+            assert P * R > 2 * (1 << 26)  # three chunks of at most 2^26 rays
